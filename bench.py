@@ -1,0 +1,531 @@
+#!/usr/bin/env python
+"""Benchmark of the NMF iteration loop on B200.
+
+A step is one NMF iteration (H update + W update) over the whole V.
+
+  value    iterations/s with V, W, H already in HBM (nmfcu_run_device),
+           K timed iterations in one call, CUDA events on the launch stream,
+           max over ranks.  Whole job: N replicas x K iterations / time.
+  e2e      iterations/s through the host-pointer C ABI (nmfcu_run, the call
+           behind nmf_rs.nmf): host->device copy of V, W0, H0, the K
+           iterations and the device->host copy of W, H, all timed.
+  roofline achieved HBM GB/s of the dominant V-streaming kernel class,
+           algorithmic bytes (one read of V per launch) / summed launch time
+           from the library's CUDA-event hooks, against MEASURED_PEAKS.json.
+  cpu_baseline  the CPU restatement of the reference loop (oracle/, the
+           Rust reference cannot be built here) on a bounded column slice of
+           the same V, extrapolated linearly in the column count.
+
+--impl reference times that CPU restatement as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+for _p in (str(ROOT), str(ROOT / "rust-nmf_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    # name: (n, p, k, alpha, rank, default iterations)
+    "atlas": (20000, 200000, 20, 0.2, 20, 25),
+    "pbmc8k": (2000, 7750, 10, 0.2, 10, 100),
+    "pbmc-subset": (1500, 3000, 8, 0.3, 8, 100),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None, help="timed iterations")
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="atlas")
+    ap.add_argument("--method", choices=["lee", "brunet", "hals", "dnmf"], default="lee")
+    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64-compare", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# Distributed plumbing (replicas: no data-path collective)
+# ---------------------------------------------------------------------------
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# Synthetic V on the device (same generator as nmf_rs.synthetic, torch RNG)
+# ---------------------------------------------------------------------------
+
+def device_workload(n, p, k, alpha, rank, seed, device):
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    f64 = torch.float64
+    w_true = torch._standard_gamma(torch.full((n, k), 0.5, dtype=f64, device=device),
+                                   generator=g)
+    w_true[torch.rand((n, k), generator=g, device=device, dtype=f64) < 0.7] = 0.0
+    ld64 = (p + 15) // 16 * 16
+    ld32 = (p + 31) // 32 * 32
+    V64 = torch.zeros((n, ld64), dtype=f64, device=device)
+    chunk = 8192
+    for c0 in range(0, p, chunk):
+        c = min(chunk, p - c0)
+        h = torch._standard_gamma(torch.full((k, c), float(alpha), dtype=f64, device=device),
+                                  generator=g)
+        h = h / h.sum(0, keepdim=True).clamp_min(1e-300)
+        lib = torch.empty(c, dtype=f64, device=device).log_normal_(7.0, 0.5, generator=g)
+        lam = (w_true @ h) * lib[None, :]
+        counts = torch.poisson(lam, generator=g)
+        col = counts.sum(0, keepdim=True)
+        scale = torch.where(col > 0, 1e4 / col.clamp_min(1e-300), torch.zeros_like(col))
+        V64[:, c0:c0 + c] = torch.log1p(counts * scale)
+        del h, lam, counts
+    V32 = torch.zeros((n, ld32), dtype=torch.float32, device=device)
+    V32[:, :p] = V64[:, :p].float()
+    vmax = float(V64[:, :p].max())
+    W0 = torch.rand((n, rank), generator=g, device=device, dtype=f64) * vmax
+    H0 = torch.rand((rank, p), generator=g, device=device, dtype=f64) * vmax
+    return V64, ld64, V32, ld32, W0, H0
+
+
+def objective_torch(V64, p, W, H, method):
+    """f64 objective of (W, H) on the device, column chunks (a check, not
+    the product path)."""
+    import torch
+
+    total = torch.zeros((), dtype=torch.float64, device=V64.device)
+    for c0 in range(0, p, 16384):
+        c1 = min(p, c0 + 16384)
+        v = V64[:, c0:c1]
+        wh = W @ H[:, c0:c1]
+        if method == "brunet":
+            pos = v > 0
+            good = pos & (wh > 0)
+            term = torch.where(good, v * torch.log(torch.where(good, v / wh, 1.0)) - v + wh,
+                               torch.zeros_like(v))
+            term = torch.where(pos, term, wh)
+            total += term.sum()
+        else:
+            total += ((v - wh) ** 2).sum()
+    return float(total) * (1.0 if method == "brunet" else 0.5)
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        if self.file is None:
+            return {}
+        self.file.flush()
+        rows = [ln.split(",") for ln in Path(self.file.name).read_text().splitlines() if ln.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (CPU restatement of the reference loop)
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(V_host_fn, n, p, rank, method, seconds, seed=0):
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    p_s = 256
+    rate = None
+    sample = None
+    for _ in range(6):
+        V_s, W0, H0 = V_host_fn(p_s)
+        t0 = time.perf_counter()
+        oracle.nmf_method(method, V_s, W0, H0, 1, num_threads=threads)
+        dt = time.perf_counter() - t0
+        rate = dt / p_s  # seconds per iteration per column
+        sample = (p_s, dt)
+        if dt > seconds / 4 or p_s >= p:
+            break
+        p_s = int(min(p, max(p_s * 2, p_s * (seconds / 2) / max(dt, 1e-3))))
+    t_full = rate * p
+    return {
+        "value": 1.0 / t_full,
+        "unit": "iters/s",
+        "cores": threads,
+        "kind": "port",
+        "sample": (f"1 {method} iteration of the CPU restatement (oracle/, OpenMP) on all "
+                   f"{n} rows x {sample[0]} of {p} columns took {sample[1]:.2f} s; "
+                   f"extrapolated linearly in columns to the full V"),
+    }
+
+
+def host_slice_fn(V64, p_full, rank, seed=0):
+    """Returns f(p_s) -> (V slice, W0, H0) on the host for the CPU baseline."""
+    def f(p_s):
+        v = V64[:, :p_s].double().cpu().numpy()
+        v = np.ascontiguousarray(v)
+        gen = np.random.default_rng(seed)
+        top = float(v.max()) if v.size else 1.0
+        W0 = gen.uniform(0, top, (v.shape[0], rank))
+        H0 = gen.uniform(0, top, (rank, p_s))
+        return v, W0, H0
+    return f
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        d = json.loads(path.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    n, p, k, alpha, r, iters = WORKLOADS[args.workload]
+    steps = args.steps or iters
+    from nmf_rs import synthetic
+
+    # A bounded column slice of the workload, generated on the host.
+    def V_host_fn(p_s):
+        V = synthetic.counts_matrix(n, p_s, k, alpha, seed=0)
+        W0, H0 = synthetic.starting_point(V, r, seed=0)
+        return V, W0, H0
+
+    vals = []
+    base = None
+    for _ in range(max(1, args.warmup)):
+        base = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds / 3)
+    for _ in range(max(1, min(steps, 3))):
+        base = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds / 3)
+        vals.append(base["value"])
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": f"{args.method} iterations/s, {args.workload} {n}x{p} rank {r}",
+        "value": value,
+        "unit": "iters/s",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded generator, column slice)",
+        "config": {"workload": args.workload, "n": n, "p": p, "rank": r,
+                   "method": args.method},
+        "cpu_baseline": {**base, "value": value},
+        "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": ("the Rust reference cannot be built in this image (no cargo/rustc); "
+                 "this arm times the C restatement of its loop (oracle/) on host cores"),
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from nmf_rs import _native
+
+    n, p, k, alpha, r, iters = WORKLOADS[args.workload]
+    steps = args.steps or iters
+    warm = max(3, args.warmup)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    V64, ld64, V32, ld32, W0, H0 = device_workload(n, p, k, alpha, r, 1234 + rank, dev)
+    torch.cuda.synchronize()
+    ctx = _native.Context(local)
+    stream = torch.cuda.current_stream(dev)
+
+    def options(precision, iters_, refine=2):
+        o = _native.default_options()
+        o.method = _native.parse_method(args.method)
+        o.stop = 0
+        o.precision = _native.PRECISIONS[precision]
+        o.max_iter = iters_
+        o.refine_iters = refine
+        o.device = local
+        return o
+
+    def device_run(precision, iters_, W, H):
+        o = options(precision, iters_)
+        if precision == "fp32":
+            return ctx.run(o, n, p, r, V32.data_ptr(), _native.F32, ld32, W.data_ptr(), H.data_ptr(), v64_ptr=V64.data_ptr(), ldv64=ld64,
+                           stream=stream.cuda_stream)
+        return ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(), H.data_ptr(),
+                       stream=stream.cuda_stream)
+
+    def timed(precision, kernel_timing):
+        W = W0.clone()
+        H = H0.clone()
+        device_run(precision, warm, W, H)  # warm-up iterations (untimed)
+        W = W0.clone()
+        H = H0.clone()
+        torch.cuda.synchronize()
+        ctx.reset_timing()
+        ctx.set_timing(kernel_timing)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        device_run(precision, steps, W, H)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+        launches = ctx.launch_count()
+        classes = {}
+        if kernel_timing:
+            for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP, _native.KCLASS_OBJECTIVE,
+                       _native.KCLASS_OTHER):
+                classes[kc] = ctx.kernel_time(kc)
+        ctx.set_timing(False)
+        return ms, launches, classes, W, H
+
+    # Headline: the requested precision, with the clock sampler running.
+    with Clocks(local) as clk:
+        ms, launches, classes, W, H = timed(args.precision, True)
+    clocks = clk.summary()
+    ms_max = max_over_ranks(ms, world)
+    value = world * steps / (ms_max / 1000.0)
+
+    extra = {}
+    if args.precision == "fp32" and not args.no_fp64_compare:
+        ms64, _, _, W64, H64 = timed("fp64", False)
+        ms64_max = max_over_ranks(ms64, world)
+        fp64_value = world * steps / (ms64_max / 1000.0)
+        o_mixed = objective_torch(V64, p, W[:, :], H, args.method)
+        o_plain = objective_torch(V64, p, W64, H64, args.method)
+        extra = {
+            "fp64_iters_per_s": fp64_value,
+            "mixed_over_fp64": value / fp64_value,
+            "rel_objective_vs_fp64": abs(o_mixed - o_plain) / abs(o_plain),
+            "max_rel_dW_vs_fp64": float((W - W64).abs().max() / W64.abs().max()),
+        }
+
+    # Roofline of the dominant V-streaming class.
+    peak, peak_kind = measured_peaks()
+    s_main = 4 if args.precision == "fp32" else 8
+    refine = 2 if args.precision == "fp32" else 0
+    main_iters = max(0, steps - refine)
+    fp64_iters = steps - main_iters
+    bytes_per_class = n * p * (main_iters * s_main + fp64_iters * 8)
+    roof = None
+    if classes:
+        cand = {kc: classes[kc] for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP)}
+        dom = max(cand, key=lambda kc: cand[kc][1])
+        nl, tot_ms = cand[dom]
+        achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
+        roof = {
+            "bound": "hbm",
+            "kernel": "hstep_contract" if dom == _native.KCLASS_HSTEP else "rowpass (W step)",
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_kind": peak_kind,
+            "launches": nl,
+            "avg_launch_ms": tot_ms / max(nl, 1),
+            "traffic": None,
+            "class_ms": {name: classes[kc][1] for name, kc in
+                         (("hstep", 0), ("wstep", 1), ("objective", 2), ("other", 3))},
+        }
+
+    # End to end through the host-pointer C ABI.
+    e2e = None
+    if not args.no_e2e:
+        V_host = torch.empty((n, p), dtype=torch.float64, pin_memory=True)
+        V_host.copy_(V64[:, :p])
+        W0h = W0.cpu().numpy()
+        H0h = H0.cpu().numpy()
+        Vh = V_host.numpy()
+        del V64, V32
+        torch.cuda.empty_cache()
+        Wout = np.empty_like(W0h)
+        Hout = np.empty_like(H0h)
+        import ctypes
+
+        lib = _native.load()
+        o = options(args.precision, steps)
+        nd, ni = ctypes.c_int64(0), ctypes.c_int64(0)
+        dp = _native._ptr
+        # warm-up (allocates the library's workspace)
+        ow = options(args.precision, 1)
+        _native.check(lib.nmfcu_run(ctypes.byref(ow), n, p, r, dp(Vh), dp(W0h), dp(H0h), dp(Wout),
+                                    dp(Hout), None, 0, ctypes.byref(nd), ctypes.byref(ni)))
+        barrier(world)
+        t0 = time.perf_counter()
+        _native.check(lib.nmfcu_run(ctypes.byref(o), n, p, r, dp(Vh), dp(W0h), dp(H0h), dp(Wout),
+                                    dp(Hout), None, 0, ctypes.byref(nd), ctypes.byref(ni)))
+        t_e2e = time.perf_counter() - t0
+        t_e2e = max_over_ranks(t_e2e, world)
+        e2e = {"value": world * steps / t_e2e, "unit": "iters/s",
+               "h2d_bytes_per_step": (n * p + n * r + r * p) * 8 / steps,
+               "d2h_bytes_per_step": (n * r + r * p) * 8 / steps,
+               "note": "one nmfcu_run call per K steps: V, W0, H0 uploaded once, W, H read back once"}
+        del V_host
+    else:
+        del V64, V32
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from nmf_rs import synthetic
+
+        def V_host_fn(p_s):
+            V = synthetic.counts_matrix(n, p_s, k, alpha, seed=0)
+            W0s, H0s = synthetic.starting_point(V, r, seed=0)
+            return V, W0s, H0s
+
+        cpu = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds)
+
+    if rank == 0:
+        line = {
+            "metric": f"{args.method} iterations/s, {args.workload} {n}x{p} rank {r}, "
+                      f"{args.precision} form",
+            "value": value,
+            "unit": "iters/s",
+            "n_gpus": world,
+            "steps": steps,
+            "warmup": warm,
+            "ms_per_step": ms_max / steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded single-cell-like generator on the device)",
+            "config": {"workload": args.workload, "n": n, "p": p, "rank": r,
+                       "method": args.method, "precision": args.precision,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "V is larger than L2 (no flush needed)"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            **extra,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,210 @@
+/*
+ * nmfcu.h -- C ABI of the B200 NMF engine (libnmfcu.so).
+ *
+ * The reference, omicverse/rust-NMF, exposes its numerics only through the
+ * PyO3 module `nmf_rs._rust` (rust/src/lib.rs:2177-2187).  Every entry point
+ * below replaces one callable of that module, or one step of the loop behind
+ * it, and is cited to it.  Plain pointers and sizes only: no allocation
+ * crosses this boundary, the caller owns every buffer it passes.
+ *
+ * Conventions
+ *   - Matrices are row-major (C-contiguous) f64: V is n x p, W is n x r,
+ *     H is r x p -- the layout numpy hands the reference
+ *     (python/nmf_rs/__init__.py:235-240).
+ *   - Every call returns an nmfcu_status; on failure nmfcu_last_error()
+ *     returns a message for the calling thread.  Nothing aborts the process.
+ *   - All compute runs on the GPU.  There is no CPU fallback: without a
+ *     usable CUDA device the compute entry points return
+ *     NMFCU_ERR_NO_DEVICE.
+ */
+#ifndef NMFCU_H
+#define NMFCU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NMFCU_ABI_VERSION 1
+/* Largest factorisation rank the GPU kernels are built for. */
+#define NMFCU_MAX_RANK 32
+
+typedef enum nmfcu_status {
+    NMFCU_OK = 0,
+    NMFCU_ERR_INVALID_ARG = 1, /* bad shape / value; Python maps to ValueError      */
+    NMFCU_ERR_UNSUPPORTED = 2, /* method or rank not built; NotImplementedError      */
+    NMFCU_ERR_OOM = 3,         /* device allocation failed; MemoryError              */
+    NMFCU_ERR_CUDA = 4,        /* CUDA runtime error; RuntimeError                   */
+    NMFCU_ERR_NUMERIC = 5,     /* non-finite value where the contract forbids one   */
+    NMFCU_ERR_TIMEOUT = 6,     /* a bounded device wait gave up; RuntimeError        */
+    NMFCU_ERR_NO_DEVICE = 7    /* no CUDA device visible; RuntimeError               */
+} nmfcu_status;
+
+/* Algorithm ids: the variants of `Algo` (lib.rs:1472-1484), same order. */
+enum {
+    NMFCU_BRUNET = 0,
+    NMFCU_LEE = 1,
+    NMFCU_OFFSET = 2, /* not built: NMFCU_ERR_UNSUPPORTED */
+    NMFCU_NSNMF = 3,  /* not built */
+    NMFCU_HALS = 4,
+    NMFCU_EHALS = 5, /* not built */
+    NMFCU_DNMF = 6,
+    NMFCU_LSNMF = 7,  /* not built */
+    NMFCU_SNMF_R = 8, /* not built */
+    NMFCU_SNMF_L = 9  /* not built */
+};
+
+/* Stop ids: the variants of `Stop` (lib.rs:1507-1513). */
+enum { NMFCU_STOP_MAX_ITER = 0, NMFCU_STOP_STATIONARY = 1 };
+
+/* Arithmetic of the V contractions.  The reference is f64 throughout.
+ *   FP64   -- f64 V, f64 products and sums (the plain method).
+ *   FP32   -- V stored f32, products and per-thread sums in f32; every
+ *             reduction across threads, all update epilogues, Gram matrices,
+ *             rescaling, objective and stop test stay f64, and the last
+ *             `refine_iters` iterations run the FP64 path on the f64 V. */
+enum { NMFCU_PREC_FP64 = 0, NMFCU_PREC_FP32 = 1 };
+
+/* Keyword arguments of py_nmf_run (lib.rs:1912-1933), plus engine knobs. */
+typedef struct nmfcu_options {
+    int32_t method;        /* NMFCU_BRUNET ...                                  */
+    int32_t stop;          /* NMFCU_STOP_*                                      */
+    int32_t precision;     /* NMFCU_PREC_*  (engine knob, default FP64)         */
+    int32_t rescale;       /* lee: W columns to sum 1 each iteration (1)        */
+    int64_t max_iter;      /* iterations (the reference has no default here)   */
+    double eps;            /* 1e-9; brunet ignores it and uses DBL_EPSILON      */
+    double theta;          /* nsNMF only (accepted, unused by built methods)    */
+    double sparsity_h;     /* dnmf L1 on H (0)                                  */
+    double sparsity_w;     /* dnmf L1 on W (0)                                  */
+    double smoothness_h;   /* dnmf L2 on H (0)                                  */
+    double smoothness_w;   /* dnmf L2 on W (0)                                  */
+    double stationary_th;  /* DBL_EPSILON                                       */
+    int64_t check_interval; /* 50                                               */
+    int64_t check_niter;    /* 10                                               */
+    int32_t refine_iters;  /* FP32 precision: trailing FP64 iterations (2)      */
+    int32_t device;        /* CUDA device ordinal (0)                           */
+} nmfcu_options;
+
+/* Fill `o` with the py_nmf_run defaults (lib.rs:1919-1932); method brunet,
+ * max_iter 2000 (the Python default, python/nmf_rs/__init__.py:403). */
+void nmfcu_options_default(nmfcu_options *o);
+
+/* Algo::from_str (lib.rs:1486-1505): case-insensitive name or alias ->
+ * method id.  NMFCU_ERR_INVALID_ARG for an unknown name. */
+nmfcu_status nmfcu_parse_method(const char *name, int32_t *method);
+
+/* Stop::from_str (lib.rs:1515-1526). */
+nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop);
+
+/*
+ * nmfcu_run -- replaces py_nmf_run (lib.rs:1934-2169) for brunet, lee, hals
+ * and dnmf: the whole iteration loop (nmf_run_brunet :1529-1586,
+ * nmf_run_lee :1589-1647, nmf_run_hals :638-688, nmf_run_dnmf :827-906).
+ *
+ * Host pointers.  V (n x p), W0 (n x r), H0 (r x p) are read; W (n x r) and
+ * H (r x p) receive the result (they may alias W0 / H0).  `deviances` must
+ * hold `deviances_cap` >= max_iter + 1 doubles when stop is stationary (it
+ * may be NULL otherwise); *n_deviances receives how many were written and
+ * *n_iter the iteration count -- the `deviances` and `n_iter` of the
+ * reference's result dict (lib.rs:2158-2168).
+ */
+nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                       const double *V, const double *W0, const double *H0, double *W,
+                       double *H, double *deviances, int64_t deviances_cap,
+                       int64_t *n_deviances, int64_t *n_iter);
+
+/* Single-step updates on host pointers; each writes a fresh factor.
+ *   py_divergence_update_h (lib.rs:1851-1862 -> divergence_update_h_impl :120-144)
+ *   py_divergence_update_w (lib.rs:1866-1877 -> divergence_update_w_impl :151-204)
+ *   py_euclidean_update_h  (lib.rs:1880-1892 -> euclidean_update_h_impl  :249-276)
+ *   py_euclidean_update_w  (lib.rs:1895-1907 -> euclidean_update_w_impl  :281-322) */
+nmfcu_status nmfcu_update_h_divergence(int64_t n, int64_t p, int64_t r, const double *V,
+                                       const double *W, const double *H, double *H_out);
+nmfcu_status nmfcu_update_w_divergence(int64_t n, int64_t p, int64_t r, const double *V,
+                                       const double *W, const double *H, double *W_out);
+nmfcu_status nmfcu_update_h_euclidean(int64_t n, int64_t p, int64_t r, const double *V,
+                                      const double *W, const double *H, double eps,
+                                      double *H_out);
+nmfcu_status nmfcu_update_w_euclidean(int64_t n, int64_t p, int64_t r, const double *V,
+                                      const double *W, const double *H, double eps,
+                                      double *W_out);
+
+/* py_smoothing_matrix (lib.rs:2172-2175 -> smoothing_matrix :458-466):
+ * S = (1 - theta) I + (theta / r) 1 1^T into S (r x r).  Host arithmetic. */
+nmfcu_status nmfcu_smoothing_matrix(int64_t r, double theta, double *S);
+
+/* set_num_threads (lib.rs:1841-1847).  The GPU engine has no CPU thread
+ * pool; returns 0 (the reference's `false`, "pool not rebuilt"). */
+int32_t nmfcu_set_num_threads(int64_t n);
+
+/* Objectives on host pointers: kl_divergence (lib.rs:1410-1431) and
+ * euclidean_distance (lib.rs:1434-1445) of V against W H, computed on the
+ * GPU in f64 without materialising W H. */
+nmfcu_status nmfcu_divergence(int64_t n, int64_t p, int64_t r, const double *V,
+                              const double *W, const double *H, double *out);
+nmfcu_status nmfcu_distance(int64_t n, int64_t p, int64_t r, const double *V, const double *W,
+                            const double *H, double *out);
+
+/* ---------------------------------------------------------------------- */
+/* Device-resident API (inputs already in HBM).                            */
+/* ---------------------------------------------------------------------- */
+
+typedef struct nmfcu_context nmfcu_context;
+
+/* A context owns the device scratch of one device and is reused across
+ * calls; one context per host thread (calls on one context serialise). */
+nmfcu_status nmfcu_context_create(int32_t device, nmfcu_context **ctx);
+void nmfcu_context_destroy(nmfcu_context *ctx);
+
+/* Element type of a device V. */
+enum { NMFCU_F64 = 0, NMFCU_F32 = 1 };
+
+/*
+ * nmfcu_run_device -- nmfcu_run on device pointers, enqueued on `stream`
+ * (a cudaStream_t, NULL for the legacy default stream).
+ *   dV      n x p, leading dimension ldv (elements), type v_dtype.  For
+ *           precision FP32 pass the f32 V here and the f64 V in dV64 (used by
+ *           the FP64 refinement iterations and the objective); for FP64 pass
+ *           the f64 V and dV64 = NULL.
+ *   dW, dH  n x r and r x p f64, W0/H0 on entry, the result on exit.
+ *   d_dev   device array of >= max_iter + 1 doubles (stationary stop) or NULL.
+ * *n_iter / *n_deviances are written after the stream has been synchronised
+ * (the call returns when the result is complete).
+ */
+nmfcu_status nmfcu_run_device(nmfcu_context *ctx, const nmfcu_options *opt, int64_t n,
+                              int64_t p, int64_t r, const void *dV, int32_t v_dtype,
+                              int64_t ldv, const double *dV64, int64_t ldv64, double *dW,
+                              double *dH, double *d_dev, int64_t *n_deviances, int64_t *n_iter,
+                              void *stream);
+
+/* Per-kernel CUDA-event timing inside nmfcu_run_device (off by default).
+ * Kernel classes: 0 = H-step V contraction, 1 = W-step V contraction,
+ * 2 = objective V pass, 3 = everything else (grams, epilogues, stop). */
+enum { NMFCU_KCLASS_HSTEP = 0, NMFCU_KCLASS_WSTEP = 1, NMFCU_KCLASS_OBJECTIVE = 2,
+       NMFCU_KCLASS_OTHER = 3, NMFCU_KCLASS_COUNT = 4 };
+nmfcu_status nmfcu_context_set_timing(nmfcu_context *ctx, int32_t enabled);
+/* Launch count and summed event time (ms) of one kernel class since the
+ * last reset; the call synchronises the context's events. */
+nmfcu_status nmfcu_context_kernel_time(nmfcu_context *ctx, int32_t kclass, int64_t *launches,
+                                       double *total_ms);
+nmfcu_status nmfcu_context_reset_timing(nmfcu_context *ctx);
+/* Kernels launched by this context since the last reset (all classes). */
+int64_t nmfcu_context_launch_count(nmfcu_context *ctx);
+
+/* ---------------------------------------------------------------------- */
+/* Misc                                                                    */
+/* ---------------------------------------------------------------------- */
+
+const char *nmfcu_last_error(void);
+const char *nmfcu_status_string(nmfcu_status s);
+int32_t nmfcu_abi_version(void);
+/* Number of visible CUDA devices (0 without a GPU; never fails). */
+int32_t nmfcu_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NMFCU_H */

@@ -1,0 +1,172 @@
+"""CPU oracle for the NMF iteration loop -- TEST INFRASTRUCTURE ONLY.
+
+A ctypes wrapper around ``liboracle.so`` (built from ``nmf_oracle.c`` by
+``oracle/Makefile``), which restates the f64 loops of omicverse/rust-NMF
+``rust/src/lib.rs`` (brunet :1529-1586, lee :1589-1647, hals :638-688,
+dnmf :827-906, objectives :1410-1445, stationary stop :1336-1401).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker / baseline.
+The shipped library never calls it.
+
+Parity status: pinned against the reference's recorded outputs in
+``examples/tutorial_quickstart.ipynb`` (fixtures in ``tests/golden/``).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+_LIB_PATH = _HERE / "liboracle.so"
+_lib = None
+
+METHODS = {"brunet": 0, "lee": 1, "hals": 4, "dnmf": 6}
+STOPS = {"max_iter": 0, "fixed": 0, "none": 0, "stationary": 1}
+
+_i64 = ctypes.c_int64
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build(force: bool = False) -> Path:
+    """Compile liboracle.so with the committed Makefile."""
+    if force or not _LIB_PATH.exists() or (
+        _LIB_PATH.stat().st_mtime < (_HERE / "nmf_oracle.c").stat().st_mtime
+    ):
+        subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
+    return _LIB_PATH
+
+
+def _load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        build()
+    lib = ctypes.CDLL(str(_LIB_PATH))
+    lib.orc_nmf_run.restype = ctypes.c_int
+    lib.orc_nmf_run.argtypes = [
+        ctypes.c_int, _i64, _i64, _i64, _dp, _dp, _dp, _i64, ctypes.c_double, ctypes.c_int,
+        ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+        ctypes.c_double, _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+        ctypes.c_int,
+    ]
+    for name in ("orc_update_h_brunet", "orc_update_w_brunet"):
+        f = getattr(lib, name)
+        f.restype = None
+        f.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp, _dp, ctypes.c_int]
+    for name in ("orc_update_h_lee", "orc_update_w_lee"):
+        f = getattr(lib, name)
+        f.restype = None
+        f.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp, ctypes.c_double, _dp, ctypes.c_int]
+    for name in ("orc_kl_divergence", "orc_euclidean_distance"):
+        f = getattr(lib, name)
+        f.restype = ctypes.c_double
+        f.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp]
+    _lib = lib
+    return lib
+
+
+def _c(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def nmf_run(method: str, V, W0, H0, max_iter: int, *, eps: float = 1e-9, rescale: bool = True,
+            sparsity_h: float = 0.0, sparsity_w: float = 0.0, smoothness_h: float = 0.0,
+            smoothness_w: float = 0.0, stop: str = "max_iter",
+            stationary_th: float = 2.220446049250313e-16, check_interval: int = 50,
+            check_niter: int = 10, num_threads: int | None = None) -> dict:
+    """Oracle counterpart of ``py_nmf_run`` (lib.rs:1934-2169) for the four
+    in-scope methods.  Returns ``{"W", "H", "n_iter", "deviances"}``."""
+    lib = _load()
+    V = _c(V)
+    W = _c(W0).copy()
+    H = _c(H0).copy()
+    n, p = V.shape
+    r = W.shape[1]
+    dev = np.zeros(max(int(max_iter) + 1, 1), dtype=np.float64)
+    nd = _i64(0)
+    ni = _i64(0)
+    rc = lib.orc_nmf_run(
+        METHODS[method], n, p, r, _ptr(V), _ptr(W), _ptr(H), int(max_iter), float(eps),
+        int(bool(rescale)), float(sparsity_h), float(sparsity_w), float(smoothness_h),
+        float(smoothness_w), STOPS[stop.lower()], float(stationary_th), int(check_interval),
+        int(check_niter), _ptr(dev), ctypes.byref(nd), ctypes.byref(ni),
+        int(num_threads or os.cpu_count() or 1),
+    )
+    if rc == -2:
+        raise ZeroDivisionError("stationary stop evaluated `iter % check_interval` with 0")
+    if rc != 0:
+        raise ValueError(f"oracle: unsupported method {method!r}")
+    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": dev[: nd.value].copy()}
+
+
+def nmf_method(method: str, V, W0, H0, max_iter: int, *, eps=1e-9, rescale=True,
+               sparsity=0.01, smoothness=1.0, stop="max_iter", **kw) -> dict:
+    """Same as :func:`nmf_run` but with the Python-level routing of
+    ``sparsity``/``smoothness`` that ``nmf()`` applies (python/nmf_rs/__init__.py:528-538):
+    dnmf gets ``sparsity`` on both factors and no L2, the others get none."""
+    if method == "dnmf":
+        sh = sw = float(sparsity)
+    else:
+        sh = sw = 0.0
+    return nmf_run(method, V, W0, H0, max_iter, eps=eps, rescale=rescale, sparsity_h=sh,
+                   sparsity_w=sw, smoothness_h=0.0, smoothness_w=0.0, stop=stop, **kw)
+
+
+def update_h_brunet(V, W, H, num_threads=None):
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    out = np.empty_like(H)
+    lib.orc_update_h_brunet(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(W), _ptr(H),
+                            _ptr(out), int(num_threads or os.cpu_count() or 1))
+    return out
+
+
+def update_w_brunet(V, W, H, num_threads=None):
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    out = np.empty_like(W)
+    lib.orc_update_w_brunet(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(W), _ptr(H),
+                            _ptr(out), int(num_threads or os.cpu_count() or 1))
+    return out
+
+
+def update_h_lee(V, W, H, eps=1e-9, num_threads=None):
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    out = np.empty_like(H)
+    lib.orc_update_h_lee(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(W), _ptr(H),
+                         float(eps), _ptr(out), int(num_threads or os.cpu_count() or 1))
+    return out
+
+
+def update_w_lee(V, W, H, eps=1e-9, num_threads=None):
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    out = np.empty_like(W)
+    lib.orc_update_w_lee(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(W), _ptr(H),
+                         float(eps), _ptr(out), int(num_threads or os.cpu_count() or 1))
+    return out
+
+
+def kl_divergence(V, W, H) -> float:
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    return float(lib.orc_kl_divergence(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(W),
+                                       _ptr(H)))
+
+
+def euclidean_distance(V, W, H) -> float:
+    lib = _load()
+    V, W, H = _c(V), _c(W), _c(H)
+    return float(lib.orc_euclidean_distance(V.shape[0], V.shape[1], W.shape[1], _ptr(V),
+                                            _ptr(W), _ptr(H)))

@@ -1,0 +1,548 @@
+/*
+ * nmf_oracle.c -- CPU restatement of the reference NMF iteration loop.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA library
+ * is compared against (parity tests, smoke(), and the CPU-baseline leg of
+ * bench.py).  Nothing in the shipped library links, loads or calls it.
+ *
+ * It restates, in plain C, the f64 algorithms of omicverse/rust-NMF
+ * `rust/src/lib.rs` (cited per function below): same loop structure, same
+ * summation order (forward / reverse exactly as cited), no FMA contraction
+ * (build with -ffp-contract=off), and OpenMP over H columns / W rows the way
+ * the reference uses rayon.  Every output element is reduced sequentially by
+ * one thread, so results do not depend on the thread count.
+ *
+ * Third-party arithmetic that the reference delegates to `matrixmultiply
+ * 0.3.10` through `ndarray 0.16.1` (rust/Cargo.lock:86-88, 105-107) -- the
+ * HALS/dnmf products W^T V and V H^T (lib.rs:514, 536) and the dense WH used
+ * by the objectives (lib.rs:57) -- is restated as a plain forward-order dot
+ * product.  matrixmultiply's own blocking order is not pinned by any
+ * reference test, so HALS/dnmf/objective parity is a tolerance, not bits.
+ *
+ * Pinned against the reference's recorded outputs in
+ * examples/tutorial_quickstart.ipynb (see tests/golden/).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* Method ids: same numbering as include/nmfcu.h. */
+enum { ORC_BRUNET = 0, ORC_LEE = 1, ORC_HALS = 4, ORC_DNMF = 6 };
+enum { ORC_STOP_MAX_ITER = 0, ORC_STOP_STATIONARY = 1 };
+
+typedef int64_t i64;
+
+/* transpose_owned, lib.rs:28-38: a (m x n) -> a_t (n x m). */
+static double *transpose(const double *a, i64 m, i64 n) {
+    double *t = (double *)malloc(sizeof(double) * (size_t)(m * n > 0 ? m * n : 1));
+    for (i64 i = 0; i < m; i++)
+        for (i64 j = 0; j < n; j++) t[j * m + i] = a[i * n + j];
+    return t;
+}
+
+static void set_threads(int nt) {
+#ifdef _OPENMP
+    if (nt > 0) omp_set_num_threads(nt);
+#else
+    (void)nt;
+#endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Brunet / KL multiplicative updates                                        */
+/* ------------------------------------------------------------------------ */
+
+/* divergence_update_h_inner, lib.rs:74-115.  v_t is p x n, w is n x r,
+ * w_t is r x n, h is r x p, sum_w has r entries.  Writes hp (r x p). */
+static void div_update_h_inner(i64 n, i64 p, i64 r, const double *v_t, const double *w,
+                               const double *w_t, const double *h, const double *sum_w,
+                               double *hp) {
+#pragma omp parallel
+    {
+        double *h_col = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+        double *wh_col = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(static)
+        for (i64 j = 0; j < p; j++) {
+            for (i64 k = 0; k < r; k++) h_col[k] = h[k * p + j];
+            for (i64 u = 0; u < n; u++) {
+                double wh = 0.0;
+                for (i64 k = 0; k < r; k++) wh += w[u * r + k] * h_col[k];
+                wh_col[u] = (wh != 0.0) ? v_t[j * n + u] / wh : 0.0;
+            }
+            for (i64 i = 0; i < r; i++) {
+                double tmp = 0.0;
+                for (i64 u = 0; u < n; u++) tmp += w_t[i * n + u] * wh_col[u];
+                hp[i * p + j] = h_col[i] * tmp / sum_w[i];
+            }
+        }
+        free(h_col);
+        free(wh_col);
+    }
+}
+
+/* Column sums of W in forward order, lib.rs:1563-1568 / 132-139. */
+static void col_sums(i64 n, i64 r, const double *w, double *sum_w) {
+    for (i64 k = 0; k < r; k++) {
+        double s = 0.0;
+        for (i64 u = 0; u < n; u++) s += w[u * r + k];
+        sum_w[k] = s;
+    }
+}
+
+/* divergence_update_w_impl, lib.rs:151-204.  Writes wp (n x r). */
+static void div_update_w(i64 n, i64 p, i64 r, const double *v, const double *w,
+                         const double *h, double *wp) {
+    double *sum_h = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    for (i64 k = 0; k < r; k++) {
+        double s = 0.0;
+        for (i64 u = 0; u < p; u++) s += h[k * p + u];
+        sum_h[k] = s;
+    }
+    double *h_t = transpose(h, r, p); /* p x r, lib.rs:175-180 */
+#pragma omp parallel
+    {
+        double *wh_row = (double *)malloc(sizeof(double) * (size_t)(p > 0 ? p : 1));
+#pragma omp for schedule(static)
+        for (i64 i = 0; i < n; i++) {
+            for (i64 u = 0; u < p; u++) {
+                double wh = 0.0;
+                for (i64 k = 0; k < r; k++) wh += w[i * r + k] * h_t[u * r + k];
+                wh_row[u] = (wh != 0.0) ? v[i * p + u] / wh : 0.0;
+            }
+            for (i64 j = 0; j < r; j++) {
+                double tmp = 0.0;
+                for (i64 u = 0; u < p; u++) tmp += h[j * p + u] * wh_row[u];
+                wp[i * r + j] = w[i * r + j] * tmp / sum_h[j];
+            }
+        }
+        free(wh_row);
+    }
+    free(h_t);
+    free(sum_h);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Lee / Frobenius multiplicative updates                                    */
+/* ------------------------------------------------------------------------ */
+
+/* W^T W with reverse-u order from w_t, lib.rs:1622-1631 and 264-273. */
+static void wtw_rev(i64 n, i64 r, const double *w_t, double *wtw) {
+    for (i64 i = 0; i < r; i++)
+        for (i64 j = 0; j < r; j++) {
+            double s = 0.0;
+            for (i64 u = n - 1; u >= 0; u--) s += w_t[i * n + u] * w_t[j * n + u];
+            wtw[i * r + j] = s;
+        }
+}
+
+/* euclidean_update_h_inner, lib.rs:213-245. */
+static void euc_update_h_inner(i64 n, i64 p, i64 r, const double *v_t, const double *w_t,
+                               const double *h, const double *wtw, double eps, double *hp) {
+#pragma omp parallel for schedule(static)
+    for (i64 j = 0; j < p; j++) {
+        for (i64 i = 0; i < r; i++) {
+            double numer = 0.0;
+            for (i64 u = n - 1; u >= 0; u--) numer += w_t[i * n + u] * v_t[j * n + u];
+            double den = 0.0;
+            for (i64 l = r - 1; l >= 0; l--) den += wtw[i * r + l] * h[l * p + j];
+            double temp = h[i * p + j] * numer;
+            hp[i * p + j] = (temp > eps ? temp : eps) / (den + eps);
+        }
+    }
+}
+
+/* euclidean_update_w_impl, lib.rs:281-322. */
+static void euc_update_w(i64 n, i64 p, i64 r, const double *v, const double *w,
+                         const double *h, double eps, double *wp) {
+    double *hht = (double *)malloc(sizeof(double) * (size_t)(r * r > 0 ? r * r : 1));
+    for (i64 j = 0; j < r; j++)
+        for (i64 i = 0; i < r; i++) {
+            double s = 0.0;
+            for (i64 u = p - 1; u >= 0; u--) s += h[j * p + u] * h[i * p + u];
+            hht[i * r + j] = s;
+        }
+#pragma omp parallel for schedule(static)
+    for (i64 i = 0; i < n; i++) {
+        for (i64 j = 0; j < r; j++) {
+            double numer = 0.0;
+            for (i64 u = p - 1; u >= 0; u--) numer += v[i * p + u] * h[j * p + u];
+            double den = 0.0;
+            for (i64 l = r - 1; l >= 0; l--) den += w[i * r + l] * hht[l * r + j];
+            double temp = w[i * r + j] * numer;
+            wp[i * r + j] = (temp < eps ? eps : temp) / (den + eps);
+        }
+    }
+    free(hht);
+}
+
+/* ------------------------------------------------------------------------ */
+/* HALS / dnmf                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Rust f64::max: returns the non-NaN operand if one is NaN. */
+static double rmax(double a, double b) {
+    if (isnan(a)) return b;
+    if (isnan(b)) return a;
+    return a > b ? a : b;
+}
+
+/* compute_wtv, lib.rs:493-519 (matrixmultiply restated as forward dots).
+ * v_t is p x n, w_t is r x n; writes wtv (r x p). */
+static void compute_wtv(i64 n, i64 p, i64 r, const double *w_t, const double *v_t, double *wtv) {
+#pragma omp parallel for schedule(static)
+    for (i64 j = 0; j < p; j++)
+        for (i64 k = 0; k < r; k++) {
+            double s = 0.0;
+            for (i64 u = 0; u < n; u++) s += w_t[k * n + u] * v_t[j * n + u];
+            wtv[k * p + j] = s;
+        }
+}
+
+/* compute_vht, lib.rs:522-540; writes vht (n x r). */
+static void compute_vht(i64 n, i64 p, i64 r, const double *v, const double *h, double *vht) {
+#pragma omp parallel for schedule(static)
+    for (i64 i = 0; i < n; i++)
+        for (i64 k = 0; k < r; k++) {
+            double s = 0.0;
+            for (i64 u = 0; u < p; u++) s += v[i * p + u] * h[k * p + u];
+            vht[i * r + k] = s;
+        }
+}
+
+/* compute_wtw_from_wt, lib.rs:543-560 (forward order). */
+static void wtw_fwd(i64 n, i64 r, const double *w_t, double *wtw) {
+    for (i64 k = 0; k < r; k++)
+        for (i64 j = 0; j < r; j++) {
+            double s = 0.0;
+            for (i64 i = 0; i < n; i++) s += w_t[k * n + i] * w_t[j * n + i];
+            wtw[k * r + j] = s;
+        }
+}
+
+/* compute_hht, lib.rs:563-579 (forward order). */
+static void hht_fwd(i64 p, i64 r, const double *h, double *hht) {
+    for (i64 k = 0; k < r; k++)
+        for (i64 j = 0; j < r; j++) {
+            double s = 0.0;
+            for (i64 u = 0; u < p; u++) s += h[k * p + u] * h[j * p + u];
+            hht[k * r + j] = s;
+        }
+}
+
+/* hals_update_h (lib.rs:582-608) when lambda = gamma = 0 and the plain
+ * max(wtw_kk, eps) denominator; hals_update_h_reg (lib.rs:1068-1092) with
+ * reg != 0.  The two differ only in `wtv - lambda` and `wtw_kk + gamma`;
+ * with lambda = gamma = 0 the reg form is bitwise the plain form
+ * (x - 0.0 == x, x + 0.0 == x for every non-NaN, non -0.0 x). */
+static void hals_update_h(i64 p, i64 r, double *h, const double *wtv, const double *wtw,
+                          double lambda, double gamma, int reg, double eps) {
+#pragma omp parallel
+    {
+        double *hc = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+#pragma omp for schedule(static)
+        for (i64 u = 0; u < p; u++) {
+            for (i64 k = 0; k < r; k++) hc[k] = h[k * p + u];
+            for (i64 k = 0; k < r; k++) {
+                double s = reg ? wtv[k * p + u] - lambda : wtv[k * p + u];
+                for (i64 j = 0; j < r; j++)
+                    if (j != k) s -= wtw[k * r + j] * hc[j];
+                double d = reg ? rmax(wtw[k * r + k] + gamma, eps) : rmax(wtw[k * r + k], eps);
+                double val = s / d;
+                hc[k] = val > eps ? val : eps;
+            }
+            for (i64 k = 0; k < r; k++) h[k * p + u] = hc[k];
+        }
+        free(hc);
+    }
+}
+
+/* hals_update_w (lib.rs:611-635) / hals_update_w_reg (lib.rs:1095-1119). */
+static void hals_update_w(i64 n, i64 r, double *w, const double *vht, const double *hht,
+                          double lambda, double gamma, int reg, double eps) {
+#pragma omp parallel for schedule(static)
+    for (i64 i = 0; i < n; i++) {
+        double *wr = w + i * r;
+        for (i64 k = 0; k < r; k++) {
+            double s = reg ? vht[i * r + k] - lambda : vht[i * r + k];
+            for (i64 j = 0; j < r; j++)
+                if (j != k) s -= hht[k * r + j] * wr[j];
+            double d = reg ? rmax(hht[k * r + k] + gamma, eps) : rmax(hht[k * r + k], eps);
+            double val = s / d;
+            wr[k] = val > eps ? val : eps;
+        }
+    }
+}
+
+/* extract_diagonal, lib.rs:808-824: unit-norm W columns / H rows; d[k]. */
+static void extract_diagonal(i64 n, i64 p, i64 r, double *w, double *h, double *d) {
+    for (i64 k = 0; k < r; k++) {
+        double nw = 0.0, nh = 0.0;
+        for (i64 i = 0; i < n; i++) nw += w[i * r + k] * w[i * r + k];
+        for (i64 j = 0; j < p; j++) nh += h[k * p + j] * h[k * p + j];
+        nw = sqrt(nw);
+        nh = sqrt(nh);
+        double dk = nw * nh;
+        if (nw > 0.0)
+            for (i64 i = 0; i < n; i++) w[i * r + k] /= nw;
+        if (nh > 0.0)
+            for (i64 j = 0; j < p; j++) h[k * p + j] /= nh;
+        d[k] = dk;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Objectives and stopping                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* wh_dense (lib.rs:43-61) element, restated as a forward dot. */
+static inline double wh_at(i64 p, i64 r, const double *w, const double *h, i64 i, i64 j) {
+    double s = 0.0;
+    for (i64 k = 0; k < r; k++) s += w[i * r + k] * h[k * p + j];
+    return s;
+}
+
+/* kl_divergence, lib.rs:1410-1431 (j outer, i inner, one running sum). */
+double orc_kl_divergence(i64 n, i64 p, i64 r, const double *v, const double *w, const double *h) {
+    double s = 0.0;
+    for (i64 j = 0; j < p; j++)
+        for (i64 i = 0; i < n; i++) {
+            double vv = v[i * p + j];
+            double ww = wh_at(p, r, w, h, i, j);
+            if (vv > 0.0) {
+                if (ww > 0.0) s += vv * log(vv / ww) - vv + ww;
+            } else {
+                s += ww;
+            }
+        }
+    return s;
+}
+
+/* euclidean_distance, lib.rs:1434-1445: 0.5 * sum((V - WH)^2). */
+double orc_euclidean_distance(i64 n, i64 p, i64 r, const double *v, const double *w,
+                              const double *h) {
+    double s = 0.0;
+    for (i64 j = 0; j < p; j++)
+        for (i64 i = 0; i < n; i++) {
+            double d = v[i * p + j] - wh_at(p, r, w, h, i, j);
+            s += d * d;
+        }
+    return 0.5 * s;
+}
+
+/* StationaryStop, lib.rs:1336-1401. */
+typedef struct {
+    i64 check_interval, check_niter;
+    double threshold, last_max, last_min;
+    i64 n_collected;
+} stationary_t;
+
+static void st_reset(stationary_t *s) {
+    s->last_max = -INFINITY;
+    s->last_min = INFINITY;
+    s->n_collected = 0;
+}
+static void st_record(stationary_t *s, double v) {
+    if (v > s->last_max) s->last_max = v;
+    if (v < s->last_min) s->last_min = v;
+    s->n_collected++;
+}
+static int st_should_stop(stationary_t *s, i64 i, double dev) {
+    if (isnan(dev)) return 1;
+    if (i == 0) {
+        st_reset(s);
+        st_record(s, dev);
+        return 0;
+    }
+    if (s->n_collected == 0) {
+        /* `i % check_interval` panics in the reference when check_interval
+         * is 0; it is only evaluated once the window is empty. */
+        if (s->check_interval == 0) return -1;
+        if (i % s->check_interval != 0) return 0;
+    }
+    st_record(s, dev);
+    if (s->n_collected == s->check_niter + 1) {
+        double crit = fabs(s->last_max - s->last_min) / (double)s->check_niter;
+        if (crit <= s->threshold) return 1;
+        st_reset(s);
+    }
+    return 0;
+}
+
+/* pmax_inplace, lib.rs:1452-1458. */
+static void pmax_inplace(double *x, i64 len, double eps) {
+    for (i64 i = 0; i < len; i++)
+        if (x[i] < eps) x[i] = eps;
+}
+
+/* col_rescale, lib.rs:1461-1470. */
+static void col_rescale(i64 n, i64 r, double *w) {
+    for (i64 j = 0; j < r; j++) {
+        double s = 0.0;
+        for (i64 i = 0; i < n; i++) s += w[i * r + j];
+        if (s > 0.0)
+            for (i64 i = 0; i < n; i++) w[i * r + j] /= s;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Public oracle entry points                                                */
+/* ------------------------------------------------------------------------ */
+
+/* Single-step updates: py_divergence_update_{h,w} / py_euclidean_update_{h,w}
+ * (lib.rs:1849-1907 -> divergence_update_h_impl :120-144,
+ * divergence_update_w_impl :151-204, euclidean_update_h_impl :249-276,
+ * euclidean_update_w_impl :281-322). */
+void orc_update_h_brunet(i64 n, i64 p, i64 r, const double *v, const double *w, const double *h,
+                         double *hp, int nt) {
+    set_threads(nt);
+    double *sum_w = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    col_sums(n, r, w, sum_w);
+    double *v_t = transpose(v, n, p);
+    double *w_t = transpose(w, n, r);
+    div_update_h_inner(n, p, r, v_t, w, w_t, h, sum_w, hp);
+    free(v_t);
+    free(w_t);
+    free(sum_w);
+}
+
+void orc_update_w_brunet(i64 n, i64 p, i64 r, const double *v, const double *w, const double *h,
+                         double *wp, int nt) {
+    set_threads(nt);
+    div_update_w(n, p, r, v, w, h, wp);
+}
+
+void orc_update_h_lee(i64 n, i64 p, i64 r, const double *v, const double *w, const double *h,
+                      double eps, double *hp, int nt) {
+    set_threads(nt);
+    double *v_t = transpose(v, n, p);
+    double *w_t = transpose(w, n, r);
+    double *wtw = (double *)malloc(sizeof(double) * (size_t)(r * r > 0 ? r * r : 1));
+    wtw_rev(n, r, w_t, wtw);
+    euc_update_h_inner(n, p, r, v_t, w_t, h, wtw, eps, hp);
+    free(wtw);
+    free(v_t);
+    free(w_t);
+}
+
+void orc_update_w_lee(i64 n, i64 p, i64 r, const double *v, const double *w, const double *h,
+                      double eps, double *wp, int nt) {
+    set_threads(nt);
+    euc_update_w(n, p, r, v, w, h, eps, wp);
+}
+
+/*
+ * orc_nmf_run: the full loop for brunet / lee / hals / dnmf.
+ *   nmf_run_brunet lib.rs:1529-1586, nmf_run_lee :1589-1647,
+ *   nmf_run_hals :638-688, nmf_run_dnmf :827-906.
+ * W (n x r) and H (r x p) hold W0/H0 on entry and the result on exit.
+ * dev must hold max_iter + 1 doubles.  Returns 0, or -1 for an unknown
+ * method, -2 when the stationary stop evaluates `i % 0` (the reference
+ * panics there, lib.rs:1388).
+ */
+int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, double *h,
+                i64 max_iter, double eps, int rescale, double sparsity_h, double sparsity_w,
+                double smoothness_h, double smoothness_w, int stop, double stationary_th,
+                i64 check_interval, i64 check_niter, double *dev, i64 *n_dev, i64 *n_iter,
+                int nt) {
+    if (method != ORC_BRUNET && method != ORC_LEE && method != ORC_HALS && method != ORC_DNMF)
+        return -1;
+    set_threads(nt);
+    stationary_t st = {check_interval, check_niter, stationary_th, -INFINITY, INFINITY, 0};
+    i64 nd = 0;
+    const int kl = (method == ORC_BRUNET);
+    const int stat = (stop == ORC_STOP_STATIONARY);
+    const double beps = DBL_EPSILON; /* lib.rs:1539 */
+
+    double *v_t = transpose(v, n, p); /* lib.rs:1546 / 1606 / 652 / 844 */
+    double *tmp_h = (double *)malloc(sizeof(double) * (size_t)(r * p > 0 ? r * p : 1));
+    double *tmp_w = (double *)malloc(sizeof(double) * (size_t)(n * r > 0 ? n * r : 1));
+    double *sq = (double *)malloc(sizeof(double) * (size_t)(r * r > 0 ? r * r : 1));
+    double *sq2 = (double *)malloc(sizeof(double) * (size_t)(r * r > 0 ? r * r : 1));
+    double *sum_w = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    double *dg = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    double *wtv = (method == ORC_HALS || method == ORC_DNMF)
+                      ? (double *)malloc(sizeof(double) * (size_t)(r * p > 0 ? r * p : 1))
+                      : NULL;
+    double *vht = (method == ORC_HALS || method == ORC_DNMF)
+                      ? (double *)malloc(sizeof(double) * (size_t)(n * r > 0 ? n * r : 1))
+                      : NULL;
+
+    i64 iter = 0;
+    int done = 0, status = 0;
+    if (stat) {
+        double d = kl ? orc_kl_divergence(n, p, r, v, w, h) : orc_euclidean_distance(n, p, r, v, w, h);
+        dev[nd++] = d;
+        if (st_should_stop(&st, 0, d) != 0) done = 1;
+    }
+    while (!done && iter < max_iter) {
+        iter++;
+        double *w_t = transpose(w, n, r);
+        if (method == ORC_BRUNET) {
+            col_sums(n, r, w, sum_w);
+            div_update_h_inner(n, p, r, v_t, w, w_t, h, sum_w, tmp_h);
+            memcpy(h, tmp_h, sizeof(double) * (size_t)(r * p));
+            div_update_w(n, p, r, v, w, h, tmp_w);
+            memcpy(w, tmp_w, sizeof(double) * (size_t)(n * r));
+            if (iter % 10 == 0) {
+                pmax_inplace(h, r * p, beps);
+                pmax_inplace(w, n * r, beps);
+            }
+        } else if (method == ORC_LEE) {
+            wtw_rev(n, r, w_t, sq);
+            euc_update_h_inner(n, p, r, v_t, w_t, h, sq, eps, tmp_h);
+            memcpy(h, tmp_h, sizeof(double) * (size_t)(r * p));
+            euc_update_w(n, p, r, v, w, h, eps, tmp_w);
+            memcpy(w, tmp_w, sizeof(double) * (size_t)(n * r));
+            if (rescale) col_rescale(n, r, w);
+        } else {
+            const int reg = (method == ORC_DNMF);
+            compute_wtv(n, p, r, w_t, v_t, wtv);
+            wtw_fwd(n, r, w_t, sq);
+            hals_update_h(p, r, h, wtv, sq, sparsity_h, smoothness_h, reg, eps);
+            compute_vht(n, p, r, v, h, vht);
+            hht_fwd(p, r, h, sq2);
+            hals_update_w(n, r, w, vht, sq2, sparsity_w, smoothness_w, reg, eps);
+            if (reg) {
+                extract_diagonal(n, p, r, w, h, dg);
+                for (i64 k = 0; k < r; k++)
+                    for (i64 j = 0; j < p; j++) h[k * p + j] *= dg[k];
+            }
+        }
+        free(w_t);
+        if (stat) {
+            double d = kl ? orc_kl_divergence(n, p, r, v, w, h)
+                          : orc_euclidean_distance(n, p, r, v, w, h);
+            dev[nd++] = d;
+            int rc = st_should_stop(&st, iter, d);
+            if (rc < 0) {
+                status = -2;
+                break;
+            }
+            if (rc) break;
+        }
+    }
+    /* dnmf stopped at iteration 0 extracts the diagonal before returning
+     * (lib.rs:852-855). */
+    if (method == ORC_DNMF && stat && iter == 0 && done) extract_diagonal(n, p, r, w, h, dg);
+
+    *n_dev = nd;
+    *n_iter = iter;
+    free(v_t);
+    free(tmp_h);
+    free(tmp_w);
+    free(sq);
+    free(sq2);
+    free(sum_w);
+    free(dg);
+    free(wtv);
+    free(vht);
+    return status;
+}
+
+/* Build identification so the Python side can tell a stale build apart. */
+int orc_version(void) { return 1; }

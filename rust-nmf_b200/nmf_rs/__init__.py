@@ -1,0 +1,302 @@
+"""nmf_rs -- non-negative matrix factorisation on one NVIDIA B200.
+
+Drop-in for the Python surface of omicverse/rust-NMF
+(``python/nmf_rs/__init__.py``): the same ``nmf()``, ``NMFResult``,
+single-step updates, ``random_init``, ``nndsvd_init``, ``smoothing_matrix``
+and ``set_num_threads``, with the iteration loop running as hand-written
+sm_100a CUDA kernels behind the C ABI of ``include/nmfcu.h``.
+
+Built methods: ``brunet`` (KL), ``lee`` (Frobenius), ``hals`` and ``dnmf``,
+each with ``stop='max_iter'`` or ``'stationary'``.  The other reference
+methods (offset, nsNMF, ehals, lsNMF, snmf/r, snmf/l) raise
+``NotImplementedError``.  There is no CPU fallback: without the CUDA library
+or a GPU every compute call raises ``RuntimeError``.
+
+Engine extensions (keyword-only, defaults keep the reference's behaviour):
+``precision='fp64'|'fp32'`` and ``refine_iters`` on :func:`nmf`.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _native
+
+__all__ = [
+    "NMFResult",
+    "nmf",
+    "update_h_brunet",
+    "update_w_brunet",
+    "update_h_lee",
+    "update_w_lee",
+    "smoothing_matrix",
+    "random_init",
+    "nndsvd_init",
+    "cv_rank",
+    "set_num_threads",
+]
+
+
+# =============================================================================
+# Result type (python/nmf_rs/__init__.py:59-99)
+# =============================================================================
+
+@dataclass
+class NMFResult:
+    """Outcome of an NMF run: ``W`` (n x rank), ``H`` (rank x p), ``n_iter``,
+    ``deviances`` (objective per iteration; empty for ``stop='max_iter'``),
+    ``method`` and ``offset`` (only for the offset algorithm)."""
+
+    W: np.ndarray
+    H: np.ndarray
+    n_iter: int
+    deviances: np.ndarray = field(default_factory=lambda: np.empty(0, dtype=np.float64))
+    method: str = "brunet"
+    offset: Optional[np.ndarray] = None
+
+    @property
+    def basis(self) -> np.ndarray:
+        return self.W
+
+    @property
+    def coef(self) -> np.ndarray:
+        return self.H
+
+    def fitted(self) -> np.ndarray:
+        """The model estimate W H (plus the offset column, when present)."""
+        wh = self.W @ self.H
+        if self.offset is not None:
+            wh = wh + self.offset[:, None]
+        return wh
+
+    def __repr__(self) -> str:
+        return (
+            f"NMFResult(method='{self.method}', n={self.W.shape[0]}, "
+            f"p={self.H.shape[1]}, rank={self.W.shape[1]}, n_iter={self.n_iter})"
+        )
+
+
+# =============================================================================
+# Initialisation (python/nmf_rs/__init__.py:110-219)
+# =============================================================================
+
+def random_init(V: np.ndarray, rank: int, seed: Optional[int] = None, *,
+                max_value: Optional[float] = None) -> tuple[np.ndarray, np.ndarray]:
+    """(W0, H0) drawn U(0, max V) from ``numpy.random.default_rng(seed)``:
+    W (n x rank) first, then H (rank x p) -- the reference's stream order,
+    so the same seed gives the same starting point."""
+    n, p = V.shape
+    gen = np.random.default_rng(seed)
+    if max_value is not None:
+        top = float(max_value)
+    else:
+        top = float(np.max(V)) if V.size else 1.0
+    W0 = gen.uniform(0.0, top, size=(n, rank))
+    H0 = gen.uniform(0.0, top, size=(rank, p))
+    return W0, H0
+
+
+def nndsvd_init(V: np.ndarray, rank: int, *, fill: str = "mean", seed: int = 0,
+                n_oversamples: int = 10) -> tuple[np.ndarray, np.ndarray]:
+    """NNDSVD start (Boutsidis & Gallopoulos 2008, "SVD based initialization:
+    A head start for nonnegative matrix factorization").
+
+    A rank-``rank`` randomized SVD of V (scikit-learn's ``randomized_svd``
+    with ``random_state=seed``) is turned into non-negative factors: the
+    leading pair by absolute value, every later pair by keeping whichever
+    sign-split half (u+, v+) or (u-, v-) has the larger norm product, scaled
+    to carry sqrt(sigma * that product).  Zeros are then kept (``'zero'``),
+    raised to 1e-9 (``'eps'``) or replaced by mean(V) (``'mean'``, NNDSVDa).
+    """
+    try:
+        from sklearn.utils.extmath import randomized_svd
+    except ImportError as exc:  # pragma: no cover - sklearn is in the image
+        raise ImportError("nndsvd_init() requires scikit-learn") from exc
+    V = np.asarray(V, dtype=np.float64)
+    if (V < 0).any():
+        raise ValueError("V must be non-negative for NNDSVD initialisation.")
+    if fill not in ("zero", "mean", "eps"):
+        raise ValueError(f"unknown fill mode '{fill}': supported zero / mean / eps")
+    U, S, Vt = randomized_svd(V, n_components=rank, n_oversamples=n_oversamples,
+                              random_state=seed)
+    n, p = V.shape
+    W = np.zeros((n, rank))
+    H = np.zeros((rank, p))
+    root = np.sqrt(S[0])
+    W[:, 0] = root * np.abs(U[:, 0])
+    H[0, :] = root * np.abs(Vt[0, :])
+    for k in range(1, rank):
+        halves = []
+        for sgn in (1.0, -1.0):
+            uh = np.maximum(sgn * U[:, k], 0.0)
+            vh = np.maximum(sgn * Vt[k, :], 0.0)
+            nu, nv = np.linalg.norm(uh), np.linalg.norm(vh)
+            halves.append((nu * nv, uh, vh, nu, nv))
+        # The positive half wins ties.
+        prod, uh, vh, nu, nv = halves[0] if halves[0][0] >= halves[1][0] else halves[1]
+        if prod > 0:
+            scale = np.sqrt(S[k] * prod)
+            W[:, k] = scale * uh / nu
+            H[k, :] = scale * vh / nv
+    if fill == "eps":
+        W[W < 1e-9] = 1e-9
+        H[H < 1e-9] = 1e-9
+    elif fill == "mean":
+        mean = float(V.mean()) if V.size else 0.0
+        W[W <= 0.0] = mean
+        H[H <= 0.0] = mean
+    return W, H
+
+
+# =============================================================================
+# Single-step updates (python/nmf_rs/__init__.py:243-264)
+# =============================================================================
+
+def _f64_c(arr, name: str) -> np.ndarray:
+    a = np.ascontiguousarray(np.asarray(arr, dtype=np.float64))
+    if a.ndim != 2:
+        raise ValueError(f"{name} must be 2-D, got shape {a.shape}")
+    return a
+
+
+def update_h_brunet(V: np.ndarray, W: np.ndarray, H: np.ndarray) -> np.ndarray:
+    """One brunet (KL) update of H (R ``std.divergence.update.h``)."""
+    return _native.py_divergence_update_h(_f64_c(V, "V"), _f64_c(W, "W"), _f64_c(H, "H"))
+
+
+def update_w_brunet(V: np.ndarray, W: np.ndarray, H: np.ndarray) -> np.ndarray:
+    """One brunet (KL) update of W (R ``std.divergence.update.w``)."""
+    return _native.py_divergence_update_w(_f64_c(V, "V"), _f64_c(W, "W"), _f64_c(H, "H"))
+
+
+def update_h_lee(V: np.ndarray, W: np.ndarray, H: np.ndarray, eps: float = 1e-9) -> np.ndarray:
+    """One lee (Frobenius) update of H (R ``std.euclidean.update.h``)."""
+    return _native.py_euclidean_update_h(_f64_c(V, "V"), _f64_c(W, "W"), _f64_c(H, "H"),
+                                         float(eps))
+
+
+def update_w_lee(V: np.ndarray, W: np.ndarray, H: np.ndarray, eps: float = 1e-9) -> np.ndarray:
+    """One lee (Frobenius) update of W (R ``std.euclidean.update.w``)."""
+    return _native.py_euclidean_update_w(_f64_c(V, "V"), _f64_c(W, "W"), _f64_c(H, "H"),
+                                         float(eps))
+
+
+def smoothing_matrix(rank: int, theta: float) -> np.ndarray:
+    """nsNMF smoothing matrix S = (1 - theta) I + (theta / r) 1 1^T."""
+    return _native.py_smoothing_matrix(int(rank), float(theta))
+
+
+def set_num_threads(n: int) -> bool:
+    """Accepted for compatibility; the GPU engine has no CPU pool (False)."""
+    return _native.set_num_threads(int(n))
+
+
+def cv_rank(V: np.ndarray, ranks: Sequence[int], **kwargs):
+    """Cross-validated rank selection.  The reference fits each fold with the
+    weighted ``ls-nmf`` method, which this engine does not build."""
+    raise NotImplementedError(
+        "cv_rank() needs method='ls-nmf', which the GPU engine does not build")
+
+
+# =============================================================================
+# Top-level driver (python/nmf_rs/__init__.py:362-568)
+# =============================================================================
+
+_METHOD_ALIASES = {
+    "brunet": "brunet", "kl": "brunet",
+    "lee": "lee", "frobenius": "lee", "euclidean": "lee",
+    "offset": "offset",
+    "nsnmf": "nsnmf", "ns": "nsnmf", "ns_nmf": "nsnmf",
+    "hals": "hals",
+    "ehals": "ehals", "e-hals": "ehals", "extrap_hals": "ehals",
+    "dnmf": "dnmf", "diag_nmf": "dnmf", "rcppml": "dnmf",
+    "ls-nmf": "lsnmf", "lsnmf": "lsnmf",
+    "snmf/r": "snmf/r", "snmf_r": "snmf/r", "snmfr": "snmf/r",
+    "snmf/l": "snmf/l", "snmf_l": "snmf/l", "snmfl": "snmf/l",
+}
+
+
+def _regularisation(method: str, sparsity: float, smoothness: float):
+    """Per-method routing of ``sparsity``/``smoothness`` to the L1/L2 terms
+    of each factor (python/nmf_rs/__init__.py:528-538)."""
+    if method == "snmf/r":
+        return float(sparsity), 0.0, 0.0, float(smoothness)
+    if method == "snmf/l":
+        return 0.0, float(sparsity), float(smoothness), 0.0
+    if method == "dnmf":
+        return float(sparsity), float(sparsity), 0.0, 0.0
+    return 0.0, 0.0, 0.0, 0.0
+
+
+def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.ndarray] = None,
+        H0: Optional[np.ndarray] = None, seed: Optional[int] = None, max_iter: int = 2000,
+        eps: float = 1e-9, rescale: bool = True, theta: float = 0.5,
+        offset: Optional[np.ndarray] = None, weight: Optional[np.ndarray] = None,
+        sparsity: float = 0.01, smoothness: float = 1.0, stop: str = "max_iter",
+        stationary_th: float = float(np.finfo(np.float64).eps), check_interval: int = 50,
+        check_niter: int = 10, num_threads: Optional[int] = None, precision: str = "fp64",
+        refine_iters: int = 2, device: int = 0) -> NMFResult:
+    """Factorise V ~ W H on the GPU.
+
+    Arguments, defaults, validation order and result follow the reference's
+    ``nmf()`` (python/nmf_rs/__init__.py:396-568): method aliases, a
+    non-negativity check on V, ``random_init(V, rank, seed)`` for a missing
+    W0/H0, shape checks, per-method sparsity routing.  ``num_threads`` is
+    accepted and ignored.
+
+    Engine extensions: ``precision='fp32'`` stores V in f32 for the two V
+    contractions (f32 products, f64 reductions, f64 updates/objective/stop)
+    and runs the last ``refine_iters`` iterations in full f64; ``device``
+    selects the GPU.
+    """
+    method_norm = _METHOD_ALIASES.get(method.lower())
+    if method_norm is None:
+        raise ValueError(
+            f"unknown method '{method}'. supported: brunet, lee, offset, nsNMF "
+            "(plus aliases KL/Frobenius/ns).")
+    V_arr = _f64_c(V, "V")
+    if (V_arr < 0).any():
+        raise ValueError("V must be non-negative.")
+    n, p = V_arr.shape
+    if W0 is None or H0 is None:
+        W0_, H0_ = random_init(V_arr, rank, seed=seed)
+        W0 = W0_ if W0 is None else W0
+        H0 = H0_ if H0 is None else H0
+    W0 = _f64_c(W0, "W0")
+    H0 = _f64_c(H0, "H0")
+    if W0.shape != (n, rank):
+        raise ValueError(f"W0.shape {W0.shape} != ({n}, {rank})")
+    if H0.shape != (rank, p):
+        raise ValueError(f"H0.shape {H0.shape} != ({rank}, {p})")
+    offset_arr = None
+    if offset is not None:
+        offset_arr = np.ascontiguousarray(np.asarray(offset, dtype=np.float64))
+        if offset_arr.shape != (n,):
+            raise ValueError(f"offset.shape {offset_arr.shape} != ({n},)")
+    weight_arr = None
+    if weight is not None:
+        weight_arr = np.ascontiguousarray(np.asarray(weight, dtype=np.float64))
+        if weight_arr.shape != V_arr.shape:
+            raise ValueError(f"weight.shape {weight_arr.shape} != V.shape {V_arr.shape}")
+    sh, sw, gh, gw = _regularisation(method_norm, sparsity, smoothness)
+    out = _native.py_nmf_run(
+        method_norm, V_arr, W0, H0, int(max_iter), eps=float(eps), rescale=bool(rescale),
+        theta=float(theta), offset=offset_arr, weight=weight_arr, sparsity_h=sh,
+        sparsity_w=sw, smoothness_h=gh, smoothness_w=gw, stop=stop,
+        stationary_th=float(stationary_th), check_interval=int(check_interval),
+        check_niter=int(check_niter),
+        num_threads=int(num_threads) if num_threads is not None else None,
+        precision=precision, refine_iters=int(refine_iters), device=int(device))
+    return NMFResult(
+        W=np.asarray(out["W"]),
+        H=np.asarray(out["H"]),
+        n_iter=int(out["n_iter"]),
+        deviances=np.asarray(out["deviances"], dtype=np.float64),
+        method=method_norm,
+        offset=np.asarray(out["offset"]) if "offset" in out else None,
+    )
+
+
+from . import synthetic  # noqa: E402,F401  (workload generator, nmf_rs.synthetic)

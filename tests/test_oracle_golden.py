@@ -1,0 +1,109 @@
+"""The CPU oracle pinned against the reference's own recorded outputs
+(examples/tutorial_quickstart.ipynb) and its Rust unit test
+(rust/src/lib.rs:2208-2227).  CPU only."""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import rel
+
+sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
+import make_golden  # noqa: E402
+
+
+def test_fixture_inputs_regenerate(quickstart, kats):
+    V, W0, H0 = quickstart
+    V2, W02, H02 = make_golden.quickstart_inputs()
+    np.testing.assert_array_equal(V, V2)
+    np.testing.assert_array_equal(W0, W02)
+    np.testing.assert_array_equal(H0, H02)
+    assert V.min() == kats["V_min"] and V.max() == kats["V_max"]
+
+
+def test_brunet_200_norm(oracle, quickstart, kats):
+    V, W0, H0 = quickstart
+    res = oracle.nmf_run("brunet", V, W0, H0, 200)
+    norm = float(np.linalg.norm(V - res["W"] @ res["H"]))
+    assert rel(norm, kats["brunet_200_frob_norm"]) < 1e-13
+    assert res["n_iter"] == 200 and res["deviances"].size == 0
+
+
+def test_lee_200_norm(oracle, quickstart, kats):
+    V, W0, H0 = quickstart
+    res = oracle.nmf_run("lee", V, W0, H0, 200)
+    norm = float(np.linalg.norm(V - res["W"] @ res["H"]))
+    assert round(norm, 4) == kats["lee_200_frob_norm_4dp"]
+
+
+def test_brunet_stationary_kat(oracle, quickstart, kats):
+    V, W0, H0 = quickstart
+    k = kats["brunet_stationary"]
+    res = oracle.nmf_run("brunet", V, W0, H0, k["max_iter"], stop="stationary",
+                         stationary_th=k["stationary_th"], check_interval=k["check_interval"],
+                         check_niter=k["check_niter"])
+    assert res["n_iter"] == k["n_iter"]
+    assert res["deviances"].size == k["n_deviances"]
+    # The KL sum is one sequential reduction in a fixed order: bit-exact.
+    assert res["deviances"][-1] == k["final_kl"]
+
+
+def test_single_step_delta_kl(oracle, quickstart, kats):
+    V, W0, H0 = quickstart
+    H1 = oracle.update_h_brunet(V, W0, H0)
+    W1 = oracle.update_w_brunet(V, W0, H1)
+
+    def kl(W, H):  # the notebook's own expression (cell 13)
+        WH = W @ H
+        return float((V * np.log(np.where(V > 0, V / (WH + 1e-30), 1)) - V + WH).sum())
+
+    assert rel(kl(W0, H0) - kl(W1, H1), kats["single_step_brunet_delta_kl"]) < 1e-13
+
+
+@pytest.mark.parametrize("method", ["brunet", "lee", "hals", "dnmf"])
+def test_thread_count_independent(oracle, quickstart, method):
+    V, W0, H0 = quickstart
+    a = oracle.nmf_method(method, V, W0, H0, 30, num_threads=1)
+    b = oracle.nmf_method(method, V, W0, H0, 30, num_threads=4)
+    np.testing.assert_array_equal(a["W"], b["W"])
+    np.testing.assert_array_equal(a["H"], b["H"])
+
+
+def test_rust_unit_brunet_reduces_kl(oracle):
+    # lib.rs:2208-2227: 3x2 V, W0 = 0.5, H0 = 1, brunet 50 it, stationary.
+    V = np.array([[1.0, 2.0], [3.0, 4.0], [5.0, 6.0]])
+    W0 = np.full((3, 2), 0.5)
+    H0 = np.ones((2, 2))
+    res = oracle.nmf_run("brunet", V, W0, H0, 50, stop="stationary", stationary_th=1e-12,
+                         check_interval=50, check_niter=10)
+    assert (res["W"] >= 0).all() and (res["H"] >= 0).all()
+    assert res["deviances"][-1] <= res["deviances"][0]
+
+
+def test_check_interval_zero_mirrors_panic(oracle, quickstart):
+    V, W0, H0 = quickstart
+    # With a window of 1 sample, the first window closes at iteration 1, the
+    # criterion fails (th = 0), the window resets and iteration 2 evaluates
+    # `2 % 0` -- the point where the reference panics.
+    with pytest.raises(ZeroDivisionError):
+        oracle.nmf_run("lee", V, W0, H0, 5, stop="stationary", stationary_th=0.0,
+                       check_interval=0, check_niter=1)
+
+
+@pytest.mark.parametrize("method", ["hals", "dnmf"])
+def test_hals_family_decreases_loss(oracle, quickstart, method):
+    V, W0, H0 = quickstart
+    res = oracle.nmf_method(method, V, W0, H0, 50, stop="stationary", check_interval=10)
+    dev = res["deviances"]
+    assert dev[-1] < dev[0]
+    assert (res["W"] > 0).all() and (res["H"] > 0).all()
+
+
+def test_dnmf_unit_norm_columns(oracle, quickstart):
+    V, W0, H0 = quickstart
+    res = oracle.nmf_method("dnmf", V, W0, H0, 20)
+    norms = np.linalg.norm(res["W"], axis=0)
+    np.testing.assert_allclose(norms, 1.0, rtol=1e-12)
