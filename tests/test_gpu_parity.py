@@ -1,11 +1,21 @@
 """GPU parity: the CUDA library (called through the C ABI via nmf_rs) against
 the CPU oracle and against the reference's recorded quickstart outputs.
 
-Tolerances (FP64 plain method):
+Tolerances (FP64 plain method), written per check below:
   factors   max|dW| / max|W| <= 1e-10 and the same for H,
   objective relative difference <= 1e-12.
 The GPU sums in a different order than the reference's scalar loops (and
 with FMA), so agreement is to rounding, not bitwise.
+
+hals and dnmf are not always well conditioned: from a random start a HALS
+component can collapse to the eps floor, after which the sweep divides by
+max(G_kk, eps) = eps and amplifies rounding by ~1e9.  The oracle itself then
+moves by up to ~1e-3 when W0 is perturbed by one ulp, and so would the
+reference (whose W^T V / V H^T summation order, matrixmultiply's, is not
+pinned either).  For those two methods the bound is therefore
+max(north-star tolerance, 100 x the oracle's own one-ulp sensitivity),
+measured in the test; from NNDSVD starts HALS is well conditioned and is
+held to the plain tolerance.
 """
 from __future__ import annotations
 
@@ -30,15 +40,41 @@ def _objective(oracle, method, V, W, H):
     return oracle.euclidean_distance(V, W, H)
 
 
+def _rel_obj(method, V, a, b):
+    """Relative objective difference; the denominator is floored at 1e-9 of
+    the objective's scale (sum V for KL, 0.5 ||V||^2 for Frobenius), so that
+    an exact fit (objective ~ 0) does not turn rounding into 100 %."""
+    scale = float(V.sum()) if method == "brunet" else 0.5 * float((V * V).sum())
+    return abs(a - b) / max(abs(b), 1e-9 * scale, 1e-300)
+
+
+def _sensitivity(oracle, method, V, W0, H0, iters, **kw):
+    """How far the oracle's own result moves when W0 is perturbed by one ulp:
+    (factor measure, objective measure)."""
+    a = oracle.nmf_method(method, V, W0, H0, iters, **kw)
+    signs = np.random.default_rng(0).choice([-1.0, 1.0], W0.shape)
+    b = oracle.nmf_method(method, V, W0 * (1 + 2.220446049250313e-16 * signs), H0, iters, **kw)
+    f = max(rel_max(b["W"], a["W"]), rel_max(b["H"], a["H"]))
+    o = _rel_obj(method, V, _objective(oracle, method, V, b["W"], b["H"]),
+                 _objective(oracle, method, V, a["W"], a["H"]))
+    return f, o
+
+
 def _check(oracle, method, V, W0, H0, iters, **kw):
     ref = oracle.nmf_method(method, V, W0, H0, iters, **kw)
     got = nmf_rs.nmf(V, W0.shape[1], method, W0=W0, H0=H0, max_iter=iters, **kw)
+    tol_f, tol_o = FACTOR_TOL, OBJ_TOL
+    if method in ("hals", "dnmf"):
+        sf, so = _sensitivity(oracle, method, V, W0, H0, iters, **kw)
+        tol_f, tol_o = max(tol_f, 100 * sf), max(tol_o, 100 * so)
     assert got.n_iter == ref["n_iter"]
-    assert rel_max(got.W, ref["W"]) <= FACTOR_TOL, rel_max(got.W, ref["W"])
-    assert rel_max(got.H, ref["H"]) <= FACTOR_TOL, rel_max(got.H, ref["H"])
+    dW, dH = rel_max(got.W, ref["W"]), rel_max(got.H, ref["H"])
+    assert dW <= tol_f, (dW, tol_f)
+    assert dH <= tol_f, (dH, tol_f)
     o_got = _objective(oracle, method, V, got.W, got.H)
     o_ref = _objective(oracle, method, V, ref["W"], ref["H"])
-    assert rel(o_got, o_ref) <= OBJ_TOL, rel(o_got, o_ref)
+    d_obj = _rel_obj(method, V, o_got, o_ref)
+    assert d_obj <= tol_o, (d_obj, tol_o)
     return got, ref
 
 
@@ -92,6 +128,26 @@ def test_quickstart_parity(oracle, quickstart, method):
     _check(oracle, method, V, W0, H0, 100)
 
 
+@pytest.mark.parametrize("method", ["hals", "dnmf"])
+@pytest.mark.parametrize("case", ["quickstart", "pbmc-subset"])
+def test_hals_family_from_nndsvd_strict(oracle, quickstart, method, case):
+    """From an NNDSVD start the HALS family is well conditioned: plain tolerance."""
+    if case == "quickstart":
+        V = quickstart[0]
+        r = 5
+    else:
+        V = synthetic.counts_matrix(1500, 3000, 8, 0.3, seed=1)
+        r = 8
+    W0, H0 = nmf_rs.nndsvd_init(V, r, fill="mean", seed=0)
+    ref = oracle.nmf_method(method, V, W0, H0, 50)
+    got = nmf_rs.nmf(V, r, method, W0=W0, H0=H0, max_iter=50)
+    assert rel_max(got.W, ref["W"]) <= FACTOR_TOL
+    assert rel_max(got.H, ref["H"]) <= FACTOR_TOL
+    o_got = _objective(oracle, method, V, got.W, got.H)
+    o_ref = _objective(oracle, method, V, ref["W"], ref["H"])
+    assert rel(o_got, o_ref) <= OBJ_TOL
+
+
 @pytest.mark.parametrize("method", METHODS)
 @pytest.mark.parametrize("shape", [(97, 131, 3), (33, 1000, 13), (517, 64, 1), (64, 33, 32),
                                    (300, 257, 17), (1, 40, 2), (40, 1, 2)])
@@ -126,6 +182,8 @@ def test_pbmc8k_shape(oracle, method):
 @pytest.mark.parametrize("method", METHODS)
 def test_stationary_stop_parity(oracle, quickstart, method):
     V, W0, H0 = quickstart
+    if method == "hals":  # well-conditioned start, so the per-iteration deviances compare
+        W0, H0 = nmf_rs.nndsvd_init(V, 5, fill="mean", seed=0)
     kw = dict(stop="stationary", stationary_th=1e-3, check_interval=5, check_niter=4)
     got, ref = _check(oracle, method, V, W0, H0, 300, **kw)
     assert got.deviances.size == ref["deviances"].size == got.n_iter + 1
@@ -192,6 +250,8 @@ def test_fp32_precision_form(oracle, method):
     """V in f32 for the contractions, f64 everywhere else, 2 f64 sweeps:
     objective within 1e-5 (relative) of the FP64 oracle."""
     V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
+    if method == "hals":  # HALS from a random start is ill conditioned (see top)
+        W0, H0 = nmf_rs.nndsvd_init(V, 8, fill="mean", seed=0)
     ref = oracle.nmf_method(method, V, W0, H0, 40)
     got = nmf_rs.nmf(V, 8, method, W0=W0, H0=H0, max_iter=40, precision="fp32")
     o_ref = _objective(oracle, method, V, ref["W"], ref["H"])
