@@ -194,6 +194,35 @@ nmfcu_status nmfcu_context_reset_timing(nmfcu_context *ctx);
 int64_t nmfcu_context_launch_count(nmfcu_context *ctx);
 
 /* ---------------------------------------------------------------------- */
+/* Allocation-free objective                                               */
+/* ---------------------------------------------------------------------- */
+
+/* No counterpart in the reference.  For callers that may not allocate
+ * device memory while they run (a server that reserves all device memory up
+ * front, code under another framework's memory pool, a loop that cannot
+ * take the synchronisation of cudaMalloc/cudaFree): the objective of V
+ * against W H on device pointers, computed without any allocation.
+ *
+ *   kind   NMFCU_OBJECTIVE_KL (kl_divergence, lib.rs:1410-1431) or
+ *          NMFCU_OBJECTIVE_FROBENIUS (0.5 ||V - WH||^2, lib.rs:1434-1445)
+ *   dV     n x p f64, leading dimension ldv;  dW n x r;  dH r x p
+ *   d_out  one f64 on the device, written when `stream` reaches the work
+ *
+ * Its scratch is a fixed 512 KB array compiled into the library (one f64 per
+ * 8 rows), which every GPU that loads the library holds until the process
+ * exits; n above NMFCU_NOALLOC_MAX_ROWS is rejected (NMFCU_ERR_INVALID_ARG).
+ * It runs on the caller's current device.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the one array: calls whose
+ * work overlaps on the GPU (different streams, or other host threads) race
+ * and may return wrong values, so serialise them. */
+#define NMFCU_NOALLOC_MAX_ROWS 524288
+enum { NMFCU_OBJECTIVE_KL = 0, NMFCU_OBJECTIVE_FROBENIUS = 1 };
+nmfcu_status nmfcu_objective_noalloc(int32_t kind, int64_t n, int64_t p, int64_t r,
+                                     const double *dV, int64_t ldv, const double *dW,
+                                     const double *dH, double *d_out, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Misc                                                                    */
 /* ---------------------------------------------------------------------- */
 

@@ -44,6 +44,19 @@ nmfcu_status cuda_fail(cudaError_t e, const char *what) {
     return fail(s, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+}  // namespace
+
+// Error reporting shared with the other translation units of the library
+// (C++ linkage, so the nmfcu_* export list does not pick it up).
+namespace nmfcu_internal {
+nmfcu_status fail(nmfcu_status s, const std::string &msg) {
+    g_last_error = msg;
+    return s;
+}
+}  // namespace nmfcu_internal
+
+namespace {
+
 #define CUDA_TRY(expr)                                        \
     do {                                                      \
         cudaError_t e_ = (expr);                              \

@@ -30,6 +30,8 @@ MAX_RANK = 32
 F64, F32 = 0, 1  # element type of a device V
 
 KCLASS_HSTEP, KCLASS_WSTEP, KCLASS_OBJECTIVE, KCLASS_OTHER = range(4)
+OBJECTIVE_KL, OBJECTIVE_FROBENIUS = 0, 1
+NOALLOC_MAX_ROWS = 524288
 
 _i32, _i64, _dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -85,6 +87,9 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_double)]),
     "nmfcu_context_reset_timing": (_i32, [ctypes.c_void_p]),
     "nmfcu_context_launch_count": (_i64, [ctypes.c_void_p]),
+    "nmfcu_objective_noalloc": (_i32, [_i32, _i64, _i64, _i64, ctypes.c_void_p, _i64,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p]),
     "nmfcu_last_error": (ctypes.c_char_p, []),
     "nmfcu_status_string": (ctypes.c_char_p, [_i32]),
     "nmfcu_abi_version": (_i32, []),
