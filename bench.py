@@ -41,6 +41,9 @@ import numpy as np  # noqa: E402
 WORKLOADS = {
     # name: (n, p, k, alpha, rank, default iterations)
     "atlas": (20000, 200000, 20, 0.2, 20, 25),
+    # a 20000 x 20000 column slice of the atlas shape (larger than L2; small
+    # enough for profiler captures)
+    "atlas-slice": (20000, 20000, 20, 0.2, 20, 25),
     "pbmc8k": (2000, 7750, 10, 0.2, 10, 100),
     "pbmc-subset": (1500, 3000, 8, 0.3, 8, 100),
 }

@@ -38,7 +38,8 @@ struct RunState {
     long long n_iter;  // iteration at which the stop fired
     int stopped;       // 1 once the loop has stopped
     int error;         // 1: `iter % check_interval` with check_interval == 0
-    int pad0, pad1;
+    int timeout;       // a bounded mbarrier wait gave up (stream.cuh codes)
+    int pad1;
 };
 
 // Fixed constants of the streaming kernels.
@@ -607,7 +608,7 @@ struct StopParams {
     double scale;         // 0.5 for the Frobenius objective, 1 for KL
 };
 
-__global__ void objective_finalize(const double *__restrict__ part, int B, double *__restrict__ dev,
+static __global__ void objective_finalize(const double *__restrict__ part, int B, double *__restrict__ dev,
                                    StopParams sp, RunState *st) {
     if (st->stopped) return;
     __shared__ double red[kThreads];
@@ -668,7 +669,21 @@ __global__ void objective_finalize(const double *__restrict__ part, int B, doubl
 // ---------------------------------------------------------------------------
 // Layout helpers.
 // ---------------------------------------------------------------------------
-__global__ void convert_f64_f32(const double *__restrict__ src, int64_t lds, float *__restrict__ dst,
+
+// H (RP x p f64) -> H^T (p x rps, type TH), zero past the first r entries.
+template <typename TH>
+__global__ void h_transpose(const double *__restrict__ H, TH *__restrict__ Ht, int p, int r,
+                            int rps) {
+    const int64_t total = (int64_t)p * rps;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = t / rps;
+        const int k = (int)(t - j * rps);
+        Ht[t] = (k < r) ? (TH)H[(int64_t)k * p + j] : (TH)0;
+    }
+}
+
+static __global__ void convert_f64_f32(const double *__restrict__ src, int64_t lds, float *__restrict__ dst,
                                 int64_t ldd, int n, int p) {
     const int64_t total = (int64_t)n * p;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;

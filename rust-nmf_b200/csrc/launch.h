@@ -1,0 +1,44 @@
+// launch.h -- host-side interface to the TMA streaming passes (stream.cuh),
+// instantiated once per V element type in stream_f32.cu / stream_f64.cu.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace nmfcu {
+
+struct StreamK;
+
+// Geometry and launchers of the two passes for one (element type, rank
+// bucket).  All pointers are device pointers.
+struct StreamOps {
+    virtual ~StreamOps() = default;
+    virtual int elem_bytes() const = 0;          // 4 or 8
+    virtual int rps() const = 0;                 // padded rank of the W / H^T copies
+    virtual int h_tcols(bool ratio) const = 0;   // H pass tile width (columns)
+    virtual int h_brows() const = 0;             // H pass rows per unit
+    virtual int h_boxc() const = 0;              // H pass V box width
+    virtual int w_trows(bool ratio) const = 0;   // W pass tile height (rows)
+    virtual int w_bcols() const = 0;             // W pass columns per unit
+    virtual cudaError_t hpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmW,
+                              const double *H, int n, int p, const StreamK &sk, double *part,
+                              RunState *st, int grid, cudaStream_t s) const = 0;
+    virtual cudaError_t wpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmH,
+                              const double *W, int n, int p, const StreamK &sk, double *part,
+                              RunState *st, int grid, cudaStream_t s) const = 0;
+    virtual void h_epi(double *H, void *Ht, int p, const double *part, const StreamK &sk,
+                       int tcols, const EpiParams &e, const RunState *st,
+                       cudaStream_t s) const = 0;
+    virtual void w_epi(double *W, int n, const double *part, const StreamK &sk, int trows,
+                       const EpiParams &e, const RunState *st, cudaStream_t s) const = 0;
+    // f32 only: W (n x RP f64) -> the f32 copy (n x rps()) that the H pass streams.
+    virtual void w_copy(const double *W, void *Wc, int n, const RunState *st,
+                        cudaStream_t s) const = 0;
+};
+
+const StreamOps *stream_ops_f32(int rp);
+const StreamOps *stream_ops_f64(int rp);
+
+}  // namespace nmfcu

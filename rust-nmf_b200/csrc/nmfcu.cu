@@ -18,8 +18,12 @@
 #include <string>
 #include <vector>
 
+#include <cudaTypedefs.h>
+
 #include "../../include/nmfcu.h"
 #include "kernels.cuh"
+#include "launch.h"
+#include "stream.cuh"
 
 using namespace nmfcu;
 
@@ -70,7 +74,7 @@ namespace {
     } while (0)
 
 // ===========================================================================
-// Rank buckets and per-bucket kernel launchers
+// Rank buckets and the small per-bucket kernels
 // ===========================================================================
 constexpr int kBuckets[] = {2, 4, 6, 8, 10, 12, 14, 16, 20, 24, 28, 32};
 
@@ -81,23 +85,16 @@ int bucket_for(int64_t r) {
 }
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
-// V element type of a pass.
-enum VType { VT_F64 = 0, VT_F32 = 1 };
-
+// Grams, rescaling, clamps and the objective pass: O(r^2 (n + p)) work plus
+// the objective's one read of V.
 struct Ops {
     virtual ~Ops() = default;
-    virtual void hstep(VType vt, const void *V, int64_t ldv, int n, int p, const double *W,
-                       const double *H, bool ratio, int S, int rows_per_split, double *part,
-                       const RunState *st, cudaStream_t s) const = 0;
-    // mode 0 plain, 1 ratio, 2 KL objective, 3 Frobenius objective
-    virtual void rowpass(VType vt, const void *V, int64_t ldv, int n, int p, const double *W,
-                         const double *H, int mode, int S2, int cols_per_split, double *part,
-                         double *obj, const RunState *st, cudaStream_t s) const = 0;
-    virtual void h_epi(double *H, int p, const double *part, int S, const EpiParams &e,
-                       const RunState *st, cudaStream_t s) const = 0;
-    virtual void w_epi(double *W, int n, const double *part, int S, const EpiParams &e,
-                       const RunState *st, cudaStream_t s) const = 0;
+    // mode 2 KL objective, 3 Frobenius objective (f64 V)
+    virtual void objective(const double *V, int64_t ldv, int n, int p, const double *W,
+                           const double *H, int mode, int S2, int cols_per_split, double *obj,
+                           const RunState *st, cudaStream_t s) const = 0;
     virtual void gram_w(const double *W, int n, int B, int rows_per_block, double *pg,
                         double *ps, const RunState *st, cudaStream_t s) const = 0;
     virtual void gram_h(const double *H, int p, int B, int cols_per_block, double *pg,
@@ -114,58 +111,17 @@ struct Ops {
 
 template <int RP>
 struct OpsT final : Ops {
-    void hstep(VType vt, const void *V, int64_t ldv, int n, int p, const double *W,
-               const double *H, bool ratio, int S, int rows_per_split, double *part,
-               const RunState *st, cudaStream_t s) const override {
-        if (p <= 0 || S <= 0) return;
-        dim3 grid(cdiv(p, 32), S), block(32, kWarps);
-        if (vt == VT_F64) {
-            if (ratio)
-                hstep_contract<double, double, RP, true><<<grid, block, 0, s>>>(
-                    (const double *)V, ldv, n, p, W, H, rows_per_split, part, st);
-            else
-                hstep_contract<double, double, RP, false><<<grid, block, 0, s>>>(
-                    (const double *)V, ldv, n, p, W, H, rows_per_split, part, st);
-        } else {
-            if (ratio)
-                hstep_contract<float, float, RP, true><<<grid, block, 0, s>>>(
-                    (const float *)V, ldv, n, p, W, H, rows_per_split, part, st);
-            else
-                hstep_contract<float, float, RP, false><<<grid, block, 0, s>>>(
-                    (const float *)V, ldv, n, p, W, H, rows_per_split, part, st);
-        }
-    }
-    void rowpass(VType vt, const void *V, int64_t ldv, int n, int p, const double *W,
-                 const double *H, int mode, int S2, int cols_per_split, double *part,
-                 double *obj, const RunState *st, cudaStream_t s) const override {
+    void objective(const double *V, int64_t ldv, int n, int p, const double *W, const double *H,
+                   int mode, int S2, int cols_per_split, double *obj, const RunState *st,
+                   cudaStream_t s) const override {
         if (n <= 0 || S2 <= 0) return;
         dim3 grid(cdiv(n, kThreads), S2), block(kThreads);
-        if (vt == VT_F64) {
-            const double *v = (const double *)V;
-            switch (mode) {
-                case 0: nmfcu::rowpass<double, double, RP, 0><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-                case 1: nmfcu::rowpass<double, double, RP, 1><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-                case 2: nmfcu::rowpass<double, double, RP, 2><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-                default: nmfcu::rowpass<double, double, RP, 3><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-            }
-        } else {
-            const float *v = (const float *)V;
-            switch (mode) {
-                case 0: nmfcu::rowpass<float, float, RP, 0><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-                case 1: nmfcu::rowpass<float, float, RP, 1><<<grid, block, 0, s>>>(v, ldv, n, p, W, H, cols_per_split, part, obj, st); break;
-                default: break;  // objectives always run on the f64 V
-            }
-        }
-    }
-    void h_epi(double *H, int p, const double *part, int S, const EpiParams &e,
-               const RunState *st, cudaStream_t s) const override {
-        if (p <= 0) return;
-        h_epilogue<RP><<<cdiv(p, kThreads), kThreads, 0, s>>>(H, p, part, S, e, st);
-    }
-    void w_epi(double *W, int n, const double *part, int S, const EpiParams &e,
-               const RunState *st, cudaStream_t s) const override {
-        if (n <= 0) return;
-        w_epilogue<RP><<<cdiv(n, kThreads), kThreads, 0, s>>>(W, n, part, S, e, st);
+        if (mode == 2)
+            nmfcu::rowpass<double, double, RP, 2><<<grid, block, 0, s>>>(
+                V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st);
+        else
+            nmfcu::rowpass<double, double, RP, 3><<<grid, block, 0, s>>>(
+                V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st);
     }
     void gram_w(const double *W, int n, int B, int rows_per_block, double *pg, double *ps,
                 const RunState *st, cudaStream_t s) const override {
@@ -230,6 +186,50 @@ const Ops *ops_for(int rp) {
 }
 
 // ===========================================================================
+// TMA tensor maps
+// ===========================================================================
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+        cudaGetLastError();
+    });
+    return fn;
+}
+
+// A 2-D row-major tensor of `rows` x `cols` elements (leading dimension ld)
+// read in boxes of box_rows x box_cols.
+nmfcu_status encode_2d(CUtensorMap *map, const void *base, bool f32, int64_t rows, int64_t cols,
+                       int64_t ld, int box_cols, int box_rows,
+                       CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_NONE) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    const size_t es = f32 ? 4 : 8;
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * es)};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                     2, const_cast<void *>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled failed (code " + std::to_string((int)r) +
+                                        ")");
+    return NMFCU_OK;
+}
+
+bool tma_layout_ok(const void *base, int64_t ld, size_t es) {
+    return (reinterpret_cast<uintptr_t>(base) % 16 == 0) && ((ld * (int64_t)es) % 16 == 0);
+}
+
+// ===========================================================================
 // Device buffers
 // ===========================================================================
 struct DevBuf {
@@ -256,11 +256,10 @@ struct DevBuf {
     T *as() const { return static_cast<T *>(ptr); }
 };
 
-// Launch geometry of one problem shape.
+// Launch geometry of the small kernels of one problem shape.
 struct Plan {
     int n = 0, p = 0, r = 0, RP = 0;
-    int S = 1, rows_per_split = 1;     // H-step row splits
-    int S2 = 1, cols_per_split = 1;    // W-step / objective column splits
+    int S2 = 1, cols_per_split = 1;    // objective pass column splits
     int Bw = 1, rows_per_gram = 1;     // W Gram blocks
     int Bh = 1, cols_per_gram = 1;     // H Gram blocks
     int obj_blocks = 0;                // objective partial count
@@ -273,14 +272,6 @@ Plan make_plan(int64_t n, int64_t p, int64_t r, int sms) {
     pl.r = (int)r;
     pl.RP = bucket_for(r);
     const int64_t target = (int64_t)sms * 8;
-    // H step: 32-column tiles, split rows until there are ~8 CTAs per SM.
-    const int64_t tiles = std::max<int64_t>(1, (p + 31) / 32);
-    int64_t S = std::max<int64_t>(1, (target + tiles - 1) / tiles);
-    S = std::min<int64_t>(S, std::max<int64_t>(1, n / 64));
-    int64_t rps = std::max<int64_t>(1, (n + S - 1) / S);
-    pl.rows_per_split = (int)rps;
-    pl.S = (int)std::max<int64_t>(1, (n + rps - 1) / rps);
-    // W step: 256-row blocks, split columns in multiples of 32.
     const int64_t rb = std::max<int64_t>(1, (n + kThreads - 1) / kThreads);
     int64_t S2 = std::max<int64_t>(1, (target + rb - 1) / rb);
     S2 = std::min<int64_t>(S2, std::max<int64_t>(1, p / 256));
@@ -288,7 +279,6 @@ Plan make_plan(int64_t n, int64_t p, int64_t r, int sms) {
     pl.cols_per_split = (int)cps;
     pl.S2 = (int)std::max<int64_t>(1, (p + cps - 1) / cps);
     pl.obj_blocks = (int)(((n + kThreads - 1) / kThreads) * pl.S2);
-    // Grams.
     pl.Bw = (int)std::max<int64_t>(1, std::min<int64_t>((n + 63) / 64, sms));
     pl.rows_per_gram = (int)std::max<int64_t>(1, (n + pl.Bw - 1) / pl.Bw);
     pl.Bh = (int)std::max<int64_t>(1, std::min<int64_t>((p + 63) / 64, sms));
@@ -296,7 +286,21 @@ Plan make_plan(int64_t n, int64_t p, int64_t r, int sms) {
     return pl;
 }
 
-inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+// Stream-K split of `tiles` tiles of `upt` units each over at most `sms` CTAs.
+StreamK plan_sk(int64_t tiles, int64_t upt, int sms) {
+    StreamK sk;
+    sk.UPT = (int)std::max<int64_t>(1, upt);
+    sk.U = tiles * upt;
+    sk.G = (int)std::min<int64_t>(sms, sk.U);
+    if (sk.G <= 0) {
+        sk.G = 0;
+        sk.slots = 0;
+        return sk;
+    }
+    const int64_t per = (sk.U + sk.G - 1) / sk.G;
+    sk.slots = (int)((per + sk.UPT - 1) / sk.UPT + 1);
+    return sk;
+}
 
 }  // namespace
 
@@ -310,9 +314,9 @@ struct nmfcu_context {
     std::mutex mu;
 
     // Workspace.
-    DevBuf V64, V32, W, H, part_h, part_w, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
-    // Pinned staging for the small run state.
-    RunState *h_state = nullptr;
+    DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
+    DevBuf Wf32, Ht64, Ht32;
+    RunState *h_state = nullptr;  // pinned
 
     // Timing.
     bool timing = false;
@@ -322,7 +326,6 @@ struct nmfcu_context {
     };
     std::vector<Ev> events;
     std::vector<cudaEvent_t> pool;
-    int64_t launches = 0;
     double total_ms[NMFCU_KCLASS_COUNT] = {0, 0, 0, 0};
     int64_t count[NMFCU_KCLASS_COUNT] = {0, 0, 0, 0};
     int64_t launch_total = 0;
@@ -352,14 +355,15 @@ struct nmfcu_context {
         return e;
     }
 
-    // Bracket one launch for the timing hooks.
+    // Brackets the launches of one scope for the timing hooks and counts them.
     struct Scope {
         nmfcu_context *c;
         cudaStream_t s;
         int kclass;
         cudaEvent_t a = nullptr;
-        Scope(nmfcu_context *c_, cudaStream_t s_, int k) : c(c_), s(s_), kclass(k) {
-            c->launch_total++;
+        Scope(nmfcu_context *c_, cudaStream_t s_, int k, int launches = 1)
+            : c(c_), s(s_), kclass(k) {
+            c->launch_total += launches;
             if (c->timing) {
                 a = c->get_event();
                 cudaEventRecord(a, s);
@@ -377,7 +381,8 @@ struct nmfcu_context {
     void drain_timing() {
         for (auto &e : events) {
             float ms = 0.f;
-            if (cudaEventSynchronize(e.b) == cudaSuccess && cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+            if (cudaEventSynchronize(e.b) == cudaSuccess &&
+                cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
                 total_ms[e.kclass] += ms;
                 count[e.kclass] += 1;
             }
@@ -391,19 +396,63 @@ struct nmfcu_context {
 namespace {
 
 // ===========================================================================
+// Pass sets: what one V element type needs for its two streaming passes
+// ===========================================================================
+struct PassSet {
+    const StreamOps *so = nullptr;
+    bool f32 = false;
+    CUtensorMap tmVh, tmVw, tmW, tmHt;
+    void *Ht = nullptr;  // H^T, written by the H epilogue, streamed by the W pass
+    void *Wc = nullptr;  // f32 copy of W (f32 only; f64 streams the master W)
+};
+
+// Partial-sum bytes the two passes of `so` need for this shape.
+size_t pass_partial_bytes(const StreamOps *so, const Plan &pl, bool ratio, int sms) {
+    const int tcols = so->h_tcols(ratio), trows = so->w_trows(ratio);
+    const StreamK skh = plan_sk((pl.p + tcols - 1) / tcols, (pl.n + so->h_brows() - 1) / so->h_brows(), sms);
+    const StreamK skw = plan_sk((pl.n + trows - 1) / trows, (pl.p + so->w_bcols() - 1) / so->w_bcols(), sms);
+    const size_t h = (size_t)skh.G * skh.slots * pl.RP * tcols;
+    const size_t w = (size_t)skw.G * skw.slots * trows * pl.RP;
+    return sizeof(double) * std::max(h, w);
+}
+
+nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, const void *V,
+                          int64_t ldv, PassSet *ps) {
+    ps->f32 = f32;
+    ps->so = f32 ? stream_ops_f32(pl.RP) : stream_ops_f64(pl.RP);
+    if (!ps->so) return fail(NMFCU_ERR_UNSUPPORTED, "no streaming kernels for this rank");
+    const int rps = ps->so->rps();
+    ps->Ht = f32 ? c->Ht32.ptr : c->Ht64.ptr;
+    ps->Wc = f32 ? c->Wf32.ptr : nullptr;
+    if (pl.n <= 0 || pl.p <= 0) return NMFCU_OK;  // no pass runs
+    if (!tma_layout_ok(V, ldv, f32 ? 4 : 8))
+        return fail(NMFCU_ERR_INVALID_ARG, "V must be 16-byte aligned with 16-byte aligned rows");
+    // The W pass reads rows of w_bcols() elements: 64 B (f32) or 128 B (f64),
+    // swizzled to match so that a warp's row-wise reads are conflict-free.
+    const CUtensorMapSwizzle wsw = f32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
+    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(), ps->so->h_brows()));
+    NMF_TRY(encode_2d(&ps->tmVw, V, f32, pl.n, pl.p, ldv, ps->so->w_bcols(), 256, wsw));
+    if (f32)
+        NMF_TRY(encode_2d(&ps->tmW, c->Wf32.ptr, true, pl.n, rps, rps, rps, ps->so->h_brows()));
+    else
+        NMF_TRY(encode_2d(&ps->tmW, c->W.ptr, false, pl.n, pl.RP, pl.RP, pl.RP, ps->so->h_brows()));
+    NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols()));
+    return NMFCU_OK;
+}
+
+// ===========================================================================
 // The iteration loop
 // ===========================================================================
 struct RunArgs {
     const nmfcu_options *opt;
     Plan pl;
     const Ops *ops;
-    VType vt_main;          // element type of Vmain
-    const void *Vmain;      // V used by the contractions (f64 or f32)
-    int64_t ldv_main;
-    const double *V64;      // f64 V for objective and refinement iterations
+    PassSet main;        // the contractions' element type (f32 in the FP32 form)
+    PassSet p64;         // f64 passes (plain method, refinement iterations)
+    const double *V64;   // f64 V for the objective
     int64_t ldv64;
-    double *W, *H;          // padded device factors
-    double *dev;            // device deviances (or nullptr)
+    double *W, *H;       // padded device factors
+    double *dev;         // device deviances (or nullptr)
 };
 
 nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
@@ -413,8 +462,8 @@ nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long ite
     const bool kl = (a.opt->method == NMFCU_BRUNET);
     {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OBJECTIVE);
-        a.ops->rowpass(VT_F64, a.V64, a.ldv64, pl.n, pl.p, a.W, a.H, kl ? 2 : 3, pl.S2,
-                       pl.cols_per_split, nullptr, c->obj.as<double>(), st, s);
+        a.ops->objective(a.V64, a.ldv64, pl.n, pl.p, a.W, a.H, kl ? 2 : 3, pl.S2,
+                         pl.cols_per_split, c->obj.as<double>(), st, s);
     }
     StopParams sp;
     sp.stationary = 1;
@@ -431,48 +480,72 @@ nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long ite
     return NMFCU_OK;
 }
 
-// Gram + sums of W (or H) into G / sums.
 void gram_w_full(nmfcu_context *c, const RunArgs &a, double *G, double *sums, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
     a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(), c->ps.as<double>(), st, s);
     a.ops->gram_fin(c->pg.as<double>(), c->ps.as<double>(), pl.Bw, G, sums, st, s);
 }
 void gram_h_full(nmfcu_context *c, const RunArgs &a, double *G, double *sums, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
     a.ops->gram_h(a.H, pl.p, pl.Bh, pl.cols_per_gram, c->pg.as<double>(), c->ps.as<double>(), st, s);
     a.ops->gram_fin(c->pg.as<double>(), c->ps.as<double>(), pl.Bh, G, sums, st, s);
 }
 
-// H step: contraction + epilogue.
-void h_step(nmfcu_context *c, const RunArgs &a, VType vt, const void *V, int64_t ldv,
-            const EpiParams &e, bool ratio, cudaStream_t s) {
+// H step: the streaming contraction over all rows, then the per-column update.
+nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const EpiParams &e,
+                    bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    {
+    const int tcols = ps.so->h_tcols(ratio);
+    const StreamK sk = plan_sk((pl.p + tcols - 1) / tcols,
+                               (pl.n + ps.so->h_brows() - 1) / ps.so->h_brows(), c->sms);
+    if (ps.f32 && pl.n > 0) {
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        ps.so->w_copy(a.W, ps.Wc, pl.n, st, s);
+    }
+    if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
-        a.ops->hstep(vt, V, ldv, pl.n, pl.p, a.W, a.H, ratio, pl.S, pl.rows_per_split,
-                     c->part_h.as<double>(), st, s);
+        CUDA_TRY(ps.so->hpass(ratio, ps.tmVh, ps.tmW, a.H, pl.n, pl.p, sk, c->part.as<double>(),
+                              st, sk.G, s));
     }
     nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-    a.ops->h_epi(a.H, pl.p, c->part_h.as<double>(), pl.p > 0 ? pl.S : 0, e, st, s);
+    ps.so->h_epi(a.H, ps.Ht, pl.p, c->part.as<double>(), sk, tcols, e, st, s);
+    return NMFCU_OK;
 }
 
-// W step: contraction + epilogue.
-void w_step(nmfcu_context *c, const RunArgs &a, VType vt, const void *V, int64_t ldv,
-            const EpiParams &e, bool ratio, cudaStream_t s) {
+// W step: the streaming contraction over all columns, then the per-row update.
+nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const EpiParams &e,
+                    bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    {
+    const int trows = ps.so->w_trows(ratio);
+    const StreamK sk = plan_sk((pl.n + trows - 1) / trows,
+                               (pl.p + ps.so->w_bcols() - 1) / ps.so->w_bcols(), c->sms);
+    if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
-        a.ops->rowpass(vt, V, ldv, pl.n, pl.p, a.W, a.H, ratio ? 1 : 0, pl.S2,
-                       pl.cols_per_split, c->part_w.as<double>(), nullptr, st, s);
+        CUDA_TRY(ps.so->wpass(ratio, ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk, c->part.as<double>(),
+                              st, sk.G, s));
     }
     nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-    a.ops->w_epi(a.W, pl.n, c->part_w.as<double>(), pl.S2, e, st, s);
+    ps.so->w_epi(a.W, pl.n, c->part.as<double>(), sk, trows, e, st, s);
+    return NMFCU_OK;
+}
+
+// H^T copy of the current H (for a W step that is not preceded by an H step).
+void transpose_h(nmfcu_context *c, const RunArgs &a, const PassSet &ps, cudaStream_t s) {
+    const Plan &pl = a.pl;
+    if (pl.p <= 0) return;
+    const int rps = ps.so->rps();
+    const unsigned blocks = std::max(1u, std::min<unsigned>(cdiv((int64_t)pl.p * rps, kThreads), 4096u));
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    if (ps.f32)
+        h_transpose<float><<<blocks, kThreads, 0, s>>>(a.H, static_cast<float *>(ps.Ht), pl.p, pl.r, rps);
+    else
+        h_transpose<double><<<blocks, kThreads, 0, s>>>(a.H, static_cast<double *>(ps.Ht), pl.p, pl.r, rps);
 }
 
 EpiParams epi(const nmfcu_options *o, int r, const double *G, const double *sums, bool hside) {
@@ -488,14 +561,12 @@ EpiParams epi(const nmfcu_options *o, int r, const double *G, const double *sums
 }
 
 // Enqueue one full iteration `it` (1-based).
-void enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp64,
-                       cudaStream_t s) {
+nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp64,
+                               cudaStream_t s) {
     const Plan &pl = a.pl;
     const nmfcu_options *o = a.opt;
     RunState *st = c->state.as<RunState>();
-    const VType vt = fp64 ? VT_F64 : a.vt_main;
-    const void *V = fp64 ? (const void *)a.V64 : a.Vmain;
-    const int64_t ldv = fp64 ? a.ldv64 : a.ldv_main;
+    const PassSet &ps = fp64 ? a.p64 : a.main;
     double *Gw = c->Gw.as<double>(), *sw = c->sw.as<double>();
     double *Gh = c->Gh.as<double>(), *sh = c->sh.as<double>();
 
@@ -503,9 +574,9 @@ void enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp
         case NMFCU_BRUNET: {
             // nmf_run_brunet lib.rs:1558-1575.
             gram_w_full(c, a, Gw, sw, s);  // sum_w (lib.rs:1563-1568)
-            h_step(c, a, vt, V, ldv, epi(o, pl.r, Gw, sw, true), true, s);
+            NMF_TRY(h_step(c, a, ps, epi(o, pl.r, Gw, sw, true), true, s));
             gram_h_full(c, a, Gh, sh, s);  // sum_h (lib.rs:161-169)
-            w_step(c, a, vt, V, ldv, epi(o, pl.r, Gh, sh, false), true, s);
+            NMF_TRY(w_step(c, a, ps, epi(o, pl.r, Gh, sh, false), true, s));
             if (it % 10 == 0) {
                 nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
                 a.ops->clamp(a.W, a.H, pl.n, pl.p, pl.r, DBL_EPSILON, st, s);
@@ -515,11 +586,11 @@ void enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp
         case NMFCU_LEE: {
             // nmf_run_lee lib.rs:1618-1636.
             gram_w_full(c, a, Gw, sw, s);  // W^T W (lib.rs:1622-1631)
-            h_step(c, a, vt, V, ldv, epi(o, pl.r, Gw, sw, true), false, s);
+            NMF_TRY(h_step(c, a, ps, epi(o, pl.r, Gw, sw, true), false, s));
             gram_h_full(c, a, Gh, sh, s);  // H H^T (lib.rs:293-302)
-            w_step(c, a, vt, V, ldv, epi(o, pl.r, Gh, sh, false), false, s);
+            NMF_TRY(w_step(c, a, ps, epi(o, pl.r, Gh, sh, false), false, s));
             if (o->rescale) {
-                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
                 a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(),
                               c->ps.as<double>(), st, s);
                 a.ops->rescale(a.W, pl.n, pl.r, c->ps.as<double>(), pl.Bw, st, s);
@@ -529,9 +600,9 @@ void enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp
         default: {
             // nmf_run_hals lib.rs:667-676; nmf_run_dnmf lib.rs:862-884.
             gram_w_full(c, a, Gw, sw, s);
-            h_step(c, a, vt, V, ldv, epi(o, pl.r, Gw, sw, true), false, s);
+            NMF_TRY(h_step(c, a, ps, epi(o, pl.r, Gw, sw, true), false, s));
             gram_h_full(c, a, Gh, sh, s);
-            w_step(c, a, vt, V, ldv, epi(o, pl.r, Gh, sh, false), false, s);
+            NMF_TRY(w_step(c, a, ps, epi(o, pl.r, Gh, sh, false), false, s));
             if (o->method == NMFCU_DNMF) {
                 gram_w_full(c, a, c->Gw2.as<double>(), c->sw2.as<double>(), s);
                 nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -540,14 +611,26 @@ void enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it, bool fp
             break;
         }
     }
+    return NMFCU_OK;
 }
 
-nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl) {
+nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32) {
     const size_t RP = pl.RP;
     NMF_TRY(c->W.ensure(sizeof(double) * (size_t)pl.n * RP));
     NMF_TRY(c->H.ensure(sizeof(double) * RP * (size_t)pl.p));
-    NMF_TRY(c->part_h.ensure(sizeof(double) * (size_t)pl.S * RP * (size_t)pl.p));
-    NMF_TRY(c->part_w.ensure(sizeof(double) * (size_t)pl.S2 * (size_t)pl.n * RP));
+    const bool ratio = true;  // sized for the larger of the two tilings
+    size_t part = 0;
+    for (bool rt : {ratio, !ratio}) {
+        part = std::max(part, pass_partial_bytes(stream_ops_f64(pl.RP), pl, rt, c->sms));
+        if (need_f32) part = std::max(part, pass_partial_bytes(stream_ops_f32(pl.RP), pl, rt, c->sms));
+    }
+    NMF_TRY(c->part.ensure(part));
+    NMF_TRY(c->Ht64.ensure(sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()));
+    if (need_f32) {
+        const size_t rps = stream_ops_f32(pl.RP)->rps();
+        NMF_TRY(c->Ht32.ensure(sizeof(float) * (size_t)pl.p * rps));
+        NMF_TRY(c->Wf32.ensure(sizeof(float) * (size_t)pl.n * rps));
+    }
     const size_t B = (size_t)std::max(pl.Bw, pl.Bh);
     NMF_TRY(c->pg.ensure(sizeof(double) * B * RP * RP));
     NMF_TRY(c->ps.ensure(sizeof(double) * B * RP));
@@ -606,7 +689,7 @@ nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_d
         (o->precision == NMFCU_PREC_FP32) ? (long long)o->max_iter - o->refine_iters : LLONG_MAX;
     for (long long it = 1; it <= o->max_iter; it++) {
         const bool fp64 = (o->precision == NMFCU_PREC_FP64) || (it > refine_from);
-        enqueue_iteration(c, a, it, fp64, s);
+        NMF_TRY(enqueue_iteration(c, a, it, fp64, s));
         if (stat) NMF_TRY(enqueue_objective(c, a, it, s));
     }
     CUDA_TRY(cudaGetLastError());
@@ -614,6 +697,9 @@ nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_d
     CUDA_TRY(cudaStreamSynchronize(s));
     if (c->timing) c->drain_timing();
     const RunState &hs = *c->h_state;
+    if (hs.timeout != 0)
+        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies (code " +
+                                           std::to_string(hs.timeout) + ")");
     if (hs.error == 1)
         return fail(NMFCU_ERR_INVALID_ARG,
                     "check_interval must be > 0 (the stationary stop evaluates iter % check_interval)");
@@ -754,7 +840,7 @@ nmfcu_status single_step(StepKind kind, int64_t n, int64_t p, int64_t r, const d
     DeviceGuard dg(c->device);
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl));
+    NMF_TRY(ensure_workspace(c, pl, false));
     int64_t ldv = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
     NMF_TRY(put_factors(c, pl, W, H, cudaMemcpyHostToDevice, s));
@@ -763,9 +849,8 @@ nmfcu_status single_step(StepKind kind, int64_t n, int64_t p, int64_t r, const d
     a.opt = &o;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    a.vt_main = VT_F64;
-    a.Vmain = c->V64.ptr;
-    a.ldv_main = ldv;
+    NMF_TRY(make_passset(c, pl, false, c->V64.ptr, ldv, &a.p64));
+    a.main = a.p64;
     a.V64 = c->V64.as<double>();
     a.ldv64 = ldv;
     a.W = c->W.as<double>();
@@ -776,27 +861,31 @@ nmfcu_status single_step(StepKind kind, int64_t n, int64_t p, int64_t r, const d
     switch (kind) {
         case STEP_H_KL:
             gram_w_full(c, a, Gw, sw, s);
-            h_step(c, a, VT_F64, a.V64, ldv, epi(&o, pl.r, Gw, sw, true), true, s);
+            NMF_TRY(h_step(c, a, a.p64, epi(&o, pl.r, Gw, sw, true), true, s));
             NMF_TRY(get_factors(c, pl, nullptr, out, cudaMemcpyDeviceToHost, s));
             break;
         case STEP_W_KL:
             gram_h_full(c, a, Gh, sh, s);
-            w_step(c, a, VT_F64, a.V64, ldv, epi(&o, pl.r, Gh, sh, false), true, s);
+            transpose_h(c, a, a.p64, s);
+            NMF_TRY(w_step(c, a, a.p64, epi(&o, pl.r, Gh, sh, false), true, s));
             NMF_TRY(get_factors(c, pl, out, nullptr, cudaMemcpyDeviceToHost, s));
             break;
         case STEP_H_EUC:
             gram_w_full(c, a, Gw, sw, s);
-            h_step(c, a, VT_F64, a.V64, ldv, epi(&o, pl.r, Gw, sw, true), false, s);
+            NMF_TRY(h_step(c, a, a.p64, epi(&o, pl.r, Gw, sw, true), false, s));
             NMF_TRY(get_factors(c, pl, nullptr, out, cudaMemcpyDeviceToHost, s));
             break;
         case STEP_W_EUC:
             gram_h_full(c, a, Gh, sh, s);
-            w_step(c, a, VT_F64, a.V64, ldv, epi(&o, pl.r, Gh, sh, false), false, s);
+            transpose_h(c, a, a.p64, s);
+            NMF_TRY(w_step(c, a, a.p64, epi(&o, pl.r, Gh, sh, false), false, s));
             NMF_TRY(get_factors(c, pl, out, nullptr, cudaMemcpyDeviceToHost, s));
             break;
     }
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s));
+    if (c->h_state->timeout != 0)
+        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies");
     return NMFCU_OK;
 }
 
@@ -813,7 +902,7 @@ nmfcu_status objective_host(bool kl, int64_t n, int64_t p, int64_t r, const doub
     DeviceGuard dg(c->device);
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl));
+    NMF_TRY(ensure_workspace(c, pl, false));
     NMF_TRY(c->dev.ensure(sizeof(double)));
     int64_t ldv = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
@@ -821,8 +910,8 @@ nmfcu_status objective_host(bool kl, int64_t n, int64_t p, int64_t r, const doub
     CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
     const Ops *ops = ops_for(pl.RP);
     RunState *st = c->state.as<RunState>();
-    ops->rowpass(VT_F64, c->V64.ptr, ldv, pl.n, pl.p, c->W.as<double>(), c->H.as<double>(),
-                 kl ? 2 : 3, pl.S2, pl.cols_per_split, nullptr, c->obj.as<double>(), st, s);
+    ops->objective(c->V64.as<double>(), ldv, pl.n, pl.p, c->W.as<double>(), c->H.as<double>(),
+                   kl ? 2 : 3, pl.S2, pl.cols_per_split, c->obj.as<double>(), st, s);
     StopParams sp{};
     sp.stationary = 0;
     sp.iter = 0;
@@ -917,21 +1006,22 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     DeviceGuard dg(c->device);
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl));
+    const bool f32 = opt->precision == NMFCU_PREC_FP32;
+    NMF_TRY(ensure_workspace(c, pl, f32));
     if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(opt->max_iter + 1)));
     int64_t ldv = 0, ld32 = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
-    if (opt->precision == NMFCU_PREC_FP32)
-        NMF_TRY(make_f32(c, c->V64.as<double>(), ldv, n, p, &ld32, s));
+    if (f32) NMF_TRY(make_f32(c, c->V64.as<double>(), ldv, n, p, &ld32, s));
     NMF_TRY(put_factors(c, pl, W0, H0, cudaMemcpyHostToDevice, s));
     RunArgs a;
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    const bool f32 = opt->precision == NMFCU_PREC_FP32;
-    a.vt_main = f32 ? VT_F32 : VT_F64;
-    a.Vmain = f32 ? c->V32.ptr : c->V64.ptr;
-    a.ldv_main = f32 ? ld32 : ldv;
+    NMF_TRY(make_passset(c, pl, false, c->V64.ptr, ldv, &a.p64));
+    if (f32)
+        NMF_TRY(make_passset(c, pl, true, c->V32.ptr, ld32, &a.main));
+    else
+        a.main = a.p64;
     a.V64 = c->V64.as<double>();
     a.ldv64 = ldv;
     a.W = c->W.as<double>();
@@ -1024,6 +1114,8 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
         return fail(NMFCU_ERR_INVALID_ARG, "precision FP64 needs an f64 V");
     const double *V64 = (v_dtype == NMFCU_F64) ? (const double *)dV : dV64;
     int64_t ld64 = (v_dtype == NMFCU_F64) ? ldv : ldv64;
+    if (V64 && dV64 && v_dtype == NMFCU_F32 && ldv64 < p)
+        return fail(NMFCU_ERR_INVALID_ARG, "ldv64 must be >= p");
     if (f32 && (stat || opt->refine_iters > 0) && !V64)
         return fail(NMFCU_ERR_INVALID_ARG,
                     "precision FP32 with a stationary stop or refinement needs the f64 V (dV64)");
@@ -1031,23 +1123,49 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     DeviceGuard dg(c->device);
     cudaStream_t s = (cudaStream_t)stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl));
-    const void *Vmain = dV;
-    int64_t ldmain = ldv;
+    NMF_TRY(ensure_workspace(c, pl, f32));
+    // The streaming passes read V through TMA, which needs a 16-byte aligned
+    // base and row pitch; a V that is not laid out so is copied into the
+    // context's pitched buffer first.
+    if (V64 && !tma_layout_ok(V64, ld64, 8)) {
+        const int64_t ld = std::max<int64_t>(16, round_up(p, 16));
+        NMF_TRY(c->V64.ensure(sizeof(double) * (size_t)(n * ld)));
+        if (n > 0 && p > 0)
+            CUDA_TRY(cudaMemcpy2DAsync(c->V64.ptr, ld * 8, V64, ld64 * 8, p * 8, n,
+                                       cudaMemcpyDeviceToDevice, s));
+        V64 = c->V64.as<double>();
+        ld64 = ld;
+    }
+    const void *Vmain = (v_dtype == NMFCU_F64) ? (const void *)V64 : dV;
+    int64_t ldmain = (v_dtype == NMFCU_F64) ? ld64 : ldv;
     if (f32 && v_dtype == NMFCU_F64) {
         int64_t ld32 = 0;
-        NMF_TRY(make_f32(c, (const double *)dV, ldv, n, p, &ld32, s));
+        NMF_TRY(make_f32(c, V64, ld64, n, p, &ld32, s));
         Vmain = c->V32.ptr;
         ldmain = ld32;
+    } else if (f32 && !tma_layout_ok(dV, ldv, 4)) {
+        const int64_t ld = std::max<int64_t>(32, round_up(p, 32));
+        NMF_TRY(c->V32.ensure(sizeof(float) * (size_t)(n * ld)));
+        if (n > 0 && p > 0)
+            CUDA_TRY(cudaMemcpy2DAsync(c->V32.ptr, ld * 4, dV, ldv * 4, p * 4, n,
+                                       cudaMemcpyDeviceToDevice, s));
+        Vmain = c->V32.ptr;
+        ldmain = ld;
     }
     NMF_TRY(put_factors(c, pl, dW, dH, cudaMemcpyDeviceToDevice, s));
     RunArgs a;
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    a.vt_main = f32 ? VT_F32 : VT_F64;
-    a.Vmain = Vmain;
-    a.ldv_main = ldmain;
+    if (V64) NMF_TRY(make_passset(c, pl, false, V64, ld64, &a.p64));
+    if (f32)
+        NMF_TRY(make_passset(c, pl, true, Vmain, ldmain, &a.main));
+    else
+        a.main = a.p64;
+    if (f32 && !V64) {
+        // No f64 V: no refinement iterations and no objective (checked above).
+        a.p64 = a.main;
+    }
     a.V64 = V64;
     a.ldv64 = ld64;
     a.W = c->W.as<double>();

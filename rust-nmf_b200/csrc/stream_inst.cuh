@@ -1,0 +1,119 @@
+// stream_inst.cuh -- StreamOps for one element type STREAM_T (included by
+// stream_f32.cu / stream_f64.cu).
+#include <algorithm>
+
+#include "launch.h"
+#include "stream.cuh"
+
+namespace nmfcu {
+namespace {
+
+template <int RP>
+struct StreamOpsT final : StreamOps {
+    using T = STREAM_T;
+    static constexpr int RPS = RankPad<T, RP>::RPS;
+
+    int elem_bytes() const override { return (int)sizeof(T); }
+    int rps() const override { return RPS; }
+    int h_tcols(bool ratio) const override {
+        return ratio ? HCfg<T, RP, true>::TCOLS : HCfg<T, RP, false>::TCOLS;
+    }
+    int h_brows() const override { return HCfg<T, RP, false>::BROWS; }
+    int h_boxc() const override { return HCfg<T, RP, false>::BOXC; }
+    int w_trows(bool ratio) const override {
+        return ratio ? WCfg<T, RP, true>::TROWS : WCfg<T, RP, false>::TROWS;
+    }
+    int w_bcols() const override { return WCfg<T, RP, false>::BCOLS; }
+
+    template <bool RATIO>
+    static cudaError_t launch_h(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
+                                int n, int p, const StreamK &sk, double *part, RunState *st,
+                                int grid, cudaStream_t s) {
+        using C = HCfg<T, RP, RATIO>;
+        static_assert(C::BOXC * C::NBOX == C::TCOLS, "tile / box mismatch");
+        cudaError_t e = cudaFuncSetAttribute(nmfcu::hpass<T, RP, RATIO>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        if (e != cudaSuccess) return e;
+        nmfcu::hpass<T, RP, RATIO><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmW, H, n, p, sk,
+                                                                        part, st);
+        return cudaGetLastError();
+    }
+    template <bool RATIO>
+    static cudaError_t launch_w(const CUtensorMap &tmV, const CUtensorMap &tmH, const double *W,
+                                int n, int p, const StreamK &sk, double *part, RunState *st,
+                                int grid, cudaStream_t s) {
+        using C = WCfg<T, RP, RATIO>;
+        cudaError_t e = cudaFuncSetAttribute(nmfcu::wpass<T, RP, RATIO>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        if (e != cudaSuccess) return e;
+        nmfcu::wpass<T, RP, RATIO><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmH, W, n, p, sk,
+                                                                        part, st);
+        return cudaGetLastError();
+    }
+
+    cudaError_t hpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmW,
+                      const double *H, int n, int p, const StreamK &sk, double *part,
+                      RunState *st, int grid, cudaStream_t s) const override {
+        return ratio ? launch_h<true>(tmV, tmW, H, n, p, sk, part, st, grid, s)
+                     : launch_h<false>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+    }
+    cudaError_t wpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmH,
+                      const double *W, int n, int p, const StreamK &sk, double *part,
+                      RunState *st, int grid, cudaStream_t s) const override {
+        return ratio ? launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s)
+                     : launch_w<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+    }
+    void h_epi(double *H, void *Ht, int p, const double *part, const StreamK &sk, int tcols,
+               const EpiParams &e, const RunState *st, cudaStream_t s) const override {
+        if (p <= 0) return;
+        h_epilogue_sk<RP, T, RPS><<<(p + kThreads - 1) / kThreads, kThreads, 0, s>>>(
+            H, static_cast<T *>(Ht), p, part, sk, tcols, e, st);
+    }
+    void w_epi(double *W, int n, const double *part, const StreamK &sk, int trows,
+               const EpiParams &e, const RunState *st, cudaStream_t s) const override {
+        if (n <= 0) return;
+        w_epilogue_sk<RP><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(W, n, part, sk,
+                                                                            trows, e, st);
+    }
+    void w_copy(const double *W, void *Wc, int n, const RunState *st,
+                cudaStream_t s) const override {
+        if (n <= 0) return;
+        const long long total = (long long)n * RPS;
+        const int blocks = (int)std::min<long long>((total + kThreads - 1) / kThreads, 4096);
+        w_to_f32<RP, RPS><<<blocks, kThreads, 0, s>>>(W, static_cast<float *>(Wc), n, st);
+    }
+};
+
+}  // namespace
+
+const StreamOps *STREAM_FACTORY(int rp) {
+    static const StreamOpsT<2> o2;
+    static const StreamOpsT<4> o4;
+    static const StreamOpsT<6> o6;
+    static const StreamOpsT<8> o8;
+    static const StreamOpsT<10> o10;
+    static const StreamOpsT<12> o12;
+    static const StreamOpsT<14> o14;
+    static const StreamOpsT<16> o16;
+    static const StreamOpsT<20> o20;
+    static const StreamOpsT<24> o24;
+    static const StreamOpsT<28> o28;
+    static const StreamOpsT<32> o32;
+    switch (rp) {
+        case 2: return &o2;
+        case 4: return &o4;
+        case 6: return &o6;
+        case 8: return &o8;
+        case 10: return &o10;
+        case 12: return &o12;
+        case 14: return &o14;
+        case 16: return &o16;
+        case 20: return &o20;
+        case 24: return &o24;
+        case 28: return &o28;
+        case 32: return &o32;
+        default: return nullptr;
+    }
+}
+
+}  // namespace nmfcu
