@@ -19,9 +19,13 @@ struct StreamOps {
     virtual int rps() const = 0;                 // padded rank of the W / H^T copies
     virtual int h_tcols(bool ratio) const = 0;   // H pass tile width (columns)
     virtual int h_brows() const = 0;             // H pass rows per unit
-    virtual int h_boxc() const = 0;              // H pass V box width
+    virtual int h_boxc(bool ratio) const = 0;    // H pass V box width
+    virtual int h_segu() const = 0;              // H pass max units per segment
     virtual int w_trows(bool ratio) const = 0;   // W pass tile height (rows)
-    virtual int w_bcols() const = 0;             // W pass columns per unit
+    virtual int w_bcols(bool ratio) const = 0;   // W pass columns per unit
+    virtual int w_segu(bool ratio) const = 0;    // W pass max units per segment
+    virtual int w_rowb(bool ratio) const = 0;    // W pass row bytes per unit (= swizzle span)
+    virtual int w_boxr(bool ratio) const = 0;    // W pass V box height (rows)
     virtual cudaError_t hpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmW,
                               const double *H, int n, int p, const StreamK &sk, double *part,
                               RunState *st, int grid, cudaStream_t s) const = 0;

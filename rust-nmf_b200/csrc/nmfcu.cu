@@ -286,11 +286,13 @@ Plan make_plan(int64_t n, int64_t p, int64_t r, int sms) {
     return pl;
 }
 
-// Stream-K split of `tiles` tiles of `upt` units each over at most `sms` CTAs.
-StreamK plan_sk(int64_t tiles, int64_t upt, int sms) {
+// Stream-K split of `majors` major tiles, each `units` units long and cut
+// into segments of at most `segu` units, over at most `sms` CTAs.
+StreamK plan_sk(int64_t majors, int64_t units, int64_t segu, int sms) {
     StreamK sk;
-    sk.UPT = (int)std::max<int64_t>(1, upt);
-    sk.U = tiles * upt;
+    sk.nseg = (int)std::max<int64_t>(1, (units + segu - 1) / segu);
+    sk.UPT = (int)std::max<int64_t>(1, (units + sk.nseg - 1) / sk.nseg);
+    sk.U = (units > 0) ? majors * sk.nseg * (int64_t)sk.UPT : 0;
     sk.G = (int)std::min<int64_t>(sms, sk.U);
     if (sk.G <= 0) {
         sk.G = 0;
@@ -300,6 +302,16 @@ StreamK plan_sk(int64_t tiles, int64_t upt, int sms) {
     const int64_t per = (sk.U + sk.G - 1) / sk.G;
     sk.slots = (int)((per + sk.UPT - 1) / sk.UPT + 1);
     return sk;
+}
+
+StreamK plan_h(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
+    const int tcols = so->h_tcols(ratio);
+    return plan_sk((p + tcols - 1) / tcols, (n + so->h_brows() - 1) / so->h_brows(), so->h_segu(),
+                   sms);
+}
+StreamK plan_w(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
+    const int trows = so->w_trows(ratio), bcols = so->w_bcols(ratio);
+    return plan_sk((n + trows - 1) / trows, (p + bcols - 1) / bcols, so->w_segu(ratio), sms);
 }
 
 }  // namespace
@@ -409,15 +421,15 @@ struct PassSet {
 // Partial-sum bytes the two passes of `so` need for this shape.
 size_t pass_partial_bytes(const StreamOps *so, const Plan &pl, bool ratio, int sms) {
     const int tcols = so->h_tcols(ratio), trows = so->w_trows(ratio);
-    const StreamK skh = plan_sk((pl.p + tcols - 1) / tcols, (pl.n + so->h_brows() - 1) / so->h_brows(), sms);
-    const StreamK skw = plan_sk((pl.n + trows - 1) / trows, (pl.p + so->w_bcols() - 1) / so->w_bcols(), sms);
+    const StreamK skh = plan_h(so, ratio, pl.n, pl.p, sms);
+    const StreamK skw = plan_w(so, ratio, pl.n, pl.p, sms);
     const size_t h = (size_t)skh.G * skh.slots * pl.RP * tcols;
     const size_t w = (size_t)skw.G * skw.slots * trows * pl.RP;
     return sizeof(double) * std::max(h, w);
 }
 
-nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, const void *V,
-                          int64_t ldv, PassSet *ps) {
+nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio,
+                          const void *V, int64_t ldv, PassSet *ps) {
     ps->f32 = f32;
     ps->so = f32 ? stream_ops_f32(pl.RP) : stream_ops_f64(pl.RP);
     if (!ps->so) return fail(NMFCU_ERR_UNSUPPORTED, "no streaming kernels for this rank");
@@ -427,16 +439,20 @@ nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, const void
     if (pl.n <= 0 || pl.p <= 0) return NMFCU_OK;  // no pass runs
     if (!tma_layout_ok(V, ldv, f32 ? 4 : 8))
         return fail(NMFCU_ERR_INVALID_ARG, "V must be 16-byte aligned with 16-byte aligned rows");
-    // The W pass reads rows of w_bcols() elements: 64 B (f32) or 128 B (f64),
-    // swizzled to match so that a warp's row-wise reads are conflict-free.
-    const CUtensorMapSwizzle wsw = f32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B;
-    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(), ps->so->h_brows()));
-    NMF_TRY(encode_2d(&ps->tmVw, V, f32, pl.n, pl.p, ldv, ps->so->w_bcols(), 256, wsw));
+    // The W pass reads rows of w_rowb() bytes (32, 64 or 128), swizzled with the
+    // same span so that a warp's row-wise reads are conflict-free.
+    const int rowb = ps->so->w_rowb(ratio);
+    const CUtensorMapSwizzle wsw = rowb == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
+                                   : rowb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                                : CU_TENSOR_MAP_SWIZZLE_128B;
+    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(ratio), ps->so->h_brows()));
+    NMF_TRY(encode_2d(&ps->tmVw, V, f32, pl.n, pl.p, ldv, ps->so->w_bcols(ratio),
+                      ps->so->w_boxr(ratio), wsw));
     if (f32)
         NMF_TRY(encode_2d(&ps->tmW, c->Wf32.ptr, true, pl.n, rps, rps, rps, ps->so->h_brows()));
     else
         NMF_TRY(encode_2d(&ps->tmW, c->W.ptr, false, pl.n, pl.RP, pl.RP, pl.RP, ps->so->h_brows()));
-    NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols()));
+    NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols(ratio)));
     return NMFCU_OK;
 }
 
@@ -501,8 +517,7 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     const int tcols = ps.so->h_tcols(ratio);
-    const StreamK sk = plan_sk((pl.p + tcols - 1) / tcols,
-                               (pl.n + ps.so->h_brows() - 1) / ps.so->h_brows(), c->sms);
+    const StreamK sk = plan_h(ps.so, ratio, pl.n, pl.p, c->sms);
     if (ps.f32 && pl.n > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
         ps.so->w_copy(a.W, ps.Wc, pl.n, st, s);
@@ -523,8 +538,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     const int trows = ps.so->w_trows(ratio);
-    const StreamK sk = plan_sk((pl.n + trows - 1) / trows,
-                               (pl.p + ps.so->w_bcols() - 1) / ps.so->w_bcols(), c->sms);
+    const StreamK sk = plan_w(ps.so, ratio, pl.n, pl.p, c->sms);
     if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
         CUDA_TRY(ps.so->wpass(ratio, ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk, c->part.as<double>(),
@@ -849,7 +863,7 @@ nmfcu_status single_step(StepKind kind, int64_t n, int64_t p, int64_t r, const d
     a.opt = &o;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    NMF_TRY(make_passset(c, pl, false, c->V64.ptr, ldv, &a.p64));
+    NMF_TRY(make_passset(c, pl, false, o.method == NMFCU_BRUNET, c->V64.ptr, ldv, &a.p64));
     a.main = a.p64;
     a.V64 = c->V64.as<double>();
     a.ldv64 = ldv;
@@ -1017,9 +1031,10 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    NMF_TRY(make_passset(c, pl, false, c->V64.ptr, ldv, &a.p64));
+    const bool ratio = (opt->method == NMFCU_BRUNET);
+    NMF_TRY(make_passset(c, pl, false, ratio, c->V64.ptr, ldv, &a.p64));
     if (f32)
-        NMF_TRY(make_passset(c, pl, true, c->V32.ptr, ld32, &a.main));
+        NMF_TRY(make_passset(c, pl, true, ratio, c->V32.ptr, ld32, &a.main));
     else
         a.main = a.p64;
     a.V64 = c->V64.as<double>();
@@ -1157,9 +1172,10 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    if (V64) NMF_TRY(make_passset(c, pl, false, V64, ld64, &a.p64));
+    const bool ratio = (opt->method == NMFCU_BRUNET);
+    if (V64) NMF_TRY(make_passset(c, pl, false, ratio, V64, ld64, &a.p64));
     if (f32)
-        NMF_TRY(make_passset(c, pl, true, Vmain, ldmain, &a.main));
+        NMF_TRY(make_passset(c, pl, true, ratio, Vmain, ldmain, &a.main));
     else
         a.main = a.p64;
     if (f32 && !V64) {

@@ -1,25 +1,29 @@
 // stream.cuh -- the two V-streaming passes of an NMF iteration, fed by TMA.
 //
-// Each pass is one kernel with one CTA (8 warps) per SM.  Lane 0 of warp 0
-// issues cp.async.bulk.tensor loads of V tiles (and of the W rows / H^T
-// columns that pair with them) into a ring of shared-memory stages guarded by
-// mbarriers; all eight warps do the FMAs out of shared memory, so no LSU
-// instruction ever waits on HBM.  The refill of a stage trails its
-// consumption by LAG units, so the issuing lane rarely waits on the other
-// warps.  (A separate producer warp would put three warps on one SM
-// sub-partition and cap every thread at 168 registers.)
+// Each pass is one kernel with one CTA (8 or 16 warps) per SM.  V tiles (and
+// the W rows / H^T columns that pair with them) arrive by
+// cp.async.bulk.tensor into a ring of shared-memory stages, each guarded by a
+// "full" mbarrier; all warps do the FMAs out of shared memory, so no LSU
+// instruction waits on HBM.  A stage is refilled by the last warp to finish
+// with it (a per-stage arrival counter in shared memory), so no warp ever
+// blocks waiting to refill and the ring keeps STAGES - 1 units in flight.
+// (A separate producer warp would put an extra warp on one SM sub-partition
+// and cap every thread below the registers the FMA loops need.)
 //
-// Work split ("stream-K"): a tile is TCOLS columns x all rows (H pass) or
-// TROWS rows x all columns (W pass); a unit is one stage of one tile.  The U
-// units of all tiles are dealt out in equal contiguous ranges, so every CTA
-// streams the same number of bytes whatever the tile count.  A CTA writes a
-// partial sum for every tile its range touches (at most `slots` of them),
-// and the epilogue adds the partials of a tile in CTA order: deterministic,
-// no atomics.
+// Work split ("stream-K"): a tile is TCOLS columns x one segment of at most
+// 2048 rows (H pass), or TROWS rows x one segment of at most 2048 columns (W
+// pass); a unit is one stage of one tile.  The U units of all tiles are dealt
+// out in equal contiguous ranges, so every CTA streams the same number of
+// bytes whatever the tile count.  A CTA writes a partial sum for every tile
+// its range touches (at most `slots` of them), and the epilogue adds the
+// partials of an output row / column over segments and CTAs in a fixed
+// order: deterministic, no atomics.  Segments bound every f32 running sum to
+// 2048 terms; all sums across segments and CTAs are f64.
 //
 //   H pass  A[k][j] = sum_u W[u][k] V[u][j]              (lee, hals, dnmf)
 //           A[k][j] = sum_u W[u][k] V[u][j] / (WH)[u][j]   (brunet)
 //     thread = CPT adjacent columns, all rows; W rows broadcast from smem.
+//     f32 products use the packed FFMA2 (two k at a time).
 //   W pass  B[i][k] = sum_j V[i][j] H[k][j]
 //           B[i][k] = sum_j H[k][j] V[i][j] / (WH)[i][j]
 //     thread = RT rows, all columns; V rows read from a 128B-swizzled tile,
@@ -38,7 +42,7 @@ namespace nmfcu {
 // try_wait may itself suspend briefly, so this bounds a wait to well under a
 // few seconds; a kernel that gives up records it in RunState::timeout.
 constexpr uint32_t kSpinLimit = 1u << 22;
-enum : int { TIMEOUT_FULL = 1, TIMEOUT_EMPTY = 2 };
+enum : int { TIMEOUT_FULL = 1 };
 
 // ---------------------------------------------------------------------------
 // PTX wrappers (mbarrier, TMA)
@@ -88,33 +92,15 @@ __device__ __forceinline__ void record_timeout(RunState *st, int code) {
     if (st) atomicCAS(&st->timeout, 0, code);
 }
 
-// Units trail: a stage is refilled for unit i + STAGES - kLag right after the
-// issuing warp has consumed unit i.
-constexpr int kLag = 2;
-
-// Producer step for local unit j (0-based within this CTA's range): wait
-// until the stage's previous occupant has been released by all warps, then
-// arm the full barrier and issue the loads.  `issue(stage_ptr, bar, j)`
-// issues the TMA copies.  Returns false on a timed-out wait.
-template <int STAGES, int STAGE_BYTES, int TX_BYTES, typename Issue>
-__device__ __forceinline__ bool produce(unsigned char *smem, uint64_t *full, uint64_t *empty,
-                                        long long j, Issue &&issue) {
-    const int s = (int)(j % STAGES);
-    const long long round = j / STAGES;
-    if (round > 0 && !mbar_wait(&empty[s], (uint32_t)((round - 1) & 1))) return false;
-    mbar_expect_tx(&full[s], TX_BYTES);
-    issue(smem + s * STAGE_BYTES, &full[s], j);
-    return true;
-}
-
 // ---------------------------------------------------------------------------
 // Stream-K bookkeeping
 // ---------------------------------------------------------------------------
 struct StreamK {
     long long U;  // units in all tiles
     int G;        // CTAs (G <= U, so no CTA is empty)
-    int UPT;      // units per tile
+    int UPT;      // units per tile (= per segment)
     int slots;    // partial slots per CTA
+    int nseg;     // segments per major tile (tile t = major * nseg + segment)
     __host__ __device__ __forceinline__ long long start(int b) const {
         return (long long)b * U / G;
     }
@@ -137,6 +123,59 @@ __device__ __forceinline__ void sk_range(const StreamK &sk, int t, int *lo, int 
         if (sk.start(m) < e) l = m; else h = m - 1;
     }
     *hi = l;
+}
+
+// Position of a unit in the tile order, advanced one unit at a time so that
+// the loops do no integer division (a runtime 64-bit division per unit costs
+// more than the arithmetic of a small unit).
+struct UnitCursor {
+    int t;       // tile = major * nseg + seg
+    int within;  // unit within the tile (segment)
+    int major;   // column tile (H pass) / row tile (W pass)
+    int seg;     // segment within the major tile
+    __device__ __forceinline__ void init(const StreamK &sk, long long u) {
+        t = (int)(u / sk.UPT);
+        within = (int)(u - (long long)t * sk.UPT);
+        major = t / sk.nseg;
+        seg = t - major * sk.nseg;
+    }
+    __device__ __forceinline__ void next(const StreamK &sk) {
+        if (++within == sk.UPT) {
+            within = 0;
+            ++t;
+            if (++seg == sk.nseg) {
+                seg = 0;
+                ++major;
+            }
+        }
+    }
+    // Unit index along the major tile (row block / column block).
+    __device__ __forceinline__ int along(const StreamK &sk) const { return seg * sk.UPT + within; }
+};
+
+// Orders this thread's earlier generic-proxy shared-memory accesses before
+// its later async-proxy (TMA) writes to shared memory.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// End of a warp's work on stage `s`: count the warp in; the last of `warps`
+// to arrive resets the counter and refills the stage with the unit `next`
+// (if `has_next`).  Called by one lane per warp after __syncwarp().
+template <int STAGE_BYTES, int TX_BYTES, typename Issue>
+__device__ __forceinline__ void release_stage(unsigned char *smem, uint64_t *full, int *arrivals,
+                                              int s, int warps, bool has_next,
+                                              const UnitCursor &next, Issue &&issue) {
+    __threadfence_block();  // this warp's reads of the stage before the count
+    if (atomicAdd(&arrivals[s], 1) == warps - 1) {
+        __threadfence_block();  // every warp's reads before the refill
+        arrivals[s] = 0;
+        if (has_next) {
+            fence_proxy_async_smem();
+            mbar_expect_tx(&full[s], TX_BYTES);
+            issue(smem + s * STAGE_BYTES, &full[s], next);
+        }
+    }
 }
 
 template <typename T, int RP>
@@ -164,188 +203,251 @@ __device__ __forceinline__ void lds_vec(T (&dst)[N], const T *src) {
     }
 }
 
-// A row of RP values (RPS-padded) from shared memory into registers.
-template <typename T, int RP>
-__device__ __forceinline__ void lds_row(T (&dst)[RP], const T *src) {
-    constexpr int V = 16 / (int)sizeof(T);
+// N consecutive values from shared memory into registers, in vectors of up to
+// 16 bytes; ALIGN is the byte alignment the caller guarantees for `src`.
+template <typename T, int N, int ALIGN = 16>
+__device__ __forceinline__ void lds_row(T (&dst)[N], const T *src) {
+    constexpr int VB = ALIGN >= 16 ? 16 : (ALIGN >= 8 ? 8 : (int)sizeof(T));
+    constexpr int V = VB / (int)sizeof(T) > 0 ? VB / (int)sizeof(T) : 1;
 #pragma unroll
-    for (int k0 = 0; k0 < RP; k0 += V) {
+    for (int k0 = 0; k0 < N; k0 += V) {
         T tmp[V];
         lds_vec<T, V>(tmp, src + k0);
 #pragma unroll
         for (int i = 0; i < V; i++)
-            if (k0 + i < RP) dst[k0 + i] = tmp[i];
+            if (k0 + i < N) dst[k0 + i] = tmp[i];
     }
 }
+
+// Byte alignment of an offset of `elems` T within a 16-byte aligned row.
+template <typename T>
+__host__ __device__ constexpr int align_of_offset(int elems) {
+    return (elems * (int)sizeof(T)) % 16 == 0 ? 16 : ((elems * (int)sizeof(T)) % 8 == 0 ? 8 : 4);
+}
+
+// acc[k] += a[k] * x for k < RP.  f32: packed FFMA2 on pairs of k (RP is
+// even); f64: one DFMA per k.
+template <int RP>
+__device__ __forceinline__ void axpy(float (&acc)[RP], const float (&a)[RP], float x) {
+    const float2 xx = make_float2(x, x);
+#pragma unroll
+    for (int k = 0; k + 1 < RP; k += 2) {
+        const float2 r = __ffma2_rn(make_float2(a[k], a[k + 1]), xx,
+                                    make_float2(acc[k], acc[k + 1]));
+        acc[k] = r.x;
+        acc[k + 1] = r.y;
+    }
+    if constexpr (RP % 2 == 1) acc[RP - 1] = fmaf(a[RP - 1], x, acc[RP - 1]);
+}
+template <int RP>
+__device__ __forceinline__ void axpy(double (&acc)[RP], const double (&a)[RP], double x) {
+#pragma unroll
+    for (int k = 0; k < RP; k++) acc[k] = fma(a[k], x, acc[k]);
+}
+
+// sum_k a[k] * b[k].  f32: two packed partial sums, added at the end.
+template <int RP>
+__device__ __forceinline__ float dot(const float (&a)[RP], const float (&b)[RP]) {
+    float2 s = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int k = 0; k + 1 < RP; k += 2)
+        s = __ffma2_rn(make_float2(a[k], a[k + 1]), make_float2(b[k], b[k + 1]), s);
+    if constexpr (RP % 2 == 1) s.x = fmaf(a[RP - 1], b[RP - 1], s.x);
+    return s.x + s.y;
+}
+template <int RP>
+__device__ __forceinline__ double dot(const double (&a)[RP], const double (&b)[RP]) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP; k++) s = fma(a[k], b[k], s);
+    return s;
+}
+
+// Register blocking.  The rank range is split in KS = 2 halves across the
+// two half-warps (lanes 0-15 take k < RP/2, lanes 16-31 the rest), so that a
+// thread can own several columns (H pass) or rows (W pass) and reuse every
+// shared-memory load for several FMAs.  Where a pass needs a full dot
+// product over k (the brunet ratio), the two halves are added with one
+// shfl_xor(16).
+constexpr int KS = 2;
+
+// Warp count from the 32-bit registers a thread's live arrays take: 16 warps
+// (128 registers a thread) when the estimate leaves room for addressing and
+// loop state, else 8 (255 registers).  `limit` is the estimate that still
+// compiled without spills at 128 registers (80; 64 for the f64 ratio
+// kernels, whose IEEE divide sequence needs more).
+__host__ __device__ constexpr int warps_for(int regs, int limit) {
+    return regs <= limit ? 16 : 8;
+}
+template <typename T, bool RATIO>
+__host__ __device__ constexpr int reg_limit() {
+    return (sizeof(T) == 8 && RATIO) ? 64 : 80;
+}
+
+// Rows / columns a segment may span (bounds every f32 running sum).
+constexpr int kSegSpan = 2048;
 
 // ---------------------------------------------------------------------------
 // H pass
 // ---------------------------------------------------------------------------
 template <typename T, int RP, bool RATIO>
 struct HCfg {
-    static constexpr int kWarps = 8;
-    static constexpr int CPT = (sizeof(T) == 8 && RATIO) ? 1 : 2;  // columns per thread
-    static constexpr int TCOLS = 32 * CPT * kWarps;
+    static constexpr int W32 = (int)sizeof(T) / 4;  // 32-bit registers per T
+    static constexpr int KB = RP / KS;               // k per thread
+    static constexpr int LPK = 32 / KS;              // lanes per k-half
+    // Columns per thread: more where one column's arithmetic is cheap.
+    static constexpr int CPT = RATIO ? 1 : (sizeof(T) == 4 ? 4 : 2);
+    static constexpr int REGS = W32 * (CPT * KB * (RATIO ? 2 : 1) + KB + CPT);
+    static constexpr int kWarps = warps_for(REGS, reg_limit<T, RATIO>());
+    static constexpr int TCOLS = LPK * CPT * kWarps;
     static constexpr int BOXC = TCOLS < 256 ? TCOLS : 256;
     static constexpr int NBOX = TCOLS / BOXC;
     static constexpr int BROWS = 8;
+    static constexpr int SEGU = kSegSpan / BROWS;  // max units per segment
     static constexpr int RPS = RankPad<T, RP>::RPS;
+    static constexpr int KALIGN = align_of_offset<T>(KB);
     static constexpr int VBYTES = BROWS * TCOLS * (int)sizeof(T);
     static constexpr int WBYTES = BROWS * RPS * (int)sizeof(T);
     static constexpr int STAGE = (VBYTES + WBYTES + 1023) / 1024 * 1024;
-    static constexpr int STAGES_FIT = (180 * 1024) / STAGE;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_FIT > 10 ? 10 : STAGES_FIT;
     static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
-    static constexpr int FLUSH2 = 32;  // f32: stages per f32 partial sum
-    // 32-bit registers a row needs: accumulators (+ H columns when RATIO)
-    // and the row of W.
-    static constexpr int REGS = (int)sizeof(T) / 4 * RP * (CPT * (RATIO ? 2 : 1) + 1);
-    // f32: the running total of the per-FLUSH2 partial sums is f64 when it
-    // fits the register budget, f32 otherwise.
-    static constexpr bool TOTAL64 = sizeof(T) == 8 || REGS + 2 * CPT * RP <= 160;
-    using Total = typename std::conditional<TOTAL64, double, float>::type;
-    static constexpr int UNROLL = (REGS + (int)sizeof(T) / 4 * RP <= 150) ? 2 : 1;
-    static_assert(STAGES >= kLag + 2, "the refill lag needs more stages");
+    static_assert(RP % KS == 0, "rank buckets are even");
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
 };
 
 template <typename T, int RP, bool RATIO>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(HCfg<T, RP, RATIO>::kWarps * 32, 1)
     hpass(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmW,
           const double *__restrict__ H, int n, int p, StreamK sk, double *__restrict__ part,
           RunState *st) {
     using C = HCfg<T, RP, RATIO>;
-    using Total = typename C::Total;
-    constexpr int CPT = C::CPT;
+    constexpr int CPT = C::CPT, KB = C::KB;
     if (run_stopped(st)) return;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char *smem = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    // 1024 B alignment for the boxes, by offsetting the shared array itself so
+    // that every access stays a shared-memory (LDS) access.
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
-    uint64_t *empty = full + C::STAGES;
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer = (threadIdx.x == 0);
     const int b = blockIdx.x;
     const long long u0 = sk.start(b), u1 = sk.start(b + 1);
     const long long nunits = u1 - u0;
 
-    // Loads of local unit j: the V boxes of its tile and rows, and its W rows.
-    auto issue = [&](unsigned char *stg, uint64_t *bar, long long j) {
-        const long long u = u0 + j;
-        const int t = (int)(u / sk.UPT), rb = (int)(u % sk.UPT);
+    // Loads of one unit: the V boxes of its columns and rows, and its W rows.
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int rb = c.along(sk);
 #pragma unroll
         for (int q = 0; q < C::NBOX; q++)
             tma_load_2d(stg + q * C::BROWS * C::BOXC * (int)sizeof(T), &tmV, bar,
-                        t * C::TCOLS + q * C::BOXC, rb * C::BROWS);
+                        c.major * C::TCOLS + q * C::BOXC, rb * C::BROWS);
         tma_load_2d(stg + C::VBYTES, &tmW, bar, 0, rb * C::BROWS);
     };
+    // `ahead`: the unit STAGES after the one being consumed (lane 0 of each
+    // warp keeps one, for the refill it may have to issue).
+    UnitCursor ahead;
+    ahead.init(sk, u0);
     if (producer) {
         for (int s = 0; s < C::STAGES; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], C::kWarps);
+            arrivals[s] = 0;
         }
         fence_mbar_init();
-        for (long long j = 0; j < nunits && j < C::STAGES; j++)
-            produce<C::STAGES, C::STAGE, C::VBYTES + C::WBYTES>(smem, full, empty, j, issue);
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::WBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
     }
     __syncthreads();
 
-    const int colw = warp * 32 * CPT + lane * CPT;  // column within the tile
+    const int kh = lane / C::LPK, cl = lane % C::LPK;
+    const int k0 = kh * KB;                                // this thread's k range
+    const int colw = (warp * C::LPK + cl) * CPT;           // first column within the tile
     const int box = colw / C::BOXC, boff = colw % C::BOXC;
-    T acc[CPT][RP];
-    Total acc2[CPT][RP];  // f32: running total of the FLUSH2-stage partial sums
-    T hcol[RATIO ? CPT : 1][RATIO ? RP : 1];
-    int cur = -1, cnt = 0;
-    const int tile0 = (int)(u0 / sk.UPT);
+    T acc[CPT][KB];
+    T hcol[RATIO ? CPT : 1][RATIO ? KB : 1];
+    int cur = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
         double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS + colw;
 #pragma unroll
-        for (int k = 0; k < RP; k++)
+        for (int k = 0; k < KB; k++)
 #pragma unroll
             for (int c = 0; c < CPT; c++)
-                dst[(size_t)k * C::TCOLS + c] =
-                    (sizeof(T) == 4) ? (double)acc2[c][k] + (double)acc[c][k] : (double)acc[c][k];
+                dst[(size_t)(k0 + k) * C::TCOLS + c] = (double)acc[c][k];
     };
 
+    int cur_major = -1;
     for (long long i = 0; i < nunits; ++i) {
-        const long long u = u0 + i;
-        const int t = (int)(u / sk.UPT);
+        const int t = uc.t;
         if (t != cur) {
             if (cur >= 0) flush(cur);
             cur = t;
-            cnt = 0;
 #pragma unroll
             for (int c = 0; c < CPT; c++)
 #pragma unroll
-                for (int k = 0; k < RP; k++) {
-                    acc[c][k] = (T)0;
-                    acc2[c][k] = (Total)0;
-                }
+                for (int k = 0; k < KB; k++) acc[c][k] = (T)0;
             if constexpr (RATIO) {
+                if (uc.major != cur_major) {
+                    cur_major = uc.major;
 #pragma unroll
-                for (int c = 0; c < CPT; c++) {
-                    const int j = t * C::TCOLS + colw + c;
+                    for (int c = 0; c < CPT; c++) {
+                        const int j = uc.major * C::TCOLS + colw + c;
 #pragma unroll
-                    for (int k = 0; k < RP; k++)
-                        hcol[c][k] = (j < p) ? (T)H[(size_t)k * p + j] : (T)0;
+                        for (int k = 0; k < KB; k++)
+                            hcol[c][k] = (j < p) ? (T)H[(size_t)(k0 + k) * p + j] : (T)0;
+                    }
                 }
             }
         }
-        const int s = (int)(i % C::STAGES);
-        if (!mbar_wait(&full[s], (uint32_t)((i / C::STAGES) & 1))) {
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
             record_timeout(st, TIMEOUT_FULL);
             ok = false;
             break;
         }
         const unsigned char *stg = smem + s * C::STAGE;
         const T *sv = reinterpret_cast<const T *>(stg) + box * C::BROWS * C::BOXC + boff;
-        const T *sw = reinterpret_cast<const T *>(stg + C::VBYTES);
-#pragma unroll(C::UNROLL)
+        const T *sw = reinterpret_cast<const T *>(stg + C::VBYTES) + k0;
+#pragma unroll 2
         for (int r = 0; r < C::BROWS; r++) {
             T v[CPT];
             lds_vec<T, CPT>(v, sv + r * C::BOXC);
-            T w[RP];
-            lds_row<T, RP>(w, sw + r * C::RPS);
-            if constexpr (RATIO) {
+            T w[KB];
+            lds_row<T, KB, C::KALIGN>(w, sw + r * C::RPS);
 #pragma unroll
-                for (int c = 0; c < CPT; c++) {
-                    T wh = (T)0;
-#pragma unroll
-                    for (int k = 0; k < RP; k++) wh = fma(w[k], hcol[c][k], wh);
+            for (int c = 0; c < CPT; c++) {
+                if constexpr (RATIO) {
+                    T wh = dot<KB>(w, hcol[c]);
+                    wh += __shfl_xor_sync(0xffffffffu, wh, C::LPK);  // the other k-half
                     const T q = (wh != (T)0) ? ratio_div(v[c], wh) : (T)0;
-#pragma unroll
-                    for (int k = 0; k < RP; k++) acc[c][k] = fma(w[k], q, acc[c][k]);
+                    axpy<KB>(acc[c], w, q);
+                } else {
+                    axpy<KB>(acc[c], w, v[c]);
                 }
-            } else {
-#pragma unroll
-                for (int c = 0; c < CPT; c++)
-#pragma unroll
-                    for (int k = 0; k < RP; k++) acc[c][k] = fma(w[k], v[c], acc[c][k]);
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-        if (producer && i >= kLag && i - kLag + C::STAGES < nunits) {
-            if (!produce<C::STAGES, C::STAGE, C::VBYTES + C::WBYTES>(
-                    smem, full, empty, i - kLag + C::STAGES, issue)) {
-                record_timeout(st, TIMEOUT_EMPTY);
-                ok = false;
-                break;
-            }
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::WBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
         }
-        if constexpr (sizeof(T) == 4) {
-            if (++cnt == C::FLUSH2) {
-                cnt = 0;
-#pragma unroll
-                for (int c = 0; c < CPT; c++)
-#pragma unroll
-                    for (int k = 0; k < RP; k++) {
-                        acc2[c][k] += (Total)acc[c][k];
-                        acc[c][k] = (T)0;
-                    }
-            }
-        }
+        uc.next(sk);
     }
     if (ok && cur >= 0) flush(cur);
 }
@@ -355,174 +457,180 @@ __global__ void __launch_bounds__(256, 1)
 // ---------------------------------------------------------------------------
 template <typename T, int RP, bool RATIO>
 struct WCfg {
-    static constexpr int kWarps = 8;
-    static constexpr int RT = (sizeof(T) == 4) ? 2 : 1;  // rows per thread
-    static constexpr int TROWS = 256 * RT;
-    static constexpr int BCOLS = 16;                       // columns per unit
-    static constexpr int ROWB = BCOLS * (int)sizeof(T);    // bytes of a row per unit
-    static constexpr int CHUNKS = ROWB / 16;               // 16 B chunks per row
-    // TMA swizzle matching the row: 128 B (f64) or 64 B (f32).  Physical chunk
-    // of logical chunk c in row r: c ^ ((r * ROWB >> 7) & (CHUNKS - 1)).
+    static constexpr int W32 = (int)sizeof(T) / 4;
+    static constexpr int KB = RP / KS;
+    static constexpr int LPK = 32 / KS;
+    // Rows per thread: more where one row's arithmetic is cheap.
+    static constexpr int RT = RATIO ? (sizeof(T) == 4 ? 2 : 1) : (sizeof(T) == 4 ? 4 : 2);
+    static constexpr int REGS = W32 * (RT * KB * (RATIO ? 2 : 1) + KB + 2 * RT);
+    static constexpr int kWarps = warps_for(REGS, reg_limit<T, RATIO>());
+    static constexpr int TROWS = LPK * RT * kWarps;       // rows per tile
+    static constexpr int BOXR = TROWS < 256 ? TROWS : 256;  // rows per V box
+    static constexpr int NBOX = TROWS / BOXR;
+    // Bytes of a row per unit: a 32 KB stage, at most one 128 B swizzle span.
+    static constexpr int ROWB = 32768 / TROWS < 128 ? 32768 / TROWS : 128;
+    static constexpr int BCOLS = ROWB / (int)sizeof(T);   // columns per unit
+    static constexpr int CHUNKS = ROWB / 16;              // 16 B chunks per row
+    static constexpr int SEGU = kSegSpan / BCOLS;         // max units per segment
+    // TMA swizzle of span ROWB: logical chunk c of row r sits at physical
+    // chunk c ^ ((r * ROWB >> 7) & (CHUNKS - 1)).
     static constexpr int RPS = RankPad<T, RP>::RPS;
+    static constexpr int KALIGN = align_of_offset<T>(KB);
     static constexpr int VBYTES = TROWS * ROWB;
     static constexpr int HBYTES = BCOLS * RPS * (int)sizeof(T);
     static constexpr int STAGE = (VBYTES + HBYTES + 1023) / 1024 * 1024;
-    static constexpr int STAGES_FIT = (200 * 1024) / STAGE;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
     static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
-    static constexpr int FLUSH2 = 32;
-    // 32-bit registers: accumulators (+ W rows when RATIO) and one H column.
-    static constexpr int REGS = (int)sizeof(T) / 4 * RP * (RT * (RATIO ? 2 : 1) + 1);
-    static constexpr bool TOTAL64 = sizeof(T) == 8 || REGS + 2 * RT * RP <= 160;
-    using Total = typename std::conditional<TOTAL64, double, float>::type;
-    static constexpr int UNROLL = (REGS + (int)sizeof(T) / 4 * RP <= 150) ? 2 : 1;
-    static_assert(STAGES >= kLag + 2, "the refill lag needs more stages");
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
+    static_assert(ROWB == 32 || ROWB == 64 || ROWB == 128, "swizzle span");
+    static_assert(TROWS % BOXR == 0, "whole boxes");
 };
 
 template <typename T, int RP, bool RATIO>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
     wpass(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmH,
           const double *__restrict__ W, int n, int p, StreamK sk, double *__restrict__ part,
           RunState *st) {
     using C = WCfg<T, RP, RATIO>;
-    using Total = typename C::Total;
-    constexpr int RT = C::RT;
+    constexpr int RT = C::RT, KB = C::KB;
     constexpr int VEC = 16 / (int)sizeof(T);  // columns per 16-byte chunk
     if (run_stopped(st)) return;
-    extern __shared__ unsigned char smem_raw[];
-    unsigned char *smem = reinterpret_cast<unsigned char *>(
-        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
-    uint64_t *empty = full + C::STAGES;
-    const int lane = threadIdx.x & 31;
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer = (threadIdx.x == 0);
     const int b = blockIdx.x;
     const long long u0 = sk.start(b), u1 = sk.start(b + 1);
     const long long nunits = u1 - u0;
 
-    // Loads of local unit j: RT boxes of 256 rows x BCOLS columns of V
+    // Loads of one unit: NBOX boxes of BOXR rows x BCOLS columns of V
     // (swizzled) and the matching BCOLS rows of H^T.
-    auto issue = [&](unsigned char *stg, uint64_t *bar, long long j) {
-        const long long u = u0 + j;
-        const int t = (int)(u / sk.UPT), cb = (int)(u % sk.UPT);
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int cb = c.along(sk);
 #pragma unroll
-        for (int q = 0; q < RT; q++)
-            tma_load_2d(stg + q * 256 * C::ROWB, &tmV, bar, cb * C::BCOLS, t * C::TROWS + q * 256);
+        for (int q = 0; q < C::NBOX; q++)
+            tma_load_2d(stg + q * C::BOXR * C::ROWB, &tmV, bar, cb * C::BCOLS,
+                        c.major * C::TROWS + q * C::BOXR);
         tma_load_2d(stg + C::VBYTES, &tmH, bar, 0, cb * C::BCOLS);
     };
+    // `ahead`: the unit STAGES after the one being consumed (lane 0 of each
+    // warp keeps one, for the refill it may have to issue).
+    UnitCursor ahead;
+    ahead.init(sk, u0);
     if (producer) {
         for (int s = 0; s < C::STAGES; s++) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], C::kWarps);
+            arrivals[s] = 0;
         }
         fence_mbar_init();
-        for (long long j = 0; j < nunits && j < C::STAGES; j++)
-            produce<C::STAGES, C::STAGE, C::VBYTES + C::HBYTES>(smem, full, empty, j, issue);
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::HBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
     }
     __syncthreads();
 
-    const int tid = threadIdx.x;  // rows tid + 256 q of the tile
-    T acc[RT][RP];
-    Total acc2[RT][RP];
-    T wrow[RATIO ? RT : 1][RATIO ? RP : 1];
-    int cur = -1, cnt = 0;
-    const int tile0 = (int)(u0 / sk.UPT);
+    const int kh = lane / C::LPK, rl = lane % C::LPK;
+    const int k0 = kh * KB;
+    // Rows of this thread within the tile: a warp owns LPK * RT consecutive
+    // rows; lane rl takes rows rl, rl + LPK, ... (a half-warp's loads touch
+    // LPK distinct rows, the other half-warp reads the same rows).
+    int rows[RT];
+    int swz[RT];
+#pragma unroll
+    for (int q = 0; q < RT; q++) {
+        rows[q] = warp * C::LPK * RT + q * C::LPK + rl;
+        swz[q] = ((rows[q] * C::ROWB) >> 7) & (C::CHUNKS - 1);
+    }
+    T acc[RT][KB];
+    T wrow[RATIO ? RT : 1][RATIO ? KB : 1];
+    int cur = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP;
+        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP + k0;
 #pragma unroll
         for (int q = 0; q < RT; q++)
 #pragma unroll
-            for (int k = 0; k < RP; k++)
-                dst[(size_t)(tid + 256 * q) * RP + k] =
-                    (sizeof(T) == 4) ? (double)acc2[q][k] + (double)acc[q][k] : (double)acc[q][k];
+            for (int k = 0; k < KB; k++) dst[(size_t)rows[q] * RP + k] = (double)acc[q][k];
     };
 
+    int cur_major = -1;
     for (long long i = 0; i < nunits; ++i) {
-        const long long u = u0 + i;
-        const int t = (int)(u / sk.UPT);
+        const int t = uc.t;
         if (t != cur) {
             if (cur >= 0) flush(cur);
             cur = t;
-            cnt = 0;
 #pragma unroll
             for (int q = 0; q < RT; q++)
 #pragma unroll
-                for (int k = 0; k < RP; k++) {
-                    acc[q][k] = (T)0;
-                    acc2[q][k] = (Total)0;
-                }
+                for (int k = 0; k < KB; k++) acc[q][k] = (T)0;
             if constexpr (RATIO) {
+                if (uc.major != cur_major) {
+                    cur_major = uc.major;
 #pragma unroll
-                for (int q = 0; q < RT; q++) {
-                    const int row = t * C::TROWS + tid + 256 * q;
+                    for (int q = 0; q < RT; q++) {
+                        const int row = uc.major * C::TROWS + rows[q];
 #pragma unroll
-                    for (int k = 0; k < RP; k++)
-                        wrow[q][k] = (row < n) ? (T)W[(size_t)row * RP + k] : (T)0;
+                        for (int k = 0; k < KB; k++)
+                            wrow[q][k] = (row < n) ? (T)W[(size_t)row * RP + k0 + k] : (T)0;
+                    }
                 }
             }
         }
-        const int s = (int)(i % C::STAGES);
-        if (!mbar_wait(&full[s], (uint32_t)((i / C::STAGES) & 1))) {
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
             record_timeout(st, TIMEOUT_FULL);
             ok = false;
             break;
         }
         const unsigned char *stg = smem + s * C::STAGE;
-        const T *sh = reinterpret_cast<const T *>(stg + C::VBYTES);
-        // Swizzle phase of this thread's row (same for every box: boxes start
-        // on 16 KB boundaries).
-        const int sw = ((tid * C::ROWB) >> 7) & (C::CHUNKS - 1);
-#pragma unroll(C::UNROLL)
+        const T *sh = reinterpret_cast<const T *>(stg + C::VBYTES) + k0;
+#pragma unroll
         for (int ci = 0; ci < C::CHUNKS; ci++) {
             T v[RT][VEC];
 #pragma unroll
             for (int q = 0; q < RT; q++)
                 lds_vec<T, VEC>(v[q], reinterpret_cast<const T *>(
-                                          stg + q * 256 * C::ROWB + tid * C::ROWB + ((ci ^ sw) << 4)));
+                                          stg + rows[q] * C::ROWB + ((ci ^ swz[q]) << 4)));
 #pragma unroll
             for (int e = 0; e < VEC; e++) {
-                T hc[RP];
-                lds_row<T, RP>(hc, sh + (ci * VEC + e) * C::RPS);
+                T hc[KB];
+                lds_row<T, KB, C::KALIGN>(hc, sh + (ci * VEC + e) * C::RPS);
 #pragma unroll
                 for (int q = 0; q < RT; q++) {
                     if constexpr (RATIO) {
-                        T wh = (T)0;
-#pragma unroll
-                        for (int k = 0; k < RP; k++) wh = fma(wrow[q][k], hc[k], wh);
+                        T wh = dot<KB>(wrow[q], hc);
+                        wh += __shfl_xor_sync(0xffffffffu, wh, C::LPK);  // the other k-half
                         const T qv = (wh != (T)0) ? ratio_div(v[q][e], wh) : (T)0;
-#pragma unroll
-                        for (int k = 0; k < RP; k++) acc[q][k] = fma(hc[k], qv, acc[q][k]);
+                        axpy<KB>(acc[q], hc, qv);
                     } else {
-#pragma unroll
-                        for (int k = 0; k < RP; k++) acc[q][k] = fma(v[q][e], hc[k], acc[q][k]);
+                        axpy<KB>(acc[q], hc, v[q][e]);
                     }
                 }
             }
         }
         __syncwarp();
-        if (lane == 0) mbar_arrive(&empty[s]);
-        if (producer && i >= kLag && i - kLag + C::STAGES < nunits) {
-            if (!produce<C::STAGES, C::STAGE, C::VBYTES + C::HBYTES>(
-                    smem, full, empty, i - kLag + C::STAGES, issue)) {
-                record_timeout(st, TIMEOUT_EMPTY);
-                ok = false;
-                break;
-            }
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::HBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
         }
-        if constexpr (sizeof(T) == 4) {
-            if (++cnt == C::FLUSH2) {
-                cnt = 0;
-#pragma unroll
-                for (int q = 0; q < RT; q++)
-#pragma unroll
-                    for (int k = 0; k < RP; k++) {
-                        acc2[q][k] += (Total)acc[q][k];
-                        acc[q][k] = (T)0;
-                    }
-            }
-        }
+        uc.next(sk);
     }
     if (ok && cur >= 0) flush(cur);
 }
@@ -531,9 +639,31 @@ __global__ void __launch_bounds__(256, 1)
 // Epilogues for the stream-K partials
 // ---------------------------------------------------------------------------
 
-// One thread per column: sum the tile's partials in CTA order, apply the H
-// update, write H (RP x p, f64) and the copy H^T (p x RPS_T, type TH) that
-// the next W pass streams.
+// Sum of the partials of output `c` of major tile `mt`, over its segments and
+// their CTAs, in that order.  `stride_k` / `stride_row` describe the partial
+// layout: element (slot base) + k * stride_k + c * stride_c.
+template <int RP>
+__device__ __forceinline__ void gather_partials(const double *__restrict__ part,
+                                                const StreamK &sk, int mt, size_t slot_elems,
+                                                size_t off, size_t stride_k, double (&num)[RP]) {
+#pragma unroll
+    for (int k = 0; k < RP; k++) num[k] = 0.0;
+    if (sk.G <= 0) return;  // no units at all: every sum is empty
+    for (int seg = 0; seg < sk.nseg; seg++) {
+        const int t = mt * sk.nseg + seg;
+        int lo, hi;
+        sk_range(sk, t, &lo, &hi);
+        for (int b = lo; b <= hi; b++) {
+            const int slot = t - (int)(sk.start(b) / sk.UPT);
+            const double *src = part + ((size_t)b * sk.slots + slot) * slot_elems + off;
+#pragma unroll
+            for (int k = 0; k < RP; k++) num[k] += src[(size_t)k * stride_k];
+        }
+    }
+}
+
+// One thread per column: sum the partials, apply the H update, write H
+// (RP x p, f64) and the copy H^T (p x RPS_T, type TH) the next W pass streams.
 template <int RP, typename TH, int RPS_T>
 __global__ void __launch_bounds__(kThreads)
     h_epilogue_sk(double *__restrict__ H, TH *__restrict__ Ht, int p,
@@ -542,21 +672,11 @@ __global__ void __launch_bounds__(kThreads)
     if (run_stopped(st)) return;
     const int j = blockIdx.x * kThreads + threadIdx.x;
     if (j >= p) return;
-    const int t = j / tcols, c = j - t * tcols;
-    int lo = 0, hi = -1;  // no units at all (n == 0): every sum is empty
-    if (sk.G > 0) sk_range(sk, t, &lo, &hi);
+    const int ct = j / tcols, c = j - ct * tcols;
     double num[RP], hc[RP];
+    gather_partials<RP>(part, sk, ct, (size_t)RP * tcols, c, tcols, num);
 #pragma unroll
-    for (int k = 0; k < RP; k++) {
-        num[k] = 0.0;
-        hc[k] = H[(size_t)k * p + j];
-    }
-    for (int b = lo; b <= hi; b++) {
-        const int slot = t - (int)(sk.start(b) / sk.UPT);
-        const double *src = part + ((size_t)b * sk.slots + slot) * RP * tcols + c;
-#pragma unroll
-        for (int k = 0; k < RP; k++) num[k] += src[(size_t)k * tcols];
-    }
+    for (int k = 0; k < RP; k++) hc[k] = H[(size_t)k * p + j];
     h_update<RP>(e, num, hc);
 #pragma unroll
     for (int k = 0; k < RP; k++)
@@ -566,7 +686,7 @@ __global__ void __launch_bounds__(kThreads)
     for (int k = 0; k < RPS_T; k++) ht[k] = (k < e.r && k < RP) ? (TH)hc[k] : (TH)0;
 }
 
-// One thread per row: sum the tile's partials in CTA order, apply the W update.
+// One thread per row: sum the partials, apply the W update.
 template <int RP>
 __global__ void __launch_bounds__(kThreads)
     w_epilogue_sk(double *__restrict__ W, int n, const double *__restrict__ part, StreamK sk,
@@ -574,21 +694,11 @@ __global__ void __launch_bounds__(kThreads)
     if (run_stopped(st)) return;
     const int i = blockIdx.x * kThreads + threadIdx.x;
     if (i >= n) return;
-    const int t = i / trows, rl = i - t * trows;
-    int lo = 0, hi = -1;  // no units at all (p == 0): every sum is empty
-    if (sk.G > 0) sk_range(sk, t, &lo, &hi);
+    const int rt = i / trows, rl = i - rt * trows;
     double num[RP], wr[RP];
+    gather_partials<RP>(part, sk, rt, (size_t)trows * RP, (size_t)rl * RP, 1, num);
 #pragma unroll
-    for (int k = 0; k < RP; k++) {
-        num[k] = 0.0;
-        wr[k] = W[(size_t)i * RP + k];
-    }
-    for (int b = lo; b <= hi; b++) {
-        const int slot = t - (int)(sk.start(b) / sk.UPT);
-        const double *src = part + (((size_t)b * sk.slots + slot) * trows + rl) * RP;
-#pragma unroll
-        for (int k = 0; k < RP; k++) num[k] += src[k];
-    }
+    for (int k = 0; k < RP; k++) wr[k] = W[(size_t)i * RP + k];
     w_update<RP>(e, num, wr);
 #pragma unroll
     for (int k = 0; k < RP; k++)

@@ -19,11 +19,25 @@ struct StreamOpsT final : StreamOps {
         return ratio ? HCfg<T, RP, true>::TCOLS : HCfg<T, RP, false>::TCOLS;
     }
     int h_brows() const override { return HCfg<T, RP, false>::BROWS; }
-    int h_boxc() const override { return HCfg<T, RP, false>::BOXC; }
+    int h_boxc(bool ratio) const override {
+        return ratio ? HCfg<T, RP, true>::BOXC : HCfg<T, RP, false>::BOXC;
+    }
+    int h_segu() const override { return HCfg<T, RP, false>::SEGU; }
     int w_trows(bool ratio) const override {
         return ratio ? WCfg<T, RP, true>::TROWS : WCfg<T, RP, false>::TROWS;
     }
-    int w_bcols() const override { return WCfg<T, RP, false>::BCOLS; }
+    int w_bcols(bool ratio) const override {
+        return ratio ? WCfg<T, RP, true>::BCOLS : WCfg<T, RP, false>::BCOLS;
+    }
+    int w_segu(bool ratio) const override {
+        return ratio ? WCfg<T, RP, true>::SEGU : WCfg<T, RP, false>::SEGU;
+    }
+    int w_rowb(bool ratio) const override {
+        return ratio ? WCfg<T, RP, true>::ROWB : WCfg<T, RP, false>::ROWB;
+    }
+    int w_boxr(bool ratio) const override {
+        return ratio ? WCfg<T, RP, true>::BOXR : WCfg<T, RP, false>::BOXR;
+    }
 
     template <bool RATIO>
     static cudaError_t launch_h(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
@@ -31,6 +45,7 @@ struct StreamOpsT final : StreamOps {
                                 int grid, cudaStream_t s) {
         using C = HCfg<T, RP, RATIO>;
         static_assert(C::BOXC * C::NBOX == C::TCOLS, "tile / box mismatch");
+        static_assert(C::BROWS == HCfg<T, RP, !RATIO>::BROWS, "one W box");
         cudaError_t e = cudaFuncSetAttribute(nmfcu::hpass<T, RP, RATIO>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
         if (e != cudaSuccess) return e;
