@@ -17,6 +17,12 @@ A step is one NMF iteration (H update + W update) over the whole V.
            the same V, extrapolated linearly in the column count.
 
 --impl reference times that CPU restatement as the reference arm.
+
+--form consensus measures the batching form instead: a consensus sweep of
+64 brunet restarts x ranks 2..10 (576 solves x 200 iterations) on a
+2000 x 5000 V, one step = one whole sweep through nmfcu_run_batch_device
+plus the nine consensus matrices, against the same solves run one by one
+through the single-solve engine.
 """
 from __future__ import annotations
 
@@ -62,6 +68,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--form", choices=["iterate", "consensus"], default="iterate")
+    ap.add_argument("--runs", type=int, default=64, help="consensus restarts per rank")
+    ap.add_argument("--seq-runs", type=int, default=None,
+                    help="consensus: restarts per rank timed one by one (default: all)")
     return ap.parse_args()
 
 
@@ -515,11 +525,216 @@ def run_ours(args, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# Batching form: consensus sweep
+# ---------------------------------------------------------------------------
+
+CONSENSUS = {"n": 2000, "p": 5000, "k": 6, "alpha": 0.3, "ranks": list(range(2, 11)),
+             "iters": 200}
+
+
+def consensus_inputs(runs, seed=7):
+    from nmf_rs import consensus, synthetic
+
+    c = CONSENSUS
+    V = synthetic.counts_matrix(c["n"], c["p"], c["k"], c["alpha"], seed)
+    starts = []
+    for r in c["ranks"]:
+        starts.extend(consensus.restart_starts(V, r, runs))
+    return V, starts
+
+
+def consensus_cpu_baseline(V, runs, seconds):
+    """The oracle's brunet iteration per rank on a column slice,
+    extrapolated to runs x 200 iterations per rank over the full V."""
+    from nmf_rs import consensus
+
+    c = CONSENSUS
+    total = 0.0
+    samples = []
+    for r in c["ranks"]:
+        def fn(p_s, r=r):
+            v = np.ascontiguousarray(V[:, :p_s])
+            W0, H0 = consensus.restart_starts(v, r, 1)[0]
+            return v, W0, H0
+        b = cpu_baseline(fn, c["n"], c["p"], r, "brunet", seconds / len(c["ranks"]))
+        total += runs * c["iters"] / b["value"]
+        samples.append(b["sample"].split(" took ")[1].split(";")[0])
+    return {"value": runs * len(c["ranks"]) / total, "unit": "solves/s",
+            "cores": os.cpu_count() or 1, "kind": "port",
+            "sample": ("1 brunet iteration of the CPU restatement (oracle/, OpenMP) per rank "
+                       "2..10 on a column slice of V (" + ", ".join(samples) + "), "
+                       f"extrapolated to {runs} restarts x {c['iters']} iterations on 2000x5000")}
+
+
+def run_consensus_reference(args, world, rank):
+    if rank != 0:
+        return
+    V, _ = consensus_inputs(1)
+    vals, base = [], None
+    for _ in range(max(1, min(args.steps or 3, 3))):
+        base = consensus_cpu_baseline(V, args.runs, args.cpu_seconds)
+        vals.append(base["value"])
+    value = statistics.median(vals)
+    c = CONSENSUS
+    print(json.dumps({
+        "impl": "reference",
+        "metric": f"consensus sweep solves/s ({args.runs} brunet restarts x ranks 2..10, "
+                  f"{c['iters']} iterations, 2000x5000)",
+        "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps or 3,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * args.runs * len(c["ranks"]) / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded single-cell-like generator)",
+        "config": {"workload": "consensus-sweep", "n": c["n"], "p": c["p"], "ranks": "2..10",
+                   "restarts": args.runs, "iters": c["iters"]},
+        "cpu_baseline": {**base, "value": value},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_consensus(args, world, rank, local):
+    import ctypes
+
+    import torch
+
+    from nmf_rs import _native, consensus
+
+    c = CONSENSUS
+    n, p, iters = c["n"], c["p"], c["iters"]
+    runs = args.runs
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    V, starts = consensus_inputs(runs)
+    ranks = np.array([w.shape[1] for w, _ in starts], dtype=np.int32)
+    offs = np.concatenate([[0], np.cumsum(ranks)[:-1]]).astype(np.int64)
+    nsolves = len(ranks)
+    rtot = int(ranks.sum())
+    W0 = np.ascontiguousarray(np.concatenate([w for w, _ in starts], axis=1))
+    H0 = np.ascontiguousarray(np.concatenate([h for _, h in starts], axis=0))
+    del starts
+    dV = torch.from_numpy(V).to(dev)
+    dW0 = torch.from_numpy(W0).to(dev)
+    dH0 = torch.from_numpy(H0).to(dev)
+    dW, dH = dW0.clone(), dH0.clone()
+    ctx = _native.Context(local)
+    lib = _native.load()
+    stream = torch.cuda.current_stream(dev)
+    prec = _native.PRECISIONS[args.precision]
+    i32p = ctypes.POINTER(ctypes.c_int32)
+    rp = ranks.ctypes.data_as(i32p)
+    cons = torch.empty((p, p), dtype=torch.float32, device=dev)
+    sels = [np.arange(ci * runs, (ci + 1) * runs, dtype=np.int32) for ci in range(len(c["ranks"]))]
+
+    def batched_sweep():
+        dW.copy_(dW0)
+        dH.copy_(dH0)
+        _native.check(lib.nmfcu_run_batch_device(
+            ctx.handle, _native.parse_method("brunet"), prec, iters, n, p,
+            ctypes.c_void_p(dV.data_ptr()), p, nsolves, rp, ctypes.c_void_p(dW.data_ptr()),
+            ctypes.c_void_p(dH.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
+        for sel in sels:
+            _native.check(lib.nmfcu_consensus_device(
+                ctx.handle, p, nsolves, rp, ctypes.c_void_p(dH.data_ptr()), runs,
+                sel.ctypes.data_as(i32p), ctypes.c_void_p(cons.data_ptr()),
+                ctypes.c_void_p(stream.cuda_stream)))
+
+    warm = max(3, args.warmup)
+    steps = args.steps or 3
+    for _ in range(warm):
+        batched_sweep()
+    torch.cuda.synchronize()
+    l0 = ctx.launch_count()
+    barrier(world)
+    with Clocks(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            batched_sweep()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    launches = ctx.launch_count() - l0
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
+    value = world * nsolves / (ms / 1000.0)
+
+    # The same solves one by one through the single-solve engine.
+    seq_runs = min(runs, args.seq_runs or runs)
+    o = _native.default_options()
+    o.method = _native.parse_method("brunet")
+    o.stop = 0
+    o.precision = prec
+    o.max_iter = iters
+    o.refine_iters = 0
+    o.device = local
+    pick = [ci * runs + i for ci in range(len(c["ranks"])) for i in range(seq_runs)]
+
+    def one(s_):
+        a, r = int(offs[s_]), int(ranks[s_])
+        w = dW0[:, a:a + r].contiguous()
+        h = dH0[a:a + r].contiguous()
+        ctx.run(o, n, p, r, dV.data_ptr(), _native.F64, p, w.data_ptr(), h.data_ptr(),
+                stream=stream.cuda_stream)
+        return h
+
+    one(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s_ in pick:
+        h = one(s_)
+    torch.cuda.synchronize()
+    t_seq = (time.perf_counter() - t0) * runs / seq_runs
+    seq_value = nsolves / t_seq
+    a, r = int(offs[pick[-1]]), int(ranks[pick[-1]])
+    dh_rel = float((h - dH[a:a + r]).abs().max() / h.abs().max())
+
+    # End to end: host V in, stacked factors and consensus matrices out.
+    t0 = time.perf_counter()
+    consensus.consensus_sweep(V, c["ranks"], runs, iters, precision=args.precision,
+                              device=local, metrics=False)
+    t_e2e = time.perf_counter() - t0
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = consensus_cpu_baseline(V, runs, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"consensus sweep solves/s ({runs} brunet restarts x ranks 2..10, "
+                      f"{iters} iterations, 2000x5000)",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded single-cell-like generator)",
+            "config": {"workload": "consensus-sweep", "n": n, "p": p, "ranks": "2..10",
+                       "restarts": runs, "iters": iters, "solves": nsolves, "sum_rank": rtot,
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "V (80 MB f64 / 40 MB f32) stays L2-resident by design"},
+            "gpu_launches": launches,
+            "clocks": clocks,
+            "one_by_one_solves_per_s": seq_value,
+            "batched_over_one_by_one": value / seq_value,
+            "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled",
+            "max_rel_dH_batched_vs_single": dh_rel,
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * nsolves / t_e2e, "unit": "solves/s",
+                    "h2d_bytes_per_step": V.nbytes + W0.nbytes + H0.nbytes,
+                    "d2h_bytes_per_step": W0.nbytes + H0.nbytes + len(c["ranks"]) * p * p * 4,
+                    "note": "consensus_sweep: host V/starts in, stacked W/H and 9 consensus "
+                            "matrices out; cophenetic/dispersion (host scipy) not timed"},
+        }), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.impl == "reference":
+        if args.form == "consensus":
+            if args.impl == "reference":
+                run_consensus_reference(args, world, rank)
+            else:
+                run_consensus(args, world, rank, local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_ours(args, world, rank, local)

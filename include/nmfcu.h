@@ -194,6 +194,44 @@ nmfcu_status nmfcu_context_reset_timing(nmfcu_context *ctx);
 int64_t nmfcu_context_launch_count(nmfcu_context *ctx);
 
 /* ---------------------------------------------------------------------- */
+/* Batched solves and consensus                                            */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * nmfcu_run_batch -- many brunet solves of one V at once: the restarts and
+ * rank sweep of the reference's consensus workflow, which calls nmf() once
+ * per (rank, run) in a Python loop (examples/build_scaling_notebook.py:
+ * 157-208, each call nmf_run_brunet lib.rs:1529-1586 with stop="max_iter").
+ * Solve s has rank ranks[s] (1..16); the factors of all solves are stacked:
+ *   W0, W  n x R f64, R = sum(ranks), solve s in columns [off_s, off_s + r_s)
+ *   H0, H  R x p f64, solve s in rows [off_s, off_s + r_s)
+ * with off_s = ranks[0] + ... + ranks[s-1].  Every solve runs exactly
+ * max_iter iterations.  method must be NMFCU_BRUNET (others:
+ * NMFCU_ERR_UNSUPPORTED).  precision FP64 gives each solve's single-solve
+ * result to rounding; FP32 computes in f32 from an f32 copy of V.
+ */
+nmfcu_status nmfcu_run_batch(int32_t method, int32_t precision, int64_t max_iter, int64_t n,
+                             int64_t p, const double *V, int32_t nsolves, const int32_t *ranks,
+                             const double *W0, const double *H0, double *W, double *H,
+                             int32_t device);
+/* The same on device pointers (V with leading dimension ldv), on `stream`;
+ * dW/dH hold the stacked starts on entry and the results on exit. */
+nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t precision,
+                                    int64_t max_iter, int64_t n, int64_t p, const double *dV,
+                                    int64_t ldv, int32_t nsolves, const int32_t *ranks,
+                                    double *dW, double *dH, void *stream);
+
+/* Consensus matrix of the selected solves `sel[0..nsel)` of a stacked H
+ * (layout as above): C[j1][j2] = fraction of the selected solves that put
+ * columns j1 and j2 in the same cluster, the cluster of column j being
+ * argmax_k H_s[k][j] (first maximum) -- connectivity_matrix and the mean over
+ * runs of examples/build_scaling_notebook.py:121-124, 179-186.  d_out is a
+ * p x p f32 device array. */
+nmfcu_status nmfcu_consensus_device(nmfcu_context *ctx, int64_t p, int32_t nsolves,
+                                    const int32_t *ranks, const double *dH, int32_t nsel,
+                                    const int32_t *sel, float *d_out, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Allocation-free objective                                               */
 /* ---------------------------------------------------------------------- */
 

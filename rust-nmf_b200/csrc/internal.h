@@ -1,0 +1,65 @@
+// internal.h -- services that nmfcu.cu offers the library's other
+// translation units (C++ linkage: the nmfcu_* export list does not see them).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../include/nmfcu.h"
+
+namespace nmfcu_internal {
+
+// Records `msg` as the calling thread's nmfcu_last_error() and returns `s`.
+nmfcu_status fail(nmfcu_status s, const std::string &msg);
+// The same for a CUDA error (maps allocation failures to NMFCU_ERR_OOM).
+nmfcu_status cuda_fail(cudaError_t e, const char *what);
+
+// The per-device context behind the host-pointer API (created on first use).
+nmfcu_status default_context(int device, nmfcu_context **out);
+
+// A scratch buffer of the context that grows to at least `bytes` (slot
+// 0..15, one owner per slot; the contents survive between calls).
+constexpr int kContextSlots = 16;
+nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out);
+
+cudaStream_t context_stream(nmfcu_context *c);
+int context_sms(nmfcu_context *c);
+int context_device(nmfcu_context *c);
+std::mutex &context_mutex(nmfcu_context *c);
+// Adds `launches` kernel launches to nmfcu_context_launch_count.
+void count_launches(nmfcu_context *c, int64_t launches);
+
+// Makes `dev` current for the scope and restores the caller's device.
+struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            prev = -1;
+            cudaGetLastError();
+        }
+        cudaSetDevice(dev);
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+    DeviceScope(const DeviceScope &) = delete;
+    DeviceScope &operator=(const DeviceScope &) = delete;
+};
+
+}  // namespace nmfcu_internal
+
+#define NMFCU_CUDA_TRY(expr)                                                  \
+    do {                                                                      \
+        cudaError_t e_ = (expr);                                              \
+        if (e_ != cudaSuccess) return nmfcu_internal::cuda_fail(e_, #expr);   \
+    } while (0)
+
+#define NMFCU_TRY(expr)                    \
+    do {                                   \
+        nmfcu_status s_ = (expr);          \
+        if (s_ != NMFCU_OK) return s_;     \
+    } while (0)

@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 
 #include "../../include/nmfcu.h"
+#include "internal.h"
 #include "kernels.cuh"
 #include "launch.h"
 #include "stream.cuh"
@@ -57,6 +58,7 @@ nmfcu_status fail(nmfcu_status s, const std::string &msg) {
     g_last_error = msg;
     return s;
 }
+nmfcu_status cuda_fail(cudaError_t e, const char *what) { return ::cuda_fail(e, what); }
 }  // namespace nmfcu_internal
 
 namespace {
@@ -328,6 +330,7 @@ struct nmfcu_context {
     // Workspace.
     DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
     DevBuf Wf32, Ht64, Ht32;
+    DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
 
     // Timing.
@@ -939,6 +942,28 @@ nmfcu_status objective_host(bool kl, int64_t n, int64_t p, int64_t r, const doub
 }
 
 }  // namespace
+
+// ===========================================================================
+// Services for the other translation units (internal.h)
+// ===========================================================================
+namespace nmfcu_internal {
+
+nmfcu_status default_context(int device, nmfcu_context **out) { return ::default_context(device, out); }
+
+nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out) {
+    if (slot < 0 || slot >= kContextSlots) return fail(NMFCU_ERR_INVALID_ARG, "bad scratch slot");
+    NMF_TRY(c->extra[slot].ensure(bytes));
+    *out = c->extra[slot].ptr;
+    return NMFCU_OK;
+}
+
+cudaStream_t context_stream(nmfcu_context *c) { return c->own_stream; }
+int context_sms(nmfcu_context *c) { return c->sms; }
+int context_device(nmfcu_context *c) { return c->device; }
+std::mutex &context_mutex(nmfcu_context *c) { return c->mu; }
+void count_launches(nmfcu_context *c, int64_t launches) { c->launch_total += launches; }
+
+}  // namespace nmfcu_internal
 
 // ===========================================================================
 // C ABI

@@ -299,4 +299,4 @@ def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.nda
     )
 
 
-from . import synthetic  # noqa: E402,F401  (workload generator, nmf_rs.synthetic)
+from . import consensus, synthetic  # noqa: E402,F401  (nmf_rs.consensus, nmf_rs.synthetic)

@@ -87,6 +87,14 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_double)]),
     "nmfcu_context_reset_timing": (_i32, [ctypes.c_void_p]),
     "nmfcu_context_launch_count": (_i64, [ctypes.c_void_p]),
+    "nmfcu_run_batch": (_i32, [_i32, _i32, _i64, _i64, _i64, _dp, _i32,
+                               ctypes.POINTER(_i32), _dp, _dp, _dp, _dp, _i32]),
+    "nmfcu_run_batch_device": (_i32, [ctypes.c_void_p, _i32, _i32, _i64, _i64, _i64,
+                                      ctypes.c_void_p, _i64, _i32, ctypes.POINTER(_i32),
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "nmfcu_consensus_device": (_i32, [ctypes.c_void_p, _i64, _i32, ctypes.POINTER(_i32),
+                                      ctypes.c_void_p, _i32, ctypes.POINTER(_i32),
+                                      ctypes.c_void_p, ctypes.c_void_p]),
     "nmfcu_objective_noalloc": (_i32, [_i32, _i64, _i64, _i64, ctypes.c_void_p, _i64,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),

@@ -178,3 +178,46 @@ def test_synthetic_generator():
     assert (V >= 0).all() and np.isfinite(V).all()
     assert 0.05 < float((V == 0).mean()) < 0.95
     np.testing.assert_array_equal(V, synthetic.counts_matrix(300, 400, 6, 0.3, seed=3))
+
+
+# ---------------------------------------------------------------------------
+# Batched solves and consensus: argument checks and the metrics (no GPU).
+# ---------------------------------------------------------------------------
+
+def test_batch_rejects_unsupported_before_touching_a_device():
+    from nmf_rs import consensus
+
+    V = np.ones((4, 5))
+    starts = [(np.ones((4, 2)), np.ones((2, 5)))]
+    with pytest.raises(NotImplementedError):
+        consensus.run_batch(V, starts, 3, method="lee")
+    with pytest.raises(NotImplementedError):
+        consensus.run_batch(V, [(np.ones((4, 17)), np.ones((17, 5)))], 3)
+    with pytest.raises(ValueError):
+        consensus.run_batch(V, starts, -1)
+
+
+def test_restart_starts_follow_the_reference_draw_order():
+    from nmf_rs import consensus
+
+    V = np.arange(1.0, 13.0).reshape(3, 4)
+    (W0, H0), (W1, _) = consensus.restart_starts(V, 2, 2)
+    gen = np.random.default_rng(2024)
+    s = float(np.sqrt(V.mean() / 2))
+    np.testing.assert_array_equal(W0, gen.uniform(0, s, (3, 2)))
+    np.testing.assert_array_equal(H0, gen.uniform(0, s, (2, 4)))
+    np.testing.assert_array_equal(W1, np.random.default_rng(2025).uniform(0, s, (3, 2)))
+
+
+def test_consensus_metrics():
+    from nmf_rs import consensus
+
+    H = np.array([[1.0, 0.9, 0.1, 0.0], [0.0, 0.1, 0.8, 1.0]])
+    C = consensus.connectivity_matrix(H)
+    np.testing.assert_array_equal(C, [[1, 1, 0, 0], [1, 1, 0, 0], [0, 0, 1, 1], [0, 0, 1, 1]])
+    assert consensus.dispersion_coefficient(C) == 1.0
+    assert consensus.cophenetic_correlation(C) == pytest.approx(1.0)
+    assert consensus.dispersion_coefficient(np.full((4, 4), 0.5)) == 0.0
+    H2 = np.array([[1.0, 0.0, 0.1, 0.0], [0.0, 0.1, 0.8, 1.0]])
+    mixed = 0.5 * (C + consensus.connectivity_matrix(H2))
+    assert 0.0 < consensus.dispersion_coefficient(mixed) < 1.0
