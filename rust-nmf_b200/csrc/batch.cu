@@ -20,6 +20,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <string>
 #include <vector>
@@ -32,141 +33,345 @@ using nmfcu_internal::fail;
 namespace {
 
 constexpr int kMaxBatchRank = 16;  // largest rank of a batched solve
+constexpr int kThreads = 128;      // threads per CTA
 constexpr int kRowChunk = 64;      // W rows staged per chunk (H step)
+constexpr int kPrefetch = 4;       // V rows in flight per thread (H step)
+constexpr int kColChunk = 16;      // V columns staged per chunk (W step)
 
-__device__ __forceinline__ double bdiv(double x, double y) { return x / y; }
-__device__ __forceinline__ float bdiv(float x, float y) { return __fdividef(x, y); }
-
-// Solves of rank R per CTA: enough that each V load serves ~32 (f32) or
-// ~16 (f64) rank components.
-template <typename T, int R>
-struct BCfg {
-    static constexpr int kComponents = sizeof(T) == 4 ? 32 : 16;
-    static constexpr int NS = kComponents / R > 0 ? kComponents / R : 1;
+// Per element type: a thread owns CPT adjacent columns (H step) or rows
+// (W step) of V, held in one "lane pack" P.  f32 packs two (float2, one
+// FFMA2 updates both), so a W value times an H pair, or an H value times a
+// W pair, is one instruction and the per-element ratio is computed for two
+// elements at once; f64 owns one (DFMA).  kComponents bounds the rank
+// components (sum of the ranks of the solves) a CTA carries.
+template <typename T>
+struct BTraits;
+template <>
+struct BTraits<float> {
+    using P = float2;
+    static constexpr int CPT = 2;
+    static constexpr int kComponents = 16;
+};
+template <>
+struct BTraits<double> {
+    using P = double;
+    static constexpr int CPT = 1;
+    static constexpr int kComponents = 16;
 };
 
-// H update of a group of NS rank-R solves for 256 columns.
-//   off[g * NS + i]: first stacked index of the group's i-th solve (or -1).
 template <typename T, int R>
-__global__ void __launch_bounds__(256)
-    batch_hstep(const T *__restrict__ V, int64_t ldv, int n, int p, const T *__restrict__ W,
-                int ldw, T *__restrict__ H, const T *__restrict__ sumW,
-                const int *__restrict__ off) {
-    constexpr int NS = BCfg<T, R>::NS;
-    __shared__ T sW[kRowChunk][NS * R];
-    const int j = blockIdx.x * 256 + threadIdx.x;
-    const bool colok = j < p;
-    const int *goff = off + blockIdx.y * NS;
-    int o[NS];
+struct BCfg {
+    static constexpr int NS = BTraits<T>::kComponents / R > 0 ? BTraits<T>::kComponents / R : 1;
+    static constexpr int ROW = NS * R;  // staged values per W row / H column
+};
+constexpr int kMaxRow = 16;             // >= ROW for every (T, R)
+template <typename T>
+constexpr int kTile = kThreads * BTraits<T>::CPT;  // columns / rows per CTA
+
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ double pfma(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float2 pdup(float x) { return make_float2(x, x); }
+__device__ __forceinline__ double pdup(double x) { return x; }
+__device__ __forceinline__ void pzero(float2 &x) { x = make_float2(0.f, 0.f); }
+__device__ __forceinline__ void pzero(double &x) { x = 0.0; }
+__device__ __forceinline__ float &plane(float2 &a, int c) { return c ? a.y : a.x; }
+__device__ __forceinline__ double &plane(double &a, int) { return a; }
+
+// The brunet ratio V / (WH), 0 where WH == 0 (lib.rs:93-99).  f32 uses the
+// hardware reciprocal approximation (rcp.approx.ftz.f32, about 1 ulp).
+__device__ __forceinline__ float ratio1(float v, float wh) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(wh));
+    return (wh != 0.f) ? v * r : 0.f;
+}
+__device__ __forceinline__ float2 ratio(float2 v, float2 wh) {
+    return make_float2(ratio1(v.x, wh.x), ratio1(v.y, wh.y));
+}
+// f64: v * (1 / wh) with the reciprocal from the hardware approximation
+// (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
+// y <- y + y (1 - wh y), each of which doubles the number of correct bits;
+// the quotient is then within about an ulp of the IEEE one.  |wh| outside
+// [2^-1000, 2^1000] (and NaN) takes the exact division.
+__device__ __forceinline__ double ratio(double v, double wh) {
+    if (wh == 0.0) return 0.0;
+    const double a = fabs(wh);
+    if (!(a > 0x1p-1000 && a < 0x1p1000)) return v / wh;
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(wh));
+    double e = fma(-wh, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-wh, y, 1.0);
+    y = fma(y, e, y);
+    return v * y;
+}
+
+// Shared memory of one CTA (the larger of the two steps' layouts).  W
+// values (H step) and H values (W step) are stored duplicated across the
+// lane pack, so one load feeds both lanes.
+template <typename T>
+struct BSmem {
+    using P = typename BTraits<T>::P;
+    union {
+        P hW[kRowChunk][kMaxRow];                 // H step: W rows of the group
+        struct {
+            T Vt[kColChunk][kTile<T> + 2];        // W step: V tile, transposed
+            P Hc[kColChunk][kMaxRow];             // W step: H columns of the group
+        } w;
+    };
+    int off[BTraits<T>::kComponents];             // stacked offset per solve (-1: none)
+};
+
+// One unit of a step: NS solves of rank R (offsets at goff[0..NS)) on one
+// tile of kTile columns (H step) or rows (W step).
+struct BItem {
+    int R;
+    int goff;  // index of the first offset in the group-offset table
+    int tile;
+    int pad;
+};
+
+// H update of one item (divergence_update_h_inner, lib.rs:74-115, per solve):
+//   H[k][j] <- H[k][j] * (sum_i W[i][k] V[i][j] / (WH)[i][j]) / sum_i W[i][k]
+// A thread owns CPT adjacent columns; W rows are staged in shared memory
+// (zero beyond n), V rows stream from L2 a few rows ahead.  V's leading
+// dimension must make a CPT-column load aligned, and V must be zero in
+// columns [p, round_up(p, CPT)).
+template <typename T, int R>
+__device__ __forceinline__ void hstep_item(BSmem<T> &sm, const T *__restrict__ V, int64_t ldv,
+                                           int n, int p, const T *__restrict__ W, int ldw,
+                                           T *__restrict__ H, const T *__restrict__ sumW,
+                                           const int *__restrict__ goff, int tile) {
+    using C = BCfg<T, R>;
+    using P = typename BTraits<T>::P;
+    constexpr int CPT = BTraits<T>::CPT;
+    constexpr int NS = C::NS, ROW = C::ROW;
+    constexpr int WPT = (kRowChunk * ROW + kThreads - 1) / kThreads;  // staged W values per thread
+    static_assert(ROW <= kMaxRow && NS <= BTraits<T>::kComponents, "staging row too long");
+    static_assert(kRowChunk % kPrefetch == 0, "row chunk must hold whole prefetch groups");
+    if (threadIdx.x < NS) sm.off[threadIdx.x] = goff[threadIdx.x];
+    __syncthreads();
+    const int j0 = tile * kTile<T> + threadIdx.x * CPT;
+    const bool colok = j0 < p;
+    P h[NS][R], acc[NS][R];
 #pragma unroll
-    for (int s = 0; s < NS; s++) o[s] = goff[s];
-    T hcol[NS][R], acc[NS][R];
-#pragma unroll
-    for (int s = 0; s < NS; s++)
+    for (int s = 0; s < NS; s++) {
+        const int o = sm.off[s];
 #pragma unroll
         for (int k = 0; k < R; k++) {
-            hcol[s][k] = (colok && o[s] >= 0) ? H[(size_t)(o[s] + k) * p + j] : (T)0;
-            acc[s][k] = (T)0;
+#pragma unroll
+            for (int c = 0; c < CPT; c++)
+                plane(h[s][k], c) = (o >= 0 && j0 + c < p) ? H[(size_t)(o + k) * p + j0 + c] : (T)0;
+            pzero(acc[s][k]);
         }
+    }
+    // W values of the next row chunk, loaded while the current one is used.
+    T wpre[WPT];
+    auto load_w = [&](int base) {
+        const int rows = min(kRowChunk, n - base);
+#pragma unroll
+        for (int t = 0; t < WPT; t++) {
+            const int e = t * kThreads + threadIdx.x;
+            const int rr = e / ROW, c = e - rr * ROW;
+            const int s = c / R, k = c - s * R;
+            const int o = (e < kRowChunk * ROW) ? sm.off[s] : -1;
+            wpre[t] = (rr < rows && o >= 0) ? W[(size_t)(base + rr) * ldw + o + k] : (T)0;
+        }
+    };
+    load_w(0);
     for (int base = 0; base < n; base += kRowChunk) {
         const int rows = min(kRowChunk, n - base);
         __syncthreads();
-        for (int e = threadIdx.x; e < kRowChunk * NS * R; e += 256) {
-            const int rr = e / (NS * R), c = e - rr * (NS * R);
-            const int s = c / R, k = c - s * R;
-            sW[rr][c] = (rr < rows && o[s] >= 0) ? W[(size_t)(base + rr) * ldw + o[s] + k] : (T)0;
+#pragma unroll
+        for (int t = 0; t < WPT; t++) {
+            const int e = t * kThreads + threadIdx.x;
+            if (e < kRowChunk * ROW) sm.hW[e / ROW][e % ROW] = pdup(wpre[t]);
         }
         __syncthreads();
-        for (int rr = 0; rr < rows; rr += 4) {
-            T v[4];
+        if (base + kRowChunk < n) load_w(base + kRowChunk);
+        const P *vp = reinterpret_cast<const P *>(V + (size_t)base * ldv + j0);
+        const int64_t ldp = ldv / CPT;
+        P vb[kPrefetch];
 #pragma unroll
-            for (int q = 0; q < 4; q++)
-                v[q] = (colok && rr + q < rows) ? V[(size_t)(base + rr + q) * ldv + j] : (T)0;
+        for (int q = 0; q < kPrefetch; q++) {
+            if (colok && q < rows) vb[q] = vp[q * ldp];
+            else pzero(vb[q]);
+        }
+        for (int r0 = 0; r0 < rows; r0 += kPrefetch) {
+            P vn[kPrefetch];
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
-                if (rr + q >= rows) break;
-                const T *wr = sW[rr + q];
+            for (int q = 0; q < kPrefetch; q++) {
+                const int rr = r0 + kPrefetch + q;
+                if (colok && rr < rows) vn[q] = vp[rr * ldp];
+                else pzero(vn[q]);
+            }
+            // Rows past the chunk's end read zero W rows and v = 0: no-ops.
+#pragma unroll
+            for (int q = 0; q < kPrefetch; q++) {
+                const P *wr = sm.hW[r0 + q];
 #pragma unroll
                 for (int s = 0; s < NS; s++) {
-                    T wh = (T)0;
+                    P d;
+                    pzero(d);
 #pragma unroll
-                    for (int k = 0; k < R; k++) wh = fma(wr[s * R + k], hcol[s][k], wh);
-                    const T qv = (wh != (T)0) ? bdiv(v[q], wh) : (T)0;
+                    for (int k = 0; k < R; k++) d = pfma(wr[s * R + k], h[s][k], d);
+                    const P qq = ratio(vb[q], d);
 #pragma unroll
-                    for (int k = 0; k < R; k++) acc[s][k] = fma(wr[s * R + k], qv, acc[s][k]);
+                    for (int k = 0; k < R; k++) acc[s][k] = pfma(wr[s * R + k], qq, acc[s][k]);
                 }
             }
+#pragma unroll
+            for (int q = 0; q < kPrefetch; q++) vb[q] = vn[q];
         }
     }
-    if (!colok) return;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        if (o[s] < 0) continue;
+        const int o = sm.off[s];
+        if (o < 0) continue;
 #pragma unroll
-        for (int k = 0; k < R; k++)  // h * tmp / sum_w (lib.rs:110)
-            H[(size_t)(o[s] + k) * p + j] = (hcol[s][k] * acc[s][k]) / sumW[o[s] + k];
+        for (int k = 0; k < R; k++)
+#pragma unroll
+            for (int c = 0; c < CPT; c++)
+                if (j0 + c < p)  // h * tmp / sum_w (lib.rs:110)
+                    H[(size_t)(o + k) * p + j0 + c] =
+                        (plane(h[s][k], c) * plane(acc[s][k], c)) / sumW[o + k];
     }
 }
 
-// W update of a group of NS rank-R solves for 256 rows.
+// W update of one item (divergence_update_w_impl, lib.rs:151-204, per solve):
+//   W[i][k] <- W[i][k] * (sum_j H[k][j] V[i][j] / (WH)[i][j]) / sum_j H[k][j]
+// A thread owns CPT adjacent rows; V tiles are staged transposed (one
+// aligned load gives a thread its rows of one column) and H columns are
+// staged, both loaded a chunk ahead into registers.
 template <typename T, int R>
-__global__ void __launch_bounds__(256)
-    batch_wstep(const T *__restrict__ V, int64_t ldv, int n, int p, T *__restrict__ W, int ldw,
-                const T *__restrict__ H, const T *__restrict__ sumH, const int *__restrict__ off) {
-    constexpr int NS = BCfg<T, R>::NS;
-    constexpr int kColChunk = 128 / (int)sizeof(T);  // V columns staged per chunk
-    __shared__ T sV[256][kColChunk + 1];
-    __shared__ T sH[kColChunk][NS * R];
-    const int row0 = blockIdx.x * 256;
-    const int i = row0 + threadIdx.x;
-    const bool rowok = i < n;
-    const int *goff = off + blockIdx.y * NS;
-    int o[NS];
+__device__ __forceinline__ void wstep_item(BSmem<T> &sm, const T *__restrict__ V, int64_t ldv,
+                                           int n, int p, T *__restrict__ W, int ldw,
+                                           const T *__restrict__ H, const T *__restrict__ sumH,
+                                           const int *__restrict__ goff, int tile) {
+    using C = BCfg<T, R>;
+    using P = typename BTraits<T>::P;
+    constexpr int CPT = BTraits<T>::CPT;
+    constexpr int NS = C::NS, ROW = C::ROW;
+    constexpr int CC = kColChunk;
+    constexpr int TILE = kTile<T>;
+    constexpr int VPT = TILE * CC / kThreads;                    // staged V values per thread
+    constexpr int HPT = (CC * ROW + kThreads - 1) / kThreads;    // staged H values per thread
+    static_assert(ROW <= kMaxRow && NS <= BTraits<T>::kComponents, "staging row too long");
+    static_assert(kThreads % CC == 0, "V staging maps a thread to one column");
+    if (threadIdx.x < NS) sm.off[threadIdx.x] = goff[threadIdx.x];
+    __syncthreads();
+    const int row0 = tile * TILE;
+    const int i0 = row0 + threadIdx.x * CPT;
+    P w[NS][R], acc[NS][R];
 #pragma unroll
-    for (int s = 0; s < NS; s++) o[s] = goff[s];
-    T wrow[NS][R], acc[NS][R];
-#pragma unroll
-    for (int s = 0; s < NS; s++)
+    for (int s = 0; s < NS; s++) {
+        const int o = sm.off[s];
 #pragma unroll
         for (int k = 0; k < R; k++) {
-            wrow[s][k] = (rowok && o[s] >= 0) ? W[(size_t)i * ldw + o[s] + k] : (T)0;
-            acc[s][k] = (T)0;
+#pragma unroll
+            for (int c = 0; c < CPT; c++)
+                plane(w[s][k], c) = (o >= 0 && i0 + c < n) ? W[(size_t)(i0 + c) * ldw + o + k] : (T)0;
+            pzero(acc[s][k]);
         }
-    for (int c0 = 0; c0 < p; c0 += kColChunk) {
-        const int cols = min(kColChunk, p - c0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < 256 * kColChunk; e += 256) {
-            const int rr = e / kColChunk, cc = e - rr * kColChunk;
-            const int gi = row0 + rr;
-            sV[rr][cc] = (gi < n && cc < cols) ? V[(size_t)gi * ldv + c0 + cc] : (T)0;
+    }
+    // Thread t stages column t % CC of rows t / CC + v * (kThreads / CC).
+    const int vcol = threadIdx.x % CC, vrow = threadIdx.x / CC;
+    T vpre[VPT], hpre[HPT];
+    auto load_chunk = [&](int c0) {
+        const int cols = min(CC, p - c0);
+#pragma unroll
+        for (int v = 0; v < VPT; v++) {
+            const int gi = row0 + vrow + v * (kThreads / CC);
+            vpre[v] = (gi < n && vcol < cols) ? V[(size_t)gi * ldv + c0 + vcol] : (T)0;
         }
-        for (int e = threadIdx.x; e < kColChunk * NS * R; e += 256) {
-            const int c = e / kColChunk, cc = e - c * kColChunk;
+#pragma unroll
+        for (int t = 0; t < HPT; t++) {
+            const int e = t * kThreads + threadIdx.x;
+            const int c = e / CC, cc = e - c * CC;
             const int s = c / R, k = c - s * R;
-            sH[cc][c] = (cc < cols && o[s] >= 0) ? H[(size_t)(o[s] + k) * p + c0 + cc] : (T)0;
+            const int o = (e < CC * ROW) ? sm.off[s] : -1;
+            hpre[t] = (cc < cols && o >= 0) ? H[(size_t)(o + k) * p + c0 + cc] : (T)0;
+        }
+    };
+    load_chunk(0);
+    for (int c0 = 0; c0 < p; c0 += CC) {
+        __syncthreads();
+#pragma unroll
+        for (int v = 0; v < VPT; v++) sm.w.Vt[vcol][vrow + v * (kThreads / CC)] = vpre[v];
+#pragma unroll
+        for (int t = 0; t < HPT; t++) {
+            const int e = t * kThreads + threadIdx.x;
+            if (e < CC * ROW) sm.w.Hc[e % CC][e / CC] = pdup(hpre[t]);
         }
         __syncthreads();
-        for (int cc = 0; cc < cols; cc++) {
-            const T v = sV[threadIdx.x][cc];
-            const T *hc = sH[cc];
+        if (c0 + CC < p) load_chunk(c0 + CC);
+        // Columns past p hold V = 0 and H = 0: no-ops.
+#pragma unroll 2
+        for (int cc = 0; cc < CC; cc++) {
+            const P v = *reinterpret_cast<const P *>(&sm.w.Vt[cc][threadIdx.x * CPT]);
+            const P *hc = sm.w.Hc[cc];
 #pragma unroll
             for (int s = 0; s < NS; s++) {
-                T wh = (T)0;
+                P d;
+                pzero(d);
 #pragma unroll
-                for (int k = 0; k < R; k++) wh = fma(wrow[s][k], hc[s * R + k], wh);
-                const T qv = (wh != (T)0) ? bdiv(v, wh) : (T)0;
+                for (int k = 0; k < R; k++) d = pfma(w[s][k], hc[s * R + k], d);
+                const P qq = ratio(v, d);
 #pragma unroll
-                for (int k = 0; k < R; k++) acc[s][k] = fma(hc[s * R + k], qv, acc[s][k]);
+                for (int k = 0; k < R; k++) acc[s][k] = pfma(hc[s * R + k], qq, acc[s][k]);
             }
         }
     }
-    if (!rowok) return;
 #pragma unroll
     for (int s = 0; s < NS; s++) {
-        if (o[s] < 0) continue;
+        const int o = sm.off[s];
+        if (o < 0) continue;
 #pragma unroll
-        for (int k = 0; k < R; k++)  // w * tmp / sum_h (lib.rs:199)
-            W[(size_t)i * ldw + o[s] + k] = (wrow[s][k] * acc[s][k]) / sumH[o[s] + k];
+        for (int k = 0; k < R; k++)
+#pragma unroll
+            for (int c = 0; c < CPT; c++)
+                if (i0 + c < n)  // w * tmp / sum_h (lib.rs:199)
+                    W[(size_t)(i0 + c) * ldw + o + k] =
+                        (plane(w[s][k], c) * plane(acc[s][k], c)) / sumH[o + k];
+    }
+}
+
+#define BATCH_RANK_CASES(X) \
+    X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
+
+// One launch per step for every rank class: CTA b runs item b.  The
+// register caps (measured best among 2..4 resident CTAs per SM) keep the
+// H step at 3 (f32) / 2 (f64) and the W step at 3 CTAs per SM.
+template <typename T>
+constexpr int kMinBlocksH = sizeof(T) == 4 ? 3 : 2;
+template <typename T>
+constexpr int kMinBlocksW = sizeof(T) == 4 ? 3 : 3;
+
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kMinBlocksH<T>)
+    batch_hstep(const T *__restrict__ V, int64_t ldv, int n, int p, const T *__restrict__ W, int ldw,
+                T *__restrict__ H, const T *__restrict__ sumW, const int *__restrict__ off,
+                const BItem *__restrict__ items) {
+    __shared__ __align__(16) BSmem<T> sm;
+    const BItem it = items[blockIdx.x];
+    switch (it.R) {
+#define H_CASE(r) \
+    case r: hstep_item<T, r>(sm, V, ldv, n, p, W, ldw, H, sumW, off + it.goff, it.tile); break;
+        BATCH_RANK_CASES(H_CASE)
+#undef H_CASE
+    }
+}
+template <typename T>
+__global__ void __launch_bounds__(kThreads, kMinBlocksW<T>)
+    batch_wstep(const T *__restrict__ V, int64_t ldv, int n, int p, T *__restrict__ W, int ldw,
+                const T *__restrict__ H, const T *__restrict__ sumH, const int *__restrict__ off,
+                const BItem *__restrict__ items) {
+    __shared__ __align__(16) BSmem<T> sm;
+    const BItem it = items[blockIdx.x];
+    switch (it.R) {
+#define W_CASE(r) \
+    case r: wstep_item<T, r>(sm, V, ldv, n, p, W, ldw, H, sumH, off + it.goff, it.tile); break;
+        BATCH_RANK_CASES(W_CASE)
+#undef W_CASE
     }
 }
 
@@ -257,90 +462,72 @@ __global__ void batch_consensus(const unsigned char *__restrict__ lab, int p, in
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-struct RankClass {
-    int R;
-    int groups;     // CTAs along the solve dimension
-    int off_index;  // first entry of this class in the group-offset table
-};
-
 template <typename T>
 int ns_for(int R) {
     switch (R) {
 #define NS_CASE(r) case r: return BCfg<T, r>::NS;
-        NS_CASE(1) NS_CASE(2) NS_CASE(3) NS_CASE(4) NS_CASE(5) NS_CASE(6) NS_CASE(7) NS_CASE(8)
-        NS_CASE(9) NS_CASE(10) NS_CASE(11) NS_CASE(12) NS_CASE(13) NS_CASE(14) NS_CASE(15) NS_CASE(16)
+        BATCH_RANK_CASES(NS_CASE)
 #undef NS_CASE
     }
     return 1;
 }
 
-template <typename T>
-void launch_class(bool hside, const RankClass &rc, const T *V, int64_t ldv, int n, int p, T *W,
-                  int ldw, T *H, const T *sums, const int *off, cudaStream_t s) {
-    const dim3 grid(hside ? (p + 255) / 256 : (n + 255) / 256, rc.groups);
-    const int *o = off + rc.off_index;
-    switch (rc.R) {
-#define CLS_CASE(r)                                                                        \
-    case r:                                                                                \
-        if (hside)                                                                         \
-            batch_hstep<T, r><<<grid, 256, 0, s>>>(V, ldv, n, p, W, ldw, H, sums, o);      \
-        else                                                                               \
-            batch_wstep<T, r><<<grid, 256, 0, s>>>(V, ldv, n, p, W, ldw, H, sums, o);      \
-        break;
-        CLS_CASE(1) CLS_CASE(2) CLS_CASE(3) CLS_CASE(4) CLS_CASE(5) CLS_CASE(6) CLS_CASE(7)
-        CLS_CASE(8) CLS_CASE(9) CLS_CASE(10) CLS_CASE(11) CLS_CASE(12) CLS_CASE(13) CLS_CASE(14)
-        CLS_CASE(15) CLS_CASE(16)
-#undef CLS_CASE
-    }
-}
-
 struct BatchPlan {
     int rtot = 0;
-    std::vector<int> offsets;      // per solve, stacked index
-    std::vector<RankClass> classes;
-    std::vector<int> group_off;    // per class, groups * NS entries (-1 padded)
+    std::vector<int> group_off;  // per group, NS offsets (-1 padded)
+    std::vector<BItem> hitems, witems;
 };
 
+// Solves of one rank form a class; a class is cut into groups of NS solves;
+// every (group, tile) pair is one CTA of the step's launch.
 template <typename T>
-BatchPlan plan_batch(int nsolves, const int32_t *ranks) {
+BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
     BatchPlan bp;
-    bp.offsets.resize(nsolves);
+    std::vector<int> offsets(nsolves);
     std::map<int, std::vector<int>> by_rank;
     for (int s = 0; s < nsolves; s++) {
-        bp.offsets[s] = bp.rtot;
+        offsets[s] = bp.rtot;
         bp.rtot += ranks[s];
         by_rank[ranks[s]].push_back(s);
     }
-    for (auto &kv : by_rank) {
-        RankClass rc;
-        rc.R = kv.first;
-        const int ns = ns_for<T>(rc.R);
-        rc.groups = (int)((kv.second.size() + ns - 1) / ns);
-        rc.off_index = (int)bp.group_off.size();
-        for (int g = 0; g < rc.groups; g++)
+    const int htiles = (p + kTile<T> - 1) / kTile<T>, wtiles = (n + kTile<T> - 1) / kTile<T>;
+    // Larger ranks first: their CTAs are the longest, so they start first.
+    for (auto it = by_rank.rbegin(); it != by_rank.rend(); ++it) {
+        const int R = it->first;
+        const auto &members = it->second;
+        const int ns = ns_for<T>(R);
+        const int groups = (int)((members.size() + ns - 1) / ns);
+        for (int g = 0; g < groups; g++) {
+            const int at = (int)bp.group_off.size();
             for (int i = 0; i < ns; i++) {
                 const size_t idx = (size_t)g * ns + i;
-                bp.group_off.push_back(idx < kv.second.size() ? bp.offsets[kv.second[idx]] : -1);
+                bp.group_off.push_back(idx < members.size() ? offsets[members[idx]] : -1);
             }
-        bp.classes.push_back(rc);
+            for (int t = 0; t < htiles; t++) bp.hitems.push_back({R, at, t, 0});
+            for (int t = 0; t < wtiles; t++) bp.witems.push_back({R, at, t, 0});
+        }
     }
     return bp;
 }
 
+struct BatchDev {
+    const int *off;
+    const BItem *hitems, *witems;
+    int nh, nw;
+};
+
 // Enqueue iterations [it0, it1] of the batched brunet loop.
 template <typename T>
-void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, const T *V,
-                         int64_t ldv, int n, int p, T *W, T *H, T *sw, T *sh, const int *doff,
+void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, const BatchDev &d,
+                         const T *V, int64_t ldv, int n, int p, T *W, T *H, T *sw, T *sh,
                          cudaStream_t s, int64_t *launches) {
     const int rtot = bp.rtot;
     for (long long it = it0; it <= it1; it++) {
         batch_colsum<T><<<(rtot + 127) / 128, 128, 0, s>>>(W, n, rtot, rtot, sw);
-        for (const auto &rc : bp.classes)
-            launch_class<T>(true, rc, V, ldv, n, p, W, rtot, H, sw, doff, s);
+        batch_hstep<T><<<d.nh, kThreads, 0, s>>>(V, ldv, n, p, W, rtot, H, sw, d.off, d.hitems);
         batch_rowsum<T><<<(rtot + 7) / 8, 256, 0, s>>>(H, p, rtot, sh);
-        for (const auto &rc : bp.classes)
-            launch_class<T>(false, rc, V, ldv, n, p, W, rtot, H, sh, doff, s);
-        *launches += 2 + 2 * (int64_t)bp.classes.size();
+        batch_wstep<T><<<d.nw, kThreads, 0, s>>>(V, ldv, n, p, W, rtot, H, sh, d.off, d.witems);
+        *launches += 4;
         if (it % 10 == 0) {
             batch_clamp<T><<<592, 256, 0, s>>>(W, (int64_t)n * rtot, H, (int64_t)rtot * p,
                                                (T)DBL_EPSILON);
@@ -353,18 +540,29 @@ template <typename T>
 nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const T *V,
                          int64_t ldv, int nsolves, const int32_t *ranks, T *W, T *H,
                          cudaStream_t s) {
-    const BatchPlan bp = plan_batch<T>(nsolves, ranks);
-    void *p_off = nullptr, *p_sw = nullptr, *p_sh = nullptr;
-    NMFCU_TRY(nmfcu_internal::context_buffer(
-        c, 0, sizeof(int) * std::max<size_t>(bp.group_off.size(), 1), &p_off));
+    const BatchPlan bp = plan_batch<T>(n, p, nsolves, ranks);
+    // One upload: group offsets, then H items, then W items (16-byte aligned).
+    const size_t off_bytes = (sizeof(int) * bp.group_off.size() + 15) / 16 * 16;
+    const size_t item_bytes = sizeof(BItem) * (bp.hitems.size() + bp.witems.size());
+    std::vector<unsigned char> table(off_bytes + item_bytes, 0);
+    std::memcpy(table.data(), bp.group_off.data(), sizeof(int) * bp.group_off.size());
+    std::memcpy(table.data() + off_bytes, bp.hitems.data(), sizeof(BItem) * bp.hitems.size());
+    std::memcpy(table.data() + off_bytes + sizeof(BItem) * bp.hitems.size(), bp.witems.data(),
+                sizeof(BItem) * bp.witems.size());
+    void *p_tab = nullptr, *p_sw = nullptr, *p_sh = nullptr;
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 0, table.size(), &p_tab));
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 1, sizeof(T) * (size_t)bp.rtot, &p_sw));
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 2, sizeof(T) * (size_t)bp.rtot, &p_sh));
-    int *doff = static_cast<int *>(p_off);
     T *sw = static_cast<T *>(p_sw), *sh = static_cast<T *>(p_sh);
-    NMFCU_CUDA_TRY(cudaMemcpyAsync(doff, bp.group_off.data(), sizeof(int) * bp.group_off.size(),
-                                   cudaMemcpyHostToDevice, s));
-    // The pageable copy above is staged before cudaMemcpyAsync returns, so
-    // the plan may go out of scope; the kernels below read doff in order.
+    // A pageable host source is staged before cudaMemcpyAsync returns, so the
+    // table may go out of scope; the kernels below read it in stream order.
+    NMFCU_CUDA_TRY(cudaMemcpyAsync(p_tab, table.data(), table.size(), cudaMemcpyHostToDevice, s));
+    BatchDev d;
+    d.off = static_cast<const int *>(p_tab);
+    d.hitems = reinterpret_cast<const BItem *>(static_cast<unsigned char *>(p_tab) + off_bytes);
+    d.witems = d.hitems + bp.hitems.size();
+    d.nh = (int)bp.hitems.size();
+    d.nw = (int)bp.witems.size();
     int64_t launches = 0;
     // The loop in blocks of 10 iterations (the clamp period), captured once
     // as a CUDA graph and replayed; the remainder is launched directly.
@@ -381,7 +579,7 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             int64_t cap_launches = 0;
-            enqueue_batch_iters<T>(1, 10, bp, V, ldv, n, p, W, H, sw, sh, doff, cs, &cap_launches);
+            enqueue_batch_iters<T>(1, 10, bp, d, V, ldv, n, p, W, H, sw, sh, cs, &cap_launches);
             e = cudaStreamEndCapture(cs, &graph);
             if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
             for (long long b = 0; e == cudaSuccess && b < blocks; b++) {
@@ -398,7 +596,7 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (ready) cudaEventDestroy(ready);
         if (e != cudaSuccess) return nmfcu_internal::cuda_fail(e, "batched iteration graph");
     }
-    enqueue_batch_iters<T>(blocks * 10 + 1, max_iter, bp, V, ldv, n, p, W, H, sw, sh, doff, s,
+    enqueue_batch_iters<T>(blocks * 10 + 1, max_iter, bp, d, V, ldv, n, p, W, H, sw, sh, s,
                            &launches);
     NMFCU_CUDA_TRY(cudaGetLastError());
     nmfcu_internal::count_launches(c, launches);
@@ -448,13 +646,17 @@ nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t 
     } else {
         // f32 copies of V and of the stacked factors (context slots 3..5).
         void *v32 = nullptr, *w32 = nullptr, *h32 = nullptr;
-        NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 3, sizeof(float) * (size_t)n * p, &v32));
+        // The f32 V's leading dimension is a multiple of 4 with the pad
+        // columns zero (the H step loads column pairs, aligned).
+        const int64_t ld32 = (p + 3) / 4 * 4;
+        NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 3, sizeof(float) * (size_t)n * ld32, &v32));
         NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 4, sizeof(float) * (size_t)n * rtot, &w32));
         NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 5, sizeof(float) * (size_t)rtot * p, &h32));
-        convert_2d<double, float><<<1184, 256, 0, s>>>(dV, ldv, (float *)v32, p, ni, pi);
+        if (ld32 > p) NMFCU_CUDA_TRY(cudaMemsetAsync(v32, 0, sizeof(float) * (size_t)n * ld32, s));
+        convert_2d<double, float><<<1184, 256, 0, s>>>(dV, ldv, (float *)v32, ld32, ni, pi);
         convert<double, float><<<1184, 256, 0, s>>>(dW, (float *)w32, n * rtot);
         convert<double, float><<<1184, 256, 0, s>>>(dH, (float *)h32, rtot * p);
-        NMFCU_TRY(run_batch_t<float>(ctx, max_iter, ni, pi, (const float *)v32, p, nsolves, ranks,
+        NMFCU_TRY(run_batch_t<float>(ctx, max_iter, ni, pi, (const float *)v32, ld32, nsolves, ranks,
                                      (float *)w32, (float *)h32, s));
         convert<float, double><<<1184, 256, 0, s>>>((const float *)w32, dW, n * rtot);
         convert<float, double><<<1184, 256, 0, s>>>((const float *)h32, dH, rtot * p);

@@ -254,6 +254,11 @@ struct DevBuf {
         bytes = want;
         return NMFCU_OK;
     }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
     template <typename T>
     T *as() const { return static_cast<T *>(ptr); }
 };
@@ -631,34 +636,48 @@ nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it,
     return NMFCU_OK;
 }
 
-nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32) {
+// Every workspace buffer one run of this plan needs, with its size: the
+// single list behind both the allocation (ensure_workspace) and the
+// serving layer's memory accounting (nmfcu_internal::context_growth).
+struct WsNeed {
+    DevBuf *buf;
+    size_t bytes;
+};
+
+std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_f32) {
+    std::vector<WsNeed> v;
     const size_t RP = pl.RP;
-    NMF_TRY(c->W.ensure(sizeof(double) * (size_t)pl.n * RP));
-    NMF_TRY(c->H.ensure(sizeof(double) * RP * (size_t)pl.p));
+    v.push_back({&c->W, sizeof(double) * (size_t)pl.n * RP});
+    v.push_back({&c->H, sizeof(double) * RP * (size_t)pl.p});
     const bool ratio = true;  // sized for the larger of the two tilings
     size_t part = 0;
     for (bool rt : {ratio, !ratio}) {
         part = std::max(part, pass_partial_bytes(stream_ops_f64(pl.RP), pl, rt, c->sms));
         if (need_f32) part = std::max(part, pass_partial_bytes(stream_ops_f32(pl.RP), pl, rt, c->sms));
     }
-    NMF_TRY(c->part.ensure(part));
-    NMF_TRY(c->Ht64.ensure(sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()));
+    v.push_back({&c->part, part});
+    v.push_back({&c->Ht64, sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()});
     if (need_f32) {
         const size_t rps = stream_ops_f32(pl.RP)->rps();
-        NMF_TRY(c->Ht32.ensure(sizeof(float) * (size_t)pl.p * rps));
-        NMF_TRY(c->Wf32.ensure(sizeof(float) * (size_t)pl.n * rps));
+        v.push_back({&c->Ht32, sizeof(float) * (size_t)pl.p * rps});
+        v.push_back({&c->Wf32, sizeof(float) * (size_t)pl.n * rps});
     }
     const size_t B = (size_t)std::max(pl.Bw, pl.Bh);
-    NMF_TRY(c->pg.ensure(sizeof(double) * B * RP * RP));
-    NMF_TRY(c->ps.ensure(sizeof(double) * B * RP));
-    NMF_TRY(c->Gw.ensure(sizeof(double) * RP * RP));
-    NMF_TRY(c->Gh.ensure(sizeof(double) * RP * RP));
-    NMF_TRY(c->Gw2.ensure(sizeof(double) * RP * RP));
-    NMF_TRY(c->sw.ensure(sizeof(double) * RP));
-    NMF_TRY(c->sh.ensure(sizeof(double) * RP));
-    NMF_TRY(c->sw2.ensure(sizeof(double) * RP));
-    NMF_TRY(c->obj.ensure(sizeof(double) * (size_t)std::max(pl.obj_blocks, 1)));
-    NMF_TRY(c->state.ensure(sizeof(RunState)));
+    v.push_back({&c->pg, sizeof(double) * B * RP * RP});
+    v.push_back({&c->ps, sizeof(double) * B * RP});
+    v.push_back({&c->Gw, sizeof(double) * RP * RP});
+    v.push_back({&c->Gh, sizeof(double) * RP * RP});
+    v.push_back({&c->Gw2, sizeof(double) * RP * RP});
+    v.push_back({&c->sw, sizeof(double) * RP});
+    v.push_back({&c->sh, sizeof(double) * RP});
+    v.push_back({&c->sw2, sizeof(double) * RP});
+    v.push_back({&c->obj, sizeof(double) * (size_t)std::max(pl.obj_blocks, 1)});
+    v.push_back({&c->state, sizeof(RunState)});
+    return v;
+}
+
+nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32) {
+    for (const WsNeed &w : workspace_needs(c, pl, need_f32)) NMF_TRY(w.buf->ensure(w.bytes));
     if (!c->h_state) CUDA_TRY(cudaMallocHost((void **)&c->h_state, sizeof(RunState)));
     return NMFCU_OK;
 }
@@ -962,6 +981,44 @@ int context_sms(nmfcu_context *c) { return c->sms; }
 int context_device(nmfcu_context *c) { return c->device; }
 std::mutex &context_mutex(nmfcu_context *c) { return c->mu; }
 void count_launches(nmfcu_context *c, int64_t launches) { c->launch_total += launches; }
+
+size_t context_bytes(nmfcu_context *c) {
+    size_t t = 0;
+    for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
+                            &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
+                            &c->Wf32, &c->Ht64, &c->Ht32})
+        t += b->bytes;
+    for (const DevBuf &b : c->extra) t += b.bytes;
+    return t;
+}
+
+// A DevBuf grows to max(want, 256) bytes (DevBuf::ensure).
+static size_t grow_by(const DevBuf &b, size_t want) {
+    want = std::max<size_t>(want, 256);
+    return want > b.bytes ? want - b.bytes : 0;
+}
+
+size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32) {
+    const Plan pl = make_plan(n, p, r, c->sms);
+    size_t g = 0;
+    for (const WsNeed &w : workspace_needs(c, pl, f32)) g += grow_by(*w.buf, w.bytes);
+    if (f32) g += grow_by(c->V32, sizeof(float) * (size_t)n * std::max<int64_t>(32, round_up(p, 32)));
+    return g;
+}
+
+size_t slot_growth(nmfcu_context *c, int slot, size_t bytes) {
+    if (slot < 0 || slot >= kContextSlots) return 0;
+    return grow_by(c->extra[slot], bytes);
+}
+
+void context_release(nmfcu_context *c) {
+    DeviceGuard dg(c->device);
+    for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
+                      &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
+                      &c->Ht64, &c->Ht32})
+        b->release();
+    for (DevBuf &b : c->extra) b.release();
+}
 
 }  // namespace nmfcu_internal
 
