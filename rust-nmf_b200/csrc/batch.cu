@@ -105,24 +105,39 @@ __device__ __forceinline__ double ratio(double v, double wh) {
     return v * y;
 }
 
-// Shared memory of one CTA (the larger of the two steps' layouts).  W
-// values (H step) and H values (W step) are stored duplicated across the
-// lane pack, so one load feeds both lanes.
+// One multiplicative update, written once for both steps.  The step
+// streams a matrix A (rows x cols) whose columns are the outputs: A = V for
+// the H step (columns = cells), A = V^T for the W step (columns = genes).
+// For each output column j and solve s it forms
+//   acc[k] = sum_r S[r][k] * A[r][j] / (sum_k' S[r][k'] X[k'][j])
+// and writes X[k][j] <- X[k][j] * acc[k] / norm[k], where S is the staged
+// factor (W for the H step, H^T for the W step) and X the updated one.
+// This is divergence_update_h_inner (lib.rs:74-115) for the H step and
+// divergence_update_w_impl (lib.rs:151-204) for the W step, per solve.
+template <typename T>
+struct MuArgs {
+    const T *A;          // rows x cols, leading dimension lda
+    int64_t lda;
+    int rows, cols;
+    const T *S;          // staged factor: S(r, c) = S[r * s_row + c * s_col]
+    int64_t s_row, s_col;
+    T *X;                // updated factor: X(c, j) = X[c * x_comp + j * x_col]
+    int64_t x_comp, x_col;
+    const T *norm;       // per stacked component
+};
+
+// Shared memory of one CTA: the staged factor's rows, duplicated across the
+// lane pack (one load feeds both lanes); rows padded so that the transposing
+// stores of the W step spread over the banks and rows stay 16-B aligned.
 template <typename T>
 struct BSmem {
     using P = typename BTraits<T>::P;
-    union {
-        P hW[kRowChunk][kMaxRow];                 // H step: W rows of the group
-        struct {
-            T Vt[kColChunk][kTile<T> + 2];        // W step: V tile, transposed
-            P Hc[kColChunk][kMaxRow];             // W step: H columns of the group
-        } w;
-    };
-    int off[BTraits<T>::kComponents];             // stacked offset per solve (-1: none)
+    P S[kRowChunk][kMaxRow + 2];
+    int off[BTraits<T>::kComponents];  // stacked offset per solve (-1: none)
 };
 
 // One unit of a step: NS solves of rank R (offsets at goff[0..NS)) on one
-// tile of kTile columns (H step) or rows (W step).
+// tile of kTile output columns.
 struct BItem {
     int R;
     int goff;  // index of the first offset in the group-offset table
@@ -130,29 +145,28 @@ struct BItem {
     int pad;
 };
 
-// H update of one item (divergence_update_h_inner, lib.rs:74-115, per solve):
-//   H[k][j] <- H[k][j] * (sum_i W[i][k] V[i][j] / (WH)[i][j]) / sum_i W[i][k]
-// A thread owns CPT adjacent columns; W rows are staged in shared memory
-// (zero beyond n), V rows stream from L2 a few rows ahead.  V's leading
-// dimension must make a CPT-column load aligned, and V must be zero in
-// columns [p, round_up(p, CPT)).
-template <typename T, int R>
-__device__ __forceinline__ void hstep_item(BSmem<T> &sm, const T *__restrict__ V, int64_t ldv,
-                                           int n, int p, const T *__restrict__ W, int ldw,
-                                           T *__restrict__ H, const T *__restrict__ sumW,
-                                           const int *__restrict__ goff, int tile) {
+// A thread owns CPT adjacent output columns; the staged factor's rows are
+// staged in shared memory a chunk ahead (zero beyond `rows`), A streams from
+// L2 a few rows ahead.  A's leading dimension must make a CPT-column load
+// aligned, and A must be zero in columns [cols, round_up(cols, CPT)).
+// kComponentFast: the staged factor is contiguous along components (W in
+// the H step) -- staging loads walk components; otherwise (H^T) they walk rows.
+template <typename T, int R, bool kComponentFast>
+__device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
+                                        const int *__restrict__ goff, int tile) {
     using C = BCfg<T, R>;
     using P = typename BTraits<T>::P;
     constexpr int CPT = BTraits<T>::CPT;
     constexpr int NS = C::NS, ROW = C::ROW;
-    constexpr int WPT = (kRowChunk * ROW + kThreads - 1) / kThreads;  // staged W values per thread
+    constexpr int SPT = (kRowChunk * ROW + kThreads - 1) / kThreads;  // staged values per thread
     static_assert(ROW <= kMaxRow && NS <= BTraits<T>::kComponents, "staging row too long");
     static_assert(kRowChunk % kPrefetch == 0, "row chunk must hold whole prefetch groups");
     if (threadIdx.x < NS) sm.off[threadIdx.x] = goff[threadIdx.x];
     __syncthreads();
+    const int rows = a.rows, cols = a.cols;
     const int j0 = tile * kTile<T> + threadIdx.x * CPT;
-    const bool colok = j0 < p;
-    P h[NS][R], acc[NS][R];
+    const bool colok = j0 < cols;
+    P x[NS][R], acc[NS][R];
 #pragma unroll
     for (int s = 0; s < NS; s++) {
         const int o = sm.off[s];
@@ -160,63 +174,79 @@ __device__ __forceinline__ void hstep_item(BSmem<T> &sm, const T *__restrict__ V
         for (int k = 0; k < R; k++) {
 #pragma unroll
             for (int c = 0; c < CPT; c++)
-                plane(h[s][k], c) = (o >= 0 && j0 + c < p) ? H[(size_t)(o + k) * p + j0 + c] : (T)0;
+                plane(x[s][k], c) = (o >= 0 && j0 + c < cols)
+                                        ? a.X[(size_t)(o + k) * a.x_comp + (size_t)(j0 + c) * a.x_col]
+                                        : (T)0;
             pzero(acc[s][k]);
         }
     }
-    // W values of the next row chunk, loaded while the current one is used.
-    T wpre[WPT];
-    auto load_w = [&](int base) {
-        const int rows = min(kRowChunk, n - base);
-#pragma unroll
-        for (int t = 0; t < WPT; t++) {
-            const int e = t * kThreads + threadIdx.x;
-            const int rr = e / ROW, c = e - rr * ROW;
-            const int s = c / R, k = c - s * R;
-            const int o = (e < kRowChunk * ROW) ? sm.off[s] : -1;
-            wpre[t] = (rr < rows && o >= 0) ? W[(size_t)(base + rr) * ldw + o + k] : (T)0;
+    // Staged values of the next row chunk, loaded while the current one is used.
+    T spre[SPT];
+    auto stage_index = [&](int e, int &rr, int &c) {
+        if (kComponentFast) {
+            rr = e / ROW;
+            c = e - rr * ROW;
+        } else {
+            c = e / kRowChunk;
+            rr = e - c * kRowChunk;
         }
     };
-    load_w(0);
-    for (int base = 0; base < n; base += kRowChunk) {
-        const int rows = min(kRowChunk, n - base);
+    auto load_s = [&](int base) {
+        const int nr = min(kRowChunk, rows - base);
+#pragma unroll
+        for (int t = 0; t < SPT; t++) {
+            const int e = t * kThreads + threadIdx.x;
+            int rr, c;
+            stage_index(e, rr, c);
+            const int s = c / R, k = c - s * R;
+            const int o = (e < kRowChunk * ROW) ? sm.off[s] : -1;
+            spre[t] = (rr < nr && o >= 0)
+                          ? a.S[(size_t)(base + rr) * a.s_row + (size_t)(o + k) * a.s_col]
+                          : (T)0;
+        }
+    };
+    load_s(0);
+    const int64_t ldp = a.lda / CPT;
+    for (int base = 0; base < rows; base += kRowChunk) {
+        const int nr = min(kRowChunk, rows - base);
         __syncthreads();
 #pragma unroll
-        for (int t = 0; t < WPT; t++) {
+        for (int t = 0; t < SPT; t++) {
             const int e = t * kThreads + threadIdx.x;
-            if (e < kRowChunk * ROW) sm.hW[e / ROW][e % ROW] = pdup(wpre[t]);
+            int rr, c;
+            stage_index(e, rr, c);
+            if (e < kRowChunk * ROW) sm.S[rr][c] = pdup(spre[t]);
         }
         __syncthreads();
-        if (base + kRowChunk < n) load_w(base + kRowChunk);
-        const P *vp = reinterpret_cast<const P *>(V + (size_t)base * ldv + j0);
-        const int64_t ldp = ldv / CPT;
+        if (base + kRowChunk < rows) load_s(base + kRowChunk);
+        const P *ap = reinterpret_cast<const P *>(a.A + (size_t)base * a.lda + j0);
         P vb[kPrefetch];
 #pragma unroll
         for (int q = 0; q < kPrefetch; q++) {
-            if (colok && q < rows) vb[q] = vp[q * ldp];
+            if (colok && q < nr) vb[q] = ap[q * ldp];
             else pzero(vb[q]);
         }
-        for (int r0 = 0; r0 < rows; r0 += kPrefetch) {
+        for (int r0 = 0; r0 < nr; r0 += kPrefetch) {
             P vn[kPrefetch];
 #pragma unroll
             for (int q = 0; q < kPrefetch; q++) {
                 const int rr = r0 + kPrefetch + q;
-                if (colok && rr < rows) vn[q] = vp[rr * ldp];
+                if (colok && rr < nr) vn[q] = ap[rr * ldp];
                 else pzero(vn[q]);
             }
-            // Rows past the chunk's end read zero W rows and v = 0: no-ops.
+            // Rows past the chunk's end read zero staged rows and a = 0: no-ops.
 #pragma unroll
             for (int q = 0; q < kPrefetch; q++) {
-                const P *wr = sm.hW[r0 + q];
+                const P *sr = sm.S[r0 + q];
 #pragma unroll
                 for (int s = 0; s < NS; s++) {
                     P d;
                     pzero(d);
 #pragma unroll
-                    for (int k = 0; k < R; k++) d = pfma(wr[s * R + k], h[s][k], d);
+                    for (int k = 0; k < R; k++) d = pfma(sr[s * R + k], x[s][k], d);
                     const P qq = ratio(vb[q], d);
 #pragma unroll
-                    for (int k = 0; k < R; k++) acc[s][k] = pfma(wr[s * R + k], qq, acc[s][k]);
+                    for (int k = 0; k < R; k++) acc[s][k] = pfma(sr[s * R + k], qq, acc[s][k]);
                 }
             }
 #pragma unroll
@@ -231,147 +261,41 @@ __device__ __forceinline__ void hstep_item(BSmem<T> &sm, const T *__restrict__ V
         for (int k = 0; k < R; k++)
 #pragma unroll
             for (int c = 0; c < CPT; c++)
-                if (j0 + c < p)  // h * tmp / sum_w (lib.rs:110)
-                    H[(size_t)(o + k) * p + j0 + c] =
-                        (plane(h[s][k], c) * plane(acc[s][k], c)) / sumW[o + k];
-    }
-}
-
-// W update of one item (divergence_update_w_impl, lib.rs:151-204, per solve):
-//   W[i][k] <- W[i][k] * (sum_j H[k][j] V[i][j] / (WH)[i][j]) / sum_j H[k][j]
-// A thread owns CPT adjacent rows; V tiles are staged transposed (one
-// aligned load gives a thread its rows of one column) and H columns are
-// staged, both loaded a chunk ahead into registers.
-template <typename T, int R>
-__device__ __forceinline__ void wstep_item(BSmem<T> &sm, const T *__restrict__ V, int64_t ldv,
-                                           int n, int p, T *__restrict__ W, int ldw,
-                                           const T *__restrict__ H, const T *__restrict__ sumH,
-                                           const int *__restrict__ goff, int tile) {
-    using C = BCfg<T, R>;
-    using P = typename BTraits<T>::P;
-    constexpr int CPT = BTraits<T>::CPT;
-    constexpr int NS = C::NS, ROW = C::ROW;
-    constexpr int CC = kColChunk;
-    constexpr int TILE = kTile<T>;
-    constexpr int VPT = TILE * CC / kThreads;                    // staged V values per thread
-    constexpr int HPT = (CC * ROW + kThreads - 1) / kThreads;    // staged H values per thread
-    static_assert(ROW <= kMaxRow && NS <= BTraits<T>::kComponents, "staging row too long");
-    static_assert(kThreads % CC == 0, "V staging maps a thread to one column");
-    if (threadIdx.x < NS) sm.off[threadIdx.x] = goff[threadIdx.x];
-    __syncthreads();
-    const int row0 = tile * TILE;
-    const int i0 = row0 + threadIdx.x * CPT;
-    P w[NS][R], acc[NS][R];
-#pragma unroll
-    for (int s = 0; s < NS; s++) {
-        const int o = sm.off[s];
-#pragma unroll
-        for (int k = 0; k < R; k++) {
-#pragma unroll
-            for (int c = 0; c < CPT; c++)
-                plane(w[s][k], c) = (o >= 0 && i0 + c < n) ? W[(size_t)(i0 + c) * ldw + o + k] : (T)0;
-            pzero(acc[s][k]);
-        }
-    }
-    // Thread t stages column t % CC of rows t / CC + v * (kThreads / CC).
-    const int vcol = threadIdx.x % CC, vrow = threadIdx.x / CC;
-    T vpre[VPT], hpre[HPT];
-    auto load_chunk = [&](int c0) {
-        const int cols = min(CC, p - c0);
-#pragma unroll
-        for (int v = 0; v < VPT; v++) {
-            const int gi = row0 + vrow + v * (kThreads / CC);
-            vpre[v] = (gi < n && vcol < cols) ? V[(size_t)gi * ldv + c0 + vcol] : (T)0;
-        }
-#pragma unroll
-        for (int t = 0; t < HPT; t++) {
-            const int e = t * kThreads + threadIdx.x;
-            const int c = e / CC, cc = e - c * CC;
-            const int s = c / R, k = c - s * R;
-            const int o = (e < CC * ROW) ? sm.off[s] : -1;
-            hpre[t] = (cc < cols && o >= 0) ? H[(size_t)(o + k) * p + c0 + cc] : (T)0;
-        }
-    };
-    load_chunk(0);
-    for (int c0 = 0; c0 < p; c0 += CC) {
-        __syncthreads();
-#pragma unroll
-        for (int v = 0; v < VPT; v++) sm.w.Vt[vcol][vrow + v * (kThreads / CC)] = vpre[v];
-#pragma unroll
-        for (int t = 0; t < HPT; t++) {
-            const int e = t * kThreads + threadIdx.x;
-            if (e < CC * ROW) sm.w.Hc[e % CC][e / CC] = pdup(hpre[t]);
-        }
-        __syncthreads();
-        if (c0 + CC < p) load_chunk(c0 + CC);
-        // Columns past p hold V = 0 and H = 0: no-ops.
-#pragma unroll 2
-        for (int cc = 0; cc < CC; cc++) {
-            const P v = *reinterpret_cast<const P *>(&sm.w.Vt[cc][threadIdx.x * CPT]);
-            const P *hc = sm.w.Hc[cc];
-#pragma unroll
-            for (int s = 0; s < NS; s++) {
-                P d;
-                pzero(d);
-#pragma unroll
-                for (int k = 0; k < R; k++) d = pfma(w[s][k], hc[s * R + k], d);
-                const P qq = ratio(v, d);
-#pragma unroll
-                for (int k = 0; k < R; k++) acc[s][k] = pfma(hc[s * R + k], qq, acc[s][k]);
-            }
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < NS; s++) {
-        const int o = sm.off[s];
-        if (o < 0) continue;
-#pragma unroll
-        for (int k = 0; k < R; k++)
-#pragma unroll
-            for (int c = 0; c < CPT; c++)
-                if (i0 + c < n)  // w * tmp / sum_h (lib.rs:199)
-                    W[(size_t)(i0 + c) * ldw + o + k] =
-                        (plane(w[s][k], c) * plane(acc[s][k], c)) / sumH[o + k];
+                if (j0 + c < cols)  // x * tmp / sum (lib.rs:110, :199)
+                    a.X[(size_t)(o + k) * a.x_comp + (size_t)(j0 + c) * a.x_col] =
+                        (plane(x[s][k], c) * plane(acc[s][k], c)) / a.norm[o + k];
     }
 }
 
 #define BATCH_RANK_CASES(X) \
     X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
-// One launch per step for every rank class: CTA b runs item b.  The
-// register caps (measured best among 2..4 resident CTAs per SM) keep the
-// H step at 3 (f32) / 2 (f64) and the W step at 3 CTAs per SM.
-template <typename T>
-constexpr int kMinBlocksH = sizeof(T) == 4 ? 3 : 2;
-template <typename T>
-constexpr int kMinBlocksW = sizeof(T) == 4 ? 3 : 3;
+// Rank buckets: ranks 1..8 and 9..16 run as separate kernels, so the
+// register budget of one bucket is not set by the other's largest rank.
+// Within a bucket one launch covers every rank class: CTA b runs item b.
+// The register cap keeps three (f32) or two (f64) CTAs resident per SM.
+constexpr int kBucketSplit = 8;  // largest rank of the low bucket
+template <typename T, int B>
+struct BBucket {
+    static constexpr int kLo = B == 0 ? 1 : kBucketSplit + 1;
+    static constexpr int kHi = B == 0 ? kBucketSplit : kMaxBatchRank;
+    static constexpr int kMinBlocks = sizeof(T) == 4 ? 3 : 2;
+};
+constexpr int bucket_of(int R) { return R <= kBucketSplit ? 0 : 1; }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads, kMinBlocksH<T>)
-    batch_hstep(const T *__restrict__ V, int64_t ldv, int n, int p, const T *__restrict__ W, int ldw,
-                T *__restrict__ H, const T *__restrict__ sumW, const int *__restrict__ off,
-                const BItem *__restrict__ items) {
+template <typename T, int B, bool kComponentFast>
+__global__ void __launch_bounds__(kThreads, (BBucket<T, B>::kMinBlocks))
+    batch_mu(MuArgs<T> a, const int *__restrict__ off, const BItem *__restrict__ items) {
     __shared__ __align__(16) BSmem<T> sm;
     const BItem it = items[blockIdx.x];
     switch (it.R) {
-#define H_CASE(r) \
-    case r: hstep_item<T, r>(sm, V, ldv, n, p, W, ldw, H, sumW, off + it.goff, it.tile); break;
-        BATCH_RANK_CASES(H_CASE)
-#undef H_CASE
-    }
-}
-template <typename T>
-__global__ void __launch_bounds__(kThreads, kMinBlocksW<T>)
-    batch_wstep(const T *__restrict__ V, int64_t ldv, int n, int p, T *__restrict__ W, int ldw,
-                const T *__restrict__ H, const T *__restrict__ sumH, const int *__restrict__ off,
-                const BItem *__restrict__ items) {
-    __shared__ __align__(16) BSmem<T> sm;
-    const BItem it = items[blockIdx.x];
-    switch (it.R) {
-#define W_CASE(r) \
-    case r: wstep_item<T, r>(sm, V, ldv, n, p, W, ldw, H, sumH, off + it.goff, it.tile); break;
-        BATCH_RANK_CASES(W_CASE)
-#undef W_CASE
+#define MU_CASE(r)                                                                     \
+    case r:                                                                            \
+        if constexpr (r >= BBucket<T, B>::kLo && r <= BBucket<T, B>::kHi)              \
+            mu_item<T, r, kComponentFast>(sm, a, off + it.goff, it.tile);              \
+        break;
+        BATCH_RANK_CASES(MU_CASE)
+#undef MU_CASE
     }
 }
 
@@ -421,6 +345,25 @@ __global__ void convert_2d(const A *__restrict__ src, int64_t lds, B *__restrict
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
         const int64_t i = t / cols, j = t - i * cols;
         dst[i * ldd + j] = (B)src[i * lds + j];
+    }
+}
+
+// dst (cols x ldd) = src (rows x cols, leading dimension lds) transposed,
+// through 32 x 32 shared-memory tiles; dst columns [rows, ldd) are zeroed.
+template <typename A, typename B>
+__global__ void transpose_2d(const A *__restrict__ src, int64_t lds, B *__restrict__ dst,
+                             int64_t ldd, int rows, int cols) {
+    __shared__ B tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+    for (int y = ty; y < 32; y += 8) {
+        const int r = r0 + y, c = c0 + tx;
+        tile[y][tx] = (r < rows && c < cols) ? (B)src[(size_t)r * lds + c] : (B)0;
+    }
+    __syncthreads();
+    for (int y = ty; y < 32; y += 8) {
+        const int c = c0 + y, r = r0 + tx;
+        if (c < cols && r < ldd) dst[(size_t)c * ldd + r] = tile[tx][y];
     }
 }
 
@@ -474,12 +417,13 @@ int ns_for(int R) {
 
 struct BatchPlan {
     int rtot = 0;
-    std::vector<int> group_off;  // per group, NS offsets (-1 padded)
-    std::vector<BItem> hitems, witems;
+    std::vector<int> group_off;           // per group, NS offsets (-1 padded)
+    std::vector<BItem> hitems, witems;    // bucket 0 items, then bucket 1 items
+    int nh[2] = {0, 0}, nw[2] = {0, 0};   // items per bucket
 };
 
 // Solves of one rank form a class; a class is cut into groups of NS solves;
-// every (group, tile) pair is one CTA of the step's launch.
+// every (group, tile) pair is one CTA of its bucket's launch.
 template <typename T>
 BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
     BatchPlan bp;
@@ -491,20 +435,25 @@ BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
         by_rank[ranks[s]].push_back(s);
     }
     const int htiles = (p + kTile<T> - 1) / kTile<T>, wtiles = (n + kTile<T> - 1) / kTile<T>;
-    // Larger ranks first: their CTAs are the longest, so they start first.
-    for (auto it = by_rank.rbegin(); it != by_rank.rend(); ++it) {
-        const int R = it->first;
-        const auto &members = it->second;
-        const int ns = ns_for<T>(R);
-        const int groups = (int)((members.size() + ns - 1) / ns);
-        for (int g = 0; g < groups; g++) {
-            const int at = (int)bp.group_off.size();
-            for (int i = 0; i < ns; i++) {
-                const size_t idx = (size_t)g * ns + i;
-                bp.group_off.push_back(idx < members.size() ? offsets[members[idx]] : -1);
+    for (int b = 0; b < 2; b++) {
+        // Larger ranks first: their CTAs are the longest, so they start first.
+        for (auto it = by_rank.rbegin(); it != by_rank.rend(); ++it) {
+            const int R = it->first;
+            if (bucket_of(R) != b) continue;
+            const auto &members = it->second;
+            const int ns = ns_for<T>(R);
+            const int groups = (int)((members.size() + ns - 1) / ns);
+            for (int g = 0; g < groups; g++) {
+                const int at = (int)bp.group_off.size();
+                for (int i = 0; i < ns; i++) {
+                    const size_t idx = (size_t)g * ns + i;
+                    bp.group_off.push_back(idx < members.size() ? offsets[members[idx]] : -1);
+                }
+                for (int t = 0; t < htiles; t++) bp.hitems.push_back({R, at, t, 0});
+                for (int t = 0; t < wtiles; t++) bp.witems.push_back({R, at, t, 0});
+                bp.nh[b] += htiles;
+                bp.nw[b] += wtiles;
             }
-            for (int t = 0; t < htiles; t++) bp.hitems.push_back({R, at, t, 0});
-            for (int t = 0; t < wtiles; t++) bp.witems.push_back({R, at, t, 0});
         }
     }
     return bp;
@@ -513,21 +462,27 @@ BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
 struct BatchDev {
     const int *off;
     const BItem *hitems, *witems;
-    int nh, nw;
+};
+
+template <typename T>
+struct BatchSteps {
+    MuArgs<T> h, w;  // the H step streams V, the W step streams V^T
 };
 
 // Enqueue iterations [it0, it1] of the batched brunet loop.
 template <typename T>
 void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, const BatchDev &d,
-                         const T *V, int64_t ldv, int n, int p, T *W, T *H, T *sw, T *sh,
+                         const BatchSteps<T> &st, int n, int p, T *W, T *H, T *sw, T *sh,
                          cudaStream_t s, int64_t *launches) {
     const int rtot = bp.rtot;
     for (long long it = it0; it <= it1; it++) {
         batch_colsum<T><<<(rtot + 127) / 128, 128, 0, s>>>(W, n, rtot, rtot, sw);
-        batch_hstep<T><<<d.nh, kThreads, 0, s>>>(V, ldv, n, p, W, rtot, H, sw, d.off, d.hitems);
+        if (bp.nh[0]) batch_mu<T, 0, true><<<bp.nh[0], kThreads, 0, s>>>(st.h, d.off, d.hitems);
+        if (bp.nh[1]) batch_mu<T, 1, true><<<bp.nh[1], kThreads, 0, s>>>(st.h, d.off, d.hitems + bp.nh[0]);
         batch_rowsum<T><<<(rtot + 7) / 8, 256, 0, s>>>(H, p, rtot, sh);
-        batch_wstep<T><<<d.nw, kThreads, 0, s>>>(V, ldv, n, p, W, rtot, H, sh, d.off, d.witems);
-        *launches += 4;
+        if (bp.nw[0]) batch_mu<T, 0, false><<<bp.nw[0], kThreads, 0, s>>>(st.w, d.off, d.witems);
+        if (bp.nw[1]) batch_mu<T, 1, false><<<bp.nw[1], kThreads, 0, s>>>(st.w, d.off, d.witems + bp.nw[0]);
+        *launches += 2 + (bp.nh[0] > 0) + (bp.nh[1] > 0) + (bp.nw[0] > 0) + (bp.nw[1] > 0);
         if (it % 10 == 0) {
             batch_clamp<T><<<592, 256, 0, s>>>(W, (int64_t)n * rtot, H, (int64_t)rtot * p,
                                                (T)DBL_EPSILON);
@@ -536,6 +491,9 @@ void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, cons
     }
 }
 
+// V (n x p, leading dimension ldv; for f32 zero in columns [p, ldv) with
+// ldv a multiple of 4) is streamed by the H step; the W step streams V^T,
+// built here once per call in context slot 12 (zero-padded the same way).
 template <typename T>
 nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const T *V,
                          int64_t ldv, int nsolves, const int32_t *ranks, T *W, T *H,
@@ -549,21 +507,28 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
     std::memcpy(table.data() + off_bytes, bp.hitems.data(), sizeof(BItem) * bp.hitems.size());
     std::memcpy(table.data() + off_bytes + sizeof(BItem) * bp.hitems.size(), bp.witems.data(),
                 sizeof(BItem) * bp.witems.size());
-    void *p_tab = nullptr, *p_sw = nullptr, *p_sh = nullptr;
+    void *p_tab = nullptr, *p_sw = nullptr, *p_sh = nullptr, *p_vt = nullptr;
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 0, table.size(), &p_tab));
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 1, sizeof(T) * (size_t)bp.rtot, &p_sw));
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 2, sizeof(T) * (size_t)bp.rtot, &p_sh));
-    T *sw = static_cast<T *>(p_sw), *sh = static_cast<T *>(p_sh);
+    const int64_t ldvt = sizeof(T) == 4 ? ((int64_t)n + 3) / 4 * 4 : (int64_t)n;
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 12, sizeof(T) * (size_t)p * ldvt, &p_vt));
+    T *sw = static_cast<T *>(p_sw), *sh = static_cast<T *>(p_sh), *Vt = static_cast<T *>(p_vt);
     // A pageable host source is staged before cudaMemcpyAsync returns, so the
     // table may go out of scope; the kernels below read it in stream order.
     NMFCU_CUDA_TRY(cudaMemcpyAsync(p_tab, table.data(), table.size(), cudaMemcpyHostToDevice, s));
+    {
+        const dim3 tg((unsigned)((p + 31) / 32), (unsigned)((ldvt + 31) / 32));
+        transpose_2d<T, T><<<tg, 256, 0, s>>>(V, ldv, Vt, ldvt, n, p);
+    }
     BatchDev d;
     d.off = static_cast<const int *>(p_tab);
     d.hitems = reinterpret_cast<const BItem *>(static_cast<unsigned char *>(p_tab) + off_bytes);
     d.witems = d.hitems + bp.hitems.size();
-    d.nh = (int)bp.hitems.size();
-    d.nw = (int)bp.witems.size();
-    int64_t launches = 0;
+    BatchSteps<T> st;
+    st.h = MuArgs<T>{V, ldv, n, p, W, (int64_t)bp.rtot, 1, H, (int64_t)p, 1, sw};
+    st.w = MuArgs<T>{Vt, ldvt, p, n, H, 1, (int64_t)p, W, 1, (int64_t)bp.rtot, sh};
+    int64_t launches = 1;
     // The loop in blocks of 10 iterations (the clamp period), captured once
     // as a CUDA graph and replayed; the remainder is launched directly.
     const long long blocks = max_iter / 10;
@@ -579,7 +544,7 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             int64_t cap_launches = 0;
-            enqueue_batch_iters<T>(1, 10, bp, d, V, ldv, n, p, W, H, sw, sh, cs, &cap_launches);
+            enqueue_batch_iters<T>(1, 10, bp, d, st, n, p, W, H, sw, sh, cs, &cap_launches);
             e = cudaStreamEndCapture(cs, &graph);
             if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
             for (long long b = 0; e == cudaSuccess && b < blocks; b++) {
@@ -596,8 +561,7 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (ready) cudaEventDestroy(ready);
         if (e != cudaSuccess) return nmfcu_internal::cuda_fail(e, "batched iteration graph");
     }
-    enqueue_batch_iters<T>(blocks * 10 + 1, max_iter, bp, d, V, ldv, n, p, W, H, sw, sh, s,
-                           &launches);
+    enqueue_batch_iters<T>(blocks * 10 + 1, max_iter, bp, d, st, n, p, W, H, sw, sh, s, &launches);
     NMFCU_CUDA_TRY(cudaGetLastError());
     nmfcu_internal::count_launches(c, launches);
     return NMFCU_OK;
