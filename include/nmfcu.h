@@ -39,7 +39,8 @@ typedef enum nmfcu_status {
     NMFCU_ERR_CUDA = 4,        /* CUDA runtime error; RuntimeError                   */
     NMFCU_ERR_NUMERIC = 5,     /* non-finite value where the contract forbids one   */
     NMFCU_ERR_TIMEOUT = 6,     /* a bounded device wait gave up; RuntimeError        */
-    NMFCU_ERR_NO_DEVICE = 7    /* no CUDA device visible; RuntimeError               */
+    NMFCU_ERR_NO_DEVICE = 7,   /* no CUDA device visible; RuntimeError               */
+    NMFCU_ERR_CANCELLED = 8    /* a served request was cancelled before it started  */
 } nmfcu_status;
 
 /* Algorithm ids: the variants of `Algo` (lib.rs:1472-1484), same order. */
@@ -230,6 +231,57 @@ nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t 
 nmfcu_status nmfcu_consensus_device(nmfcu_context *ctx, int64_t p, int32_t nsolves,
                                     const int32_t *ranks, const double *dH, int32_t nsel,
                                     const int32_t *sel, float *d_out, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Serving: continuous batching of independent factorisations              */
+/* ---------------------------------------------------------------------- */
+
+/*
+ * No counterpart in the reference, whose nmf() runs each factorisation to
+ * completion on the calling thread (python/nmf_rs/__init__.py:396-568).  A
+ * server runs requests of any shape, rank and method concurrently on one
+ * GPU: `slots` workers, each with its own engine context and stream, take
+ * queued requests as slots and device memory free up; a request is admitted
+ * when the device bytes its slot must add fit in `budget_bytes` (0: 90% of
+ * the device's free memory at creation) next to what all slots hold.  Each
+ * request computes exactly what nmfcu_run computes for the same arguments.
+ */
+typedef struct nmfcu_server nmfcu_server;
+
+typedef struct nmfcu_server_stats {
+    int64_t submitted, completed, failed, cancelled, queued, running;
+    int64_t iterations;       /* iterations of the completed requests            */
+    double wall_ms;           /* first submission to the last completion         */
+    double p50_ms, p99_ms, max_ms; /* submit-to-complete latency, completed ones  */
+    double mean_queue_ms;     /* submit-to-start, completed requests             */
+    int64_t budget_bytes, in_use_bytes, peak_bytes; /* device memory of the slots */
+    int32_t slots, peak_running;
+} nmfcu_server_stats;
+
+nmfcu_status nmfcu_server_create(int32_t device, int32_t slots, int64_t budget_bytes,
+                                 nmfcu_server **out);
+/* Cancels queued requests, waits for running ones, frees everything. */
+void nmfcu_server_destroy(nmfcu_server *srv);
+/* Queues one factorisation (arguments as nmfcu_run; V has leading dimension
+ * ldv).  Every buffer stays owned by the caller and must stay valid until
+ * nmfcu_server_wait has returned for the request.  A request that would not
+ * fit in the budget even alone fails here with NMFCU_ERR_OOM. */
+nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, int64_t n,
+                                 int64_t p, int64_t r, const double *V, int64_t ldv,
+                                 const double *W0, const double *H0, double *W, double *H,
+                                 double *deviances, int64_t dev_cap, int64_t *request_id);
+/* state: 0 queued, 1 running, 2 done. */
+nmfcu_status nmfcu_server_poll(nmfcu_server *srv, int64_t request_id, int32_t *state);
+/* Waits up to timeout_ms (< 0: no limit) and returns the request's own
+ * status (NMFCU_ERR_TIMEOUT if it has not finished; the request stays).
+ * Once a final status is returned the id is released. */
+nmfcu_status nmfcu_server_wait(nmfcu_server *srv, int64_t request_id, int64_t timeout_ms,
+                               int64_t *n_iter, int64_t *n_deviances);
+/* Cancels a request that has not started (its wait returns
+ * NMFCU_ERR_CANCELLED); running requests finish. */
+nmfcu_status nmfcu_server_cancel(nmfcu_server *srv, int64_t request_id);
+nmfcu_status nmfcu_server_get_stats(nmfcu_server *srv, nmfcu_server_stats *out);
+nmfcu_status nmfcu_server_reset_stats(nmfcu_server *srv);
 
 /* ---------------------------------------------------------------------- */
 /* Allocation-free objective                                               */

@@ -36,7 +36,6 @@ constexpr int kMaxBatchRank = 16;  // largest rank of a batched solve
 constexpr int kThreads = 128;      // threads per CTA
 constexpr int kRowChunk = 64;      // W rows staged per chunk (H step)
 constexpr int kPrefetch = 4;       // V rows in flight per thread (H step)
-constexpr int kColChunk = 16;      // V columns staged per chunk (W step)
 
 // Per element type: a thread owns CPT adjacent columns (H step) or rows
 // (W step) of V, held in one "lane pack" P.  f32 packs two (float2, one

@@ -18,6 +18,9 @@ nmfcu_status fail(nmfcu_status s, const std::string &msg);
 // The same for a CUDA error (maps allocation failures to NMFCU_ERR_OOM).
 nmfcu_status cuda_fail(cudaError_t e, const char *what);
 
+// The option checks every run entry point applies (method, stop, sizes...).
+nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r);
+
 // The per-device context behind the host-pointer API (created on first use).
 nmfcu_status default_context(int device, nmfcu_context **out);
 

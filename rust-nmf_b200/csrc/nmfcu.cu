@@ -969,6 +969,10 @@ namespace nmfcu_internal {
 
 nmfcu_status default_context(int device, nmfcu_context **out) { return ::default_context(device, out); }
 
+nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r) {
+    return ::validate_options(o, n, p, r);
+}
+
 nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out) {
     if (slot < 0 || slot >= kContextSlots) return fail(NMFCU_ERR_INVALID_ARG, "bad scratch slot");
     NMF_TRY(c->extra[slot].ensure(bytes));
@@ -1325,6 +1329,7 @@ const char *nmfcu_status_string(nmfcu_status s) {
         case NMFCU_ERR_NUMERIC: return "numeric error";
         case NMFCU_ERR_TIMEOUT: return "device wait timed out";
         case NMFCU_ERR_NO_DEVICE: return "no CUDA device";
+        case NMFCU_ERR_CANCELLED: return "request cancelled";
     }
     return "unknown status";
 }

@@ -230,27 +230,10 @@ def _regularisation(method: str, sparsity: float, smoothness: float):
     return 0.0, 0.0, 0.0, 0.0
 
 
-def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.ndarray] = None,
-        H0: Optional[np.ndarray] = None, seed: Optional[int] = None, max_iter: int = 2000,
-        eps: float = 1e-9, rescale: bool = True, theta: float = 0.5,
-        offset: Optional[np.ndarray] = None, weight: Optional[np.ndarray] = None,
-        sparsity: float = 0.01, smoothness: float = 1.0, stop: str = "max_iter",
-        stationary_th: float = float(np.finfo(np.float64).eps), check_interval: int = 50,
-        check_niter: int = 10, num_threads: Optional[int] = None, precision: str = "fp64",
-        refine_iters: int = 2, device: int = 0) -> NMFResult:
-    """Factorise V ~ W H on the GPU.
-
-    Arguments, defaults, validation order and result follow the reference's
-    ``nmf()`` (python/nmf_rs/__init__.py:396-568): method aliases, a
-    non-negativity check on V, ``random_init(V, rank, seed)`` for a missing
-    W0/H0, shape checks, per-method sparsity routing.  ``num_threads`` is
-    accepted and ignored.
-
-    Engine extensions: ``precision='fp32'`` stores V in f32 for the two V
-    contractions (f32 products, f64 reductions, f64 updates/objective/stop)
-    and runs the last ``refine_iters`` iterations in full f64; ``device``
-    selects the GPU.
-    """
+def _prepare(V, rank, method, W0, H0, seed, offset, weight, sparsity, smoothness):
+    """nmf()'s argument handling before the native call, in the reference's
+    order (python/nmf_rs/__init__.py:487-538): method aliases, V >= 0, a
+    random start for a missing W0/H0, shape checks, sparsity routing."""
     method_norm = _METHOD_ALIASES.get(method.lower())
     if method_norm is None:
         raise ValueError(
@@ -281,6 +264,32 @@ def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.nda
         if weight_arr.shape != V_arr.shape:
             raise ValueError(f"weight.shape {weight_arr.shape} != V.shape {V_arr.shape}")
     sh, sw, gh, gw = _regularisation(method_norm, sparsity, smoothness)
+    return method_norm, V_arr, W0, H0, offset_arr, weight_arr, (sh, sw, gh, gw)
+
+
+def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.ndarray] = None,
+        H0: Optional[np.ndarray] = None, seed: Optional[int] = None, max_iter: int = 2000,
+        eps: float = 1e-9, rescale: bool = True, theta: float = 0.5,
+        offset: Optional[np.ndarray] = None, weight: Optional[np.ndarray] = None,
+        sparsity: float = 0.01, smoothness: float = 1.0, stop: str = "max_iter",
+        stationary_th: float = float(np.finfo(np.float64).eps), check_interval: int = 50,
+        check_niter: int = 10, num_threads: Optional[int] = None, precision: str = "fp64",
+        refine_iters: int = 2, device: int = 0) -> NMFResult:
+    """Factorise V ~ W H on the GPU.
+
+    Arguments, defaults, validation order and result follow the reference's
+    ``nmf()`` (python/nmf_rs/__init__.py:396-568): method aliases, a
+    non-negativity check on V, ``random_init(V, rank, seed)`` for a missing
+    W0/H0, shape checks, per-method sparsity routing.  ``num_threads`` is
+    accepted and ignored.
+
+    Engine extensions: ``precision='fp32'`` stores V in f32 for the two V
+    contractions (f32 products, f64 reductions, f64 updates/objective/stop)
+    and runs the last ``refine_iters`` iterations in full f64; ``device``
+    selects the GPU.
+    """
+    method_norm, V_arr, W0, H0, offset_arr, weight_arr, (sh, sw, gh, gw) = _prepare(
+        V, rank, method, W0, H0, seed, offset, weight, sparsity, smoothness)
     out = _native.py_nmf_run(
         method_norm, V_arr, W0, H0, int(max_iter), eps=float(eps), rescale=bool(rescale),
         theta=float(theta), offset=offset_arr, weight=weight_arr, sparsity_h=sh,
@@ -299,4 +308,4 @@ def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.nda
     )
 
 
-from . import consensus, synthetic  # noqa: E402,F401  (nmf_rs.consensus, nmf_rs.synthetic)
+from . import consensus, serve, synthetic  # noqa: E402,F401

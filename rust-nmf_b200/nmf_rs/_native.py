@@ -20,7 +20,7 @@ _HERE = Path(__file__).resolve().parent
 LIB_PATH = Path(os.environ.get("NMFCU_LIBRARY", _HERE / "libnmfcu.so"))
 
 # Status codes (nmfcu_status).
-OK, INVALID_ARG, UNSUPPORTED, OOM, CUDA, NUMERIC, TIMEOUT, NO_DEVICE = range(8)
+OK, INVALID_ARG, UNSUPPORTED, OOM, CUDA, NUMERIC, TIMEOUT, NO_DEVICE, CANCELLED = range(9)
 
 # Method ids (Algo, lib.rs:1472-1484) and stop ids (Stop, lib.rs:1507-1513).
 BRUNET, LEE, OFFSET, NSNMF, HALS, EHALS, DNMF, LSNMF, SNMF_R, SNMF_L = range(10)
@@ -36,6 +36,18 @@ NOALLOC_MAX_ROWS = 524288
 _i32, _i64, _dbl = ctypes.c_int32, ctypes.c_int64, ctypes.c_double
 _dp = ctypes.POINTER(ctypes.c_double)
 _i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class ServerStats(ctypes.Structure):
+    """Mirror of ``nmfcu_server_stats``."""
+
+    _fields_ = [
+        ("submitted", _i64), ("completed", _i64), ("failed", _i64), ("cancelled", _i64),
+        ("queued", _i64), ("running", _i64), ("iterations", _i64), ("wall_ms", _dbl),
+        ("p50_ms", _dbl), ("p99_ms", _dbl), ("max_ms", _dbl), ("mean_queue_ms", _dbl),
+        ("budget_bytes", _i64), ("in_use_bytes", _i64), ("peak_bytes", _i64),
+        ("slots", _i32), ("peak_running", _i32),
+    ]
 
 
 class Options(ctypes.Structure):
@@ -95,6 +107,15 @@ SIGNATURES = {
     "nmfcu_consensus_device": (_i32, [ctypes.c_void_p, _i64, _i32, ctypes.POINTER(_i32),
                                       ctypes.c_void_p, _i32, ctypes.POINTER(_i32),
                                       ctypes.c_void_p, ctypes.c_void_p]),
+    "nmfcu_server_create": (_i32, [_i32, _i32, _i64, ctypes.POINTER(ctypes.c_void_p)]),
+    "nmfcu_server_destroy": (None, [ctypes.c_void_p]),
+    "nmfcu_server_submit": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64, _i64,
+                                   _dp, _i64, _dp, _dp, _dp, _dp, _dp, _i64, _i64p]),
+    "nmfcu_server_poll": (_i32, [ctypes.c_void_p, _i64, ctypes.POINTER(_i32)]),
+    "nmfcu_server_wait": (_i32, [ctypes.c_void_p, _i64, _i64, _i64p, _i64p]),
+    "nmfcu_server_cancel": (_i32, [ctypes.c_void_p, _i64]),
+    "nmfcu_server_get_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
+    "nmfcu_server_reset_stats": (_i32, [ctypes.c_void_p]),
     "nmfcu_objective_noalloc": (_i32, [_i32, _i64, _i64, _i64, ctypes.c_void_p, _i64,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),
@@ -149,6 +170,10 @@ def check(status: int) -> None:
         raise NotImplementedError(msg)
     if status == OOM:
         raise MemoryError(msg)
+    if status == CANCELLED:
+        import concurrent.futures
+
+        raise concurrent.futures.CancelledError(msg)
     raise RuntimeError(f"nmfcu: {load().nmfcu_status_string(status).decode()}: {msg}")
 
 
@@ -256,6 +281,33 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     and defaults; ``precision``, ``refine_iters`` and ``device`` are engine
     extensions.  ``num_threads`` is accepted and ignored (there is no CPU
     thread pool).  Returns ``{"W", "H", "n_iter", "deviances"}``."""
+    o, v, w0, h0, n, p, r = build_run_options(
+        algo, v, w0, h0, max_iter, eps=eps, rescale=rescale, theta=theta, offset=offset,
+        weight=weight, sparsity_h=sparsity_h, sparsity_w=sparsity_w, smoothness_h=smoothness_h,
+        smoothness_w=smoothness_w, stop=stop, stationary_th=stationary_th,
+        check_interval=check_interval, check_niter=check_niter, num_threads=num_threads,
+        precision=precision, refine_iters=refine_iters, device=device)
+    W = np.empty((n, r), dtype=np.float64)
+    H = np.empty((r, p), dtype=np.float64)
+    cap = o.max_iter + 1
+    dev = np.empty(cap, dtype=np.float64)
+    nd, ni = _i64(0), _i64(0)
+    check(load().nmfcu_run(ctypes.byref(o), n, p, r, _ptr(v), _ptr(w0), _ptr(h0), _ptr(W),
+                           _ptr(H), _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
+    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}
+
+
+def build_run_options(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
+                      rescale: bool = True, theta: float = 0.5, offset=None, weight=None,
+                      sparsity_h: float = 0.0, sparsity_w: float = 0.0,
+                      smoothness_h: float = 0.0, smoothness_w: float = 0.0,
+                      stop: str = "max_iter", stationary_th: float = 2.220446049250313e-16,
+                      check_interval: int = 50, check_niter: int = 10,
+                      num_threads: Optional[int] = None, precision: str = "fp64",
+                      refine_iters: int = 2, device: int = 0):
+    """py_nmf_run's argument handling (lib.rs:1934-1971): the checks in the
+    reference's order and the ``nmfcu_options`` they produce.  Returns
+    ``(options, V, W0, H0, n, p, r)`` with the arrays as C-contiguous f64."""
     o = default_options()
     o.method = parse_method(algo)            # Algo::from_str, lib.rs:1956
     o.stop = parse_stop(stop)                # Stop::from_str, lib.rs:1957
@@ -282,14 +334,7 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     o.check_niter = int(check_niter)
     o.refine_iters = int(refine_iters)
     o.device = int(device)
-    W = np.empty((n, r), dtype=np.float64)
-    H = np.empty((r, p), dtype=np.float64)
-    cap = o.max_iter + 1
-    dev = np.empty(cap, dtype=np.float64)
-    nd, ni = _i64(0), _i64(0)
-    check(load().nmfcu_run(ctypes.byref(o), n, p, r, _ptr(v), _ptr(w0), _ptr(h0), _ptr(W),
-                           _ptr(H), _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
-    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}
+    return o, v, w0, h0, n, p, r
 
 
 def divergence(v, w, h) -> float:

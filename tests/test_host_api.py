@@ -221,3 +221,16 @@ def test_consensus_metrics():
     H2 = np.array([[1.0, 0.0, 0.1, 0.0], [0.0, 0.1, 0.8, 1.0]])
     mixed = 0.5 * (C + consensus.connectivity_matrix(H2))
     assert 0.0 < consensus.dispersion_coefficient(mixed) < 1.0
+
+
+def test_server_needs_a_device_and_checks_its_arguments():
+    from nmf_rs import _native, serve
+
+    import ctypes
+    lib = _native.load()
+    h = ctypes.c_void_p()
+    assert lib.nmfcu_server_create(0, 0, 0, ctypes.byref(h)) == _native.INVALID_ARG
+    assert lib.nmfcu_server_create(0, 4, -1, ctypes.byref(h)) == _native.INVALID_ARG
+    if _native.device_count() == 0:
+        with pytest.raises(RuntimeError):
+            serve.Server(slots=2)
