@@ -18,6 +18,11 @@ A step is one NMF iteration (H update + W update) over the whole V.
 
 --impl reference times that CPU restatement as the reference arm.
 
+--form serve measures the serving form: a stream of Poisson-arriving
+requests (shapes log-uniform 500x1000 .. 5000x50000, rank U{5..30}, methods
+lee 40% / brunet 30% / hals 20% / dnmf 10%, 25..200 iterations, FP32 form)
+through nmfcu_server_*, reporting p50/p99 latency and aggregate iters/s.
+
 --form consensus measures the batching form instead: a consensus sweep of
 64 brunet restarts x ranks 2..10 (576 solves x 200 iterations) on a
 2000 x 5000 V, one step = one whole sweep through nmfcu_run_batch_device
@@ -68,10 +73,15 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--form", choices=["iterate", "consensus"], default="iterate")
+    ap.add_argument("--form", choices=["iterate", "consensus", "serve"], default="iterate")
+    ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
+    ap.add_argument("--slots", type=int, default=4, help="serve: server slots")
+    ap.add_argument("--load", type=float, default=0.8,
+                    help="serve: Poisson arrival rate as a fraction of the measured capacity")
     ap.add_argument("--runs", type=int, default=64, help="consensus restarts per rank")
     ap.add_argument("--seq-runs", type=int, default=None,
-                    help="consensus: restarts per rank timed one by one (default: all)")
+                    help="consensus: restarts per rank timed one by one (default: all; 0: skip)")
+    ap.add_argument("--iters", type=int, default=200, help="consensus: iterations per solve")
     return ap.parse_args()
 
 
@@ -435,7 +445,7 @@ def run_ours(args, world, rank, local):
         achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
         roof = {
             "bound": "hbm",
-            "kernel": "hstep_contract" if dom == _native.KCLASS_HSTEP else "rowpass (W step)",
+            "kernel": "hpass (H step)" if dom == _native.KCLASS_HSTEP else "wpass (W step)",
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -544,7 +554,7 @@ def consensus_inputs(runs, seed=7):
     return V, starts
 
 
-def consensus_cpu_baseline(V, runs, seconds):
+def consensus_cpu_baseline(V, runs, seconds, iters=200):
     """The oracle's brunet iteration per rank on a column slice,
     extrapolated to runs x 200 iterations per rank over the full V."""
     from nmf_rs import consensus
@@ -558,13 +568,13 @@ def consensus_cpu_baseline(V, runs, seconds):
             W0, H0 = consensus.restart_starts(v, r, 1)[0]
             return v, W0, H0
         b = cpu_baseline(fn, c["n"], c["p"], r, "brunet", seconds / len(c["ranks"]))
-        total += runs * c["iters"] / b["value"]
+        total += runs * iters / b["value"]
         samples.append(b["sample"].split(" took ")[1].split(";")[0])
     return {"value": runs * len(c["ranks"]) / total, "unit": "solves/s",
             "cores": os.cpu_count() or 1, "kind": "port",
             "sample": ("1 brunet iteration of the CPU restatement (oracle/, OpenMP) per rank "
                        "2..10 on a column slice of V (" + ", ".join(samples) + "), "
-                       f"extrapolated to {runs} restarts x {c['iters']} iterations on 2000x5000")}
+                       f"extrapolated to {runs} restarts x {iters} iterations on 2000x5000")}
 
 
 def run_consensus_reference(args, world, rank):
@@ -573,20 +583,20 @@ def run_consensus_reference(args, world, rank):
     V, _ = consensus_inputs(1)
     vals, base = [], None
     for _ in range(max(1, min(args.steps or 3, 3))):
-        base = consensus_cpu_baseline(V, args.runs, args.cpu_seconds)
+        base = consensus_cpu_baseline(V, args.runs, args.cpu_seconds, args.iters)
         vals.append(base["value"])
     value = statistics.median(vals)
     c = CONSENSUS
     print(json.dumps({
         "impl": "reference",
         "metric": f"consensus sweep solves/s ({args.runs} brunet restarts x ranks 2..10, "
-                  f"{c['iters']} iterations, 2000x5000)",
+                  f"{args.iters} iterations, 2000x5000)",
         "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps or 3,
         "warmup": args.warmup, "ms_per_step": 1000.0 * args.runs * len(c["ranks"]) / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded single-cell-like generator)",
         "config": {"workload": "consensus-sweep", "n": c["n"], "p": c["p"], "ranks": "2..10",
-                   "restarts": args.runs, "iters": c["iters"]},
+                   "restarts": args.runs, "iters": args.iters},
         "cpu_baseline": {**base, "value": value},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -601,7 +611,7 @@ def run_consensus(args, world, rank, local):
     from nmf_rs import _native, consensus
 
     c = CONSENSUS
-    n, p, iters = c["n"], c["p"], c["iters"]
+    n, p, iters = c["n"], c["p"], args.iters
     runs = args.runs
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -660,34 +670,36 @@ def run_consensus(args, world, rank, local):
     value = world * nsolves / (ms / 1000.0)
 
     # The same solves one by one through the single-solve engine.
-    seq_runs = min(runs, args.seq_runs or runs)
-    o = _native.default_options()
-    o.method = _native.parse_method("brunet")
-    o.stop = 0
-    o.precision = prec
-    o.max_iter = iters
-    o.refine_iters = 0
-    o.device = local
-    pick = [ci * runs + i for ci in range(len(c["ranks"])) for i in range(seq_runs)]
+    seq_runs = min(runs, runs if args.seq_runs is None else args.seq_runs)
+    seq_value = dh_rel = None
+    if seq_runs > 0:
+        o = _native.default_options()
+        o.method = _native.parse_method("brunet")
+        o.stop = 0
+        o.precision = prec
+        o.max_iter = iters
+        o.refine_iters = 0
+        o.device = local
+        pick = [ci * runs + i for ci in range(len(c["ranks"])) for i in range(seq_runs)]
 
-    def one(s_):
-        a, r = int(offs[s_]), int(ranks[s_])
-        w = dW0[:, a:a + r].contiguous()
-        h = dH0[a:a + r].contiguous()
-        ctx.run(o, n, p, r, dV.data_ptr(), _native.F64, p, w.data_ptr(), h.data_ptr(),
-                stream=stream.cuda_stream)
-        return h
+        def one(s_):
+            a, r = int(offs[s_]), int(ranks[s_])
+            w = dW0[:, a:a + r].contiguous()
+            h = dH0[a:a + r].contiguous()
+            ctx.run(o, n, p, r, dV.data_ptr(), _native.F64, p, w.data_ptr(), h.data_ptr(),
+                    stream=stream.cuda_stream)
+            return h
 
-    one(0)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for s_ in pick:
-        h = one(s_)
-    torch.cuda.synchronize()
-    t_seq = (time.perf_counter() - t0) * runs / seq_runs
-    seq_value = nsolves / t_seq
-    a, r = int(offs[pick[-1]]), int(ranks[pick[-1]])
-    dh_rel = float((h - dH[a:a + r]).abs().max() / h.abs().max())
+        one(0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s_ in pick:
+            h = one(s_)
+        torch.cuda.synchronize()
+        t_seq = (time.perf_counter() - t0) * runs / seq_runs
+        seq_value = nsolves / t_seq
+        a, r = int(offs[pick[-1]]), int(ranks[pick[-1]])
+        dh_rel = float((h - dH[a:a + r]).abs().max() / h.abs().max())
 
     # End to end: host V in, stacked factors and consensus matrices out.
     t0 = time.perf_counter()
@@ -696,7 +708,7 @@ def run_consensus(args, world, rank, local):
     t_e2e = time.perf_counter() - t0
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = consensus_cpu_baseline(V, runs, args.cpu_seconds)
+        cpu = consensus_cpu_baseline(V, runs, args.cpu_seconds, iters)
     if rank == 0:
         print(json.dumps({
             "metric": f"consensus sweep solves/s ({runs} brunet restarts x ranks 2..10, "
@@ -712,7 +724,7 @@ def run_consensus(args, world, rank, local):
             "gpu_launches": launches,
             "clocks": clocks,
             "one_by_one_solves_per_s": seq_value,
-            "batched_over_one_by_one": value / seq_value,
+            "batched_over_one_by_one": value / seq_value if seq_value else None,
             "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled",
             "max_rel_dH_batched_vs_single": dh_rel,
             "cpu_baseline": cpu,
@@ -725,11 +737,215 @@ def run_consensus(args, world, rank, local):
     ctx.close()
 
 
+# ---------------------------------------------------------------------------
+# Serving form: Poisson request stream
+# ---------------------------------------------------------------------------
+
+SERVE_METHODS = (("lee", 0.4), ("brunet", 0.3), ("hals", 0.2), ("dnmf", 0.1))
+SERVE_MAX = (5000, 50000)
+
+
+def serve_requests(count, seed=11):
+    """The request mix: (n, p, rank, method, iterations) per request."""
+    gen = np.random.default_rng(seed)
+    names = [m for m, _ in SERVE_METHODS]
+    probs = [w for _, w in SERVE_METHODS]
+    out = []
+    for _ in range(count):
+        n = int(round(np.exp(gen.uniform(np.log(500), np.log(5000)))))
+        p = int(round(np.exp(gen.uniform(np.log(1000), np.log(50000)))))
+        out.append((n, p, int(gen.integers(5, 31)), str(gen.choice(names, p=probs)),
+                    int(gen.integers(25, 201))))
+    return out
+
+
+def serve_cpu_rate(V_host, reqs, seconds):
+    """Oracle seconds per (row x column x iteration), from 1 iteration of each
+    method on a block of V; returns (iters/s for the whole mix, sample)."""
+    import oracle
+
+    oracle.build()
+    threads = os.cpu_count() or 1
+    n_s, p_s = 1000, 2000
+    v = np.ascontiguousarray(V_host[:n_s, :p_s])
+    per = {}
+    for m, _ in SERVE_METHODS:
+        gen = np.random.default_rng(0)
+        W0 = gen.uniform(0, 1, (n_s, 15))
+        H0 = gen.uniform(0, 1, (15, p_s))
+        t0 = time.perf_counter()
+        oracle.nmf_method(m, v, W0, H0, 1, num_threads=threads)
+        per[m] = (time.perf_counter() - t0) / (n_s * p_s * 15)
+    total_s = sum(per[m] * n * p * r * it for n, p, r, m, it in reqs)
+    iters = sum(it for *_, it in reqs)
+    return iters / total_s, {
+        "cores": threads,
+        "sample": (f"1 iteration per method of the CPU restatement (oracle/, OpenMP) on a "
+                   f"{n_s}x{p_s} rank-15 block, scaled by rows x columns x rank x iterations "
+                   f"to the {len(reqs)}-request mix")}
+
+
+def run_serve_reference(args, world, rank):
+    if rank != 0:
+        return
+    from nmf_rs import synthetic
+
+    reqs = serve_requests(args.requests)
+    V = synthetic.counts_matrix(1000, 2000, 12, 0.3, 4321)
+    value, info = serve_cpu_rate(V, reqs, args.cpu_seconds)
+    iters = sum(it for *_, it in reqs)
+    print(json.dumps({
+        "impl": "reference",
+        "metric": f"served iterations/s ({len(reqs)} Poisson-arriving mixed requests, "
+                  f"FP32 form, {args.slots} slots)",
+        "value": value, "unit": "iters/s", "n_gpus": args.gpus, "steps": len(reqs),
+        "warmup": args.warmup, "ms_per_step": 1000.0 * iters / value / len(reqs),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded single-cell-like generator)",
+        "config": {"workload": "serve-stream", "requests": len(reqs)},
+        "cpu_baseline": {"value": value, "unit": "iters/s", "kind": "port", **info},
+        "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "note": "the reference runs requests one after another on the host cores",
+    }), flush=True)
+
+
+def run_serve(args, world, rank, local):
+    import ctypes
+
+    import torch
+
+    from nmf_rs import _native
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    reqs = serve_requests(args.requests)
+    N, P = SERVE_MAX
+    # One pinned host V; request i reads its top-left n x p block (ldv = P).
+    V64, ld64, V32, ld32, _, _ = device_workload(N, P, 12, 0.3, 5, 4321 + rank, dev)
+    V_host = torch.empty((N, P), dtype=torch.float64, pin_memory=True)
+    V_host.copy_(V64[:, :P])
+    del V64, V32
+    torch.cuda.empty_cache()
+    Vh = V_host.numpy()
+    lib = _native.load()
+    h = ctypes.c_void_p()
+    _native.check(lib.nmfcu_server_create(local, args.slots, 0, ctypes.byref(h)))
+    gen = np.random.default_rng(5)
+    bufs = []
+    for n, p, r, m, it in reqs:
+        top = 1.0
+        W0 = gen.uniform(0, top, (n, r))
+        H0 = gen.uniform(0, top, (r, p))
+        o = _native.default_options()
+        o.method = _native.parse_method(m)
+        o.precision = _native.PRECISIONS["fp32"]
+        o.max_iter = it
+        o.refine_iters = 2
+        o.device = local
+        bufs.append((o, W0, H0, np.empty((n, r)), np.empty((r, p))))
+    dp = _native._ptr
+
+    def submit(i):
+        n, p, r, m, it = reqs[i]
+        o, W0, H0, W, H = bufs[i]
+        rid = ctypes.c_int64(0)
+        _native.check(lib.nmfcu_server_submit(
+            h, ctypes.byref(o), n, p, r, dp(Vh), P, dp(W0), dp(H0), dp(W), dp(H), None, 0,
+            ctypes.byref(rid)))
+        return rid.value
+
+    def wait(rid):
+        ni, nd = ctypes.c_int64(0), ctypes.c_int64(0)
+        _native.check(lib.nmfcu_server_wait(h, rid, -1, ctypes.byref(ni), ctypes.byref(nd)))
+        return ni.value
+
+    # Warm-up and capacity: the first requests as one burst.
+    warm = list(range(min(len(reqs), max(3, args.warmup) * args.slots)))
+    t0 = time.perf_counter()
+    ids = [submit(i) for i in warm]
+    for rid in ids:
+        wait(rid)
+    burst_s = time.perf_counter() - t0
+    # Capacity in requests/s: work units (rows x columns x rank x iterations)
+    # per second in the burst, over the mean work of a request of the mix.
+    units = [n * p * r * it for n, p, r, _, it in reqs]
+    rate_cap = sum(units[i] for i in warm) / burst_s / float(np.mean(units))
+    lam = args.load * rate_cap  # requests per second
+    _native.check(lib.nmfcu_server_reset_stats(h))
+    arrivals = np.cumsum(np.random.default_rng(17).exponential(1.0 / lam, len(reqs)))
+    barrier(world)
+    with Clocks(local) as clk:
+        t_start = time.perf_counter()
+        ids = []
+        for i, ta in enumerate(arrivals):
+            delay = ta - (time.perf_counter() - t_start)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(submit(i))
+        total_iters = sum(wait(rid) for rid in ids)
+        elapsed = time.perf_counter() - t_start
+    clocks = clk.summary()
+    st = _native.ServerStats()
+    _native.check(lib.nmfcu_server_get_stats(h, ctypes.byref(st)))
+    lib.nmfcu_server_destroy(h)
+    # FP64 objective checks: a few requests again alone in FP64.
+    from nmf_rs import _native as nv
+
+    rel = []
+    for i in range(min(4, len(reqs))):
+        n, p, r, m, it = reqs[i]
+        o, W0, H0, W, H = bufs[i]
+        Vi = np.ascontiguousarray(Vh[:n, :p])
+        ref = nv.py_nmf_run(m, Vi, W0, H0, it, precision="fp64", device=local)
+        f = nv.divergence if m == "brunet" else nv.distance
+        a, b = f(Vi, W, H), f(Vi, ref["W"], ref["H"])
+        rel.append(abs(a - b) / abs(b))
+    value = world * total_iters / elapsed
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, info = serve_cpu_rate(Vh, reqs, args.cpu_seconds)
+        cpu = {"value": cv, "unit": "iters/s", "kind": "port", **info}
+    h2d = sum(n * p * 8 + (n * r + r * p) * 8 for n, p, r, _, _ in reqs)
+    d2h = sum((n * r + r * p) * 8 for n, p, r, _, _ in reqs)
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"served iterations/s ({len(reqs)} Poisson-arriving mixed requests, "
+                      f"FP32 form, {args.slots} slots)",
+            "value": value, "unit": "iters/s", "n_gpus": world, "steps": len(reqs),
+            "warmup": len(warm), "ms_per_step": 1000.0 * elapsed / len(reqs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded single-cell-like generator; request blocks of one V)",
+            "config": {"workload": "serve-stream", "requests": len(reqs), "slots": args.slots,
+                       "shapes": "log-uniform 500x1000..5000x50000", "ranks": "5..30",
+                       "iters": "25..200", "mix": "lee .4 brunet .3 hals .2 dnmf .1",
+                       "arrival_rate_per_s": lam, "load": args.load,
+                       "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "max": st.max_ms,
+                           "mean_queue": st.mean_queue_ms},
+            "server": {"completed": st.completed, "failed": st.failed,
+                       "peak_running": st.peak_running, "peak_bytes": st.peak_bytes,
+                       "budget_bytes": st.budget_bytes},
+            "rel_objective_vs_fp64_alone": rel,
+            "gpu_launches": st.launches,
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": h2d / len(reqs),
+                    "d2h_bytes_per_step": d2h / len(reqs),
+                    "note": "already end to end: host V/W0/H0 in, host W/H out, per request"},
+        }), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.form == "consensus":
+        if args.form == "serve":
+            if args.impl == "reference":
+                run_serve_reference(args, world, rank)
+            else:
+                run_serve(args, world, rank, local)
+        elif args.form == "consensus":
             if args.impl == "reference":
                 run_consensus_reference(args, world, rank)
             else:

@@ -255,6 +255,7 @@ typedef struct nmfcu_server_stats {
     double p50_ms, p99_ms, max_ms; /* submit-to-complete latency, completed ones  */
     double mean_queue_ms;     /* submit-to-start, completed requests             */
     int64_t budget_bytes, in_use_bytes, peak_bytes; /* device memory of the slots */
+    int64_t launches;         /* engine kernel launches of the completed requests */
     int32_t slots, peak_running;
 } nmfcu_server_stats;
 

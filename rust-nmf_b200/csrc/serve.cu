@@ -117,6 +117,7 @@ struct nmfcu_server {
 
     // Statistics since creation or the last reset.
     int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, iterations = 0;
+    int64_t launches = 0;
     std::vector<double> latency_ms, queue_ms;
     bool have_first = false;
     Clock::time_point first_submit, last_done;
@@ -175,7 +176,9 @@ void nmfcu_server::worker(int k) {
         q->state = kRunning;
         q->t_start = Clock::now();
         lk.unlock();
+        const int64_t l0 = nmfcu_context_launch_count(sl.ctx);
         run(k, q);
+        const int64_t dl = nmfcu_context_launch_count(sl.ctx) - l0;
         const size_t now_held = nmfcu_internal::context_bytes(sl.ctx);
         lk.lock();
         in_use = in_use - sl.held + now_held;
@@ -188,6 +191,7 @@ void nmfcu_server::worker(int k) {
         if (q->status == NMFCU_OK) {
             completed++;
             iterations += q->n_iter;
+            launches += dl;
             latency_ms.push_back(ms_between(q->t_submit, q->t_done));
             queue_ms.push_back(ms_between(q->t_submit, q->t_start));
         } else {
@@ -438,6 +442,7 @@ nmfcu_status nmfcu_server_get_stats(nmfcu_server *srv, nmfcu_server_stats *out) 
     st.budget_bytes = (int64_t)srv->budget;
     st.in_use_bytes = (int64_t)srv->in_use;
     st.peak_bytes = (int64_t)srv->peak;
+    st.launches = srv->launches;
     st.slots = (int32_t)srv->slots.size();
     st.peak_running = srv->peak_running;
     *out = st;
@@ -448,6 +453,7 @@ nmfcu_status nmfcu_server_reset_stats(nmfcu_server *srv) {
     if (!srv) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     std::lock_guard<std::mutex> lk(srv->mu);
     srv->submitted = srv->completed = srv->failed = srv->cancelled = srv->iterations = 0;
+    srv->launches = 0;
     srv->latency_ms.clear();
     srv->queue_ms.clear();
     srv->have_first = false;

@@ -46,7 +46,7 @@ class ServerStats(ctypes.Structure):
         ("queued", _i64), ("running", _i64), ("iterations", _i64), ("wall_ms", _dbl),
         ("p50_ms", _dbl), ("p99_ms", _dbl), ("max_ms", _dbl), ("mean_queue_ms", _dbl),
         ("budget_bytes", _i64), ("in_use_bytes", _i64), ("peak_bytes", _i64),
-        ("slots", _i32), ("peak_running", _i32),
+        ("launches", _i64), ("slots", _i32), ("peak_running", _i32),
     ]
 
 
