@@ -286,6 +286,19 @@ def host_slice_fn(V64, p_full, rank, seed=0):
     return f
 
 
+# DRAM bytes (read + write) per V element of one launch of each streaming
+# pass, from an ncu capture (dram__bytes_read.sum + dram__bytes_write.sum)
+# of the 20000 x 20000 slice (V larger than L2), rank 20.  Traffic grows with
+# the V elements a launch streams, so a launch over n x p moves this times
+# n * p bytes.
+PASS_DRAM_BYTES_PER_ELEMENT = {
+    ("hpass", "fp32"): (1634701568 + 35060736) / 4e8,
+    ("wpass", "fp32"): (1637906432 + 33353984) / 4e8,
+    ("hpass", "fp64"): (3232219392 + 31828224) / 4e8,
+    ("wpass", "fp64"): (3242305792 + 32467968) / 4e8,
+}
+
+
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -443,6 +456,12 @@ def run_ours(args, world, rank, local):
         dom = max(cand, key=lambda kc: cand[kc][1])
         nl, tot_ms = cand[dom]
         achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
+        kname = "hpass" if dom == _native.KCLASS_HSTEP else "wpass"
+        traffic = None
+        if args.workload in ("atlas", "atlas-slice") and r == 20:
+            per = (main_iters * PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] +
+                   fp64_iters * PASS_DRAM_BYTES_PER_ELEMENT[(kname, "fp64")]) / max(steps, 1)
+            traffic = per * n * p  # bytes per launch, averaged over the timed launches
         roof = {
             "bound": "hbm",
             "kernel": "hpass (H step)" if dom == _native.KCLASS_HSTEP else "wpass (W step)",
@@ -453,7 +472,10 @@ def run_ours(args, world, rank, local):
             "peak_kind": peak_kind,
             "launches": nl,
             "avg_launch_ms": tot_ms / max(nl, 1),
-            "traffic": None,
+            "traffic": traffic,
+            "traffic_note": ("ncu DRAM bytes per launch, measured on the 20000x20000 slice and "
+                             "scaled by V elements") if traffic else None,
+            "algorithmic_bytes_per_launch": bytes_per_class / max(steps, 1),
             "class_ms": {name: classes[kc][1] for name, kc in
                          (("hstep", 0), ("wstep", 1), ("objective", 2), ("other", 3))},
         }
