@@ -1,7 +1,10 @@
 #!/usr/bin/env python
 """Benchmark of the NMF iteration loop on B200.
 
-A step is one NMF iteration (H update + W update) over the whole V.
+A step is one NMF iteration (H update + W update) over the whole V.  The
+default is the split-bf16 precision form (V as bf16 hi + lo, products on the
+tensor cores, f64 elsewhere, 2 trailing f64 iterations); --precision fp32
+(CUDA-core f32 products) and fp64 (the plain method) measure the others.
 
   value    iterations/s with V, W, H already in HBM (nmfcu_run_device),
            K timed iterations in one call, CUDA events on the launch stream,
@@ -68,7 +71,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="atlas")
     ap.add_argument("--method", choices=["lee", "brunet", "hals", "dnmf"], default="lee")
-    ap.add_argument("--precision", choices=["fp32", "fp64"], default="fp32")
+    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp64"], default="bf16x3")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -388,6 +391,9 @@ def run_ours(args, world, rank, local):
 
     def device_run(precision, iters_, W, H):
         o = options(precision, iters_)
+        if precision == "bf16x3":
+            return ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(),
+                           H.data_ptr(), stream=stream.cuda_stream)
         if precision == "fp32":
             return ctx.run(o, n, p, r, V32.data_ptr(), _native.F32, ld32, W.data_ptr(), H.data_ptr(), v64_ptr=V64.data_ptr(), ldv64=ld64,
                            stream=stream.cuda_stream)
@@ -417,7 +423,8 @@ def run_ours(args, world, rank, local):
         classes = {}
         if kernel_timing:
             for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP, _native.KCLASS_OBJECTIVE,
-                       _native.KCLASS_OTHER):
+                       _native.KCLASS_OTHER, _native.KCLASS_HSTEP_REFINE,
+                       _native.KCLASS_WSTEP_REFINE):
                 classes[kc] = ctx.kernel_time(kc)
         ctx.set_timing(False)
         return ms, launches, classes, W, H
@@ -430,26 +437,32 @@ def run_ours(args, world, rank, local):
     value = world * steps / (ms_max / 1000.0)
 
     extra = {}
-    if args.precision == "fp32" and not args.no_fp64_compare:
+    if args.precision != "fp64" and not args.no_fp64_compare:
         ms64, _, _, W64, H64 = timed("fp64", False)
         ms64_max = max_over_ranks(ms64, world)
         fp64_value = world * steps / (ms64_max / 1000.0)
         o_mixed = objective_torch(V64, p, W[:, :], H, args.method)
         o_plain = objective_torch(V64, p, W64, H64, args.method)
-        extra = {
+        extra = {}
+        if args.precision == "bf16x3":
+            ms32, _, _, _, _ = timed("fp32", False)
+            extra["fp32_form_iters_per_s"] = world * steps / (max_over_ranks(ms32, world) / 1000.0)
+        extra.update({
             "fp64_iters_per_s": fp64_value,
             "mixed_over_fp64": value / fp64_value,
             "rel_objective_vs_fp64": abs(o_mixed - o_plain) / abs(o_plain),
             "max_rel_dW_vs_fp64": float((W - W64).abs().max() / W64.abs().max()),
-        }
+        })
 
     # Roofline of the dominant V-streaming class.
     peak, peak_kind = measured_peaks()
-    s_main = 4 if args.precision == "fp32" else 8
-    refine = 2 if args.precision == "fp32" else 0
+    s_main = 8 if args.precision == "fp64" else 4  # f32 V, or bf16 hi + lo
+    refine = 0 if args.precision == "fp64" else 2
     main_iters = max(0, steps - refine)
     fp64_iters = steps - main_iters
-    bytes_per_class = n * p * (main_iters * s_main + fp64_iters * 8)
+    # The dominant class's launches are the main-form passes only (the FP64
+    # refinement passes are timed in their own classes).
+    bytes_per_class = n * p * main_iters * s_main
     roof = None
     if classes:
         cand = {kc: classes[kc] for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP)}
@@ -458,13 +471,14 @@ def run_ours(args, world, rank, local):
         achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
         kname = "hpass" if dom == _native.KCLASS_HSTEP else "wpass"
         traffic = None
-        if args.workload in ("atlas", "atlas-slice") and r == 20:
-            per = (main_iters * PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] +
-                   fp64_iters * PASS_DRAM_BYTES_PER_ELEMENT[(kname, "fp64")]) / max(steps, 1)
-            traffic = per * n * p  # bytes per launch, averaged over the timed launches
+        if (args.workload in ("atlas", "atlas-slice") and r == 20 and
+                (kname, args.precision) in PASS_DRAM_BYTES_PER_ELEMENT):
+            traffic = PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] * n * p  # per launch
         roof = {
             "bound": "hbm",
-            "kernel": "hpass (H step)" if dom == _native.KCLASS_HSTEP else "wpass (W step)",
+            "kernel": ((("tc_pass<H>" if dom == _native.KCLASS_HSTEP else "tc_pass<W>")
+                        if args.precision == "bf16x3" and args.method != "brunet" else
+                        ("hpass (H step)" if dom == _native.KCLASS_HSTEP else "wpass (W step)"))),
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
@@ -475,9 +489,10 @@ def run_ours(args, world, rank, local):
             "traffic": traffic,
             "traffic_note": ("ncu DRAM bytes per launch, measured on the 20000x20000 slice and "
                              "scaled by V elements") if traffic else None,
-            "algorithmic_bytes_per_launch": bytes_per_class / max(steps, 1),
+            "algorithmic_bytes_per_launch": bytes_per_class / max(nl, 1),
             "class_ms": {name: classes[kc][1] for name, kc in
-                         (("hstep", 0), ("wstep", 1), ("objective", 2), ("other", 3))},
+                         (("hstep", 0), ("wstep", 1), ("objective", 2), ("other", 3),
+                          ("hstep_refine", 4), ("wstep_refine", 5))},
         }
 
     # End to end through the host-pointer C ABI.
@@ -540,7 +555,8 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "dtype": {"fp32": "f32", "bf16x3": "bf16x3 (split bf16, f32 accumulation)",
+                      "fp64": "f64"}[args.precision],
             "data": "synthetic (seeded single-cell-like generator on the device)",
             "config": {"workload": args.workload, "n": n, "p": p, "rank": r,
                        "method": args.method, "precision": args.precision,

@@ -65,8 +65,13 @@ enum { NMFCU_STOP_MAX_ITER = 0, NMFCU_STOP_STATIONARY = 1 };
  *   FP32   -- V stored f32, products and per-thread sums in f32; every
  *             reduction across threads, all update epilogues, Gram matrices,
  *             rescaling, objective and stop test stay f64, and the last
- *             `refine_iters` iterations run the FP64 path on the f64 V. */
-enum { NMFCU_PREC_FP64 = 0, NMFCU_PREC_FP32 = 1 };
+ *             `refine_iters` iterations run the FP64 path on the f64 V.
+ *   BF16X3 -- lee / hals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
+ *             an element), the factor of each contraction split into three
+ *             bf16 terms, products on the tensor cores with f32 sums of at
+ *             most 2048 terms; everything else as FP32.  brunet (whose ratio
+ *             is formed per element) runs as FP32.  Needs the f64 V. */
+enum { NMFCU_PREC_FP64 = 0, NMFCU_PREC_FP32 = 1, NMFCU_PREC_BF16X3 = 2 };
 
 /* Keyword arguments of py_nmf_run (lib.rs:1912-1933), plus engine knobs. */
 typedef struct nmfcu_options {
@@ -182,9 +187,12 @@ nmfcu_status nmfcu_run_device(nmfcu_context *ctx, const nmfcu_options *opt, int6
 
 /* Per-kernel CUDA-event timing inside nmfcu_run_device (off by default).
  * Kernel classes: 0 = H-step V contraction, 1 = W-step V contraction,
- * 2 = objective V pass, 3 = everything else (grams, epilogues, stop). */
+ * 2 = objective V pass, 3 = everything else (grams, epilogues, stop),
+ * 4 / 5 = the H / W contractions of FP64 refinement iterations. */
 enum { NMFCU_KCLASS_HSTEP = 0, NMFCU_KCLASS_WSTEP = 1, NMFCU_KCLASS_OBJECTIVE = 2,
-       NMFCU_KCLASS_OTHER = 3, NMFCU_KCLASS_COUNT = 4 };
+       NMFCU_KCLASS_OTHER = 3,
+       /* the FP64 refinement iterations of the FP32 / BF16X3 forms */
+       NMFCU_KCLASS_HSTEP_REFINE = 4, NMFCU_KCLASS_WSTEP_REFINE = 5, NMFCU_KCLASS_COUNT = 6 };
 nmfcu_status nmfcu_context_set_timing(nmfcu_context *ctx, int32_t enabled);
 /* Launch count and summed event time (ms) of one kernel class since the
  * last reset; the call synchronises the context's events. */

@@ -45,4 +45,21 @@ struct StreamOps {
 const StreamOps *stream_ops_f32(int rp);
 const StreamOps *stream_ops_f64(int rp);
 
+// Tensor-core passes of the split-bf16 form (stream_tc.cu).  Tiles are 128
+// outputs wide, units 64 streamed elements, segments at most 32 units.
+constexpr int kTcTile = 128, kTcUnit = 64, kTcSegUnits = 32;
+// hpass: D[j][k] = sum_i V[i][j] W[i][k] (ah/al: the split V^T, p x n);
+// otherwise D[i][k] = sum_j V[i][j] H[k][j] (ah/al: the split V).  Maps of
+// A have box {64, 128}; b3: the factor's three bf16 terms (box {64, RPN});
+// RPN 16 or 32.
+cudaError_t tc_pass_launch(bool hpass, int RPN, const CUtensorMap &ah, const CUtensorMap &al,
+                           const CUtensorMap *b3, int kext, int RP, const StreamK &sk,
+                           double *part, RunState *st, cudaStream_t s);
+// V (f64) -> Vh, Vl (bf16, n x ldb) and Vth, Vtl (bf16 V^T, p x ldbt), one read of V.
+void tc_split_v(const double *V, int64_t ldv, void *Vh, void *Vl, int64_t ldb, void *Vth,
+                void *Vtl, int64_t ldbt, int n, int p, cudaStream_t s);
+// F(k, x) = F[k * fk + x * fx] (R x K) -> three bf16 planes of RPN x ldk.
+void tc_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *out, int RPN,
+                     int64_t ldk, const RunState *st, int sms, cudaStream_t s);
+
 }  // namespace nmfcu

@@ -231,6 +231,25 @@ bool tma_layout_ok(const void *base, int64_t ld, size_t es) {
     return (reinterpret_cast<uintptr_t>(base) % 16 == 0) && ((ld * (int64_t)es) % 16 == 0);
 }
 
+// bf16 matrix (rows x cols, leading dimension ld elements) with a
+// 128-byte-swizzled box of box_cols x box_rows (box_cols * 2 <= 128).
+nmfcu_status encode_2d_bf16(CUtensorMap *map, const void *base, int64_t rows, int64_t cols,
+                            int64_t ld, int box_cols, int box_rows) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)(ld * 2)};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS)
+        return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled (bf16) failed (code " +
+                                        std::to_string((int)r) + ")");
+    return NMFCU_OK;
+}
+
 // ===========================================================================
 // Device buffers
 // ===========================================================================
@@ -335,6 +354,7 @@ struct nmfcu_context {
     // Workspace.
     DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
     DevBuf Wf32, Ht64, Ht32;
+    DevBuf Vs, Fs;     // split-bf16 form: V hi/lo, the factor's three terms
     DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
 
@@ -346,8 +366,8 @@ struct nmfcu_context {
     };
     std::vector<Ev> events;
     std::vector<cudaEvent_t> pool;
-    double total_ms[NMFCU_KCLASS_COUNT] = {0, 0, 0, 0};
-    int64_t count[NMFCU_KCLASS_COUNT] = {0, 0, 0, 0};
+    double total_ms[NMFCU_KCLASS_COUNT] = {};
+    int64_t count[NMFCU_KCLASS_COUNT] = {};
     int64_t launch_total = 0;
 
     ~nmfcu_context() {
@@ -424,7 +444,36 @@ struct PassSet {
     CUtensorMap tmVh, tmVw, tmW, tmHt;
     void *Ht = nullptr;  // H^T, written by the H epilogue, streamed by the W pass
     void *Wc = nullptr;  // f32 copy of W (f32 only; f64 streams the master W)
+    // Split-bf16 form (tensor-core passes): V hi/lo maps for the H pass (box
+    // 64 x 64) and the W pass (box 64 x 128), and the factor terms' maps.
+    bool tc = false;
+    int rpn = 0;
+    int64_t ldw = 0, ldh = 0;  // leading dimensions of the W / H term planes
+    CUtensorMap tmVhH, tmVlH, tmVhW, tmVlW, tmFw[3], tmFh[3];  // H: V^T planes; W: V planes
 };
+
+// The split-bf16 form runs lee / hals / dnmf on the tensor cores; brunet's
+// ratio is formed per element, so it keeps the FP32 CUDA-core passes.
+bool tc_form(const nmfcu_options *o) {
+    return o->precision == NMFCU_PREC_BF16X3 && o->method != NMFCU_BRUNET;
+}
+// Element type of the main passes is f32 (FP32 form, or brunet in the split form).
+bool f32_form(const nmfcu_options *o) {
+    return o->precision == NMFCU_PREC_FP32 || (o->precision == NMFCU_PREC_BF16X3 && !tc_form(o));
+}
+int64_t round8(int64_t x) { return std::max<int64_t>(8, (x + 7) / 8 * 8); }
+int tc_rpn(int RP) { return RP <= 16 ? 16 : 32; }
+StreamK plan_tc_h(int64_t n, int64_t p, int sms) {
+    return plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms);
+}
+StreamK plan_tc_w(int64_t n, int64_t p, int sms) {
+    return plan_sk((n + kTcTile - 1) / kTcTile, (p + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms);
+}
+size_t tc_partial_bytes(const Plan &pl, int sms) {
+    const StreamK h = plan_tc_h(pl.n, pl.p, sms), w = plan_tc_w(pl.n, pl.p, sms);
+    return sizeof(double) * (size_t)pl.RP * kTcTile *
+           std::max((size_t)h.G * h.slots, (size_t)w.G * w.slots);
+}
 
 // Partial-sum bytes the two passes of `so` need for this shape.
 size_t pass_partial_bytes(const StreamOps *so, const Plan &pl, bool ratio, int sms) {
@@ -461,6 +510,47 @@ nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio
     else
         NMF_TRY(encode_2d(&ps->tmW, c->W.ptr, false, pl.n, pl.RP, pl.RP, pl.RP, ps->so->h_brows()));
     NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols(ratio)));
+    return NMFCU_OK;
+}
+
+// The split-bf16 passes over the f64 V (leading dimension ldv): splits V into
+// the context's hi/lo planes and encodes every tensor map.
+nmfcu_status make_tc_passset(nmfcu_context *c, const Plan &pl, const double *V64, int64_t ldv,
+                             cudaStream_t s, PassSet *ps) {
+    ps->tc = true;
+    ps->f32 = false;
+    ps->so = stream_ops_f32(pl.RP);  // its epilogues read the tensor-core partials
+    if (!ps->so) return fail(NMFCU_ERR_UNSUPPORTED, "no streaming kernels for this rank");
+    ps->Ht = nullptr;  // no H^T copy: the W pass streams the split terms of H
+    ps->Wc = nullptr;
+    ps->rpn = tc_rpn(pl.RP);
+    ps->ldw = round8(pl.n);
+    ps->ldh = round8(pl.p);
+    if (pl.n <= 0 || pl.p <= 0) return NMFCU_OK;
+    // Planes: V hi, V lo (n x ldb), V^T hi, V^T lo (p x ldbt).
+    const int64_t ldb = round8(pl.p), ldbt = round8(pl.n);
+    if ((ldbt + 31) / 32 > 65535)
+        return fail(NMFCU_ERR_UNSUPPORTED, "the split-bf16 form supports at most 2097120 rows");
+    unsigned char *vh = c->Vs.as<unsigned char>();
+    unsigned char *vl = vh + (size_t)pl.n * ldb * 2;
+    unsigned char *vth = vl + (size_t)pl.n * ldb * 2;
+    unsigned char *vtl = vth + (size_t)pl.p * ldbt * 2;
+    {
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        tc_split_v(V64, ldv, vh, vl, ldb, vth, vtl, ldbt, pl.n, pl.p, s);
+    }
+    CUDA_TRY(cudaGetLastError());
+    NMF_TRY(encode_2d_bf16(&ps->tmVhH, vth, pl.p, pl.n, ldbt, kTcUnit, kTcTile));
+    NMF_TRY(encode_2d_bf16(&ps->tmVlH, vtl, pl.p, pl.n, ldbt, kTcUnit, kTcTile));
+    NMF_TRY(encode_2d_bf16(&ps->tmVhW, vh, pl.n, pl.p, ldb, kTcUnit, kTcTile));
+    NMF_TRY(encode_2d_bf16(&ps->tmVlW, vl, pl.n, pl.p, ldb, kTcUnit, kTcTile));
+    unsigned char *f = c->Fs.as<unsigned char>();
+    for (int i = 0; i < 3; i++) {
+        NMF_TRY(encode_2d_bf16(&ps->tmFw[i], f + (size_t)i * ps->rpn * ps->ldw * 2, ps->rpn, pl.n,
+                               ps->ldw, kTcUnit, ps->rpn));
+        NMF_TRY(encode_2d_bf16(&ps->tmFh[i], f + (size_t)i * ps->rpn * ps->ldh * 2, ps->rpn, pl.p,
+                               ps->ldh, kTcUnit, ps->rpn));
+    }
     return NMFCU_OK;
 }
 
@@ -524,14 +614,32 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                     bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
+    if (ps.tc) {
+        // W (n x RP f64) -> three bf16 terms of W^T; tensor-core pass; update.
+        const StreamK sk = plan_tc_h(pl.n, pl.p, c->sms);
+        if (pl.n > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            tc_split_factor(a.W, 1, pl.RP, pl.r, pl.n, c->Fs.ptr, ps.rpn, ps.ldw, st, c->sms, s);
+        }
+        if (sk.G > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
+            CUDA_TRY(tc_pass_launch(true, ps.rpn, ps.tmVhH, ps.tmVlH, ps.tmFw, pl.n, pl.RP, sk,
+                                    c->part.as<double>(), st, s));
+        }
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        ps.so->h_epi(a.H, ps.Ht, pl.p, c->part.as<double>(), sk, kTcTile, e, st, s);
+        return NMFCU_OK;
+    }
     const int tcols = ps.so->h_tcols(ratio);
     const StreamK sk = plan_h(ps.so, ratio, pl.n, pl.p, c->sms);
+    const int kclass = (&ps == &a.p64 && a.opt->precision != NMFCU_PREC_FP64)
+                           ? NMFCU_KCLASS_HSTEP_REFINE : NMFCU_KCLASS_HSTEP;
     if (ps.f32 && pl.n > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
         ps.so->w_copy(a.W, ps.Wc, pl.n, st, s);
     }
     if (sk.G > 0) {
-        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
+        nmfcu_context::Scope sc(c, s, kclass);
         CUDA_TRY(ps.so->hpass(ratio, ps.tmVh, ps.tmW, a.H, pl.n, pl.p, sk, c->part.as<double>(),
                               st, sk.G, s));
     }
@@ -545,10 +653,28 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                     bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
+    if (ps.tc) {
+        // H (RP x p f64) -> three bf16 terms; tensor-core pass; update.
+        const StreamK sk = plan_tc_w(pl.n, pl.p, c->sms);
+        if (pl.p > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            tc_split_factor(a.H, pl.p, 1, pl.r, pl.p, c->Fs.ptr, ps.rpn, ps.ldh, st, c->sms, s);
+        }
+        if (sk.G > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
+            CUDA_TRY(tc_pass_launch(false, ps.rpn, ps.tmVhW, ps.tmVlW, ps.tmFh, pl.p, pl.RP, sk,
+                                    c->part.as<double>(), st, s));
+        }
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        ps.so->w_epi(a.W, pl.n, c->part.as<double>(), sk, kTcTile, e, st, s);
+        return NMFCU_OK;
+    }
     const int trows = ps.so->w_trows(ratio);
     const StreamK sk = plan_w(ps.so, ratio, pl.n, pl.p, c->sms);
+    const int kclass = (&ps == &a.p64 && a.opt->precision != NMFCU_PREC_FP64)
+                           ? NMFCU_KCLASS_WSTEP_REFINE : NMFCU_KCLASS_WSTEP;
     if (sk.G > 0) {
-        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
+        nmfcu_context::Scope sc(c, s, kclass);
         CUDA_TRY(ps.so->wpass(ratio, ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk, c->part.as<double>(),
                               st, sk.G, s));
     }
@@ -644,7 +770,8 @@ struct WsNeed {
     size_t bytes;
 };
 
-std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_f32) {
+std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_f32,
+                                    bool need_tc) {
     std::vector<WsNeed> v;
     const size_t RP = pl.RP;
     v.push_back({&c->W, sizeof(double) * (size_t)pl.n * RP});
@@ -655,7 +782,14 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         part = std::max(part, pass_partial_bytes(stream_ops_f64(pl.RP), pl, rt, c->sms));
         if (need_f32) part = std::max(part, pass_partial_bytes(stream_ops_f32(pl.RP), pl, rt, c->sms));
     }
+    if (need_tc) part = std::max(part, tc_partial_bytes(pl, c->sms));
     v.push_back({&c->part, part});
+    if (need_tc) {
+        const size_t rpn = (size_t)tc_rpn(pl.RP);
+        v.push_back({&c->Vs, 2 * 2 * ((size_t)pl.n * (size_t)round8(pl.p) +
+                                      (size_t)pl.p * (size_t)round8(pl.n))});
+        v.push_back({&c->Fs, 3 * 2 * rpn * (size_t)std::max(round8(pl.n), round8(pl.p))});
+    }
     v.push_back({&c->Ht64, sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()});
     if (need_f32) {
         const size_t rps = stream_ops_f32(pl.RP)->rps();
@@ -676,8 +810,10 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
     return v;
 }
 
-nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32) {
-    for (const WsNeed &w : workspace_needs(c, pl, need_f32)) NMF_TRY(w.buf->ensure(w.bytes));
+nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32,
+                              bool need_tc = false) {
+    for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc))
+        NMF_TRY(w.buf->ensure(w.bytes));
     if (!c->h_state) CUDA_TRY(cudaMallocHost((void **)&c->h_state, sizeof(RunState)));
     return NMFCU_OK;
 }
@@ -705,7 +841,8 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
     }
     if (o->stop != NMFCU_STOP_MAX_ITER && o->stop != NMFCU_STOP_STATIONARY)
         return fail(NMFCU_ERR_INVALID_ARG, "unknown stop id");
-    if (o->precision != NMFCU_PREC_FP64 && o->precision != NMFCU_PREC_FP32)
+    if (o->precision != NMFCU_PREC_FP64 && o->precision != NMFCU_PREC_FP32 &&
+        o->precision != NMFCU_PREC_BF16X3)
         return fail(NMFCU_ERR_INVALID_ARG, "unknown precision id");
     if (o->max_iter < 0) return fail(NMFCU_ERR_INVALID_ARG, "max_iter must be >= 0");
     if (o->check_niter < 0 || o->check_interval < 0)
@@ -722,7 +859,7 @@ nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_d
     CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
     if (stat) NMF_TRY(enqueue_objective(c, a, 0, s));
     const long long refine_from =
-        (o->precision == NMFCU_PREC_FP32) ? (long long)o->max_iter - o->refine_iters : LLONG_MAX;
+        (o->precision != NMFCU_PREC_FP64) ? (long long)o->max_iter - o->refine_iters : LLONG_MAX;
     for (long long it = 1; it <= o->max_iter; it++) {
         const bool fp64 = (o->precision == NMFCU_PREC_FP64) || (it > refine_from);
         NMF_TRY(enqueue_iteration(c, a, it, fp64, s));
@@ -990,7 +1127,7 @@ size_t context_bytes(nmfcu_context *c) {
     size_t t = 0;
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
-                            &c->Wf32, &c->Ht64, &c->Ht32})
+                            &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs})
         t += b->bytes;
     for (const DevBuf &b : c->extra) t += b.bytes;
     return t;
@@ -1002,11 +1139,11 @@ static size_t grow_by(const DevBuf &b, size_t want) {
     return want > b.bytes ? want - b.bytes : 0;
 }
 
-size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32) {
+size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32, bool tc) {
     const Plan pl = make_plan(n, p, r, c->sms);
     size_t g = 0;
-    for (const WsNeed &w : workspace_needs(c, pl, f32)) g += grow_by(*w.buf, w.bytes);
-    if (f32) g += grow_by(c->V32, sizeof(float) * (size_t)n * std::max<int64_t>(32, round_up(p, 32)));
+    for (const WsNeed &w : workspace_needs(c, pl, f32 || tc, tc)) g += grow_by(*w.buf, w.bytes);
+    if (f32 && !tc) g += grow_by(c->V32, sizeof(float) * (size_t)n * std::max<int64_t>(32, round_up(p, 32)));
     return g;
 }
 
@@ -1019,7 +1156,7 @@ void context_release(nmfcu_context *c) {
     DeviceGuard dg(c->device);
     for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
-                      &c->Ht64, &c->Ht32})
+                      &c->Ht64, &c->Ht32, &c->Vs, &c->Fs})
         b->release();
     for (DevBuf &b : c->extra) b.release();
 }
@@ -1106,8 +1243,8 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     DeviceGuard dg(c->device);
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    const bool f32 = opt->precision == NMFCU_PREC_FP32;
-    NMF_TRY(ensure_workspace(c, pl, f32));
+    const bool f32 = f32_form(opt), tc = tc_form(opt);
+    NMF_TRY(ensure_workspace(c, pl, f32, tc));
     if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(opt->max_iter + 1)));
     int64_t ldv = 0, ld32 = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
@@ -1119,7 +1256,9 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     a.ops = ops_for(pl.RP);
     const bool ratio = (opt->method == NMFCU_BRUNET);
     NMF_TRY(make_passset(c, pl, false, ratio, c->V64.ptr, ldv, &a.p64));
-    if (f32)
+    if (tc)
+        NMF_TRY(make_tc_passset(c, pl, c->V64.as<double>(), ldv, s, &a.main));
+    else if (f32)
         NMF_TRY(make_passset(c, pl, true, ratio, c->V32.ptr, ld32, &a.main));
     else
         a.main = a.p64;
@@ -1209,10 +1348,10 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     if (v_dtype != NMFCU_F64 && v_dtype != NMFCU_F32)
         return fail(NMFCU_ERR_INVALID_ARG, "v_dtype must be NMFCU_F64 or NMFCU_F32");
     if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
-    const bool f32 = (opt->precision == NMFCU_PREC_FP32);
+    const bool f32 = f32_form(opt), tc = tc_form(opt);
     const bool stat = opt->stop == NMFCU_STOP_STATIONARY;
-    if (!f32 && v_dtype != NMFCU_F64)
-        return fail(NMFCU_ERR_INVALID_ARG, "precision FP64 needs an f64 V");
+    if (!f32 && v_dtype != NMFCU_F64 && !(tc && dV64))
+        return fail(NMFCU_ERR_INVALID_ARG, "precision FP64 and the split-bf16 form need an f64 V");
     const double *V64 = (v_dtype == NMFCU_F64) ? (const double *)dV : dV64;
     int64_t ld64 = (v_dtype == NMFCU_F64) ? ldv : ldv64;
     if (V64 && dV64 && v_dtype == NMFCU_F32 && ldv64 < p)
@@ -1224,7 +1363,7 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     DeviceGuard dg(c->device);
     cudaStream_t s = (cudaStream_t)stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl, f32));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc));
     // The streaming passes read V through TMA, which needs a 16-byte aligned
     // base and row pitch; a V that is not laid out so is copied into the
     // context's pitched buffer first.
@@ -1260,7 +1399,9 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     a.ops = ops_for(pl.RP);
     const bool ratio = (opt->method == NMFCU_BRUNET);
     if (V64) NMF_TRY(make_passset(c, pl, false, ratio, V64, ld64, &a.p64));
-    if (f32)
+    if (tc)
+        NMF_TRY(make_tc_passset(c, pl, V64, ld64, s, &a.main));
+    else if (f32)
         NMF_TRY(make_passset(c, pl, true, ratio, Vmain, ldmain, &a.main));
     else
         a.main = a.p64;

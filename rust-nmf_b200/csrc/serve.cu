@@ -79,8 +79,9 @@ size_t dev_slots(const Request &q) {
 
 // Bytes context `c` would add to run request q.
 size_t growth_on(nmfcu_context *c, const Request &q) {
-    const bool f32 = q.opt.precision == NMFCU_PREC_FP32;
-    return nmfcu_internal::context_growth(c, q.n, q.p, q.r, f32) +
+    const bool tc = q.opt.precision == NMFCU_PREC_BF16X3 && q.opt.method != NMFCU_BRUNET;
+    const bool f32 = q.opt.precision == NMFCU_PREC_FP32 || (q.opt.precision == NMFCU_PREC_BF16X3 && !tc);
+    return nmfcu_internal::context_growth(c, q.n, q.p, q.r, f32, tc) +
            nmfcu_internal::slot_growth(c, kSlotV, v_bytes(q)) +
            nmfcu_internal::slot_growth(c, kSlotW, sizeof(double) * (size_t)(q.n * q.r)) +
            nmfcu_internal::slot_growth(c, kSlotH, sizeof(double) * (size_t)(q.r * q.p)) +

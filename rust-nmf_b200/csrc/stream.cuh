@@ -88,6 +88,25 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, u
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
         : "memory");
 }
+// The same with an L2 cache policy (createpolicy) for the loaded lines.
+__device__ __forceinline__ void tma_load_2d_hint(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                                 int x, int y, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint64_t l2_evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
 __device__ __forceinline__ void record_timeout(RunState *st, int code) {
     if (st) atomicCAS(&st->timeout, 0, code);
 }
@@ -681,22 +700,48 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) H[(size_t)k * p + j] = hc[k];
+    if (Ht == nullptr) return;  // the tensor-core passes stream their own H terms
     TH *ht = Ht + (size_t)j * RPS_T;
 #pragma unroll
     for (int k = 0; k < RPS_T; k++) ht[k] = (k < e.r && k < RP) ? (TH)hc[k] : (TH)0;
 }
 
-// One thread per row: sum the partials, apply the W update.
+// One warp per row: lane l adds the partials of segments l, l + 32, ...
+// (each over its CTAs in order), a fixed xor butterfly adds the lanes, and
+// lane 0 applies the W update -- a long row (many column segments) is
+// gathered 32 segments at a time.  Deterministic.
 template <int RP>
 __global__ void __launch_bounds__(kThreads)
     w_epilogue_sk(double *__restrict__ W, int n, const double *__restrict__ part, StreamK sk,
                   int trows, EpiParams e, const RunState *st) {
     if (run_stopped(st)) return;
-    const int i = blockIdx.x * kThreads + threadIdx.x;
-    if (i >= n) return;
+    const int i = (int)(((size_t)blockIdx.x * kThreads + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;  // uniform across the warp
     const int rt = i / trows, rl = i - rt * trows;
-    double num[RP], wr[RP];
-    gather_partials<RP>(part, sk, rt, (size_t)trows * RP, (size_t)rl * RP, 1, num);
+    double num[RP];
+#pragma unroll
+    for (int k = 0; k < RP; k++) num[k] = 0.0;
+    if (sk.G > 0) {
+        const size_t slot_elems = (size_t)trows * RP;
+        for (int seg = lane; seg < sk.nseg; seg += 32) {
+            const int t = rt * sk.nseg + seg;
+            int lo, hi;
+            sk_range(sk, t, &lo, &hi);
+            for (int b = lo; b <= hi; b++) {
+                const int slot = t - (int)(sk.start(b) / sk.UPT);
+                const double *src = part + ((size_t)b * sk.slots + slot) * slot_elems + (size_t)rl * RP;
+#pragma unroll
+                for (int k = 0; k < RP; k++) num[k] += src[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < RP; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) num[k] += __shfl_xor_sync(0xffffffffu, num[k], o);
+    if (lane != 0) return;
+    double wr[RP];
 #pragma unroll
     for (int k = 0; k < RP; k++) wr[k] = W[(size_t)i * RP + k];
     w_update<RP>(e, num, wr);

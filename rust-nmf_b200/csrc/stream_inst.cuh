@@ -87,7 +87,7 @@ struct StreamOpsT final : StreamOps {
     void w_epi(double *W, int n, const double *part, const StreamK &sk, int trows,
                const EpiParams &e, const RunState *st, cudaStream_t s) const override {
         if (n <= 0) return;
-        w_epilogue_sk<RP><<<(n + kThreads - 1) / kThreads, kThreads, 0, s>>>(W, n, part, sk,
+        w_epilogue_sk<RP><<<(unsigned)(((size_t)n * 32 + kThreads - 1) / kThreads), kThreads, 0, s>>>(W, n, part, sk,
                                                                             trows, e, st);
     }
     void w_copy(const double *W, void *Wc, int n, const RunState *st,

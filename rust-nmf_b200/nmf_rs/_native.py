@@ -25,11 +25,12 @@ OK, INVALID_ARG, UNSUPPORTED, OOM, CUDA, NUMERIC, TIMEOUT, NO_DEVICE, CANCELLED 
 # Method ids (Algo, lib.rs:1472-1484) and stop ids (Stop, lib.rs:1507-1513).
 BRUNET, LEE, OFFSET, NSNMF, HALS, EHALS, DNMF, LSNMF, SNMF_R, SNMF_L = range(10)
 STOP_MAX_ITER, STOP_STATIONARY = 0, 1
-PRECISIONS = {"fp64": 0, "fp32": 1}
+PRECISIONS = {"fp64": 0, "fp32": 1, "bf16x3": 2}
 MAX_RANK = 32
 F64, F32 = 0, 1  # element type of a device V
 
-KCLASS_HSTEP, KCLASS_WSTEP, KCLASS_OBJECTIVE, KCLASS_OTHER = range(4)
+(KCLASS_HSTEP, KCLASS_WSTEP, KCLASS_OBJECTIVE, KCLASS_OTHER, KCLASS_HSTEP_REFINE,
+ KCLASS_WSTEP_REFINE) = range(6)
 OBJECTIVE_KL, OBJECTIVE_FROBENIUS = 0, 1
 NOALLOC_MAX_ROWS = 524288
 
@@ -320,7 +321,7 @@ def build_run_options(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     try:
         o.precision = PRECISIONS[str(precision).lower()]
     except KeyError:
-        raise ValueError(f"unknown precision {precision!r}: supported fp64, fp32") from None
+        raise ValueError(f"unknown precision {precision!r}: supported fp64, fp32, bf16x3") from None
     o.max_iter = int(max_iter)
     if o.max_iter < 0:
         raise OverflowError("max_iter must be a non-negative integer")
