@@ -299,6 +299,9 @@ PASS_DRAM_BYTES_PER_ELEMENT = {
     ("wpass", "fp32"): (1637906432 + 33353984) / 4e8,
     ("hpass", "fp64"): (3232219392 + 31828224) / 4e8,
     ("wpass", "fp64"): (3242305792 + 32467968) / 4e8,
+    # split-bf16 form: the tensor-core passes (H pass streams the split V^T)
+    ("hpass", "bf16x3"): (1614820000 + 7405568) / 4e8,
+    ("wpass", "bf16x3"): (1614029000 + 9831936) / 4e8,
 }
 
 
