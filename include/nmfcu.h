@@ -47,10 +47,10 @@ typedef enum nmfcu_status {
 enum {
     NMFCU_BRUNET = 0,
     NMFCU_LEE = 1,
-    NMFCU_OFFSET = 2, /* not built: NMFCU_ERR_UNSUPPORTED */
-    NMFCU_NSNMF = 3,  /* not built */
+    NMFCU_OFFSET = 2, /* through nmfcu_run / nmfcu_run_offset (host buffers) */
+    NMFCU_NSNMF = 3,
     NMFCU_HALS = 4,
-    NMFCU_EHALS = 5, /* not built */
+    NMFCU_EHALS = 5, /* not built: NMFCU_ERR_UNSUPPORTED */
     NMFCU_DNMF = 6,
     NMFCU_LSNMF = 7,  /* not built */
     NMFCU_SNMF_R = 8, /* not built */
@@ -66,11 +66,12 @@ enum { NMFCU_STOP_MAX_ITER = 0, NMFCU_STOP_STATIONARY = 1 };
  *             reduction across threads, all update epilogues, Gram matrices,
  *             rescaling, objective and stop test stay f64, and the last
  *             `refine_iters` iterations run the FP64 path on the f64 V.
- *   BF16X3 -- lee / hals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
+ *   BF16X3 -- lee / offset / hals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
  *             an element), the factor of each contraction split into three
  *             bf16 terms, products on the tensor cores with f32 sums of at
- *             most 2048 terms; everything else as FP32.  brunet (whose ratio
- *             is formed per element) runs as FP32.  Needs the f64 V. */
+ *             most 2048 terms; everything else as FP32.  brunet and nsNMF
+ *             (whose ratio is formed per element) run as FP32.  Needs the
+ *             f64 V. */
 enum { NMFCU_PREC_FP64 = 0, NMFCU_PREC_FP32 = 1, NMFCU_PREC_BF16X3 = 2 };
 
 /* Keyword arguments of py_nmf_run (lib.rs:1912-1933), plus engine knobs. */
@@ -81,7 +82,7 @@ typedef struct nmfcu_options {
     int32_t rescale;       /* lee: W columns to sum 1 each iteration (1)        */
     int64_t max_iter;      /* iterations (the reference has no default here)   */
     double eps;            /* 1e-9; brunet ignores it and uses DBL_EPSILON      */
-    double theta;          /* nsNMF only (accepted, unused by built methods)    */
+    double theta;          /* nsNMF smoothing (0.5)                             */
     double sparsity_h;     /* dnmf L1 on H (0)                                  */
     double sparsity_w;     /* dnmf L1 on W (0)                                  */
     double smoothness_h;   /* dnmf L2 on H (0)                                  */
@@ -105,9 +106,12 @@ nmfcu_status nmfcu_parse_method(const char *name, int32_t *method);
 nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop);
 
 /*
- * nmfcu_run -- replaces py_nmf_run (lib.rs:1934-2169) for brunet, lee, hals
- * and dnmf: the whole iteration loop (nmf_run_brunet :1529-1586,
- * nmf_run_lee :1589-1647, nmf_run_hals :638-688, nmf_run_dnmf :827-906).
+ * nmfcu_run -- replaces py_nmf_run (lib.rs:1934-2169) for brunet, lee,
+ * offset, nsNMF, hals and dnmf: the whole iteration loop (nmf_run_brunet
+ * :1529-1586, nmf_run_lee :1589-1647, nmf_run_offset :1650-1760,
+ * nmf_run_nsnmf :1762-1830, nmf_run_hals :638-688, nmf_run_dnmf :827-906).
+ * For offset it starts from rowMeans(V) and drops the final offsets; use
+ * nmfcu_run_offset to pass and receive them.
  *
  * Host pointers.  V (n x p), W0 (n x r), H0 (r x p) are read; W (n x r) and
  * H (r x p) receive the result (they may alias W0 / H0).  `deviances` must
@@ -120,6 +124,19 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
                        const double *V, const double *W0, const double *H0, double *W,
                        double *H, double *deviances, int64_t deviances_cap,
                        int64_t *n_deviances, int64_t *n_iter);
+
+/*
+ * nmfcu_run_offset -- py_nmf_run with method "offset" (lib.rs:2023-2037, 2163-2165): as
+ * nmfcu_run, plus the row offsets.  offset0 (n doubles) is the `offset`
+ * keyword (NULL: rowMeans(V), lib.rs:1667-1679); `offset` (n doubles)
+ * receives the final offsets, the result dict's "offset" entry.  opt->method
+ * must be NMFCU_OFFSET.
+ */
+nmfcu_status nmfcu_run_offset(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                              const double *V, const double *W0, const double *H0,
+                              const double *offset0, double *W, double *H, double *offset,
+                              double *deviances, int64_t deviances_cap, int64_t *n_deviances,
+                              int64_t *n_iter);
 
 /* Single-step updates on host pointers; each writes a fresh factor.
  *   py_divergence_update_h (lib.rs:1851-1862 -> divergence_update_h_impl :120-144)

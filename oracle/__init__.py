@@ -2,8 +2,9 @@
 
 A ctypes wrapper around ``liboracle.so`` (built from ``nmf_oracle.c`` by
 ``oracle/Makefile``), which restates the f64 loops of omicverse/rust-NMF
-``rust/src/lib.rs`` (brunet :1529-1586, lee :1589-1647, hals :638-688,
-dnmf :827-906, objectives :1410-1445, stationary stop :1336-1401).
+``rust/src/lib.rs`` (brunet :1529-1586, lee :1589-1647, offset :1650-1760,
+nsNMF :1762-1830, hals :638-688, dnmf :827-906, objectives :1410-1445,
+stationary stop :1336-1401).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package, and only as the checker / baseline.
@@ -67,6 +68,21 @@ def _load():
         f = getattr(lib, name)
         f.restype = ctypes.c_double
         f.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp]
+    lib.orc_euclidean_distance_offset.restype = ctypes.c_double
+    lib.orc_euclidean_distance_offset.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp, _dp]
+    lib.orc_nmf_run_nsnmf.restype = ctypes.c_int
+    lib.orc_nmf_run_nsnmf.argtypes = [
+        _i64, _i64, _i64, _dp, _dp, _dp, _i64, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+        _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64), ctypes.c_int,
+    ]
+    lib.orc_nmf_run_offset.restype = ctypes.c_int
+    lib.orc_nmf_run_offset.argtypes = [
+        _i64, _i64, _i64, _dp, _dp, _dp, _dp, _i64, ctypes.c_double, ctypes.c_int,
+        ctypes.c_double, _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+        ctypes.c_int,
+    ]
+    if lib.orc_version() < 2:
+        raise RuntimeError("liboracle.so is stale: rebuild it (make -C oracle)")
     _lib = lib
     return lib
 
@@ -109,11 +125,80 @@ def nmf_run(method: str, V, W0, H0, max_iter: int, *, eps: float = 1e-9, rescale
     return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": dev[: nd.value].copy()}
 
 
+def _row_means_fwd(V: np.ndarray) -> np.ndarray:
+    """rowMeans(V) with forward-order sums (the default offset, lib.rs:1667-1679)."""
+    n, p = V.shape
+    if p == 0:
+        return np.full(n, np.nan)
+    return np.cumsum(V, axis=1)[:, -1] / float(p)
+
+
+def _stat_args(stop, stationary_th, check_interval, check_niter):
+    return (STOPS[stop.lower()], float(stationary_th), int(check_interval), int(check_niter))
+
+
+def nmf_nsnmf(V, W0, H0, max_iter: int, *, theta: float = 0.5, stop: str = "max_iter",
+              stationary_th: float = 2.220446049250313e-16, check_interval: int = 50,
+              check_niter: int = 10, num_threads: int | None = None) -> dict:
+    """Oracle of ``py_nmf_run`` with method nsNMF (nmf_run_nsnmf, lib.rs:1762-1830)."""
+    lib = _load()
+    V = _c(V)
+    W = _c(W0).copy()
+    H = _c(H0).copy()
+    n, p = V.shape
+    r = W.shape[1]
+    dev = np.zeros(max(int(max_iter) + 1, 1), dtype=np.float64)
+    nd, ni = _i64(0), _i64(0)
+    rc = lib.orc_nmf_run_nsnmf(
+        n, p, r, _ptr(V), _ptr(W), _ptr(H), int(max_iter), float(theta),
+        *_stat_args(stop, stationary_th, check_interval, check_niter), _ptr(dev),
+        ctypes.byref(nd), ctypes.byref(ni), int(num_threads or os.cpu_count() or 1),
+    )
+    if rc == -2:
+        raise ZeroDivisionError("stationary stop evaluated `iter % check_interval` with 0")
+    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": dev[: nd.value].copy()}
+
+
+def nmf_offset(V, W0, H0, max_iter: int, *, offset=None, eps: float = 1e-9,
+               stop: str = "max_iter", stationary_th: float = 2.220446049250313e-16,
+               check_interval: int = 50, check_niter: int = 10,
+               num_threads: int | None = None) -> dict:
+    """Oracle of ``py_nmf_run`` with method offset (nmf_run_offset, lib.rs:1650-1760).
+    Returns ``{"W", "H", "offset", "n_iter", "deviances"}``."""
+    lib = _load()
+    V = _c(V)
+    W = _c(W0).copy()
+    H = _c(H0).copy()
+    n, p = V.shape
+    r = W.shape[1]
+    off = _row_means_fwd(V) if offset is None else _c(offset).copy()
+    if off.shape != (n,):
+        raise ValueError(f"offset must have {n} entries")
+    dev = np.zeros(max(int(max_iter) + 1, 1), dtype=np.float64)
+    nd, ni = _i64(0), _i64(0)
+    rc = lib.orc_nmf_run_offset(
+        n, p, r, _ptr(V), _ptr(W), _ptr(H), _ptr(off), int(max_iter), float(eps),
+        *_stat_args(stop, stationary_th, check_interval, check_niter), _ptr(dev),
+        ctypes.byref(nd), ctypes.byref(ni), int(num_threads or os.cpu_count() or 1),
+    )
+    if rc == -2:
+        raise ZeroDivisionError("stationary stop evaluated `iter % check_interval` with 0")
+    return {"W": W, "H": H, "offset": off, "n_iter": int(ni.value),
+            "deviances": dev[: nd.value].copy()}
+
+
 def nmf_method(method: str, V, W0, H0, max_iter: int, *, eps=1e-9, rescale=True,
-               sparsity=0.01, smoothness=1.0, stop="max_iter", **kw) -> dict:
+               sparsity=0.01, smoothness=1.0, stop="max_iter", theta=0.5, offset=None,
+               **kw) -> dict:
     """Same as :func:`nmf_run` but with the Python-level routing of
     ``sparsity``/``smoothness`` that ``nmf()`` applies (python/nmf_rs/__init__.py:528-538):
-    dnmf gets ``sparsity`` on both factors and no L2, the others get none."""
+    dnmf gets ``sparsity`` on both factors and no L2, the others get none.
+    nsNMF and offset go to their own loops."""
+    m = method.lower()
+    if m in ("nsnmf", "ns", "ns_nmf"):
+        return nmf_nsnmf(V, W0, H0, max_iter, theta=theta, stop=stop, **kw)
+    if m == "offset":
+        return nmf_offset(V, W0, H0, max_iter, offset=offset, eps=eps, stop=stop, **kw)
     if method == "dnmf":
         sh = sw = float(sparsity)
     else:
@@ -170,3 +255,10 @@ def euclidean_distance(V, W, H) -> float:
     V, W, H = _c(V), _c(W), _c(H)
     return float(lib.orc_euclidean_distance(V.shape[0], V.shape[1], W.shape[1], _ptr(V),
                                             _ptr(W), _ptr(H)))
+
+
+def euclidean_distance_offset(V, W, H, offset) -> float:
+    lib = _load()
+    V, W, H, off = _c(V), _c(W), _c(H), _c(offset)
+    return float(lib.orc_euclidean_distance_offset(V.shape[0], V.shape[1], W.shape[1], _ptr(V),
+                                                   _ptr(W), _ptr(H), _ptr(off)))

@@ -544,5 +544,214 @@ int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, dou
     return status;
 }
 
+/* ------------------------------------------------------------------------ */
+/* nsNMF and offset                                                          */
+/* ------------------------------------------------------------------------ */
+
+/* smoothing_matrix, lib.rs:458-466: S = (1 - theta) I + (theta / r) 1 1^T. */
+static void smoothing(i64 r, double theta, double *s) {
+    const double off = theta / (double)r;
+    for (i64 i = 0; i < r; i++)
+        for (i64 j = 0; j < r; j++) s[i * r + j] = (i == j) ? (1.0 - theta) + off : off;
+}
+
+/* c = a (m x k) * b (k x q), forward dots (ndarray `dot`, lib.rs:1811 and
+ * :1819, restated). */
+static void mul_rs(i64 m, i64 k, i64 q, const double *a, const double *b, double *c) {
+    for (i64 i = 0; i < m; i++)
+        for (i64 j = 0; j < q; j++) {
+            double acc = 0.0;
+            for (i64 l = 0; l < k; l++) acc += a[i * k + l] * b[l * q + j];
+            c[i * q + j] = acc;
+        }
+}
+
+/*
+ * orc_nmf_run_nsnmf: nmf_run_nsnmf, lib.rs:1762-1830.  Each iteration: the
+ * KL H update with W S in place of W, the KL W update with S H in place of H,
+ * then col_rescale(W); objective KL(V, (W S) H).  No clamp.
+ */
+int orc_nmf_run_nsnmf(i64 n, i64 p, i64 r, const double *v, double *w, double *h, i64 max_iter,
+                      double theta, int stop, double stationary_th, i64 check_interval,
+                      i64 check_niter, double *dev, i64 *n_dev, i64 *n_iter, int nt) {
+    set_threads(nt);
+    stationary_t st = {check_interval, check_niter, stationary_th, -INFINITY, INFINITY, 0};
+    const int stat = (stop == ORC_STOP_STATIONARY);
+    const size_t rr = (size_t)(r * r > 0 ? r * r : 1);
+    const size_t nr = (size_t)(n * r > 0 ? n * r : 1), rp = (size_t)(r * p > 0 ? r * p : 1);
+    double *S = (double *)malloc(sizeof(double) * rr);
+    double *ws = (double *)malloc(sizeof(double) * nr);
+    double *sh = (double *)malloc(sizeof(double) * rp);
+    double *tmp_h = (double *)malloc(sizeof(double) * rp);
+    double *tmp_w = (double *)malloc(sizeof(double) * nr);
+    double *sum_ws = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    smoothing(r, theta, S);
+    double *v_t = transpose(v, n, p);
+    i64 nd = 0, iter = 0;
+    int done = 0, status = 0;
+    if (stat) {
+        mul_rs(n, r, r, w, S, ws);
+        double d = orc_kl_divergence(n, p, r, v, ws, h);
+        dev[nd++] = d;
+        if (st_should_stop(&st, 0, d) != 0) done = 1;
+    }
+    while (!done && iter < max_iter) {
+        iter++;
+        mul_rs(n, r, r, w, S, ws);
+        double *ws_t = transpose(ws, n, r);
+        col_sums(n, r, ws, sum_ws);
+        div_update_h_inner(n, p, r, v_t, ws, ws_t, h, sum_ws, tmp_h);
+        memcpy(h, tmp_h, sizeof(double) * (size_t)(r * p));
+        free(ws_t);
+        mul_rs(r, r, p, S, h, sh);
+        div_update_w(n, p, r, v, w, sh, tmp_w);
+        memcpy(w, tmp_w, sizeof(double) * (size_t)(n * r));
+        col_rescale(n, r, w);
+        if (stat) {
+            mul_rs(n, r, r, w, S, ws);
+            double d = orc_kl_divergence(n, p, r, v, ws, h);
+            dev[nd++] = d;
+            int rc = st_should_stop(&st, iter, d);
+            if (rc < 0) {
+                status = -2;
+                break;
+            }
+            if (rc) break;
+        }
+    }
+    *n_dev = nd;
+    *n_iter = iter;
+    free(S);
+    free(ws);
+    free(sh);
+    free(tmp_h);
+    free(tmp_w);
+    free(sum_ws);
+    free(v_t);
+    return status;
+}
+
+/* euclidean_distance of V against W H + off 1^T (lib.rs:1688-1694,
+ * :1745-1752): 0.5 * sum((V - WH - off)^2), j outer. */
+double orc_euclidean_distance_offset(i64 n, i64 p, i64 r, const double *v, const double *w,
+                                     const double *h, const double *off) {
+    double s = 0.0;
+    for (i64 j = 0; j < p; j++)
+        for (i64 i = 0; i < n; i++) {
+            double d = v[i * p + j] - (wh_at(p, r, w, h, i, j) + off[i]);
+            s += d * d;
+        }
+    return 0.5 * s;
+}
+
+/*
+ * orc_nmf_run_offset: nmf_run_offset, lib.rs:1650-1760.  off (n) holds the
+ * starting offsets on entry (rowMeans(V) by default, computed by the caller)
+ * and the result on exit.  Per iteration: the Frobenius H update with
+ * W^T off added to its denominator (offset_update_h_inner :330-361), the W
+ * update with off[i] rowSums(H)[j] added (offset_update_w_impl :398-450), then
+ * off_i <- off_i max(rowSums(V)_i, eps) / (rowSums(W H + off)_i + eps).
+ */
+int orc_nmf_run_offset(i64 n, i64 p, i64 r, const double *v, double *w, double *h, double *off,
+                       i64 max_iter, double eps, int stop, double stationary_th,
+                       i64 check_interval, i64 check_niter, double *dev, i64 *n_dev,
+                       i64 *n_iter, int nt) {
+    set_threads(nt);
+    stationary_t st = {check_interval, check_niter, stationary_th, -INFINITY, INFINITY, 0};
+    const int stat = (stop == ORC_STOP_STATIONARY);
+    const size_t rr = (size_t)(r * r > 0 ? r * r : 1);
+    const size_t nr = (size_t)(n * r > 0 ? n * r : 1), rp = (size_t)(r * p > 0 ? r * p : 1);
+    double *wtw = (double *)malloc(sizeof(double) * rr);
+    double *hht = (double *)malloc(sizeof(double) * rr);
+    double *addon = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    double *rsh = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
+    double *hp = (double *)malloc(sizeof(double) * rp);
+    double *wp = (double *)malloc(sizeof(double) * nr);
+    double *v_t = transpose(v, n, p);
+    i64 nd = 0, iter = 0;
+    int done = 0, status = 0;
+    if (stat) {
+        double d = orc_euclidean_distance_offset(n, p, r, v, w, h, off);
+        dev[nd++] = d;
+        if (st_should_stop(&st, 0, d) != 0) done = 1;
+    }
+    while (!done && iter < max_iter) {
+        iter++;
+        double *w_t = transpose(w, n, r);
+        wtw_rev(n, r, w_t, wtw);
+        for (i64 i = 0; i < r; i++) {
+            double a = 0.0;
+            for (i64 u = n - 1; u >= 0; u--) a += w_t[i * n + u] * off[u];
+            addon[i] = a;
+        }
+#pragma omp parallel for schedule(static)
+        for (i64 j = 0; j < p; j++)
+            for (i64 i = 0; i < r; i++) {
+                double numer = 0.0;
+                for (i64 u = n - 1; u >= 0; u--) numer += w_t[i * n + u] * v_t[j * n + u];
+                double den = 0.0;
+                for (i64 l = r - 1; l >= 0; l--) den += wtw[i * r + l] * h[l * p + j];
+                den += addon[i];
+                double temp = h[i * p + j] * numer;
+                hp[i * p + j] = (temp > eps ? temp : eps) / (den + eps);
+            }
+        memcpy(h, hp, sizeof(double) * (size_t)(r * p));
+        free(w_t);
+        for (i64 j = 0; j < r; j++)
+            for (i64 i = 0; i < r; i++) {
+                double a = 0.0;
+                for (i64 u = p - 1; u >= 0; u--) a += h[j * p + u] * h[i * p + u];
+                hht[i * r + j] = a;
+            }
+        for (i64 i = 0; i < r; i++) {
+            double a = 0.0;
+            for (i64 u = p - 1; u >= 0; u--) a += h[i * p + u];
+            rsh[i] = a;
+        }
+#pragma omp parallel for schedule(static)
+        for (i64 i = 0; i < n; i++)
+            for (i64 j = 0; j < r; j++) {
+                double numer = 0.0;
+                for (i64 u = p - 1; u >= 0; u--) numer += v[i * p + u] * h[j * p + u];
+                double den = 0.0;
+                for (i64 l = r - 1; l >= 0; l--) den += w[i * r + l] * hht[l * r + j];
+                den += off[i] * rsh[j];
+                double temp = w[i * r + j] * numer;
+                wp[i * r + j] = (temp < eps ? eps : temp) / (den + eps);
+            }
+        memcpy(w, wp, sizeof(double) * (size_t)(n * r));
+#pragma omp parallel for schedule(static)
+        for (i64 i = 0; i < n; i++) {
+            double rs_v = 0.0, rs_whpo = 0.0;
+            for (i64 j = 0; j < p; j++) {
+                rs_v += v[i * p + j];
+                rs_whpo += wh_at(p, r, w, h, i, j) + off[i];
+            }
+            const double num = rs_v > eps ? rs_v : eps;
+            off[i] = off[i] * num / (rs_whpo + eps);
+        }
+        if (stat) {
+            double d = orc_euclidean_distance_offset(n, p, r, v, w, h, off);
+            dev[nd++] = d;
+            int rc = st_should_stop(&st, iter, d);
+            if (rc < 0) {
+                status = -2;
+                break;
+            }
+            if (rc) break;
+        }
+    }
+    *n_dev = nd;
+    *n_iter = iter;
+    free(wtw);
+    free(hht);
+    free(addon);
+    free(rsh);
+    free(hp);
+    free(wp);
+    free(v_t);
+    return status;
+}
+
 /* Build identification so the Python side can tell a stale build apart. */
-int orc_version(void) { return 1; }
+int orc_version(void) { return 2; }

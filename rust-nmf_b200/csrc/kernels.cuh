@@ -26,7 +26,7 @@
 namespace nmfcu {
 
 // Method ids, same values as include/nmfcu.h.
-enum : int { M_BRUNET = 0, M_LEE = 1, M_HALS = 4, M_DNMF = 6 };
+enum : int { M_BRUNET = 0, M_LEE = 1, M_OFFSET = 2, M_NSNMF = 3, M_HALS = 4, M_DNMF = 6 };
 
 // Device-side state of the stationary stop (lib.rs:1336-1401) and of the
 // run: written by single-thread kernels, read by every kernel of an
@@ -193,7 +193,7 @@ template <typename TV, typename TA, int RP, int MODE>
 __global__ void __launch_bounds__(kThreads)
     rowpass(const TV *__restrict__ V, int64_t ldv, int n, int p, const double *__restrict__ W,
             const double *__restrict__ H, int cols_per_split, double *__restrict__ part,
-            double *__restrict__ obj, const RunState *st) {
+            double *__restrict__ obj, const RunState *st, const double *__restrict__ roff = nullptr) {
     if (run_stopped(st)) return;
     constexpr int TC = (sizeof(TV) == 8) ? 16 : 32;  // 128 B of a V row per tile
     __shared__ TV sV[kThreads][TC + 1];
@@ -216,6 +216,8 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int k = 0; k < (MODE <= 1 ? RP : 1); k++) acc[k] = 0.0;
     double objacc = 0.0;
+    // offset method: the row's offset is part of the estimate (lib.rs:1746-1752)
+    const double ro = (MODE == 3 && roff != nullptr && rowok) ? roff[i] : 0.0;
 
     constexpr int NA = (MODE <= 1) ? RP : 1;
     TA accf[NA];  // f64: the accumulator; f32: one tile's sums
@@ -259,7 +261,7 @@ __global__ void __launch_bounds__(kThreads)
                         objacc += ww;
                     }
                 } else {
-                    const double d = (double)v - (double)wh;
+                    const double d = (double)v - ((double)wh + ro);
                     objacc += d * d;
                 }
             }
@@ -297,6 +299,113 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------
+// nsNMF and offset helpers
+// ---------------------------------------------------------------------------
+// Smoothing matrix entry S[k][j] = (1 - theta) I + (theta / r) (lib.rs:458-466).
+__device__ __forceinline__ double smooth_at(int k, int j, int r, double theta) {
+    const double off = theta / (double)r;
+    return (k == j) ? (1.0 - theta) + off : off;
+}
+// out = X S for X (rows x RP, row-major; columns >= r zero), forward k
+// (W S of nmf_run_nsnmf, lib.rs:1811).
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    ns_right_s(const double *__restrict__ X, int rows, int r, double theta,
+               double *__restrict__ out, const RunState *st) {
+    if (run_stopped(st)) return;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= rows) return;
+    double x[RP];
+#pragma unroll
+    for (int k = 0; k < RP; k++) x[k] = X[(size_t)i * RP + k];
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < RP; k++)
+            if (k < r && j < r) acc = add(acc, mul(x[k], smooth_at(k, j, r, theta)));
+        out[(size_t)i * RP + j] = acc;
+    }
+}
+// out = S H for H (RP x p; rows >= r zero), forward l (S H, lib.rs:1819).
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    ns_left_s(const double *__restrict__ H, int p, int r, double theta, double *__restrict__ out,
+              const RunState *st) {
+    if (run_stopped(st)) return;
+    const int j = blockIdx.x * kThreads + threadIdx.x;
+    if (j >= p) return;
+    double h[RP];
+#pragma unroll
+    for (int l = 0; l < RP; l++) h[l] = H[(size_t)l * p + j];
+#pragma unroll
+    for (int k = 0; k < RP; k++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int l = 0; l < RP; l++)
+            if (k < r && l < r) acc = add(acc, mul(smooth_at(k, l, r, theta), h[l]));
+        out[(size_t)k * p + j] = acc;
+    }
+}
+// addon[k] = sum_u W[u][k] off[u] (den_addon, lib.rs:1705-1709); one block a
+// component, a fixed-order tree over the rows.
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    off_addon(const double *__restrict__ W, int n, int r, const double *__restrict__ off,
+              double *__restrict__ addon, const RunState *st) {
+    if (run_stopped(st)) return;
+    const int k = blockIdx.x;
+    __shared__ double red[kThreads];
+    double acc = 0.0;
+    if (k < r)
+        for (int u = threadIdx.x; u < n; u += kThreads) acc = add(acc, mul(W[(size_t)u * RP + k], off[u]));
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) addon[k] = (k < r) ? red[0] : 0.0;
+}
+// Row sums of V (one warp a row, fixed-order lanes + butterfly).
+static __global__ void __launch_bounds__(kThreads)
+    v_row_sums(const double *__restrict__ V, int64_t ldv, int n, int p, double *__restrict__ out) {
+    const int i = (int)(((size_t)blockIdx.x * kThreads + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n) return;
+    double acc = 0.0;
+    for (int j = lane; j < p; j += 32) acc += V[(size_t)i * ldv + j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) out[i] = acc;
+}
+// Default offset: rowMeans(V) (lib.rs:1667-1679).
+static __global__ void off_init(const double *__restrict__ rsv, int n, int p,
+                                double *__restrict__ off) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) off[i] = rsv[i] / (double)p;
+}
+// off_i <- off_i max(rowSums(V)_i, eps) / (rowSums(W H + off)_i + eps)
+// (lib.rs:1729-1742), with rowSums(W H)_i = sum_k W[i][k] rowSums(H)_k.
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    off_update(const double *__restrict__ W, int n, int r, const double *__restrict__ rsh,
+               const double *__restrict__ rsv, int p, double eps, double *__restrict__ off,
+               const RunState *st) {
+    if (run_stopped(st)) return;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < RP; k++)
+        if (k < r) s = add(s, mul(W[(size_t)i * RP + k], rsh[k]));
+    const double o = off[i];
+    const double rsw = add(s, mul((double)p, o));
+    const double num = rsv[i] > eps ? rsv[i] : eps;
+    off[i] = mul(o, num) / add(rsw, eps);
+}
+
+// ---------------------------------------------------------------------------
 // Epilogues.  Parameters shared by the H and W epilogues.
 // ---------------------------------------------------------------------------
 struct EpiParams {
@@ -307,6 +416,8 @@ struct EpiParams {
     double gamma;   // dnmf L2 (smoothness)
     const double *G;    // RP x RP Gram (W^T W for H, H H^T for W)
     const double *sums; // colsum(W) for the brunet H step, rowsum(H) for the W step
+    const double *addon = nullptr;  // offset, H step: (W^T off)[k] added to the denominator
+    const double *roff = nullptr;   // offset, W step: the row offsets off[i]
 };
 
 // Per-column H update from the reduced contraction num[] (old column hc[]).
@@ -317,7 +428,8 @@ struct EpiParams {
 template <int RP>
 __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, double *hc) {
     const int r = e.r;
-    if (e.method == M_LEE) {
+    if (e.method == M_LEE || e.method == M_OFFSET) {
+        // offset (offset_update_h_inner, lib.rs:330-361): + (W^T off)[i]
         double out[RP];
 #pragma unroll
         for (int i = 0; i < RP; i++) {
@@ -326,6 +438,7 @@ __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, 
 #pragma unroll
                 for (int l = RP - 1; l >= 0; l--)
                     if (l < r) den = add(den, mul(e.G[i * RP + l], hc[l]));
+                if (e.addon) den = add(den, e.addon[i]);
                 const double temp = mul(hc[i], num[i]);
                 out[i] = (temp > e.eps ? temp : e.eps) / add(den, e.eps);
             }
@@ -333,7 +446,7 @@ __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, 
 #pragma unroll
         for (int i = 0; i < RP; i++)
             if (i < r) hc[i] = out[i];
-    } else if (e.method == M_BRUNET) {
+    } else if (e.method == M_BRUNET || e.method == M_NSNMF) {
 #pragma unroll
         for (int i = 0; i < RP; i++)
             if (i < r) hc[i] = mul(hc[i], num[i]) / e.sums[i];
@@ -360,10 +473,12 @@ __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, 
 //   brunet : divergence_update_w_impl lib.rs:194-200
 //   hals   : hals_update_w           lib.rs:622-632
 //   dnmf   : hals_update_w_reg       lib.rs:1106-1116
+// ro: the row's offset (offset method; lib.rs:441-446), else unused.
 template <int RP>
-__device__ __forceinline__ void w_update(const EpiParams &e, const double *num, double *wr) {
+__device__ __forceinline__ void w_update(const EpiParams &e, const double *num, double *wr,
+                                         double ro = 0.0) {
     const int r = e.r;
-    if (e.method == M_LEE) {
+    if (e.method == M_LEE || e.method == M_OFFSET) {
         double out[RP];
 #pragma unroll
         for (int j = 0; j < RP; j++) {
@@ -372,6 +487,7 @@ __device__ __forceinline__ void w_update(const EpiParams &e, const double *num, 
 #pragma unroll
                 for (int l = RP - 1; l >= 0; l--)
                     if (l < r) den = add(den, mul(wr[l], e.G[l * RP + j]));
+                if (e.method == M_OFFSET) den = add(den, mul(ro, e.sums[j]));
                 const double temp = mul(wr[j], num[j]);
                 out[j] = (temp < e.eps ? e.eps : temp) / add(den, e.eps);
             }
@@ -379,7 +495,7 @@ __device__ __forceinline__ void w_update(const EpiParams &e, const double *num, 
 #pragma unroll
         for (int j = 0; j < RP; j++)
             if (j < r) wr[j] = out[j];
-    } else if (e.method == M_BRUNET) {
+    } else if (e.method == M_BRUNET || e.method == M_NSNMF) {
 #pragma unroll
         for (int j = 0; j < RP; j++)
             if (j < r) wr[j] = mul(wr[j], num[j]) / e.sums[j];
@@ -439,7 +555,7 @@ __global__ void __launch_bounds__(kThreads)
         num[k] = s;
         wr[k] = W[(int64_t)i * RP + k];
     }
-    w_update<RP>(e, num, wr);
+    w_update<RP>(e, num, wr, e.roff ? e.roff[i] : 0.0);
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) W[(int64_t)i * RP + k] = wr[k];

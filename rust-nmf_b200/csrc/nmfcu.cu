@@ -93,10 +93,23 @@ inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 // the objective's one read of V.
 struct Ops {
     virtual ~Ops() = default;
-    // mode 2 KL objective, 3 Frobenius objective (f64 V)
+    // mode 2 KL objective, 3 Frobenius objective (f64 V); roff: row offsets
+    // added to W H (offset method) or nullptr
     virtual void objective(const double *V, int64_t ldv, int n, int p, const double *W,
                            const double *H, int mode, int S2, int cols_per_split, double *obj,
+                           const RunState *st, cudaStream_t s,
+                           const double *roff = nullptr) const = 0;
+    // nsNMF: out = X S (rows x RP) and out = S H (RP x p)
+    virtual void ns_right(const double *X, int rows, int r, double theta, double *out,
+                          const RunState *st, cudaStream_t s) const = 0;
+    virtual void ns_left(const double *H, int p, int r, double theta, double *out,
+                         const RunState *st, cudaStream_t s) const = 0;
+    // offset: addon = W^T off; off update from rowSums(H) and rowSums(V)
+    virtual void off_addon(const double *W, int n, int r, const double *off, double *addon,
                            const RunState *st, cudaStream_t s) const = 0;
+    virtual void off_update(const double *W, int n, int r, const double *rsh, const double *rsv,
+                            int p, double eps, double *off, const RunState *st,
+                            cudaStream_t s) const = 0;
     virtual void gram_w(const double *W, int n, int B, int rows_per_block, double *pg,
                         double *ps, const RunState *st, cudaStream_t s) const = 0;
     virtual void gram_h(const double *H, int p, int B, int cols_per_block, double *pg,
@@ -115,7 +128,7 @@ template <int RP>
 struct OpsT final : Ops {
     void objective(const double *V, int64_t ldv, int n, int p, const double *W, const double *H,
                    int mode, int S2, int cols_per_split, double *obj, const RunState *st,
-                   cudaStream_t s) const override {
+                   cudaStream_t s, const double *roff) const override {
         if (n <= 0 || S2 <= 0) return;
         dim3 grid(cdiv(n, kThreads), S2), block(kThreads);
         if (mode == 2)
@@ -123,7 +136,25 @@ struct OpsT final : Ops {
                 V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st);
         else
             nmfcu::rowpass<double, double, RP, 3><<<grid, block, 0, s>>>(
-                V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st);
+                V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st, roff);
+    }
+    void ns_right(const double *X, int rows, int r, double theta, double *out, const RunState *st,
+                  cudaStream_t s) const override {
+        if (rows > 0)
+            nmfcu::ns_right_s<RP><<<cdiv(rows, kThreads), kThreads, 0, s>>>(X, rows, r, theta, out, st);
+    }
+    void ns_left(const double *H, int p, int r, double theta, double *out, const RunState *st,
+                 cudaStream_t s) const override {
+        if (p > 0) nmfcu::ns_left_s<RP><<<cdiv(p, kThreads), kThreads, 0, s>>>(H, p, r, theta, out, st);
+    }
+    void off_addon(const double *W, int n, int r, const double *off, double *addon,
+                   const RunState *st, cudaStream_t s) const override {
+        nmfcu::off_addon<RP><<<RP, kThreads, 0, s>>>(W, n, r, off, addon, st);
+    }
+    void off_update(const double *W, int n, int r, const double *rsh, const double *rsv, int p,
+                    double eps, double *off, const RunState *st, cudaStream_t s) const override {
+        if (n > 0)
+            nmfcu::off_update<RP><<<cdiv(n, kThreads), kThreads, 0, s>>>(W, n, r, rsh, rsv, p, eps, off, st);
     }
     void gram_w(const double *W, int n, int B, int rows_per_block, double *pg, double *ps,
                 const RunState *st, cudaStream_t s) const override {
@@ -355,6 +386,8 @@ struct nmfcu_context {
     DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
     DevBuf Wf32, Ht64, Ht32;
     DevBuf Vs, Fs;     // split-bf16 form: V hi/lo, the factor's three terms
+    DevBuf Wns, Hns;   // nsNMF: W S (n x RP), S H (RP x p)
+    DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
     DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
 
@@ -452,10 +485,12 @@ struct PassSet {
     CUtensorMap tmVhH, tmVlH, tmVhW, tmVlW, tmFw[3], tmFh[3];  // H: V^T planes; W: V planes
 };
 
-// The split-bf16 form runs lee / hals / dnmf on the tensor cores; brunet's
-// ratio is formed per element, so it keeps the FP32 CUDA-core passes.
+// The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
+// brunet's and nsNMF's ratio is formed per element, so they keep the FP32
+// CUDA-core passes.
 bool tc_form(const nmfcu_options *o) {
-    return o->precision == NMFCU_PREC_BF16X3 && o->method != NMFCU_BRUNET;
+    return o->precision == NMFCU_PREC_BF16X3 && o->method != NMFCU_BRUNET &&
+           o->method != NMFCU_NSNMF;
 }
 // Element type of the main passes is f32 (FP32 form, or brunet in the split form).
 bool f32_form(const nmfcu_options *o) {
@@ -485,8 +520,10 @@ size_t pass_partial_bytes(const StreamOps *so, const Plan &pl, bool ratio, int s
     return sizeof(double) * std::max(h, w);
 }
 
+// wsrc: the f64 matrix the H pass streams as W (W itself, or W S for nsNMF).
 nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio,
-                          const void *V, int64_t ldv, PassSet *ps) {
+                          const void *V, int64_t ldv, PassSet *ps,
+                          const double *wsrc = nullptr) {
     ps->f32 = f32;
     ps->so = f32 ? stream_ops_f32(pl.RP) : stream_ops_f64(pl.RP);
     if (!ps->so) return fail(NMFCU_ERR_UNSUPPORTED, "no streaming kernels for this rank");
@@ -508,7 +545,8 @@ nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio
     if (f32)
         NMF_TRY(encode_2d(&ps->tmW, c->Wf32.ptr, true, pl.n, rps, rps, rps, ps->so->h_brows()));
     else
-        NMF_TRY(encode_2d(&ps->tmW, c->W.ptr, false, pl.n, pl.RP, pl.RP, pl.RP, ps->so->h_brows()));
+        NMF_TRY(encode_2d(&ps->tmW, wsrc ? wsrc : c->W.as<double>(), false, pl.n, pl.RP, pl.RP,
+                          pl.RP, ps->so->h_brows()));
     NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols(ratio)));
     return NMFCU_OK;
 }
@@ -567,17 +605,26 @@ struct RunArgs {
     int64_t ldv64;
     double *W, *H;       // padded device factors
     double *dev;         // device deviances (or nullptr)
+    double *Wns = nullptr, *Hns = nullptr;  // nsNMF: W S, S H
+    double *off = nullptr, *rsv = nullptr, *addon = nullptr;  // offset
 };
 
 nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
                                cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    const bool kl = (a.opt->method == NMFCU_BRUNET);
+    const bool kl = (a.opt->method == NMFCU_BRUNET || a.opt->method == NMFCU_NSNMF);
+    const double *West = a.W;
+    if (a.opt->method == NMFCU_NSNMF) {  // KL of V against (W S) H, lib.rs:1779-1783
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        a.ops->ns_right(a.W, pl.n, pl.r, a.opt->theta, a.Wns, st, s);
+        West = a.Wns;
+    }
     {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OBJECTIVE);
-        a.ops->objective(a.V64, a.ldv64, pl.n, pl.p, a.W, a.H, kl ? 2 : 3, pl.S2,
-                         pl.cols_per_split, c->obj.as<double>(), st, s);
+        a.ops->objective(a.V64, a.ldv64, pl.n, pl.p, West, a.H, kl ? 2 : 3, pl.S2,
+                         pl.cols_per_split, c->obj.as<double>(), st, s,
+                         a.opt->method == NMFCU_OFFSET ? a.off : nullptr);
     }
     StopParams sp;
     sp.stationary = 1;
@@ -745,6 +792,55 @@ nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it,
             }
             break;
         }
+        case NMFCU_NSNMF: {
+            // nmf_run_nsnmf lib.rs:1804-1821: H update with W S, W update with
+            // S H, then col_rescale(W).
+            RunArgs aw = a;
+            aw.W = a.Wns;
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->ns_right(a.W, pl.n, pl.r, o->theta, a.Wns, st, s);
+            }
+            gram_w_full(c, aw, Gw, sw, s);  // colsum(W S)
+            NMF_TRY(h_step(c, aw, ps, epi(o, pl.r, Gw, sw, true), true, s));
+            RunArgs ah = a;
+            ah.H = a.Hns;
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->ns_left(a.H, pl.p, pl.r, o->theta, a.Hns, st, s);
+            }
+            transpose_h(c, ah, ps, s);      // the W pass streams (S H)^T
+            gram_h_full(c, ah, Gh, sh, s);  // rowsum(S H)
+            NMF_TRY(w_step(c, a, ps, epi(o, pl.r, Gh, sh, false), true, s));
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
+                a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(),
+                              c->ps.as<double>(), st, s);
+                a.ops->rescale(a.W, pl.n, pl.r, c->ps.as<double>(), pl.Bw, st, s);
+            }
+            break;
+        }
+        case NMFCU_OFFSET: {
+            // nmf_run_offset lib.rs:1694-1742: lee updates with the offset
+            // terms, then the offset update.
+            gram_w_full(c, a, Gw, sw, s);  // W^T W
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->off_addon(a.W, pl.n, pl.r, a.off, a.addon, st, s);
+            }
+            EpiParams eh = epi(o, pl.r, Gw, sw, true);
+            eh.addon = a.addon;
+            NMF_TRY(h_step(c, a, ps, eh, false, s));
+            gram_h_full(c, a, Gh, sh, s);  // H H^T, rowSums(H)
+            EpiParams ew = epi(o, pl.r, Gh, sh, false);
+            ew.roff = a.off;
+            NMF_TRY(w_step(c, a, ps, ew, false, s));
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->off_update(a.W, pl.n, pl.r, sh, a.rsv, pl.p, o->eps, a.off, st, s);
+            }
+            break;
+        }
         default: {
             // nmf_run_hals lib.rs:667-676; nmf_run_dnmf lib.rs:862-884.
             gram_w_full(c, a, Gw, sw, s);
@@ -771,7 +867,7 @@ struct WsNeed {
 };
 
 std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_f32,
-                                    bool need_tc) {
+                                    bool need_tc, int method) {
     std::vector<WsNeed> v;
     const size_t RP = pl.RP;
     v.push_back({&c->W, sizeof(double) * (size_t)pl.n * RP});
@@ -807,12 +903,21 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
     v.push_back({&c->sw2, sizeof(double) * RP});
     v.push_back({&c->obj, sizeof(double) * (size_t)std::max(pl.obj_blocks, 1)});
     v.push_back({&c->state, sizeof(RunState)});
+    if (method == NMFCU_NSNMF) {
+        v.push_back({&c->Wns, sizeof(double) * (size_t)pl.n * RP});
+        v.push_back({&c->Hns, sizeof(double) * RP * (size_t)pl.p});
+    }
+    if (method == NMFCU_OFFSET) {
+        v.push_back({&c->off, sizeof(double) * (size_t)pl.n});
+        v.push_back({&c->rsv, sizeof(double) * (size_t)pl.n});
+        v.push_back({&c->addon, sizeof(double) * RP});
+    }
     return v;
 }
 
 nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32,
-                              bool need_tc = false) {
-    for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc))
+                              bool need_tc = false, int method = -1) {
+    for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc, method))
         NMF_TRY(w.buf->ensure(w.bytes));
     if (!c->h_state) CUDA_TRY(cudaMallocHost((void **)&c->h_state, sizeof(RunState)));
     return NMFCU_OK;
@@ -831,12 +936,14 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
     switch (o->method) {
         case NMFCU_BRUNET:
         case NMFCU_LEE:
+        case NMFCU_OFFSET:
+        case NMFCU_NSNMF:
         case NMFCU_HALS:
         case NMFCU_DNMF: break;
-        case NMFCU_OFFSET: case NMFCU_NSNMF: case NMFCU_EHALS: case NMFCU_LSNMF:
-        case NMFCU_SNMF_R: case NMFCU_SNMF_L:
+        case NMFCU_EHALS: case NMFCU_LSNMF: case NMFCU_SNMF_R: case NMFCU_SNMF_L:
             return fail(NMFCU_ERR_UNSUPPORTED,
-                        "method is not built in the GPU engine (built: brunet, lee, hals, dnmf)");
+                        "method is not built in the GPU engine (built: brunet, lee, offset, nsNMF, "
+                        "hals, dnmf)");
         default: return fail(NMFCU_ERR_INVALID_ARG, "unknown method id");
     }
     if (o->stop != NMFCU_STOP_MAX_ITER && o->stop != NMFCU_STOP_STATIONARY)
@@ -1127,7 +1234,8 @@ size_t context_bytes(nmfcu_context *c) {
     size_t t = 0;
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
-                            &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs})
+                            &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
+                            &c->off, &c->rsv, &c->addon})
         t += b->bytes;
     for (const DevBuf &b : c->extra) t += b.bytes;
     return t;
@@ -1139,10 +1247,12 @@ static size_t grow_by(const DevBuf &b, size_t want) {
     return want > b.bytes ? want - b.bytes : 0;
 }
 
-size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32, bool tc) {
+size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32, bool tc,
+                      int method) {
     const Plan pl = make_plan(n, p, r, c->sms);
     size_t g = 0;
-    for (const WsNeed &w : workspace_needs(c, pl, f32 || tc, tc)) g += grow_by(*w.buf, w.bytes);
+    for (const WsNeed &w : workspace_needs(c, pl, f32 || tc, tc, method))
+        g += grow_by(*w.buf, w.bytes);
     if (f32 && !tc) g += grow_by(c->V32, sizeof(float) * (size_t)n * std::max<int64_t>(32, round_up(p, 32)));
     return g;
 }
@@ -1156,7 +1266,8 @@ void context_release(nmfcu_context *c) {
     DeviceGuard dg(c->device);
     for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
-                      &c->Ht64, &c->Ht32, &c->Vs, &c->Fs})
+                      &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
+                            &c->off, &c->rsv, &c->addon})
         b->release();
     for (DevBuf &b : c->extra) b.release();
 }
@@ -1227,10 +1338,46 @@ nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop) {
                                            "': supported: max_iter, stationary");
 }
 
-nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
-                       const double *V, const double *W0, const double *H0, double *W,
-                       double *H, double *deviances, int64_t deviances_cap,
-                       int64_t *n_deviances, int64_t *n_iter) {
+}  // extern "C"
+
+namespace {
+
+// Method state set up before the first iteration: nsNMF's W S / S H buffers;
+// the offset method's row sums of V and its starting offsets (off0 when
+// given, on the host or the device, else rowMeans(V) as in lib.rs:1667-1679).
+nmfcu_status setup_method(nmfcu_context *c, const Plan &pl, const nmfcu_options *o, RunArgs &a,
+                          const double *off0, bool off0_host, cudaStream_t s) {
+    if (o->method == NMFCU_NSNMF) {
+        a.Wns = c->Wns.as<double>();
+        a.Hns = c->Hns.as<double>();
+    }
+    if (o->method == NMFCU_OFFSET) {
+        a.off = c->off.as<double>();
+        a.rsv = c->rsv.as<double>();
+        a.addon = c->addon.as<double>();
+        if (pl.n > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, off0 ? 1 : 2);
+            v_row_sums<<<(unsigned)cdiv((int64_t)pl.n * 32, kThreads), kThreads, 0, s>>>(
+                a.V64, a.ldv64, pl.n, pl.p, a.rsv);
+            if (off0)
+                CUDA_TRY(cudaMemcpyAsync(a.off, off0, sizeof(double) * (size_t)pl.n,
+                                         off0_host ? cudaMemcpyHostToDevice
+                                                   : cudaMemcpyDeviceToDevice, s));
+            else
+                off_init<<<(unsigned)cdiv(pl.n, kThreads), kThreads, 0, s>>>(a.rsv, pl.n, pl.p,
+                                                                            a.off);
+        }
+    }
+    CUDA_TRY(cudaGetLastError());
+    return NMFCU_OK;
+}
+
+// The host-buffer run shared by nmfcu_run and nmfcu_run_offset.
+nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                      const double *V, const double *W0, const double *H0,
+                      const double *offset0, double *W, double *H, double *offset,
+                      double *deviances, int64_t deviances_cap, int64_t *n_deviances,
+                      int64_t *n_iter) {
     NMF_TRY(validate_options(opt, n, p, r));
     if (!V || !W0 || !H0 || !W || !H || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
@@ -1244,7 +1391,7 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
     const bool f32 = f32_form(opt), tc = tc_form(opt);
-    NMF_TRY(ensure_workspace(c, pl, f32, tc));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method));
     if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(opt->max_iter + 1)));
     int64_t ldv = 0, ld32 = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
@@ -1254,8 +1401,9 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    const bool ratio = (opt->method == NMFCU_BRUNET);
-    NMF_TRY(make_passset(c, pl, false, ratio, c->V64.ptr, ldv, &a.p64));
+    const bool ratio = (opt->method == NMFCU_BRUNET || opt->method == NMFCU_NSNMF);
+    const double *wsrc = (opt->method == NMFCU_NSNMF) ? c->Wns.as<double>() : nullptr;
+    NMF_TRY(make_passset(c, pl, false, ratio, c->V64.ptr, ldv, &a.p64, wsrc));
     if (tc)
         NMF_TRY(make_tc_passset(c, pl, c->V64.as<double>(), ldv, s, &a.main));
     else if (f32)
@@ -1267,9 +1415,13 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     a.W = c->W.as<double>();
     a.H = c->H.as<double>();
     a.dev = stat ? c->dev.as<double>() : nullptr;
+    NMF_TRY(setup_method(c, pl, opt, a, offset0, true, s));
     int64_t nd = 0, ni = 0;
     NMF_TRY(run_loop(c, a, s, &nd, &ni));
     NMF_TRY(get_factors(c, pl, W, H, cudaMemcpyDeviceToHost, s));
+    if (offset && opt->method == NMFCU_OFFSET && n > 0)
+        CUDA_TRY(cudaMemcpyAsync(offset, a.off, sizeof(double) * (size_t)n,
+                                 cudaMemcpyDeviceToHost, s));
     if (stat && nd > 0)
         CUDA_TRY(cudaMemcpyAsync(deviances, c->dev.ptr, sizeof(double) * (size_t)nd,
                                  cudaMemcpyDeviceToHost, s));
@@ -1277,6 +1429,31 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
     *n_deviances = nd;
     *n_iter = ni;
     return NMFCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                       const double *V, const double *W0, const double *H0, double *W,
+                       double *H, double *deviances, int64_t deviances_cap,
+                       int64_t *n_deviances, int64_t *n_iter) {
+    return run_host(opt, n, p, r, V, W0, H0, nullptr, W, H, nullptr, deviances, deviances_cap,
+                    n_deviances, n_iter);
+}
+
+nmfcu_status nmfcu_run_offset(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                              const double *V, const double *W0, const double *H0,
+                              const double *offset0, double *W, double *H, double *offset,
+                              double *deviances, int64_t deviances_cap, int64_t *n_deviances,
+                              int64_t *n_iter) {
+    if (!opt) return fail(NMFCU_ERR_INVALID_ARG, "NULL options");
+    if (opt->method != NMFCU_OFFSET)
+        return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_run_offset runs method NMFCU_OFFSET only");
+    if (!offset && n > 0) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    return run_host(opt, n, p, r, V, W0, H0, offset0, W, H, offset, deviances, deviances_cap,
+                    n_deviances, n_iter);
 }
 
 nmfcu_status nmfcu_update_h_divergence(int64_t n, int64_t p, int64_t r, const double *V,
@@ -1343,6 +1520,9 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
                               void *stream) {
     if (!c) return fail(NMFCU_ERR_INVALID_ARG, "NULL context");
     NMF_TRY(validate_options(opt, n, p, r));
+    if (opt->method == NMFCU_OFFSET)
+        return fail(NMFCU_ERR_UNSUPPORTED,
+                    "the offset method returns its row offsets: run it through nmfcu_run_offset");
     if (!dV || !dW || !dH || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (v_dtype != NMFCU_F64 && v_dtype != NMFCU_F32)
@@ -1363,7 +1543,7 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     DeviceGuard dg(c->device);
     cudaStream_t s = (cudaStream_t)stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl, f32, tc));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method));
     // The streaming passes read V through TMA, which needs a 16-byte aligned
     // base and row pitch; a V that is not laid out so is copied into the
     // context's pitched buffer first.
@@ -1397,8 +1577,9 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     a.opt = opt;
     a.pl = pl;
     a.ops = ops_for(pl.RP);
-    const bool ratio = (opt->method == NMFCU_BRUNET);
-    if (V64) NMF_TRY(make_passset(c, pl, false, ratio, V64, ld64, &a.p64));
+    const bool ratio = (opt->method == NMFCU_BRUNET || opt->method == NMFCU_NSNMF);
+    const double *wsrc = (opt->method == NMFCU_NSNMF) ? c->Wns.as<double>() : nullptr;
+    if (V64) NMF_TRY(make_passset(c, pl, false, ratio, V64, ld64, &a.p64, wsrc));
     if (tc)
         NMF_TRY(make_tc_passset(c, pl, V64, ld64, s, &a.main));
     else if (f32)
@@ -1415,6 +1596,7 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     a.H = c->H.as<double>();
     a.dev = stat ? d_dev : nullptr;
     if (stat && !d_dev) return fail(NMFCU_ERR_INVALID_ARG, "stationary stop needs d_dev");
+    NMF_TRY(setup_method(c, pl, opt, a, nullptr, false, s));
     int64_t nd = 0, ni = 0;
     NMF_TRY(run_loop(c, a, s, &nd, &ni));
     NMF_TRY(get_factors(c, pl, dW, dH, cudaMemcpyDeviceToDevice, s));

@@ -79,9 +79,10 @@ size_t dev_slots(const Request &q) {
 
 // Bytes context `c` would add to run request q.
 size_t growth_on(nmfcu_context *c, const Request &q) {
-    const bool tc = q.opt.precision == NMFCU_PREC_BF16X3 && q.opt.method != NMFCU_BRUNET;
+    const bool tc = q.opt.precision == NMFCU_PREC_BF16X3 && q.opt.method != NMFCU_BRUNET &&
+                    q.opt.method != NMFCU_NSNMF;
     const bool f32 = q.opt.precision == NMFCU_PREC_FP32 || (q.opt.precision == NMFCU_PREC_BF16X3 && !tc);
-    return nmfcu_internal::context_growth(c, q.n, q.p, q.r, f32, tc) +
+    return nmfcu_internal::context_growth(c, q.n, q.p, q.r, f32, tc, q.opt.method) +
            nmfcu_internal::slot_growth(c, kSlotV, v_bytes(q)) +
            nmfcu_internal::slot_growth(c, kSlotW, sizeof(double) * (size_t)(q.n * q.r)) +
            nmfcu_internal::slot_growth(c, kSlotH, sizeof(double) * (size_t)(q.r * q.p)) +
@@ -329,6 +330,9 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
                                  double *deviances, int64_t dev_cap, int64_t *request_id) {
     if (!srv || !opt || !request_id) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     NMFCU_TRY(nmfcu_internal::validate_options(opt, n, p, r));
+    if (opt->method == NMFCU_OFFSET)
+        return fail(NMFCU_ERR_UNSUPPORTED,
+                    "the offset method returns its row offsets: run it through nmfcu_run_offset");
     if (!V || !W0 || !H0 || !W || !H) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
     if (dev_cap < 0 || (dev_cap > 0 && !deviances))

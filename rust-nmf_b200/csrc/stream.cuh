@@ -744,7 +744,7 @@ __global__ void __launch_bounds__(kThreads)
     double wr[RP];
 #pragma unroll
     for (int k = 0; k < RP; k++) wr[k] = W[(size_t)i * RP + k];
-    w_update<RP>(e, num, wr);
+    w_update<RP>(e, num, wr, e.roff ? e.roff[i] : 0.0);
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) W[(size_t)i * RP + k] = wr[k];

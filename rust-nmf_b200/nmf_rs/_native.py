@@ -81,6 +81,8 @@ SIGNATURES = {
     "nmfcu_parse_stop": (_i32, [ctypes.c_char_p, ctypes.POINTER(_i32)]),
     "nmfcu_run": (_i32, [ctypes.POINTER(Options), _i64, _i64, _i64, _dp, _dp, _dp, _dp, _dp,
                          _dp, _i64, _i64p, _i64p]),
+    "nmfcu_run_offset": (_i32, [ctypes.POINTER(Options), _i64, _i64, _i64, _dp, _dp, _dp, _dp,
+                                _dp, _dp, _dp, _dp, _i64, _i64p, _i64p]),
     "nmfcu_update_h_divergence": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dp]),
     "nmfcu_update_w_divergence": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dp]),
     "nmfcu_update_h_euclidean": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dbl, _dp]),
@@ -281,7 +283,8 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     """The full loop (lib.rs:1934-2169).  Same positional / keyword signature
     and defaults; ``precision``, ``refine_iters`` and ``device`` are engine
     extensions.  ``num_threads`` is accepted and ignored (there is no CPU
-    thread pool).  Returns ``{"W", "H", "n_iter", "deviances"}``."""
+    thread pool).  Returns ``{"W", "H", "n_iter", "deviances"}``, plus
+    ``"offset"`` for the offset method (lib.rs:2161-2165)."""
     o, v, w0, h0, n, p, r = build_run_options(
         algo, v, w0, h0, max_iter, eps=eps, rescale=rescale, theta=theta, offset=offset,
         weight=weight, sparsity_h=sparsity_h, sparsity_w=sparsity_w, smoothness_h=smoothness_h,
@@ -293,6 +296,19 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     cap = o.max_iter + 1
     dev = np.empty(cap, dtype=np.float64)
     nd, ni = _i64(0), _i64(0)
+    if o.method == OFFSET:
+        off0 = None
+        if offset is not None:
+            off0 = np.ascontiguousarray(np.asarray(offset, dtype=np.float64))
+            if off0.shape != (n,):
+                raise ValueError(f"offset.shape {off0.shape} != ({n},)")
+        off = np.empty(n, dtype=np.float64)
+        check(load().nmfcu_run_offset(
+            ctypes.byref(o), n, p, r, _ptr(v), _ptr(w0), _ptr(h0),
+            _ptr(off0) if off0 is not None else None, _ptr(W), _ptr(H), _ptr(off), _ptr(dev),
+            cap, ctypes.byref(nd), ctypes.byref(ni)))
+        return {"W": W, "H": H, "offset": off, "n_iter": int(ni.value),
+                "deviances": list(dev[: nd.value])}
     check(load().nmfcu_run(ctypes.byref(o), n, p, r, _ptr(v), _ptr(w0), _ptr(h0), _ptr(W),
                            _ptr(H), _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
     return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}

@@ -40,6 +40,9 @@ KATS = {
     "V_max": 8.061756004056358,             # cell 1
     "brunet_200_frob_norm": 9.11162723892749,   # cell 5: ||V - WH||_F, brunet, 200 it
     "lee_200_frob_norm_4dp": 8.0928,        # cell 7: lee, 200 it, printed to 4 d.p.
+    "offset_200_frob_norm_4dp": 8.4113,     # cell 7: ||V - (WH + off)||_F, offset, 200 it
+    "offset_200_range_2dp": [0.61, 2.21],   # cell 7: min / max of the final offsets
+    "nsnmf_200_frob_norm_4dp": 30.8650,     # cell 7: ||V - WH||_F (fitted() omits S), nsNMF
     "brunet_stationary": {                  # cell 9
         "max_iter": 2000, "stationary_th": 1e-6, "check_interval": 10, "check_niter": 10,
         "n_iter": 2000, "final_kl": 0.5964519986834893, "n_deviances": 2001,

@@ -1,0 +1,134 @@
+"""GPU parity of the offset and nsNMF methods (nmf_run_offset, lib.rs:1650-1760;
+nmf_run_nsnmf, lib.rs:1762-1830) against the CPU oracle and the reference's
+recorded quickstart outputs.
+
+Tolerances (FP64), as for the other methods:
+  factors and offsets  max|d| / max|ref| <= 1e-10,
+  objective            relative 1e-12 beyond the evaluation's rounding floor.
+Reduced precisions (fp32, bf16x3 with their trailing FP64 iterations): the
+objective within 1e-5 relative of the FP64 oracle.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import rel, rel_max
+
+import nmf_rs
+from nmf_rs import synthetic
+
+pytestmark = pytest.mark.gpu
+
+FACTOR_TOL = 1e-10
+OBJ_TOL = 1e-12
+EPS = float(np.finfo(np.float64).eps)
+
+
+def _smooth(r, theta):
+    return (1.0 - theta) * np.eye(r) + theta / r
+
+
+def _objective(oracle, method, V, W, H, off=None, theta=0.5):
+    if method == "offset":
+        return oracle.euclidean_distance_offset(V, W, H, off)
+    return oracle.kl_divergence(V, W @ _smooth(W.shape[1], theta), H)
+
+
+def _rel_obj(method, V, a, b):
+    scale = 0.5 * float((V * V).sum()) if method == "offset" else float(V.sum())
+    excess = max(0.0, abs(a - b) - 10 * EPS * scale)
+    return excess / max(abs(b), 1e-300)
+
+
+def _check(oracle, method, V, W0, H0, iters, **kw):
+    ref = oracle.nmf_method(method, V, W0, H0, iters, **kw)
+    got = nmf_rs.nmf(V, W0.shape[1], method, W0=W0, H0=H0, max_iter=iters, **kw)
+    assert got.n_iter == ref["n_iter"]
+    assert rel_max(got.W, ref["W"]) <= FACTOR_TOL, rel_max(got.W, ref["W"])
+    assert rel_max(got.H, ref["H"]) <= FACTOR_TOL, rel_max(got.H, ref["H"])
+    if method == "offset":
+        assert got.offset is not None and got.offset.shape == (V.shape[0],)
+        assert rel_max(got.offset, ref["offset"]) <= FACTOR_TOL
+    else:
+        assert got.offset is None
+    theta = kw.get("theta", 0.5)
+    o_got = _objective(oracle, method, V, got.W, got.H, got.offset, theta)
+    o_ref = _objective(oracle, method, V, ref["W"], ref["H"], ref.get("offset"), theta)
+    assert _rel_obj(method, V, o_got, o_ref) <= OBJ_TOL
+    return got, ref
+
+
+def test_kat_offset_200(quickstart, kats):
+    V, W0, H0 = quickstart
+    res = nmf_rs.nmf(V, 5, "offset", W0=W0, H0=H0, max_iter=200)
+    assert round(float(np.linalg.norm(V - res.fitted())), 4) == kats["offset_200_frob_norm_4dp"]
+    lo, hi = kats["offset_200_range_2dp"]
+    assert round(float(res.offset.min()), 2) == lo and round(float(res.offset.max()), 2) == hi
+
+
+def test_kat_nsnmf_200(quickstart, kats):
+    V, W0, H0 = quickstart
+    res = nmf_rs.nmf(V, 5, "nsNMF", W0=W0, H0=H0, max_iter=200)
+    assert round(float(np.linalg.norm(V - res.fitted())), 4) == kats["nsnmf_200_frob_norm_4dp"]
+
+
+@pytest.mark.parametrize("method", ["offset", "nsNMF"])
+def test_quickstart_parity(oracle, quickstart, method):
+    V, W0, H0 = quickstart
+    _check(oracle, method, V, W0, H0, 100)
+
+
+@pytest.mark.parametrize("method", ["offset", "nsNMF"])
+@pytest.mark.parametrize("shape", [(300, 517, 7), (1, 40, 3), (64, 1, 2), (129, 257, 32)])
+def test_ragged_shapes(oracle, method, shape):
+    n, p, r = shape
+    V = synthetic.counts_matrix(n, p, max(1, r // 2), 0.3, seed=n + p)
+    V += 0.01  # keep every row sum positive (the offset update divides by it)
+    W0, H0 = nmf_rs.random_init(V, r, seed=3)
+    _check(oracle, method, V, W0, H0, 25)
+
+
+def test_offset_given_start(oracle, quickstart):
+    V, W0, H0 = quickstart
+    off0 = np.linspace(0.2, 1.3, V.shape[0])
+    got, ref = _check(oracle, "offset", V, W0, H0, 30, offset=off0)
+    assert not np.array_equal(got.offset, oracle.nmf_offset(V, W0, H0, 30)["offset"])
+
+
+@pytest.mark.parametrize("theta", [0.0, 0.25, 0.9])
+def test_nsnmf_theta(oracle, quickstart, theta):
+    V, W0, H0 = quickstart
+    _check(oracle, "nsNMF", V, W0, H0, 40, theta=theta)
+
+
+@pytest.mark.parametrize("method", ["offset", "nsNMF"])
+def test_stationary(oracle, quickstart, method):
+    V, W0, H0 = quickstart
+    kw = dict(stop="stationary", stationary_th=1e-6, check_interval=10, check_niter=5)
+    got, ref = _check(oracle, method, V, W0, H0, 300, **kw)
+    assert got.deviances.size == ref["deviances"].size == got.n_iter + 1
+    d = np.abs(got.deviances - ref["deviances"]) / np.abs(ref["deviances"])
+    assert d.max() <= 1e-10, d.max()
+
+
+@pytest.mark.parametrize("method", ["offset", "nsNMF"])
+@pytest.mark.parametrize("precision", ["fp32", "bf16x3"])
+def test_reduced_precision(oracle, method, precision):
+    V = synthetic.counts_matrix(700, 900, 6, 0.3, seed=11) + 0.01
+    W0, H0 = nmf_rs.random_init(V, 8, seed=5)
+    ref = oracle.nmf_method(method, V, W0, H0, 40)
+    got = nmf_rs.nmf(V, 8, method, W0=W0, H0=H0, max_iter=40, precision=precision)
+    o_ref = _objective(oracle, method, V, ref["W"], ref["H"], ref.get("offset"))
+    o_got = _objective(oracle, method, V, got.W, got.H, got.offset)
+    assert rel(o_got, o_ref) <= 1e-5, rel(o_got, o_ref)
+
+
+def test_offset_rejected_where_offsets_cannot_be_returned():
+    V = synthetic.counts_matrix(40, 50, 3, 0.3, seed=1)
+    W0, H0 = nmf_rs.random_init(V, 3, seed=1)
+    with nmf_rs.serve.Server(slots=1) as srv:
+        with pytest.raises(NotImplementedError, match="nmfcu_run_offset"):
+            srv.submit(V, 3, "offset", W0=W0, H0=H0, max_iter=5)
+        ok = srv.submit(V, 3, "nsNMF", W0=W0, H0=H0, max_iter=5).result(timeout=120)
+    assert ok.n_iter == 5

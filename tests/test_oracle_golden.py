@@ -39,6 +39,46 @@ def test_lee_200_norm(oracle, quickstart, kats):
     assert round(norm, 4) == kats["lee_200_frob_norm_4dp"]
 
 
+def test_offset_200_kat(oracle, quickstart, kats):
+    # The notebook prints ||V - fitted()|| with fitted() = W H + offset.
+    V, W0, H0 = quickstart
+    res = oracle.nmf_method("offset", V, W0, H0, 200)
+    fitted = res["W"] @ res["H"] + res["offset"][:, None]
+    assert round(float(np.linalg.norm(V - fitted)), 4) == kats["offset_200_frob_norm_4dp"]
+    lo, hi = kats["offset_200_range_2dp"]
+    assert round(float(res["offset"].min()), 2) == lo
+    assert round(float(res["offset"].max()), 2) == hi
+
+
+def test_nsnmf_200_kat(oracle, quickstart, kats):
+    # fitted() is W H for nsNMF (no smoothing matrix).
+    V, W0, H0 = quickstart
+    res = oracle.nmf_method("nsNMF", V, W0, H0, 200)
+    assert round(float(np.linalg.norm(V - res["W"] @ res["H"])), 4) == \
+        kats["nsnmf_200_frob_norm_4dp"]
+
+
+def test_offset_default_is_row_means(oracle, quickstart):
+    V, W0, H0 = quickstart
+    a = oracle.nmf_offset(V, W0, H0, 5)
+    b = oracle.nmf_offset(V, W0, H0, 5, offset=np.cumsum(V, axis=1)[:, -1] / V.shape[1])
+    np.testing.assert_array_equal(a["W"], b["W"])
+    np.testing.assert_array_equal(a["offset"], b["offset"])
+
+
+def test_offset_nsnmf_stationary_deviances(oracle, quickstart):
+    V, W0, H0 = quickstart
+    res = oracle.nmf_offset(V, W0, H0, 20, stop="stationary", check_interval=5, check_niter=2)
+    d = res["deviances"]
+    assert d.size == res["n_iter"] + 1
+    assert d[-1] == oracle.euclidean_distance_offset(V, res["W"], res["H"], res["offset"])
+    assert np.all(np.diff(d) <= 1e-9 * d[0])  # the offset updates do not raise the loss
+    res = oracle.nmf_nsnmf(V, W0, H0, 20, stop="stationary", check_interval=5, check_niter=2)
+    S = np.full((5, 5), 0.1) + 0.5 * np.eye(5)
+    assert res["deviances"].size == res["n_iter"] + 1
+    assert rel(res["deviances"][-1], oracle.kl_divergence(V, res["W"] @ S, res["H"])) < 1e-12
+
+
 def test_brunet_stationary_kat(oracle, quickstart, kats):
     V, W0, H0 = quickstart
     k = kats["brunet_stationary"]
@@ -63,7 +103,7 @@ def test_single_step_delta_kl(oracle, quickstart, kats):
     assert rel(kl(W0, H0) - kl(W1, H1), kats["single_step_brunet_delta_kl"]) < 1e-13
 
 
-@pytest.mark.parametrize("method", ["brunet", "lee", "hals", "dnmf"])
+@pytest.mark.parametrize("method", ["brunet", "lee", "offset", "nsNMF", "hals", "dnmf"])
 def test_thread_count_independent(oracle, quickstart, method):
     V, W0, H0 = quickstart
     a = oracle.nmf_method(method, V, W0, H0, 30, num_threads=1)
