@@ -202,6 +202,21 @@ nmfcu_status nmfcu_run_device(nmfcu_context *ctx, const nmfcu_options *opt, int6
                               double *dH, double *d_dev, int64_t *n_deviances, int64_t *n_iter,
                               void *stream);
 
+/*
+ * nmfcu_v_product_device -- one V contraction of the randomized range finder
+ * behind nndsvd_init (python/nmf_rs/__init__.py:129-219, which calls
+ * scikit-learn's randomized_svd at :172-174; its products A @ Q, A.T @ Q and
+ * Q.T @ A are these two with A = V or V^T):
+ *   trans = 0:  out (n x l) = V X,    X (p x l)
+ *   trans = 1:  out (p x l) = V^T X,  X (n x l)
+ * All device pointers, f64, row-major, leading dimensions ldv / ldx / ldo,
+ * enqueued on `stream`; returns once the product is complete.  One FP64
+ * streaming pass over V per 32 columns of X.
+ */
+nmfcu_status nmfcu_v_product_device(nmfcu_context *ctx, int32_t trans, int64_t n, int64_t p,
+                                    int64_t l, const double *dV, int64_t ldv, const double *dX,
+                                    int64_t ldx, double *dOut, int64_t ldo, void *stream);
+
 /* Per-kernel CUDA-event timing inside nmfcu_run_device (off by default).
  * Kernel classes: 0 = H-step V contraction, 1 = W-step V contraction,
  * 2 = objective V pass, 3 = everything else (grams, epilogues, stop),

@@ -27,6 +27,9 @@ namespace nmfcu {
 
 // Method ids, same values as include/nmfcu.h.
 enum : int { M_BRUNET = 0, M_LEE = 1, M_OFFSET = 2, M_NSNMF = 3, M_HALS = 4, M_DNMF = 6 };
+// Not a method: the epilogues store the contraction itself (the products of
+// the randomized range finder behind the NNDSVD start).
+constexpr int M_PRODUCT = 100;
 
 // Device-side state of the stationary stop (lib.rs:1336-1401) and of the
 // run: written by single-thread kernels, read by every kernel of an
@@ -428,7 +431,11 @@ struct EpiParams {
 template <int RP>
 __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, double *hc) {
     const int r = e.r;
-    if (e.method == M_LEE || e.method == M_OFFSET) {
+    if (e.method == M_PRODUCT) {
+#pragma unroll
+        for (int i = 0; i < RP; i++)
+            if (i < r) hc[i] = num[i];
+    } else if (e.method == M_LEE || e.method == M_OFFSET) {
         // offset (offset_update_h_inner, lib.rs:330-361): + (W^T off)[i]
         double out[RP];
 #pragma unroll
@@ -478,7 +485,11 @@ template <int RP>
 __device__ __forceinline__ void w_update(const EpiParams &e, const double *num, double *wr,
                                          double ro = 0.0) {
     const int r = e.r;
-    if (e.method == M_LEE || e.method == M_OFFSET) {
+    if (e.method == M_PRODUCT) {
+#pragma unroll
+        for (int j = 0; j < RP; j++)
+            if (j < r) wr[j] = num[j];
+    } else if (e.method == M_LEE || e.method == M_OFFSET) {
         double out[RP];
 #pragma unroll
         for (int j = 0; j < RP; j++) {

@@ -1103,6 +1103,44 @@ bool ieq(const char *a, const char *b) {
     return *a == 0 && *b == 0;
 }
 
+// Waits for the stream and reports a streaming kernel that gave up waiting
+// for its copies (the device state's timeout flag).
+nmfcu_status finish_checked(nmfcu_context *c, cudaStream_t s) {
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c->h_state, c->state.ptr, sizeof(RunState), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (c->h_state->timeout != 0)
+        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies (code " +
+                                           std::to_string(c->h_state->timeout) + ")");
+    return NMFCU_OK;
+}
+
+// Columns [c0, c0 + kc) of X (rows x ldx) into out (rows x ld, zero padded).
+__global__ void pack_cols(const double *__restrict__ X, int64_t ldx, int rows, int c0, int kc,
+                          double *__restrict__ out, int ld) {
+    const int64_t total = (int64_t)rows * ld;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / ld;
+        const int k = (int)(t - i * ld);
+        out[t] = (k < kc) ? X[i * ldx + c0 + k] : 0.0;
+    }
+}
+// Rows [0, kc) of H (RP x p) into columns [c0, c0 + kc) of out (p x ldo).
+__global__ void unpack_rows_t(const double *__restrict__ H, int p, int kc, double *__restrict__ out,
+                              int64_t ldo, int c0) {
+    const int64_t total = (int64_t)p * kc;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = t / kc;
+        const int k = (int)(t - j * kc);
+        out[j * ldo + c0 + k] = H[(int64_t)k * p + j];
+    }
+}
+unsigned grid_for(int64_t total) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, kThreads), 4096));
+}
+
 // Single-step driver used by the four update entry points.
 enum StepKind { STEP_H_KL, STEP_W_KL, STEP_H_EUC, STEP_W_EUC };
 
@@ -1162,11 +1200,7 @@ nmfcu_status single_step(StepKind kind, int64_t n, int64_t p, int64_t r, const d
             NMF_TRY(get_factors(c, pl, out, nullptr, cudaMemcpyDeviceToHost, s));
             break;
     }
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(s));
-    if (c->h_state->timeout != 0)
-        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies");
-    return NMFCU_OK;
+    return finish_checked(c, s);
 }
 
 nmfcu_status objective_host(bool kl, int64_t n, int64_t p, int64_t r, const double *V,
@@ -1604,6 +1638,87 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     *n_deviances = nd;
     *n_iter = ni;
     return NMFCU_OK;
+}
+
+nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, int64_t p,
+                                    int64_t l, const double *dV, int64_t ldv, const double *dX,
+                                    int64_t ldx, double *dOut, int64_t ldo, void *stream) {
+    if (!c) return fail(NMFCU_ERR_INVALID_ARG, "NULL context");
+    if (trans != 0 && trans != 1) return fail(NMFCU_ERR_INVALID_ARG, "trans must be 0 or 1");
+    if (n < 0 || p < 0 || l < 0) return fail(NMFCU_ERR_INVALID_ARG, "negative dimension");
+    if (n > INT32_MAX || p > INT32_MAX)
+        return fail(NMFCU_ERR_UNSUPPORTED, "n and p must each fit in 32 bits");
+    if (ldv < p || ldx < l || ldo < l)
+        return fail(NMFCU_ERR_INVALID_ARG, "leading dimensions must be >= the row lengths");
+    const int64_t xrows = trans ? n : p, orows = trans ? p : n;
+    if (l == 0 || orows == 0) return NMFCU_OK;
+    if (!dOut || (xrows > 0 && (!dV || !dX))) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (xrows == 0) {  // an empty sum: the product is zero
+        CUDA_TRY(cudaMemset2DAsync(dOut, ldo * 8, 0, l * 8, orows, s));
+        return finish_checked(c, s);
+    }
+    // TMA needs a 16-byte aligned base and row pitch: otherwise V is copied
+    // into the context's pitched buffer once for all column chunks.
+    if (!tma_layout_ok(dV, ldv, 8)) {
+        const int64_t ld = std::max<int64_t>(16, round_up(p, 16));
+        NMF_TRY(c->V64.ensure(sizeof(double) * (size_t)(n * ld)));
+        CUDA_TRY(cudaMemcpy2DAsync(c->V64.ptr, ld * 8, dV, ldv * 8, p * 8, n,
+                                   cudaMemcpyDeviceToDevice, s));
+        dV = c->V64.as<double>();
+        ldv = ld;
+    }
+    nmfcu_options o;
+    nmfcu_options_default(&o);
+    o.method = NMFCU_LEE;
+    CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
+    // Column chunks of at most the largest built rank; each is one pass over V.
+    for (int64_t c0 = 0; c0 < l; c0 += NMFCU_MAX_RANK) {
+        const int kc = (int)std::min<int64_t>(NMFCU_MAX_RANK, l - c0);
+        const Plan pl = make_plan(n, p, kc, c->sms);
+        NMF_TRY(ensure_workspace(c, pl, false));
+        RunArgs a;
+        a.opt = &o;
+        a.pl = pl;
+        a.ops = ops_for(pl.RP);
+        NMF_TRY(make_passset(c, pl, false, false, dV, ldv, &a.p64));
+        a.main = a.p64;
+        a.V64 = dV;
+        a.ldv64 = ldv;
+        a.W = c->W.as<double>();
+        a.H = c->H.as<double>();
+        a.dev = nullptr;
+        EpiParams e = epi(&o, kc, nullptr, nullptr, trans != 0);
+        e.method = nmfcu::M_PRODUCT;
+        if (trans) {
+            // V^T X: X's columns as the H pass's W (n x RP); the product lands
+            // in H (RP x p) and is transposed out.
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                pack_cols<<<grid_for(n * pl.RP), kThreads, 0, s>>>(dX, ldx, (int)n, (int)c0, kc,
+                                                                   a.W, pl.RP);
+            }
+            NMF_TRY(h_step(c, a, a.p64, e, false, s));
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            unpack_rows_t<<<grid_for(p * kc), kThreads, 0, s>>>(a.H, (int)p, kc, dOut, ldo,
+                                                                (int)c0);
+        } else {
+            // V X: X's columns as the W pass's H^T (p x rps); the product lands
+            // in W (n x RP).
+            const int rps = a.p64.so->rps();
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                pack_cols<<<grid_for(p * rps), kThreads, 0, s>>>(
+                    dX, ldx, (int)p, (int)c0, kc, static_cast<double *>(a.p64.Ht), rps);
+            }
+            NMF_TRY(w_step(c, a, a.p64, e, false, s));
+            CUDA_TRY(cudaMemcpy2DAsync(dOut + c0, ldo * 8, a.W, (size_t)pl.RP * 8, (size_t)kc * 8,
+                                       n, cudaMemcpyDeviceToDevice, s));
+        }
+    }
+    return finish_checked(c, s);
 }
 
 nmfcu_status nmfcu_context_set_timing(nmfcu_context *ctx, int32_t enabled) {

@@ -99,55 +99,33 @@ def random_init(V: np.ndarray, rank: int, seed: Optional[int] = None, *,
 
 
 def nndsvd_init(V: np.ndarray, rank: int, *, fill: str = "mean", seed: int = 0,
-                n_oversamples: int = 10) -> tuple[np.ndarray, np.ndarray]:
+                n_oversamples: int = 10, device: int = 0) -> tuple[np.ndarray, np.ndarray]:
     """NNDSVD start (Boutsidis & Gallopoulos 2008, "SVD based initialization:
-    A head start for nonnegative matrix factorization").
+    A head start for nonnegative matrix factorization"), the reference's
+    ``nndsvd_init`` (python/nmf_rs/__init__.py:129-219).
 
-    A rank-``rank`` randomized SVD of V (scikit-learn's ``randomized_svd``
-    with ``random_state=seed``) is turned into non-negative factors: the
+    A rank-``rank`` randomized SVD of V -- the algorithm of scikit-learn's
+    ``randomized_svd`` with ``random_state=seed``, its passes over V on the
+    GPU (``nmf_rs.nndsvd``) -- is turned into non-negative factors: the
     leading pair by absolute value, every later pair by keeping whichever
     sign-split half (u+, v+) or (u-, v-) has the larger norm product, scaled
     to carry sqrt(sigma * that product).  Zeros are then kept (``'zero'``),
     raised to 1e-9 (``'eps'``) or replaced by mean(V) (``'mean'``, NNDSVDa).
+    ``device`` (engine extension) selects the GPU.
     """
-    try:
-        from sklearn.utils.extmath import randomized_svd
-    except ImportError as exc:  # pragma: no cover - sklearn is in the image
-        raise ImportError("nndsvd_init() requires scikit-learn") from exc
     V = np.asarray(V, dtype=np.float64)
     if (V < 0).any():
         raise ValueError("V must be non-negative for NNDSVD initialisation.")
     if fill not in ("zero", "mean", "eps"):
         raise ValueError(f"unknown fill mode '{fill}': supported zero / mean / eps")
-    U, S, Vt = randomized_svd(V, n_components=rank, n_oversamples=n_oversamples,
-                              random_state=seed)
-    n, p = V.shape
-    W = np.zeros((n, rank))
-    H = np.zeros((rank, p))
-    root = np.sqrt(S[0])
-    W[:, 0] = root * np.abs(U[:, 0])
-    H[0, :] = root * np.abs(Vt[0, :])
-    for k in range(1, rank):
-        halves = []
-        for sgn in (1.0, -1.0):
-            uh = np.maximum(sgn * U[:, k], 0.0)
-            vh = np.maximum(sgn * Vt[k, :], 0.0)
-            nu, nv = np.linalg.norm(uh), np.linalg.norm(vh)
-            halves.append((nu * nv, uh, vh, nu, nv))
-        # The positive half wins ties.
-        prod, uh, vh, nu, nv = halves[0] if halves[0][0] >= halves[1][0] else halves[1]
-        if prod > 0:
-            scale = np.sqrt(S[k] * prod)
-            W[:, k] = scale * uh / nu
-            H[k, :] = scale * vh / nv
-    if fill == "eps":
-        W[W < 1e-9] = 1e-9
-        H[H < 1e-9] = 1e-9
-    elif fill == "mean":
-        mean = float(V.mean()) if V.size else 0.0
-        W[W <= 0.0] = mean
-        H[H <= 0.0] = mean
-    return W, H
+    if _native.device_count() < 1:
+        raise RuntimeError("nndsvd_init() runs its passes over V on a CUDA device; none is visible")
+    from . import nndsvd
+
+    Vd = nndsvd.upload(V, int(device))
+    W, H = nndsvd.nndsvd_device(Vd, int(rank), fill=fill, seed=int(seed),
+                                n_oversamples=int(n_oversamples))
+    return W.cpu().numpy(), H.cpu().numpy()
 
 
 # =============================================================================

@@ -97,6 +97,9 @@ SIGNATURES = {
                                 ctypes.c_void_p, _i32, _i64, ctypes.c_void_p, _i64,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64p, _i64p,
                                 ctypes.c_void_p]),
+    "nmfcu_v_product_device": (_i32, [ctypes.c_void_p, _i32, _i64, _i64, _i64, ctypes.c_void_p,
+                                      _i64, ctypes.c_void_p, _i64, ctypes.c_void_p, _i64,
+                                      ctypes.c_void_p]),
     "nmfcu_context_set_timing": (_i32, [ctypes.c_void_p, _i32]),
     "nmfcu_context_kernel_time": (_i32, [ctypes.c_void_p, _i32, _i64p,
                                          ctypes.POINTER(ctypes.c_double)]),
@@ -408,6 +411,13 @@ class Context:
             ctypes.c_void_p(h_ptr), ctypes.c_void_p(dev_ptr or None), ctypes.byref(nd),
             ctypes.byref(ni), ctypes.c_void_p(stream or None)))
         return int(ni.value), int(nd.value)
+
+    def v_product(self, trans: int, n: int, p: int, l: int, v_ptr: int, ldv: int, x_ptr: int,
+                  ldx: int, out_ptr: int, ldo: int, stream: int = 0):
+        """out = V X (trans 0) or V^T X (trans 1) on device pointers."""
+        check(self._lib.nmfcu_v_product_device(
+            self.handle, int(trans), n, p, l, ctypes.c_void_p(v_ptr), ldv, ctypes.c_void_p(x_ptr),
+            ldx, ctypes.c_void_p(out_ptr), ldo, ctypes.c_void_p(stream or None)))
 
     def set_timing(self, on: bool):
         check(self._lib.nmfcu_context_set_timing(self.handle, int(bool(on))))
