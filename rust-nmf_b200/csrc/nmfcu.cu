@@ -1658,7 +1658,8 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, 
     cudaStream_t s = (cudaStream_t)stream;
     if (xrows == 0) {  // an empty sum: the product is zero
         CUDA_TRY(cudaMemset2DAsync(dOut, ldo * 8, 0, l * 8, orows, s));
-        return finish_checked(c, s);
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return NMFCU_OK;
     }
     // TMA needs a 16-byte aligned base and row pitch: otherwise V is copied
     // into the context's pitched buffer once for all column chunks.
@@ -1673,12 +1674,12 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, 
     nmfcu_options o;
     nmfcu_options_default(&o);
     o.method = NMFCU_LEE;
-    CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
     // Column chunks of at most the largest built rank; each is one pass over V.
     for (int64_t c0 = 0; c0 < l; c0 += NMFCU_MAX_RANK) {
         const int kc = (int)std::min<int64_t>(NMFCU_MAX_RANK, l - c0);
         const Plan pl = make_plan(n, p, kc, c->sms);
-        NMF_TRY(ensure_workspace(c, pl, false));
+        NMF_TRY(ensure_workspace(c, pl, false));  // allocates the device state too
+        if (c0 == 0) CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
         RunArgs a;
         a.opt = &o;
         a.pl = pl;

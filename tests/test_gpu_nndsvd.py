@@ -93,8 +93,9 @@ def test_nndsvd_matches_reference(golden, name):
 
 def test_nndsvd_large_against_cpu_products():
     # 3000 x 5000, rank 20: the device passes against the same host logic on
-    # CPU torch products.
-    V = synthetic.counts_matrix(3000, 5000, 10, 0.3, seed=21)
+    # CPU torch products.  No all-zero row (there the factors' entries are
+    # rounding noise whose sign picks between the fill and ~1e-16).
+    V = synthetic.counts_matrix(3000, 5000, 30, 0.3, seed=21) + 0.01
     Vt = torch.from_numpy(V)
     W_ref, H_ref = nndsvd.nndsvd_device(
         Vt, 20, fill="mean", seed=0,
