@@ -26,6 +26,13 @@ requests (shapes log-uniform 500x1000 .. 5000x50000, rank U{5..30}, methods
 lee 40% / brunet 30% / hals 20% / dnmf 10%, 25..200 iterations, FP32 form)
 through nmfcu_server_*, reporting p50/p99 latency and aggregate iters/s.
 
+--form nndsvd measures the NNDSVD start (nmf_rs.nndsvd_init, the reference's
+nndsvd_init over scikit-learn's randomized_svd) at the atlas shape: one step
+= one rank-20 NNDSVD of V with its 16 FP64 passes over V on the device
+(nmfcu_v_product_device) and the small factorizations on the device;
+cpu_baseline = scikit-learn's randomized_svd (the reference's own call) on a
+column slice of the same V.
+
 --form consensus measures the batching form instead: a consensus sweep of
 64 brunet restarts x ranks 2..10 (576 solves x 200 iterations) on a
 2000 x 5000 V, one step = one whole sweep through nmfcu_run_batch_device
@@ -76,7 +83,8 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--form", choices=["iterate", "consensus", "serve"], default="iterate")
+    ap.add_argument("--form", choices=["iterate", "consensus", "serve", "nndsvd"],
+                    default="iterate")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="serve: server slots")
     ap.add_argument("--load", type=float, default=0.8,
@@ -977,11 +985,178 @@ def run_serve(args, world, rank, local):
         }), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# NNDSVD start
+# ---------------------------------------------------------------------------
+
+FP64_PEAK_TFLOPS = 37.0  # B200 nominal dense FP64 (CUDA-core FMA and DMMA alike)
+
+
+def nndsvd_passes(n, p, rank, over=10):
+    """Passes over V of one randomized SVD (power iterations x 2, the final
+    range product, the projection), and the test-vector count."""
+    l = rank + over
+    n_iter = 7 if rank < 0.1 * min(n, p) else 4
+    return 2 * n_iter + 2, l
+
+
+def nndsvd_cpu_baseline(n, k, alpha, rank, p_full, seconds, seed=0):
+    """scikit-learn's randomized_svd -- the call the reference's nndsvd_init
+    makes (python/nmf_rs/__init__.py:172-174) -- on all rows x a column
+    slice, extrapolated linearly in columns (each pass over V is linear in
+    p); the O((n + p) rank) post-processing is left out of the sample."""
+    from sklearn.utils.extmath import randomized_svd
+
+    from nmf_rs import synthetic
+
+    p_s = 1024
+    for _ in range(6):
+        V = synthetic.counts_matrix(n, p_s, k, alpha, seed=seed)
+        t0 = time.perf_counter()
+        randomized_svd(V, n_components=rank, n_oversamples=10, random_state=0)
+        dt = time.perf_counter() - t0
+        if dt > seconds / 4 or p_s >= p_full:
+            break
+        p_s = int(min(p_full, max(p_s * 2, p_s * (seconds / 2) / max(dt, 1e-3))))
+    t_full = dt * p_full / p_s
+    return {"value": 1.0 / t_full, "unit": "starts/s", "cores": os.cpu_count() or 1,
+            "kind": "reference",
+            "sample": (f"scikit-learn {__import__('sklearn').__version__} randomized_svd "
+                       f"(rank {rank}, 10 oversamples, numpy BLAS threads) on {n} rows x {p_s} "
+                       f"of {p_full} columns took {dt:.2f} s; extrapolated linearly in columns")}
+
+
+def run_nndsvd_reference(args, world, rank):
+    if rank != 0:
+        return
+    n, p, k, alpha, r, _ = WORKLOADS[args.workload]
+    vals = []
+    base = None
+    for _ in range(max(1, min(args.steps or 2, 3))):
+        base = nndsvd_cpu_baseline(n, k, alpha, r, p, args.cpu_seconds / 2)
+        vals.append(base["value"])
+    value = statistics.median(vals)
+    print(json.dumps({
+        "impl": "reference",
+        "metric": f"NNDSVD starts/s, {args.workload} {n}x{p} rank {r}",
+        "value": value, "unit": "starts/s", "n_gpus": args.gpus, "steps": len(vals),
+        "warmup": 0, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, column slice)",
+        "config": {"workload": args.workload, "n": n, "p": p, "rank": r, "form": "nndsvd"},
+        "cpu_baseline": {**base, "value": value},
+        "e2e": {"value": value, "unit": "starts/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_nndsvd(args, world, rank, local):
+    import torch
+
+    import nmf_rs
+    from nmf_rs import _native, nndsvd
+
+    n, p, k, alpha, r, _ = WORKLOADS[args.workload]
+    steps = args.steps or 5
+    warm = max(3, args.warmup)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    V64, ld64, V32, ld32, _, _ = device_workload(n, p, k, alpha, r, 1234 + rank, dev)
+    del V32
+    torch.cuda.empty_cache()
+    V = V64[:, :p]
+    ctx = nndsvd._context(local)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(warm):
+        nndsvd.nndsvd_device(V, r, fill="mean", seed=0)
+    torch.cuda.synchronize()
+    ctx.reset_timing()
+    ctx.set_timing(True)
+    launches0 = ctx.launch_count()
+    barrier(world)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            W, H = nndsvd.nndsvd_device(V, r, fill="mean", seed=0)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    clocks = clk.summary()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    launches = ctx.launch_count() - launches0
+    hk = ctx.kernel_time(_native.KCLASS_HSTEP)
+    wk = ctx.kernel_time(_native.KCLASS_WSTEP)
+    ctx.set_timing(False)
+    value = world * steps / (ms / 1000.0)
+    passes, l = nndsvd_passes(n, p, r)
+    peak, peak_kind = measured_peaks()
+    nl = hk[0] + wk[0]
+    avg_ms = (hk[1] + wk[1]) / max(nl, 1)
+    bytes_launch = n * p * 8
+    achieved = bytes_launch / (avg_ms / 1000.0) / 1e9
+    flops_launch = 2.0 * n * p * l
+    roof = {
+        "bound": "hbm", "kernel": "hpass/wpass (FP64, V product)", "achieved": achieved,
+        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+        "traffic": PASS_DRAM_BYTES_PER_ELEMENT[("hpass", "fp64")] * n * p
+        if args.workload in ("atlas", "atlas-slice") else None,
+        "traffic_note": "the FP64 H pass's ncu DRAM bytes per V element (rank-20 capture), "
+                        "scaled to n x p",
+        "launches": nl, "avg_launch_ms": avg_ms, "algorithmic_bytes_per_launch": bytes_launch,
+        "passes_per_step": passes, "test_vectors": l,
+        "fp64_flops_per_launch": flops_launch,
+        "fp64_tflops": flops_launch / (avg_ms / 1000.0) / 1e12,
+        "fp64_frac_of_nominal": flops_launch / (avg_ms / 1000.0) / 1e12 / FP64_PEAK_TFLOPS,
+        "pass_ms_of_step": (hk[1] + wk[1]) / steps,
+    }
+    e2e = None
+    if not args.no_e2e:
+        V_host = torch.empty((n, p), dtype=torch.float64, pin_memory=True)
+        V_host.copy_(V)
+        Vh = V_host.numpy()
+        del V64, V
+        torch.cuda.empty_cache()
+        nmf_rs.nndsvd_init(Vh[:, :256], r, fill="mean", seed=0, device=local)  # warm-up
+        barrier(world)
+        t0 = time.perf_counter()
+        Wh, Hh = nmf_rs.nndsvd_init(Vh, r, fill="mean", seed=0, device=local)
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+        e2e = {"value": world / t_e2e, "unit": "starts/s", "h2d_bytes_per_step": n * p * 8,
+               "d2h_bytes_per_step": (n + p) * r * 8,
+               "note": "nmf_rs.nndsvd_init on a host V: upload, the start, W0/H0 read back"}
+        del V_host
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = nndsvd_cpu_baseline(n, k, alpha, r, p, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"NNDSVD starts/s, {args.workload} {n}x{p} rank {r}",
+            "value": value, "unit": "starts/s", "n_gpus": world, "steps": steps,
+            "warmup": warm, "ms_per_step": ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded single-cell-like generator on the device)",
+            "config": {"workload": args.workload, "n": n, "p": p, "rank": r, "form": "nndsvd",
+                       "fill": "mean", "n_oversamples": 10,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "V is larger than L2 (no flush needed)"},
+            "gpu_launches": launches, "clocks": clocks, "roofline": roof,
+            "cpu_baseline": cpu, "e2e": e2e,
+        }), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
     try:
-        if args.form == "serve":
+        if args.form == "nndsvd":
+            if args.impl == "reference":
+                run_nndsvd_reference(args, world, rank)
+            else:
+                run_nndsvd(args, world, rank, local)
+        elif args.form == "serve":
             if args.impl == "reference":
                 run_serve_reference(args, world, rank)
             else:

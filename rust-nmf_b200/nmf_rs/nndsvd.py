@@ -163,15 +163,31 @@ def nndsvd_factors(V, U, S, Vt, fill: str):
     return W, H
 
 
+class _Cusolver:
+    """torch.linalg on CUDA through cuSOLVER for the scope (its default
+    backend choice may pick MAGMA's batched routines for these tall, narrow
+    factorizations); the caller's choice is restored on exit."""
+
+    def __enter__(self):
+        torch = _torch()
+        self.prev = torch.backends.cuda.preferred_linalg_library()
+        torch.backends.cuda.preferred_linalg_library("cusolver")
+
+    def __exit__(self, *exc):
+        _torch().backends.cuda.preferred_linalg_library(self.prev)
+        return False
+
+
 def nndsvd_device(V, rank: int, *, fill: str = "mean", seed: int = 0,
                   n_oversamples: int = 10, product: Optional[Callable] = None):
     """NNDSVD of a device-resident V (f64 torch tensor, n x p).  Returns
     (W0, H0) as torch tensors on V's device."""
     if fill not in ("zero", "mean", "eps"):
         raise ValueError(f"unknown fill mode '{fill}': supported zero / mean / eps")
-    U, S, Vt = randomized_svd(V, int(rank), n_oversamples=int(n_oversamples), seed=int(seed),
-                              product=product)
-    return nndsvd_factors(V, U, S, Vt, fill)
+    with _Cusolver():
+        U, S, Vt = randomized_svd(V, int(rank), n_oversamples=int(n_oversamples),
+                                  seed=int(seed), product=product)
+        return nndsvd_factors(V, U, S, Vt, fill)
 
 
 def upload(V: np.ndarray, device: int = 0):
