@@ -50,9 +50,9 @@ enum {
     NMFCU_OFFSET = 2, /* through nmfcu_run / nmfcu_run_offset (host buffers) */
     NMFCU_NSNMF = 3,
     NMFCU_HALS = 4,
-    NMFCU_EHALS = 5, /* not built: NMFCU_ERR_UNSUPPORTED */
+    NMFCU_EHALS = 5,
     NMFCU_DNMF = 6,
-    NMFCU_LSNMF = 7,  /* not built */
+    NMFCU_LSNMF = 7,  /* not built: NMFCU_ERR_UNSUPPORTED */
     NMFCU_SNMF_R = 8, /* not built */
     NMFCU_SNMF_L = 9  /* not built */
 };
@@ -66,7 +66,7 @@ enum { NMFCU_STOP_MAX_ITER = 0, NMFCU_STOP_STATIONARY = 1 };
  *             reduction across threads, all update epilogues, Gram matrices,
  *             rescaling, objective and stop test stay f64, and the last
  *             `refine_iters` iterations run the FP64 path on the f64 V.
- *   BF16X3 -- lee / offset / hals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
+ *   BF16X3 -- lee / offset / hals / ehals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
  *             an element), the factor of each contraction split into three
  *             bf16 terms, products on the tensor cores with f32 sums of at
  *             most 2048 terms; everything else as FP32.  brunet and nsNMF
@@ -107,9 +107,10 @@ nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop);
 
 /*
  * nmfcu_run -- replaces py_nmf_run (lib.rs:1934-2169) for brunet, lee,
- * offset, nsNMF, hals and dnmf: the whole iteration loop (nmf_run_brunet
- * :1529-1586, nmf_run_lee :1589-1647, nmf_run_offset :1650-1760,
- * nmf_run_nsnmf :1762-1830, nmf_run_hals :638-688, nmf_run_dnmf :827-906).
+ * offset, nsNMF, hals, ehals and dnmf: the whole iteration loop
+ * (nmf_run_brunet :1529-1586, nmf_run_lee :1589-1647, nmf_run_offset
+ * :1650-1760, nmf_run_nsnmf :1762-1830, nmf_run_hals :638-688,
+ * nmf_run_ehals :711-786, nmf_run_dnmf :827-906).
  * For offset it starts from rowMeans(V) and drops the final offsets; use
  * nmfcu_run_offset to pass and receive them.
  *

@@ -3,7 +3,7 @@
 A ctypes wrapper around ``liboracle.so`` (built from ``nmf_oracle.c`` by
 ``oracle/Makefile``), which restates the f64 loops of omicverse/rust-NMF
 ``rust/src/lib.rs`` (brunet :1529-1586, lee :1589-1647, offset :1650-1760,
-nsNMF :1762-1830, hals :638-688, dnmf :827-906, objectives :1410-1445,
+nsNMF :1762-1830, hals :638-688, ehals :711-786, dnmf :827-906, objectives :1410-1445,
 stationary stop :1336-1401).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
@@ -26,7 +26,7 @@ _HERE = Path(__file__).resolve().parent
 _LIB_PATH = _HERE / "liboracle.so"
 _lib = None
 
-METHODS = {"brunet": 0, "lee": 1, "hals": 4, "dnmf": 6}
+METHODS = {"brunet": 0, "lee": 1, "hals": 4, "ehals": 5, "dnmf": 6}
 STOPS = {"max_iter": 0, "fixed": 0, "none": 0, "stationary": 1}
 
 _i64 = ctypes.c_int64

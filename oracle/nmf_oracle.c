@@ -32,7 +32,7 @@
 #endif
 
 /* Method ids: same numbering as include/nmfcu.h. */
-enum { ORC_BRUNET = 0, ORC_LEE = 1, ORC_HALS = 4, ORC_DNMF = 6 };
+enum { ORC_BRUNET = 0, ORC_LEE = 1, ORC_HALS = 4, ORC_EHALS = 5, ORC_DNMF = 6 };
 enum { ORC_STOP_MAX_ITER = 0, ORC_STOP_STATIONARY = 1 };
 
 typedef int64_t i64;
@@ -436,9 +436,9 @@ void orc_update_w_lee(i64 n, i64 p, i64 r, const double *v, const double *w, con
 }
 
 /*
- * orc_nmf_run: the full loop for brunet / lee / hals / dnmf.
+ * orc_nmf_run: the full loop for brunet / lee / hals / ehals / dnmf.
  *   nmf_run_brunet lib.rs:1529-1586, nmf_run_lee :1589-1647,
- *   nmf_run_hals :638-688, nmf_run_dnmf :827-906.
+ *   nmf_run_hals :638-688, nmf_run_ehals :711-786, nmf_run_dnmf :827-906.
  * W (n x r) and H (r x p) hold W0/H0 on entry and the result on exit.
  * dev must hold max_iter + 1 doubles.  Returns 0, or -1 for an unknown
  * method, -2 when the stationary stop evaluates `i % 0` (the reference
@@ -449,7 +449,8 @@ int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, dou
                 double smoothness_h, double smoothness_w, int stop, double stationary_th,
                 i64 check_interval, i64 check_niter, double *dev, i64 *n_dev, i64 *n_iter,
                 int nt) {
-    if (method != ORC_BRUNET && method != ORC_LEE && method != ORC_HALS && method != ORC_DNMF)
+    if (method != ORC_BRUNET && method != ORC_LEE && method != ORC_HALS && method != ORC_EHALS &&
+        method != ORC_DNMF)
         return -1;
     set_threads(nt);
     stationary_t st = {check_interval, check_niter, stationary_th, -INFINITY, INFINITY, 0};
@@ -465,12 +466,20 @@ int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, dou
     double *sq2 = (double *)malloc(sizeof(double) * (size_t)(r * r > 0 ? r * r : 1));
     double *sum_w = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
     double *dg = (double *)malloc(sizeof(double) * (size_t)(r > 0 ? r : 1));
-    double *wtv = (method == ORC_HALS || method == ORC_DNMF)
+    double *wtv = (method == ORC_HALS || method == ORC_EHALS || method == ORC_DNMF)
                       ? (double *)malloc(sizeof(double) * (size_t)(r * p > 0 ? r * p : 1))
                       : NULL;
-    double *vht = (method == ORC_HALS || method == ORC_DNMF)
+    double *vht = (method == ORC_HALS || method == ORC_EHALS || method == ORC_DNMF)
                       ? (double *)malloc(sizeof(double) * (size_t)(n * r > 0 ? n * r : 1))
                       : NULL;
+    /* ehals: the previous iterate, initially the start (lib.rs:743-744). */
+    double *w_prev = NULL, *h_prev = NULL;
+    if (method == ORC_EHALS) {
+        w_prev = (double *)malloc(sizeof(double) * (size_t)(n * r > 0 ? n * r : 1));
+        h_prev = (double *)malloc(sizeof(double) * (size_t)(r * p > 0 ? r * p : 1));
+        memcpy(w_prev, w, sizeof(double) * (size_t)(n * r));
+        memcpy(h_prev, h, sizeof(double) * (size_t)(r * p));
+    }
 
     i64 iter = 0;
     int done = 0, status = 0;
@@ -501,6 +510,21 @@ int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, dou
             if (rescale) col_rescale(n, r, w);
         } else {
             const int reg = (method == ORC_DNMF);
+            if (method == ORC_EHALS) {
+                /* x <- max(eps, x + 0.5 (x - prev)); prev <- old x (lib.rs:755-767) */
+                for (i64 t = 0; t < n * r; t++) {
+                    const double x = w[t], ext = x + 0.5 * (x - w_prev[t]);
+                    w[t] = ext > eps ? ext : eps;
+                    w_prev[t] = x;
+                }
+                for (i64 t = 0; t < r * p; t++) {
+                    const double x = h[t], ext = x + 0.5 * (x - h_prev[t]);
+                    h[t] = ext > eps ? ext : eps;
+                    h_prev[t] = x;
+                }
+                free(w_t);
+                w_t = transpose(w, n, r);
+            }
             compute_wtv(n, p, r, w_t, v_t, wtv);
             wtw_fwd(n, r, w_t, sq);
             hals_update_h(p, r, h, wtv, sq, sparsity_h, smoothness_h, reg, eps);
@@ -541,6 +565,8 @@ int orc_nmf_run(int method, i64 n, i64 p, i64 r, const double *v, double *w, dou
     free(dg);
     free(wtv);
     free(vht);
+    free(w_prev);
+    free(h_prev);
     return status;
 }
 

@@ -26,7 +26,8 @@
 namespace nmfcu {
 
 // Method ids, same values as include/nmfcu.h.
-enum : int { M_BRUNET = 0, M_LEE = 1, M_OFFSET = 2, M_NSNMF = 3, M_HALS = 4, M_DNMF = 6 };
+enum : int { M_BRUNET = 0, M_LEE = 1, M_OFFSET = 2, M_NSNMF = 3, M_HALS = 4, M_EHALS = 5,
+             M_DNMF = 6 };
 // Not a method: the epilogues store the contraction itself (the products of
 // the randomized range finder behind the NNDSVD start).
 constexpr int M_PRODUCT = 100;
@@ -370,6 +371,25 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (threadIdx.x == 0) addon[k] = (k < r) ? red[0] : 0.0;
 }
+// E-HALS extrapolation (nmf_run_ehals, lib.rs:755-767) of the first `cols`
+// entries of each of `rows` rows (leading dimension ld):
+//   x <- max(eps, x + beta (x - prev)),  prev <- the old x.
+static __global__ void ehals_extrapolate(double *__restrict__ X, double *__restrict__ prev,
+                                         int64_t rows, int ld, int cols, double beta, double eps,
+                                         const RunState *st) {
+    if (run_stopped(st)) return;
+    const int64_t total = rows * cols;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / cols;
+        const int64_t at = i * ld + (t - i * cols);
+        const double x = X[at];
+        const double ext = add(x, mul(beta, sub(x, prev[at])));
+        X[at] = ext > eps ? ext : eps;
+        prev[at] = x;
+    }
+}
+
 // Row sums of V (one warp a row, fixed-order lanes + butterfly).
 static __global__ void __launch_bounds__(kThreads)
     v_row_sums(const double *__restrict__ V, int64_t ldv, int n, int p, double *__restrict__ out) {

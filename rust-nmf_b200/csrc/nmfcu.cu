@@ -87,6 +87,10 @@ int bucket_for(int64_t r) {
 }
 
 inline unsigned cdiv(int64_t a, int64_t b) { return (unsigned)((a + b - 1) / b); }
+// Blocks of a grid-stride loop over `total` elements.
+inline unsigned grid_for(int64_t total) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, kThreads), 4096));
+}
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
 // Grams, rescaling, clamps and the objective pass: O(r^2 (n + p)) work plus
@@ -388,6 +392,7 @@ struct nmfcu_context {
     DevBuf Vs, Fs;     // split-bf16 form: V hi/lo, the factor's three terms
     DevBuf Wns, Hns;   // nsNMF: W S (n x RP), S H (RP x p)
     DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
+    DevBuf Wprev, Hprev;     // ehals: the iterate before the last extrapolation
     DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
 
@@ -607,6 +612,7 @@ struct RunArgs {
     double *dev;         // device deviances (or nullptr)
     double *Wns = nullptr, *Hns = nullptr;  // nsNMF: W S, S H
     double *off = nullptr, *rsv = nullptr, *addon = nullptr;  // offset
+    double *Wprev = nullptr, *Hprev = nullptr;                // ehals
 };
 
 nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
@@ -841,6 +847,16 @@ nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it,
             }
             break;
         }
+        case NMFCU_EHALS: {
+            // nmf_run_ehals lib.rs:753-776: extrapolate W and H (beta 0.5),
+            // then one HALS sweep from there.
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
+            ehals_extrapolate<<<grid_for((int64_t)pl.n * pl.r), kThreads, 0, s>>>(
+                a.W, a.Wprev, pl.n, pl.RP, pl.r, 0.5, o->eps, st);
+            ehals_extrapolate<<<grid_for((int64_t)pl.r * pl.p), kThreads, 0, s>>>(
+                a.H, a.Hprev, pl.r, pl.p, pl.p, 0.5, o->eps, st);
+        }
+            [[fallthrough]];
         default: {
             // nmf_run_hals lib.rs:667-676; nmf_run_dnmf lib.rs:862-884.
             gram_w_full(c, a, Gw, sw, s);
@@ -907,6 +923,10 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         v.push_back({&c->Wns, sizeof(double) * (size_t)pl.n * RP});
         v.push_back({&c->Hns, sizeof(double) * RP * (size_t)pl.p});
     }
+    if (method == NMFCU_EHALS) {
+        v.push_back({&c->Wprev, sizeof(double) * (size_t)pl.n * RP});
+        v.push_back({&c->Hprev, sizeof(double) * RP * (size_t)pl.p});
+    }
     if (method == NMFCU_OFFSET) {
         v.push_back({&c->off, sizeof(double) * (size_t)pl.n});
         v.push_back({&c->rsv, sizeof(double) * (size_t)pl.n});
@@ -939,11 +959,12 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
         case NMFCU_OFFSET:
         case NMFCU_NSNMF:
         case NMFCU_HALS:
+        case NMFCU_EHALS:
         case NMFCU_DNMF: break;
-        case NMFCU_EHALS: case NMFCU_LSNMF: case NMFCU_SNMF_R: case NMFCU_SNMF_L:
+        case NMFCU_LSNMF: case NMFCU_SNMF_R: case NMFCU_SNMF_L:
             return fail(NMFCU_ERR_UNSUPPORTED,
                         "method is not built in the GPU engine (built: brunet, lee, offset, nsNMF, "
-                        "hals, dnmf)");
+                        "hals, ehals, dnmf)");
         default: return fail(NMFCU_ERR_INVALID_ARG, "unknown method id");
     }
     if (o->stop != NMFCU_STOP_MAX_ITER && o->stop != NMFCU_STOP_STATIONARY)
@@ -1137,9 +1158,6 @@ __global__ void unpack_rows_t(const double *__restrict__ H, int p, int kc, doubl
         out[j * ldo + c0 + k] = H[(int64_t)k * p + j];
     }
 }
-unsigned grid_for(int64_t total) {
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>(cdiv(total, kThreads), 4096));
-}
 
 // Single-step driver used by the four update entry points.
 enum StepKind { STEP_H_KL, STEP_W_KL, STEP_H_EUC, STEP_W_EUC };
@@ -1269,7 +1287,7 @@ size_t context_bytes(nmfcu_context *c) {
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
                             &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
-                            &c->off, &c->rsv, &c->addon})
+                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev})
         t += b->bytes;
     for (const DevBuf &b : c->extra) t += b.bytes;
     return t;
@@ -1301,7 +1319,7 @@ void context_release(nmfcu_context *c) {
     for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
                       &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
-                            &c->off, &c->rsv, &c->addon})
+                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev})
         b->release();
     for (DevBuf &b : c->extra) b.release();
 }
@@ -1384,6 +1402,14 @@ nmfcu_status setup_method(nmfcu_context *c, const Plan &pl, const nmfcu_options 
     if (o->method == NMFCU_NSNMF) {
         a.Wns = c->Wns.as<double>();
         a.Hns = c->Hns.as<double>();
+    }
+    if (o->method == NMFCU_EHALS) {  // the previous iterate starts as the start
+        a.Wprev = c->Wprev.as<double>();
+        a.Hprev = c->Hprev.as<double>();
+        CUDA_TRY(cudaMemcpyAsync(a.Wprev, a.W, sizeof(double) * (size_t)pl.n * pl.RP,
+                                 cudaMemcpyDeviceToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(a.Hprev, a.H, sizeof(double) * (size_t)pl.RP * pl.p,
+                                 cudaMemcpyDeviceToDevice, s));
     }
     if (o->method == NMFCU_OFFSET) {
         a.off = c->off.as<double>();

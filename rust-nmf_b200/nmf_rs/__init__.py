@@ -7,8 +7,8 @@ and ``set_num_threads``, with the iteration loop running as hand-written
 sm_100a CUDA kernels behind the C ABI of ``include/nmfcu.h``.
 
 Built methods: ``brunet`` (KL), ``lee`` (Frobenius), ``offset``, ``nsNMF``,
-``hals`` and ``dnmf``, each with ``stop='max_iter'`` or ``'stationary'``.
-The other reference methods (ehals, lsNMF, snmf/r, snmf/l) raise
+``hals``, ``ehals`` and ``dnmf``, each with ``stop='max_iter'`` or
+``'stationary'``.  The other reference methods (lsNMF, snmf/r, snmf/l) raise
 ``NotImplementedError``.  There is no CPU fallback: without the CUDA library
 or a GPU every compute call raises ``RuntimeError``.
 

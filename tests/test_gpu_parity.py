@@ -33,7 +33,7 @@ pytestmark = pytest.mark.gpu
 
 FACTOR_TOL = 1e-10
 OBJ_TOL = 1e-12
-METHODS = ["brunet", "lee", "hals", "dnmf"]
+METHODS = ["brunet", "lee", "hals", "ehals", "dnmf"]
 
 
 def _objective(oracle, method, V, W, H):
@@ -76,7 +76,7 @@ def _check(oracle, method, V, W0, H0, iters, **kw):
     ref = oracle.nmf_method(method, V, W0, H0, iters, **kw)
     got = nmf_rs.nmf(V, W0.shape[1], method, W0=W0, H0=H0, max_iter=iters, **kw)
     tol_f, tol_o = FACTOR_TOL, OBJ_TOL
-    if method in ("hals", "dnmf"):
+    if method in ("hals", "ehals", "dnmf"):
         sf, so = _sensitivity(oracle, method, V, W0, H0, iters, **kw)
         tol_f, tol_o = max(tol_f, 100 * sf), max(tol_o, 100 * so)
     assert got.n_iter == ref["n_iter"]
@@ -140,7 +140,7 @@ def test_quickstart_parity(oracle, quickstart, method):
     _check(oracle, method, V, W0, H0, 100)
 
 
-@pytest.mark.parametrize("method", ["hals", "dnmf"])
+@pytest.mark.parametrize("method", ["hals", "ehals", "dnmf"])
 @pytest.mark.parametrize("case", ["quickstart", "pbmc-subset"])
 def test_hals_family_from_nndsvd_strict(oracle, quickstart, method, case):
     """From an NNDSVD start the HALS family is well conditioned: plain tolerance."""
@@ -194,7 +194,7 @@ def test_pbmc8k_shape(oracle, method):
 @pytest.mark.parametrize("method", METHODS)
 def test_stationary_stop_parity(oracle, quickstart, method):
     V, W0, H0 = quickstart
-    if method == "hals":  # well-conditioned start, so the per-iteration deviances compare
+    if method in ("hals", "ehals"):  # well-conditioned start: the deviances compare
         W0, H0 = nmf_rs.nndsvd_init(V, 5, fill="mean", seed=0)
     kw = dict(stop="stationary", stationary_th=1e-3, check_interval=5, check_niter=4)
     got, ref = _check(oracle, method, V, W0, H0, 300, **kw)
@@ -257,12 +257,12 @@ def test_deterministic(quickstart, method):
     np.testing.assert_array_equal(a.H, b.H)
 
 
-@pytest.mark.parametrize("method", ["lee", "brunet", "hals", "dnmf"])
+@pytest.mark.parametrize("method", ["lee", "brunet", "hals", "ehals", "dnmf"])
 def test_fp32_precision_form(oracle, method):
     """V in f32 for the contractions, f64 everywhere else, 2 f64 sweeps:
     objective within 1e-5 (relative) of the FP64 oracle."""
     V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
-    if method == "hals":  # HALS from a random start is ill conditioned (see top)
+    if method in ("hals", "ehals"):  # ill conditioned from a random start (see top)
         W0, H0 = nmf_rs.nndsvd_init(V, 8, fill="mean", seed=0)
     ref = oracle.nmf_method(method, V, W0, H0, 40)
     got = nmf_rs.nmf(V, 8, method, W0=W0, H0=H0, max_iter=40, precision="fp32")
@@ -274,7 +274,7 @@ def test_fp32_precision_form(oracle, method):
 def test_unsupported_method_and_rank(quickstart):
     V, W0, H0 = quickstart
     with pytest.raises(NotImplementedError):
-        nmf_rs.nmf(V, 5, "ehals", W0=W0, H0=H0, max_iter=2)
+        nmf_rs.nmf(V, 5, "snmf/r", W0=W0, H0=H0, max_iter=2)
     V2 = synthetic.counts_matrix(50, 60, 4, 0.3, seed=1)
     with pytest.raises(NotImplementedError, match="rank 33"):
         nmf_rs.nmf(V2, 33, "lee", max_iter=2, seed=0)

@@ -37,10 +37,10 @@ def test_one_iteration_matches_oracle(oracle, n, p, r):
     assert rel_max(got.W, ref["W"]) <= 5e-4, rel_max(got.W, ref["W"])
 
 
-@pytest.mark.parametrize("method", ["lee", "hals", "dnmf", "brunet"])
+@pytest.mark.parametrize("method", ["lee", "hals", "ehals", "dnmf", "brunet"])
 def test_split_bf16_form(oracle, method):
     V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
-    if method == "hals":  # HALS from a random start is ill conditioned
+    if method in ("hals", "ehals"):  # ill conditioned from a random start
         W0, H0 = nmf_rs.nndsvd_init(V, 8, fill="mean", seed=0)
     ref = oracle.nmf_method(method, V, W0, H0, 40)
     got = nmf_rs.nmf(V, 8, method, W0=W0, H0=H0, max_iter=40, precision="bf16x3")

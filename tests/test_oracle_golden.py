@@ -103,7 +103,8 @@ def test_single_step_delta_kl(oracle, quickstart, kats):
     assert rel(kl(W0, H0) - kl(W1, H1), kats["single_step_brunet_delta_kl"]) < 1e-13
 
 
-@pytest.mark.parametrize("method", ["brunet", "lee", "offset", "nsNMF", "hals", "dnmf"])
+@pytest.mark.parametrize("method", ["brunet", "lee", "offset", "nsNMF", "hals", "ehals",
+                                    "dnmf"])
 def test_thread_count_independent(oracle, quickstart, method):
     V, W0, H0 = quickstart
     a = oracle.nmf_method(method, V, W0, H0, 30, num_threads=1)
@@ -133,7 +134,7 @@ def test_check_interval_zero_mirrors_panic(oracle, quickstart):
                        check_interval=0, check_niter=1)
 
 
-@pytest.mark.parametrize("method", ["hals", "dnmf"])
+@pytest.mark.parametrize("method", ["hals", "ehals", "dnmf"])
 def test_hals_family_decreases_loss(oracle, quickstart, method):
     V, W0, H0 = quickstart
     res = oracle.nmf_method(method, V, W0, H0, 50, stop="stationary", check_interval=10)
@@ -147,3 +148,19 @@ def test_dnmf_unit_norm_columns(oracle, quickstart):
     res = oracle.nmf_method("dnmf", V, W0, H0, 20)
     norms = np.linalg.norm(res["W"], axis=0)
     np.testing.assert_allclose(norms, 1.0, rtol=1e-12)
+
+
+def test_ehals_is_hals_from_the_extrapolated_point(oracle, quickstart):
+    # One ehals iteration from (W0, H0) with no history is max(eps, .) of the
+    # start followed by a HALS sweep (lib.rs:743-776).
+    V, W0, H0 = quickstart
+    W0 = W0.copy()
+    W0[0, 0] = 0.0  # raised to eps by the extrapolation
+    a = oracle.nmf_method("ehals", V, W0, H0, 1)
+    b = oracle.nmf_method("hals", V, np.maximum(W0, 1e-9), np.maximum(H0, 1e-9), 1)
+    np.testing.assert_array_equal(a["W"], b["W"])
+    np.testing.assert_array_equal(a["H"], b["H"])
+    # Two iterations differ from HALS: the second extrapolates.
+    a2 = oracle.nmf_method("ehals", V, W0, H0, 2)
+    b2 = oracle.nmf_method("hals", V, np.maximum(W0, 1e-9), np.maximum(H0, 1e-9), 2)
+    assert not np.array_equal(a2["W"], b2["W"])
