@@ -52,7 +52,7 @@ enum {
     NMFCU_HALS = 4,
     NMFCU_EHALS = 5,
     NMFCU_DNMF = 6,
-    NMFCU_LSNMF = 7,  /* not built: NMFCU_ERR_UNSUPPORTED */
+    NMFCU_LSNMF = 7,  /* through nmfcu_run_weighted (FP64) */
     NMFCU_SNMF_R = 8, /* not built */
     NMFCU_SNMF_L = 9  /* not built */
 };
@@ -138,6 +138,17 @@ nmfcu_status nmfcu_run_offset(const nmfcu_options *opt, int64_t n, int64_t p, in
                               const double *offset0, double *W, double *H, double *offset,
                               double *deviances, int64_t deviances_cap, int64_t *n_deviances,
                               int64_t *n_iter);
+
+/*
+ * nmfcu_run_weighted -- py_nmf_run with method "lsnmf" (lib.rs:2101-2115 ->
+ * nmf_run_lsnmf :945-1043): as nmfcu_run, plus the per-entry weights
+ * `weight` (n x p, the `weight` keyword), minimising 0.5 ||(V - W H) o
+ * weight||^2.  opt->method must be NMFCU_LSNMF and opt->precision FP64.
+ */
+nmfcu_status nmfcu_run_weighted(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                                const double *V, const double *weight, const double *W0,
+                                const double *H0, double *W, double *H, double *deviances,
+                                int64_t deviances_cap, int64_t *n_deviances, int64_t *n_iter);
 
 /* Single-step updates on host pointers; each writes a fresh factor.
  *   py_divergence_update_h (lib.rs:1851-1862 -> divergence_update_h_impl :120-144)

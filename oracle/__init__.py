@@ -3,7 +3,7 @@
 A ctypes wrapper around ``liboracle.so`` (built from ``nmf_oracle.c`` by
 ``oracle/Makefile``), which restates the f64 loops of omicverse/rust-NMF
 ``rust/src/lib.rs`` (brunet :1529-1586, lee :1589-1647, offset :1650-1760,
-nsNMF :1762-1830, hals :638-688, ehals :711-786, dnmf :827-906, objectives :1410-1445,
+nsNMF :1762-1830, hals :638-688, ehals :711-786, dnmf :827-906, lsNMF :945-1043, objectives :1410-1445,
 stationary stop :1336-1401).
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
@@ -81,7 +81,15 @@ def _load():
         ctypes.c_double, _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
         ctypes.c_int,
     ]
-    if lib.orc_version() < 2:
+    lib.orc_weighted_distance.restype = ctypes.c_double
+    lib.orc_weighted_distance.argtypes = [_i64, _i64, _i64, _dp, _dp, _dp, _dp]
+    lib.orc_nmf_run_lsnmf.restype = ctypes.c_int
+    lib.orc_nmf_run_lsnmf.argtypes = [
+        _i64, _i64, _i64, _dp, _dp, _dp, _dp, _i64, ctypes.c_double, ctypes.c_int,
+        ctypes.c_double, _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
+        ctypes.c_int,
+    ]
+    if lib.orc_version() < 3:
         raise RuntimeError("liboracle.so is stale: rebuild it (make -C oracle)")
     _lib = lib
     return lib
@@ -187,9 +195,40 @@ def nmf_offset(V, W0, H0, max_iter: int, *, offset=None, eps: float = 1e-9,
             "deviances": dev[: nd.value].copy()}
 
 
+def nmf_lsnmf(V, weight, W0, H0, max_iter: int, *, eps: float = 1e-9, stop: str = "max_iter",
+              stationary_th: float = 2.220446049250313e-16, check_interval: int = 50,
+              check_niter: int = 10, num_threads: int | None = None) -> dict:
+    """Oracle of ``py_nmf_run`` with method lsnmf (nmf_run_lsnmf, lib.rs:945-1043)."""
+    lib = _load()
+    V, S = _c(V), _c(weight)
+    W = _c(W0).copy()
+    H = _c(H0).copy()
+    n, p = V.shape
+    if S.shape != V.shape:
+        raise ValueError("weight must have V's shape")
+    r = W.shape[1]
+    dev = np.zeros(max(int(max_iter) + 1, 1), dtype=np.float64)
+    nd, ni = _i64(0), _i64(0)
+    rc = lib.orc_nmf_run_lsnmf(
+        n, p, r, _ptr(V), _ptr(S), _ptr(W), _ptr(H), int(max_iter), float(eps),
+        *_stat_args(stop, stationary_th, check_interval, check_niter), _ptr(dev),
+        ctypes.byref(nd), ctypes.byref(ni), int(num_threads or os.cpu_count() or 1),
+    )
+    if rc == -2:
+        raise ZeroDivisionError("stationary stop evaluated `iter % check_interval` with 0")
+    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": dev[: nd.value].copy()}
+
+
+def weighted_distance(V, weight, W, H) -> float:
+    lib = _load()
+    V, S, W, H = _c(V), _c(weight), _c(W), _c(H)
+    return float(lib.orc_weighted_distance(V.shape[0], V.shape[1], W.shape[1], _ptr(V), _ptr(S),
+                                           _ptr(W), _ptr(H)))
+
+
 def nmf_method(method: str, V, W0, H0, max_iter: int, *, eps=1e-9, rescale=True,
                sparsity=0.01, smoothness=1.0, stop="max_iter", theta=0.5, offset=None,
-               **kw) -> dict:
+               weight=None, **kw) -> dict:
     """Same as :func:`nmf_run` but with the Python-level routing of
     ``sparsity``/``smoothness`` that ``nmf()`` applies (python/nmf_rs/__init__.py:528-538):
     dnmf gets ``sparsity`` on both factors and no L2, the others get none.
@@ -199,6 +238,10 @@ def nmf_method(method: str, V, W0, H0, max_iter: int, *, eps=1e-9, rescale=True,
         return nmf_nsnmf(V, W0, H0, max_iter, theta=theta, stop=stop, **kw)
     if m == "offset":
         return nmf_offset(V, W0, H0, max_iter, offset=offset, eps=eps, stop=stop, **kw)
+    if m in ("lsnmf", "ls-nmf"):
+        if weight is None:
+            raise ValueError("method='lsnmf' requires a `weight` matrix of the same shape as V")
+        return nmf_lsnmf(V, weight, W0, H0, max_iter, eps=eps, stop=stop, **kw)
     if method == "dnmf":
         sh = sw = float(sparsity)
     else:

@@ -779,5 +779,95 @@ int orc_nmf_run_offset(i64 n, i64 p, i64 r, const double *v, double *w, double *
     return status;
 }
 
+/* 0.5 sum ((V - W H) o S)^2, rows outer (lib.rs:962-975 / 1024-1035). */
+double orc_weighted_distance(i64 n, i64 p, i64 r, const double *v, const double *weight,
+                             const double *w, const double *h) {
+    double s = 0.0;
+    for (i64 u = 0; u < n; u++)
+        for (i64 j = 0; j < p; j++) {
+            const double d = (v[u * p + j] - wh_at(p, r, w, h, u, j)) * weight[u * p + j];
+            s += d * d;
+        }
+    return 0.5 * s;
+}
+
+/* est o S for the current W, H (wh_dense then elementwise_mul, lib.rs:980-981). */
+static void est_weighted(i64 n, i64 p, i64 r, const double *w, const double *h,
+                         const double *weight, double *out) {
+#pragma omp parallel for schedule(static)
+    for (i64 u = 0; u < n; u++)
+        for (i64 j = 0; j < p; j++) out[u * p + j] = wh_at(p, r, w, h, u, j) * weight[u * p + j];
+}
+
+/*
+ * orc_nmf_run_lsnmf: nmf_run_lsnmf, lib.rs:945-1043 (weighted Frobenius).
+ * Per iteration: H <- max(eps, H o W^T(V o S)) / (W^T((W H) o S) + eps), then
+ * W <- max(eps, W o (V o S) H^T) / (((W H) o S) H^T + eps) with the new H.
+ */
+int orc_nmf_run_lsnmf(i64 n, i64 p, i64 r, const double *v, const double *weight, double *w,
+                      double *h, i64 max_iter, double eps, int stop, double stationary_th,
+                      i64 check_interval, i64 check_niter, double *dev, i64 *n_dev,
+                      i64 *n_iter, int nt) {
+    set_threads(nt);
+    stationary_t st = {check_interval, check_niter, stationary_th, -INFINITY, INFINITY, 0};
+    const int stat = (stop == ORC_STOP_STATIONARY);
+    const size_t np = (size_t)(n * p > 0 ? n * p : 1);
+    const size_t nr = (size_t)(n * r > 0 ? n * r : 1), rp = (size_t)(r * p > 0 ? r * p : 1);
+    double *v_w = (double *)malloc(sizeof(double) * np);
+    double *est_w = (double *)malloc(sizeof(double) * np);
+    double *num = (double *)malloc(sizeof(double) * (rp > nr ? rp : nr));
+    double *den = (double *)malloc(sizeof(double) * (rp > nr ? rp : nr));
+    for (i64 t = 0; t < n * p; t++) v_w[t] = v[t] * weight[t];
+    double *v_w_t = transpose(v_w, n, p);
+    i64 nd = 0, iter = 0;
+    int done = 0, status = 0;
+    if (stat) {
+        const double d = orc_weighted_distance(n, p, r, v, weight, w, h);
+        dev[nd++] = d;
+        if (st_should_stop(&st, 0, d) != 0) done = 1;
+    }
+    while (!done && iter < max_iter) {
+        iter++;
+        est_weighted(n, p, r, w, h, weight, est_w);
+        double *est_w_t = transpose(est_w, n, p);
+        double *w_t = transpose(w, n, r);
+        compute_wtv(n, p, r, w_t, v_w_t, num);
+        compute_wtv(n, p, r, w_t, est_w_t, den);
+        for (i64 k = 0; k < r; k++)
+            for (i64 u = 0; u < p; u++) {
+                const double temp = h[k * p + u] * num[k * p + u];
+                h[k * p + u] = (temp > eps ? temp : eps) / (den[k * p + u] + eps);
+            }
+        free(est_w_t);
+        free(w_t);
+        est_weighted(n, p, r, w, h, weight, est_w);
+        compute_vht(n, p, r, v_w, h, num);
+        compute_vht(n, p, r, est_w, h, den);
+        for (i64 u = 0; u < n; u++)
+            for (i64 k = 0; k < r; k++) {
+                const double temp = w[u * r + k] * num[u * r + k];
+                w[u * r + k] = (temp > eps ? temp : eps) / (den[u * r + k] + eps);
+            }
+        if (stat) {
+            const double d = orc_weighted_distance(n, p, r, v, weight, w, h);
+            dev[nd++] = d;
+            int rc = st_should_stop(&st, iter, d);
+            if (rc < 0) {
+                status = -2;
+                break;
+            }
+            if (rc) break;
+        }
+    }
+    *n_dev = nd;
+    *n_iter = iter;
+    free(v_w);
+    free(v_w_t);
+    free(est_w);
+    free(num);
+    free(den);
+    return status;
+}
+
 /* Build identification so the Python side can tell a stale build apart. */
-int orc_version(void) { return 2; }
+int orc_version(void) { return 3; }

@@ -27,7 +27,7 @@ namespace nmfcu {
 
 // Method ids, same values as include/nmfcu.h.
 enum : int { M_BRUNET = 0, M_LEE = 1, M_OFFSET = 2, M_NSNMF = 3, M_HALS = 4, M_EHALS = 5,
-             M_DNMF = 6 };
+             M_DNMF = 6, M_LSNMF = 7 };
 // Not a method: the epilogues store the contraction itself (the products of
 // the randomized range finder behind the NNDSVD start).
 constexpr int M_PRODUCT = 100;
@@ -371,6 +371,53 @@ __global__ void __launch_bounds__(kThreads)
     }
     if (threadIdx.x == 0) addon[k] = (k < r) ? red[0] : 0.0;
 }
+// lsNMF objective partials (lib.rs:1024-1035): sum_ij (Vs_ij - (W H)_ij S_ij)^2
+// with Vs = V o S precomputed, i.e. ((V - W H) o S)^2.  Block b takes rows
+// b, b + nblocks, ... one warp a row (lanes over columns in a fixed order, a
+// xor butterfly), and writes its sum to part[b].
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    ls_objective(const double *__restrict__ Vs, const double *__restrict__ S, int64_t ld, int n,
+                 int p, const double *__restrict__ W, const double *__restrict__ H,
+                 double *__restrict__ part, const RunState *st) {
+    if (run_stopped(st)) return;
+    constexpr int kWarps = kThreads / 32;
+    __shared__ double red[kWarps];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double acc = 0.0;
+    for (int i = blockIdx.x * kWarps + warp; i < n; i += gridDim.x * kWarps) {
+        double w[RP];
+#pragma unroll
+        for (int k = 0; k < RP; k++) w[k] = W[(size_t)i * RP + k];
+        for (int j = lane; j < p; j += 32) {
+            double wh = 0.0;
+#pragma unroll
+            for (int k = 0; k < RP; k++) wh = fma(w[k], H[(size_t)k * p + j], wh);
+            const double d = Vs[(size_t)i * ld + j] - wh * S[(size_t)i * ld + j];
+            acc = fma(d, d, acc);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int q = 0; q < kWarps; q++) s += red[q];
+        part[blockIdx.x] = s;
+    }
+}
+// Vs <- V o S in place (the weighted target of lsNMF, lib.rs:961).
+static __global__ void mul_weight(double *__restrict__ V, const double *__restrict__ S,
+                                  int64_t ld, int n, int p) {
+    const int64_t total = (int64_t)n * p;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / p, at = i * ld + (t - i * p);
+        V[at] = mul(V[at], S[at]);
+    }
+}
+
 // E-HALS extrapolation (nmf_run_ehals, lib.rs:755-767) of the first `cols`
 // entries of each of `rows` rows (leading dimension ld):
 //   x <- max(eps, x + beta (x - prev)),  prev <- the old x.
@@ -441,6 +488,9 @@ struct EpiParams {
     const double *sums; // colsum(W) for the brunet H step, rowsum(H) for the W step
     const double *addon = nullptr;  // offset, H step: (W^T off)[k] added to the denominator
     const double *roff = nullptr;   // offset, W step: the row offsets off[i]
+    // lsNMF: the numerator contraction (W^T (V o S) as RP x p for the H step,
+    // (V o S) H^T as n x RP for the W step); the pass supplies the denominator.
+    const double *aux = nullptr;
 };
 
 // Per-column H update from the reduced contraction num[] (old column hc[]).
@@ -449,9 +499,18 @@ struct EpiParams {
 //   hals   : hals_update_h             lib.rs:595-605
 //   dnmf   : hals_update_h_reg         lib.rs:1079-1089
 template <int RP>
-__device__ __forceinline__ void h_update(const EpiParams &e, const double *num, double *hc) {
+__device__ __forceinline__ void h_update(const EpiParams &e, const double *num, double *hc,
+                                         const double *ax = nullptr) {
     const int r = e.r;
-    if (e.method == M_PRODUCT) {
+    if (e.method == M_LSNMF) {
+        // nmf_run_lsnmf lib.rs:990-999: max(eps, H numer) / (denom + eps)
+#pragma unroll
+        for (int i = 0; i < RP; i++)
+            if (i < r) {
+                const double temp = mul(hc[i], ax[i]);
+                hc[i] = (temp > e.eps ? temp : e.eps) / add(num[i], e.eps);
+            }
+    } else if (e.method == M_PRODUCT) {
 #pragma unroll
         for (int i = 0; i < RP; i++)
             if (i < r) hc[i] = num[i];
@@ -503,9 +562,17 @@ __device__ __forceinline__ void h_update(const EpiParams &e, const double *num, 
 // ro: the row's offset (offset method; lib.rs:441-446), else unused.
 template <int RP>
 __device__ __forceinline__ void w_update(const EpiParams &e, const double *num, double *wr,
-                                         double ro = 0.0) {
+                                         double ro = 0.0, const double *ax = nullptr) {
     const int r = e.r;
-    if (e.method == M_PRODUCT) {
+    if (e.method == M_LSNMF) {
+        // nmf_run_lsnmf lib.rs:1011-1018
+#pragma unroll
+        for (int j = 0; j < RP; j++)
+            if (j < r) {
+                const double temp = mul(wr[j], ax[j]);
+                wr[j] = (temp > e.eps ? temp : e.eps) / add(num[j], e.eps);
+            }
+    } else if (e.method == M_PRODUCT) {
 #pragma unroll
         for (int j = 0; j < RP; j++)
             if (j < r) wr[j] = num[j];

@@ -32,6 +32,16 @@ struct StreamOps {
     virtual cudaError_t wpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmH,
                               const double *W, int n, int p, const StreamK &sk, double *part,
                               RunState *st, int grid, cudaStream_t s) const = 0;
+    // The ratio passes' tiling with each V element entering as v (W H)_ij
+    // (lsNMF's denominators; V holds the weights).  f64 only.
+    virtual cudaError_t hpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmW,
+                                       const double *H, int n, int p, const StreamK &sk,
+                                       double *part, RunState *st, int grid,
+                                       cudaStream_t s) const = 0;
+    virtual cudaError_t wpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmH,
+                                       const double *W, int n, int p, const StreamK &sk,
+                                       double *part, RunState *st, int grid,
+                                       cudaStream_t s) const = 0;
     virtual void h_epi(double *H, void *Ht, int p, const double *part, const StreamK &sk,
                        int tcols, const EpiParams &e, const RunState *st,
                        cudaStream_t s) const = 0;

@@ -103,6 +103,10 @@ struct Ops {
                            const double *H, int mode, int S2, int cols_per_split, double *obj,
                            const RunState *st, cudaStream_t s,
                            const double *roff = nullptr) const = 0;
+    // lsNMF objective partials over V o S and S: one per block, nblocks blocks
+    virtual void ls_objective(const double *Vs, const double *S, int64_t ld, int n, int p,
+                              const double *W, const double *H, int nblocks, double *part,
+                              const RunState *st, cudaStream_t s) const = 0;
     // nsNMF: out = X S (rows x RP) and out = S H (RP x p)
     virtual void ns_right(const double *X, int rows, int r, double theta, double *out,
                           const RunState *st, cudaStream_t s) const = 0;
@@ -141,6 +145,12 @@ struct OpsT final : Ops {
         else
             nmfcu::rowpass<double, double, RP, 3><<<grid, block, 0, s>>>(
                 V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st, roff);
+    }
+    void ls_objective(const double *Vs, const double *S, int64_t ld, int n, int p,
+                      const double *W, const double *H, int nblocks, double *part,
+                      const RunState *st, cudaStream_t s) const override {
+        if (nblocks > 0)
+            nmfcu::ls_objective<RP><<<nblocks, kThreads, 0, s>>>(Vs, S, ld, n, p, W, H, part, st);
     }
     void ns_right(const double *X, int rows, int r, double theta, double *out, const RunState *st,
                   cudaStream_t s) const override {
@@ -393,6 +403,7 @@ struct nmfcu_context {
     DevBuf Wns, Hns;   // nsNMF: W S (n x RP), S H (RP x p)
     DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
     DevBuf Wprev, Hprev;     // ehals: the iterate before the last extrapolation
+    DevBuf S64, NH, NW;      // lsNMF: weights (pitched like V), the numerator contractions
     DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
 
@@ -613,6 +624,12 @@ struct RunArgs {
     double *Wns = nullptr, *Hns = nullptr;  // nsNMF: W S, S H
     double *off = nullptr, *rsv = nullptr, *addon = nullptr;  // offset
     double *Wprev = nullptr, *Hprev = nullptr;                // ehals
+    // lsNMF: V holds V o S; S the weights (same pitch); NH / NW the
+    // numerator contractions; pden the weighted passes' maps over S.
+    const double *S64 = nullptr;
+    double *NH = nullptr, *NW = nullptr;
+    PassSet pden;
+    bool weighted = false;  // h_step / w_step run the weighted passes
 };
 
 nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
@@ -626,7 +643,11 @@ nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long ite
         a.ops->ns_right(a.W, pl.n, pl.r, a.opt->theta, a.Wns, st, s);
         West = a.Wns;
     }
-    {
+    if (a.opt->method == NMFCU_LSNMF) {  // 0.5 ||(V - W H) o S||^2, lib.rs:1024-1035
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OBJECTIVE);
+        a.ops->ls_objective(a.V64, a.S64, a.ldv64, pl.n, pl.p, a.W, a.H,
+                            pl.n > 0 ? pl.obj_blocks : 0, c->obj.as<double>(), st, s);
+    } else {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OBJECTIVE);
         a.ops->objective(a.V64, a.ldv64, pl.n, pl.p, West, a.H, kl ? 2 : 3, pl.S2,
                          pl.cols_per_split, c->obj.as<double>(), st, s,
@@ -693,8 +714,12 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     }
     if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, kclass);
-        CUDA_TRY(ps.so->hpass(ratio, ps.tmVh, ps.tmW, a.H, pl.n, pl.p, sk, c->part.as<double>(),
-                              st, sk.G, s));
+        if (a.weighted)
+            CUDA_TRY(ps.so->hpass_weighted(ps.tmVh, ps.tmW, a.H, pl.n, pl.p, sk,
+                                           c->part.as<double>(), st, sk.G, s));
+        else
+            CUDA_TRY(ps.so->hpass(ratio, ps.tmVh, ps.tmW, a.H, pl.n, pl.p, sk,
+                                  c->part.as<double>(), st, sk.G, s));
     }
     nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
     ps.so->h_epi(a.H, ps.Ht, pl.p, c->part.as<double>(), sk, tcols, e, st, s);
@@ -728,8 +753,12 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                            ? NMFCU_KCLASS_WSTEP_REFINE : NMFCU_KCLASS_WSTEP;
     if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, kclass);
-        CUDA_TRY(ps.so->wpass(ratio, ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk, c->part.as<double>(),
-                              st, sk.G, s));
+        if (a.weighted)
+            CUDA_TRY(ps.so->wpass_weighted(ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk,
+                                           c->part.as<double>(), st, sk.G, s));
+        else
+            CUDA_TRY(ps.so->wpass(ratio, ps.tmVw, ps.tmHt, a.W, pl.n, pl.p, sk,
+                                  c->part.as<double>(), st, sk.G, s));
     }
     nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
     ps.so->w_epi(a.W, pl.n, c->part.as<double>(), sk, trows, e, st, s);
@@ -847,6 +876,29 @@ nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it,
             }
             break;
         }
+        case NMFCU_LSNMF: {
+            // nmf_run_lsnmf lib.rs:978-1019.  H: numerator W^T (V o S) by a
+            // plain pass over V o S into NH, denominator W^T ((W H) o S) by
+            // the weighted pass over S, whose epilogue applies the update.
+            // W: the same with the new H (its H^T copy from the H epilogue).
+            RunArgs an = a;
+            an.H = a.NH;
+            EpiParams ep = epi(o, pl.r, nullptr, nullptr, true);
+            ep.method = nmfcu::M_PRODUCT;
+            NMF_TRY(h_step(c, an, a.p64, ep, false, s));
+            RunArgs ad = a;
+            ad.weighted = true;
+            EpiParams eh = epi(o, pl.r, nullptr, nullptr, true);
+            eh.aux = a.NH;
+            NMF_TRY(h_step(c, ad, a.pden, eh, true, s));
+            an = a;
+            an.W = a.NW;
+            NMF_TRY(w_step(c, an, a.p64, ep, false, s));
+            EpiParams ew = epi(o, pl.r, nullptr, nullptr, false);
+            ew.aux = a.NW;
+            NMF_TRY(w_step(c, ad, a.pden, ew, true, s));
+            break;
+        }
         case NMFCU_EHALS: {
             // nmf_run_ehals lib.rs:753-776: extrapolate W and H (beta 0.5),
             // then one HALS sweep from there.
@@ -923,6 +975,10 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         v.push_back({&c->Wns, sizeof(double) * (size_t)pl.n * RP});
         v.push_back({&c->Hns, sizeof(double) * RP * (size_t)pl.p});
     }
+    if (method == NMFCU_LSNMF) {
+        v.push_back({&c->NW, sizeof(double) * (size_t)pl.n * RP});
+        v.push_back({&c->NH, sizeof(double) * RP * (size_t)pl.p});
+    }
     if (method == NMFCU_EHALS) {
         v.push_back({&c->Wprev, sizeof(double) * (size_t)pl.n * RP});
         v.push_back({&c->Hprev, sizeof(double) * RP * (size_t)pl.p});
@@ -960,11 +1016,12 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
         case NMFCU_NSNMF:
         case NMFCU_HALS:
         case NMFCU_EHALS:
+        case NMFCU_LSNMF:
         case NMFCU_DNMF: break;
-        case NMFCU_LSNMF: case NMFCU_SNMF_R: case NMFCU_SNMF_L:
+        case NMFCU_SNMF_R: case NMFCU_SNMF_L:
             return fail(NMFCU_ERR_UNSUPPORTED,
                         "method is not built in the GPU engine (built: brunet, lee, offset, nsNMF, "
-                        "hals, ehals, dnmf)");
+                        "hals, ehals, dnmf, lsNMF)");
         default: return fail(NMFCU_ERR_INVALID_ARG, "unknown method id");
     }
     if (o->stop != NMFCU_STOP_MAX_ITER && o->stop != NMFCU_STOP_STATIONARY)
@@ -973,6 +1030,8 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
         o->precision != NMFCU_PREC_BF16X3)
         return fail(NMFCU_ERR_INVALID_ARG, "unknown precision id");
     if (o->max_iter < 0) return fail(NMFCU_ERR_INVALID_ARG, "max_iter must be >= 0");
+    if (o->method == NMFCU_LSNMF && o->precision != NMFCU_PREC_FP64)
+        return fail(NMFCU_ERR_UNSUPPORTED, "lsNMF runs in FP64 only");
     if (o->check_niter < 0 || o->check_interval < 0)
         return fail(NMFCU_ERR_INVALID_ARG, "check_interval / check_niter must be >= 0");
     if (o->refine_iters < 0) return fail(NMFCU_ERR_INVALID_ARG, "refine_iters must be >= 0");
@@ -1287,7 +1346,8 @@ size_t context_bytes(nmfcu_context *c) {
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
                             &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
-                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev})
+                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
+                            &c->S64, &c->NH, &c->NW})
         t += b->bytes;
     for (const DevBuf &b : c->extra) t += b.bytes;
     return t;
@@ -1319,7 +1379,8 @@ void context_release(nmfcu_context *c) {
     for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
                       &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
-                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev})
+                            &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
+                            &c->S64, &c->NH, &c->NW})
         b->release();
     for (DevBuf &b : c->extra) b.release();
 }
@@ -1432,15 +1493,21 @@ nmfcu_status setup_method(nmfcu_context *c, const Plan &pl, const nmfcu_options 
     return NMFCU_OK;
 }
 
-// The host-buffer run shared by nmfcu_run and nmfcu_run_offset.
+// The host-buffer run shared by nmfcu_run, nmfcu_run_offset and
+// nmfcu_run_weighted.
 nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
-                      const double *V, const double *W0, const double *H0,
-                      const double *offset0, double *W, double *H, double *offset,
-                      double *deviances, int64_t deviances_cap, int64_t *n_deviances,
-                      int64_t *n_iter) {
+                      const double *V, const double *weight, const double *W0,
+                      const double *H0, const double *offset0, double *W, double *H,
+                      double *offset, double *deviances, int64_t deviances_cap,
+                      int64_t *n_deviances, int64_t *n_iter) {
     NMF_TRY(validate_options(opt, n, p, r));
     if (!V || !W0 || !H0 || !W || !H || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    const bool ls = opt->method == NMFCU_LSNMF;
+    if (ls && !weight)  // py_nmf_run, lib.rs:1967-1971
+        return fail(NMFCU_ERR_INVALID_ARG,
+                    "method='lsnmf' requires a `weight` matrix of the same shape as V "
+                    "(nmfcu_run_weighted)");
     const bool stat = opt->stop == NMFCU_STOP_STATIONARY;
     if (stat && (!deviances || deviances_cap < opt->max_iter + 1))
         return fail(NMFCU_ERR_INVALID_ARG, "deviances must hold max_iter + 1 values");
@@ -1475,6 +1542,22 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
     a.W = c->W.as<double>();
     a.H = c->H.as<double>();
     a.dev = stat ? c->dev.as<double>() : nullptr;
+    if (ls) {
+        // S next to V with V's pitch, then V <- V o S (lib.rs:961).
+        NMF_TRY(c->S64.ensure(sizeof(double) * (size_t)(n * ldv)));
+        if (n > 0 && p > 0) {
+            CUDA_TRY(cudaMemcpy2DAsync(c->S64.ptr, ldv * 8, weight, p * 8, p * 8, n,
+                                       cudaMemcpyHostToDevice, s));
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            mul_weight<<<grid_for(n * p), kThreads, 0, s>>>(c->V64.as<double>(),
+                                                            c->S64.as<double>(), ldv, (int)n,
+                                                            (int)p);
+        }
+        a.S64 = c->S64.as<double>();
+        a.NH = c->NH.as<double>();
+        a.NW = c->NW.as<double>();
+        NMF_TRY(make_passset(c, pl, false, true, c->S64.ptr, ldv, &a.pden));
+    }
     NMF_TRY(setup_method(c, pl, opt, a, offset0, true, s));
     int64_t nd = 0, ni = 0;
     NMF_TRY(run_loop(c, a, s, &nd, &ni));
@@ -1499,8 +1582,21 @@ nmfcu_status nmfcu_run(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r
                        const double *V, const double *W0, const double *H0, double *W,
                        double *H, double *deviances, int64_t deviances_cap,
                        int64_t *n_deviances, int64_t *n_iter) {
-    return run_host(opt, n, p, r, V, W0, H0, nullptr, W, H, nullptr, deviances, deviances_cap,
-                    n_deviances, n_iter);
+    return run_host(opt, n, p, r, V, nullptr, W0, H0, nullptr, W, H, nullptr, deviances,
+                    deviances_cap, n_deviances, n_iter);
+}
+
+nmfcu_status nmfcu_run_weighted(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                                const double *V, const double *weight, const double *W0,
+                                const double *H0, double *W, double *H, double *deviances,
+                                int64_t deviances_cap, int64_t *n_deviances, int64_t *n_iter) {
+    if (!opt) return fail(NMFCU_ERR_INVALID_ARG, "NULL options");
+    if (opt->method != NMFCU_LSNMF)
+        return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_run_weighted runs method NMFCU_LSNMF only");
+    if (!weight && n > 0 && p > 0) return fail(NMFCU_ERR_INVALID_ARG, "NULL weight");
+    static const double kNone = 0.0;
+    return run_host(opt, n, p, r, V, weight ? weight : &kNone, W0, H0, nullptr, W, H, nullptr,
+                    deviances, deviances_cap, n_deviances, n_iter);
 }
 
 nmfcu_status nmfcu_run_offset(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
@@ -1512,8 +1608,8 @@ nmfcu_status nmfcu_run_offset(const nmfcu_options *opt, int64_t n, int64_t p, in
     if (opt->method != NMFCU_OFFSET)
         return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_run_offset runs method NMFCU_OFFSET only");
     if (!offset && n > 0) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
-    return run_host(opt, n, p, r, V, W0, H0, offset0, W, H, offset, deviances, deviances_cap,
-                    n_deviances, n_iter);
+    return run_host(opt, n, p, r, V, nullptr, W0, H0, offset0, W, H, offset, deviances,
+                    deviances_cap, n_deviances, n_iter);
 }
 
 nmfcu_status nmfcu_update_h_divergence(int64_t n, int64_t p, int64_t r, const double *V,
@@ -1583,6 +1679,9 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     if (opt->method == NMFCU_OFFSET)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "the offset method returns its row offsets: run it through nmfcu_run_offset");
+    if (opt->method == NMFCU_LSNMF)
+        return fail(NMFCU_ERR_UNSUPPORTED,
+                    "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
     if (!dV || !dW || !dH || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (v_dtype != NMFCU_F64 && v_dtype != NMFCU_F32)

@@ -333,6 +333,9 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
     if (opt->method == NMFCU_OFFSET)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "the offset method returns its row offsets: run it through nmfcu_run_offset");
+    if (opt->method == NMFCU_LSNMF)
+        return fail(NMFCU_ERR_UNSUPPORTED,
+                    "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
     if (!V || !W0 || !H0 || !W || !H) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
     if (dev_cap < 0 || (dev_cap > 0 && !deviances))

@@ -335,7 +335,9 @@ struct HCfg {
     static_assert(STAGES >= 3, "a ring needs stages in flight");
 };
 
-template <typename T, int RP, bool RATIO>
+// RATIO: each V element enters as v / (W H)_ij (0 where W H is 0); with
+// WEIGHTED as v (W H)_ij instead (lsNMF's denominator, V holding the weights).
+template <typename T, int RP, bool RATIO, bool WEIGHTED = false>
 __global__ void __launch_bounds__(HCfg<T, RP, RATIO>::kWarps * 32, 1)
     hpass(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmW,
           const double *__restrict__ H, int n, int p, StreamK sk, double *__restrict__ part,
@@ -450,7 +452,11 @@ __global__ void __launch_bounds__(HCfg<T, RP, RATIO>::kWarps * 32, 1)
                 if constexpr (RATIO) {
                     T wh = dot<KB>(w, hcol[c]);
                     wh += __shfl_xor_sync(0xffffffffu, wh, C::LPK);  // the other k-half
-                    const T q = (wh != (T)0) ? ratio_div(v[c], wh) : (T)0;
+                    T q;
+                    if constexpr (WEIGHTED)
+                        q = v[c] * wh;
+                    else
+                        q = (wh != (T)0) ? ratio_div(v[c], wh) : (T)0;
                     axpy<KB>(acc[c], w, q);
                 } else {
                     axpy<KB>(acc[c], w, v[c]);
@@ -506,7 +512,7 @@ struct WCfg {
     static_assert(TROWS % BOXR == 0, "whole boxes");
 };
 
-template <typename T, int RP, bool RATIO>
+template <typename T, int RP, bool RATIO, bool WEIGHTED = false>
 __global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
     wpass(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmH,
           const double *__restrict__ W, int n, int p, StreamK sk, double *__restrict__ part,
@@ -632,7 +638,11 @@ __global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
                     if constexpr (RATIO) {
                         T wh = dot<KB>(wrow[q], hc);
                         wh += __shfl_xor_sync(0xffffffffu, wh, C::LPK);  // the other k-half
-                        const T qv = (wh != (T)0) ? ratio_div(v[q][e], wh) : (T)0;
+                        T qv;
+                        if constexpr (WEIGHTED)
+                            qv = v[q][e] * wh;
+                        else
+                            qv = (wh != (T)0) ? ratio_div(v[q][e], wh) : (T)0;
                         axpy<KB>(acc[q], hc, qv);
                     } else {
                         axpy<KB>(acc[q], hc, v[q][e]);
@@ -696,7 +706,10 @@ __global__ void __launch_bounds__(kThreads)
     gather_partials<RP>(part, sk, ct, (size_t)RP * tcols, c, tcols, num);
 #pragma unroll
     for (int k = 0; k < RP; k++) hc[k] = H[(size_t)k * p + j];
-    h_update<RP>(e, num, hc);
+    double ax[RP];
+#pragma unroll
+    for (int k = 0; k < RP; k++) ax[k] = (e.aux != nullptr && k < e.r) ? e.aux[(size_t)k * p + j] : 0.0;
+    h_update<RP>(e, num, hc, ax);
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) H[(size_t)k * p + j] = hc[k];
@@ -741,10 +754,13 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) num[k] += __shfl_xor_sync(0xffffffffu, num[k], o);
     if (lane != 0) return;
-    double wr[RP];
+    double wr[RP], ax[RP];
 #pragma unroll
-    for (int k = 0; k < RP; k++) wr[k] = W[(size_t)i * RP + k];
-    w_update<RP>(e, num, wr, e.roff ? e.roff[i] : 0.0);
+    for (int k = 0; k < RP; k++) {
+        wr[k] = W[(size_t)i * RP + k];
+        ax[k] = e.aux != nullptr ? e.aux[(size_t)i * RP + k] : 0.0;
+    }
+    w_update<RP>(e, num, wr, e.roff ? e.roff[i] : 0.0, ax);
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) W[(size_t)i * RP + k] = wr[k];

@@ -39,30 +39,30 @@ struct StreamOpsT final : StreamOps {
         return ratio ? WCfg<T, RP, true>::BOXR : WCfg<T, RP, false>::BOXR;
     }
 
-    template <bool RATIO>
+    template <bool RATIO, bool WEIGHTED = false>
     static cudaError_t launch_h(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
                                 int n, int p, const StreamK &sk, double *part, RunState *st,
                                 int grid, cudaStream_t s) {
         using C = HCfg<T, RP, RATIO>;
         static_assert(C::BOXC * C::NBOX == C::TCOLS, "tile / box mismatch");
         static_assert(C::BROWS == HCfg<T, RP, !RATIO>::BROWS, "one W box");
-        cudaError_t e = cudaFuncSetAttribute(nmfcu::hpass<T, RP, RATIO>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        auto *kern = nmfcu::hpass<T, RP, RATIO, WEIGHTED>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
         if (e != cudaSuccess) return e;
-        nmfcu::hpass<T, RP, RATIO><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmW, H, n, p, sk,
-                                                                        part, st);
+        kern<<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmW, H, n, p, sk, part, st);
         return cudaGetLastError();
     }
-    template <bool RATIO>
+    template <bool RATIO, bool WEIGHTED = false>
     static cudaError_t launch_w(const CUtensorMap &tmV, const CUtensorMap &tmH, const double *W,
                                 int n, int p, const StreamK &sk, double *part, RunState *st,
                                 int grid, cudaStream_t s) {
         using C = WCfg<T, RP, RATIO>;
-        cudaError_t e = cudaFuncSetAttribute(nmfcu::wpass<T, RP, RATIO>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        auto *kern = nmfcu::wpass<T, RP, RATIO, WEIGHTED>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
         if (e != cudaSuccess) return e;
-        nmfcu::wpass<T, RP, RATIO><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmH, W, n, p, sk,
-                                                                        part, st);
+        kern<<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmH, W, n, p, sk, part, st);
         return cudaGetLastError();
     }
 
@@ -77,6 +77,22 @@ struct StreamOpsT final : StreamOps {
                       RunState *st, int grid, cudaStream_t s) const override {
         return ratio ? launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s)
                      : launch_w<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+    }
+    cudaError_t hpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
+                               int n, int p, const StreamK &sk, double *part, RunState *st,
+                               int grid, cudaStream_t s) const override {
+        if constexpr (sizeof(T) == 8)
+            return launch_h<true, true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+        else
+            return cudaErrorNotSupported;
+    }
+    cudaError_t wpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmH, const double *W,
+                               int n, int p, const StreamK &sk, double *part, RunState *st,
+                               int grid, cudaStream_t s) const override {
+        if constexpr (sizeof(T) == 8)
+            return launch_w<true, true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+        else
+            return cudaErrorNotSupported;
     }
     void h_epi(double *H, void *Ht, int p, const double *part, const StreamK &sk, int tcols,
                const EpiParams &e, const RunState *st, cudaStream_t s) const override {

@@ -7,9 +7,9 @@ and ``set_num_threads``, with the iteration loop running as hand-written
 sm_100a CUDA kernels behind the C ABI of ``include/nmfcu.h``.
 
 Built methods: ``brunet`` (KL), ``lee`` (Frobenius), ``offset``, ``nsNMF``,
-``hals``, ``ehals`` and ``dnmf``, each with ``stop='max_iter'`` or
-``'stationary'``.  The other reference methods (lsNMF, snmf/r, snmf/l) raise
-``NotImplementedError``.  There is no CPU fallback: without the CUDA library
+``hals``, ``ehals``, ``dnmf`` and ``lsnmf`` (weighted, FP64), each with
+``stop='max_iter'`` or ``'stationary'``.  The Kim-Park ``snmf/r`` and
+``snmf/l`` raise ``NotImplementedError``.  There is no CPU fallback: without the CUDA library
 or a GPU every compute call raises ``RuntimeError``.
 
 Engine extensions (keyword-only, defaults keep the reference's behaviour):
@@ -171,11 +171,48 @@ def set_num_threads(n: int) -> bool:
     return _native.set_num_threads(int(n))
 
 
-def cv_rank(V: np.ndarray, ranks: Sequence[int], **kwargs):
-    """Cross-validated rank selection.  The reference fits each fold with the
-    weighted ``ls-nmf`` method, which this engine does not build."""
-    raise NotImplementedError(
-        "cv_rank() needs method='ls-nmf', which the GPU engine does not build")
+def cv_rank(V: np.ndarray, ranks: Sequence[int], *, method: str = "hals", n_folds: int = 4,
+            mask_frac: float = 0.05, max_iter: int = 100, init: str = "nndsvd", seed: int = 0,
+            num_threads: Optional[int] = None, device: int = 0, **nmf_kwargs):
+    """Cross-validated rank selection by held-out reconstruction error, the
+    reference's ``cv_rank`` (python/nmf_rs/__init__.py:273-355).
+
+    For every rank and fold a fresh seed from ``default_rng(seed)`` draws a
+    mask holding out ``mask_frac`` of V's entries; the fold is fitted with
+    the weighted ``lsnmf`` method (held-out entries weigh 0) from an NNDSVD
+    (``init='nndsvd'``) or uniform start of the masked V, and scored by the
+    0.5 weighted squared residual on the kept entries and the mean squared
+    error on the held-out ones.  ``method`` is accepted as in the reference
+    (which does not use it).  Returns a pandas DataFrame with columns rank,
+    fold, train_loss, test_mse.
+    """
+    import pandas as pd
+
+    V = _f64_c(V, "V")
+    if (V < 0).any():
+        raise ValueError("V must be non-negative")
+    n, p = V.shape
+    master = np.random.default_rng(seed)
+    rows = []
+    for k in ranks:
+        for fold in range(n_folds):
+            fold_seed = int(master.integers(0, 2**31 - 1))
+            keep = np.random.default_rng(fold_seed).random((n, p)) > mask_frac
+            weight = keep.astype(np.float64)
+            V_train = V * weight
+            if init == "nndsvd":
+                W0, H0 = nndsvd_init(V_train, k, fill="mean", seed=fold_seed, device=device)
+            else:
+                W0, H0 = random_init(V_train, k, seed=fold_seed)
+            res = nmf(V_train, rank=k, method="ls-nmf", W0=W0, H0=H0, weight=weight,
+                      max_iter=max_iter, num_threads=num_threads, device=device, **nmf_kwargs)
+            recon = res.fitted()
+            train_loss = 0.5 * float((((V - recon) * weight) ** 2).sum())
+            held = ~keep
+            test_mse = float(((V[held] - recon[held]) ** 2).mean())
+            rows.append({"rank": int(k), "fold": fold, "train_loss": train_loss,
+                         "test_mse": test_mse})
+    return pd.DataFrame(rows)
 
 
 # =============================================================================

@@ -83,6 +83,8 @@ SIGNATURES = {
                          _dp, _i64, _i64p, _i64p]),
     "nmfcu_run_offset": (_i32, [ctypes.POINTER(Options), _i64, _i64, _i64, _dp, _dp, _dp, _dp,
                                 _dp, _dp, _dp, _dp, _i64, _i64p, _i64p]),
+    "nmfcu_run_weighted": (_i32, [ctypes.POINTER(Options), _i64, _i64, _i64, _dp, _dp, _dp, _dp,
+                                  _dp, _dp, _dp, _i64, _i64p, _i64p]),
     "nmfcu_update_h_divergence": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dp]),
     "nmfcu_update_w_divergence": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dp]),
     "nmfcu_update_h_euclidean": (_i32, [_i64, _i64, _i64, _dp, _dp, _dp, _dbl, _dp]),
@@ -312,6 +314,14 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
             cap, ctypes.byref(nd), ctypes.byref(ni)))
         return {"W": W, "H": H, "offset": off, "n_iter": int(ni.value),
                 "deviances": list(dev[: nd.value])}
+    if o.method == LSNMF:
+        S = np.ascontiguousarray(np.asarray(weight, dtype=np.float64))
+        if S.shape != v.shape:
+            raise ValueError(f"weight.shape {S.shape} != V.shape {v.shape}")
+        check(load().nmfcu_run_weighted(
+            ctypes.byref(o), n, p, r, _ptr(v), _ptr(S), _ptr(w0), _ptr(h0), _ptr(W), _ptr(H),
+            _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
+        return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}
     check(load().nmfcu_run(ctypes.byref(o), n, p, r, _ptr(v), _ptr(w0), _ptr(h0), _ptr(W),
                            _ptr(H), _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
     return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}

@@ -132,3 +132,78 @@ def test_offset_rejected_where_offsets_cannot_be_returned():
             srv.submit(V, 3, "offset", W0=W0, H0=H0, max_iter=5)
         ok = srv.submit(V, 3, "nsNMF", W0=W0, H0=H0, max_iter=5).result(timeout=120)
     assert ok.n_iter == 5
+
+
+# ---------------------------------------------------------------------------
+# lsNMF (nmf_run_lsnmf, lib.rs:945-1043) and cv_rank (__init__.py:273-355)
+# ---------------------------------------------------------------------------
+
+def _ls_check(oracle, V, S, W0, H0, iters, **kw):
+    ref = oracle.nmf_method("lsnmf", V, W0, H0, iters, weight=S, **kw)
+    got = nmf_rs.nmf(V, W0.shape[1], "lsnmf", W0=W0, H0=H0, weight=S, max_iter=iters, **kw)
+    assert got.n_iter == ref["n_iter"]
+    assert rel_max(got.W, ref["W"]) <= FACTOR_TOL, rel_max(got.W, ref["W"])
+    assert rel_max(got.H, ref["H"]) <= FACTOR_TOL, rel_max(got.H, ref["H"])
+    o_got = oracle.weighted_distance(V, S, got.W, got.H)
+    o_ref = oracle.weighted_distance(V, S, ref["W"], ref["H"])
+    assert _rel_obj("offset", V * S, o_got, o_ref) <= OBJ_TOL
+    return got, ref
+
+
+@pytest.mark.parametrize("kind", ["mask", "uniform", "ones"])
+def test_lsnmf_quickstart(oracle, quickstart, kind):
+    V, W0, H0 = quickstart
+    gen = np.random.default_rng(1)
+    S = {"mask": (gen.random(V.shape) > 0.05).astype(float),
+         "uniform": gen.uniform(0.1, 2.0, V.shape),
+         "ones": np.ones_like(V)}[kind]
+    _ls_check(oracle, V, S, W0, H0, 60)
+
+
+@pytest.mark.parametrize("shape", [(300, 517, 7), (1, 40, 3), (64, 1, 2), (129, 257, 32)])
+def test_lsnmf_ragged(oracle, shape):
+    n, p, r = shape
+    V = synthetic.counts_matrix(n, p, max(1, r // 2), 0.3, seed=n * 3 + p)
+    S = np.random.default_rng(n + p).uniform(0.0, 1.0, V.shape)
+    W0, H0 = nmf_rs.random_init(V, r, seed=4)
+    _ls_check(oracle, V, S, W0, H0, 20)
+
+
+def test_lsnmf_stationary(oracle, quickstart):
+    V, W0, H0 = quickstart
+    S = (np.random.default_rng(2).random(V.shape) > 0.1).astype(float)
+    kw = dict(stop="stationary", stationary_th=1e-6, check_interval=10, check_niter=5)
+    got, ref = _ls_check(oracle, V, S, W0, H0, 200, **kw)
+    assert got.deviances.size == ref["deviances"].size == got.n_iter + 1
+    d = np.abs(got.deviances - ref["deviances"]) / np.abs(ref["deviances"])
+    assert d.max() <= 1e-10
+
+
+def test_lsnmf_arguments(quickstart):
+    V, W0, H0 = quickstart
+    with pytest.raises(ValueError, match="weight"):
+        nmf_rs.nmf(V, 5, "lsnmf", W0=W0, H0=H0, max_iter=2)
+    with pytest.raises(NotImplementedError, match="FP64"):
+        nmf_rs.nmf(V, 5, "lsnmf", W0=W0, H0=H0, weight=np.ones_like(V), max_iter=2,
+                   precision="fp32")
+
+
+def test_cv_rank_prefers_the_true_rank():
+    V = synthetic.counts_matrix(200, 300, 4, 0.3, seed=8) + 0.01
+    df = nmf_rs.cv_rank(V, [1, 4], n_folds=2, max_iter=60, seed=1)
+    assert list(df.columns) == ["rank", "fold", "train_loss", "test_mse"]
+    assert len(df) == 4
+    mse = df.groupby("rank")["test_mse"].mean()
+    assert mse[4] < mse[1]
+    again = nmf_rs.cv_rank(V, [1, 4], n_folds=2, max_iter=60, seed=1)
+    np.testing.assert_array_equal(df.to_numpy(), again.to_numpy())
+
+
+def test_ehals_kat_free_parity_from_nndsvd(oracle, quickstart):
+    # ehals has no recorded output in the reference; from an NNDSVD start its
+    # HALS sweeps are well conditioned, so the plain tolerance applies.
+    V = quickstart[0]
+    W0, H0 = nmf_rs.nndsvd_init(V, 5, fill="mean", seed=0)
+    ref = oracle.nmf_method("ehals", V, W0, H0, 80)
+    got = nmf_rs.nmf(V, 5, "ehals", W0=W0, H0=H0, max_iter=80)
+    assert rel_max(got.W, ref["W"]) <= FACTOR_TOL and rel_max(got.H, ref["H"]) <= FACTOR_TOL

@@ -134,9 +134,9 @@ def test_nmf_validation_errors():
         nmf_rs.nmf(V, 2, precision="fp16")
 
 
-def test_cv_rank_not_built():
-    with pytest.raises(NotImplementedError):
-        nmf_rs.cv_rank(np.ones((4, 4)), [2])
+def test_cv_rank_rejects_negative_v_before_any_device_work():
+    with pytest.raises(ValueError, match="non-negative"):
+        nmf_rs.cv_rank(-np.ones((4, 4)), [2])
 
 
 def test_regularisation_routing():

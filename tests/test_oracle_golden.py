@@ -9,7 +9,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import rel
+from conftest import rel, rel_max
 
 sys.path.insert(0, str(Path(__file__).resolve().parent / "golden"))
 import make_golden  # noqa: E402
@@ -164,3 +164,38 @@ def test_ehals_is_hals_from_the_extrapolated_point(oracle, quickstart):
     a2 = oracle.nmf_method("ehals", V, W0, H0, 2)
     b2 = oracle.nmf_method("hals", V, np.maximum(W0, 1e-9), np.maximum(H0, 1e-9), 2)
     assert not np.array_equal(a2["W"], b2["W"])
+
+
+def test_lsnmf_unit_weights_is_lee_without_rescale(oracle, quickstart):
+    # W^T((W H) o 1) = W^T W H and ((W H) o 1) H^T = W H H^T: lee's updates
+    # (lib.rs:990-1018 vs 213-322) up to summation order; lee's W clamp
+    # differs only for NaN.
+    V, W0, H0 = quickstart
+    a = oracle.nmf_method("lsnmf", V, W0, H0, 50, weight=np.ones_like(V))
+    b = oracle.nmf_method("lee", V, W0, H0, 50, rescale=False)
+    assert rel_max(a["W"], b["W"]) < 1e-12 and rel_max(a["H"], b["H"]) < 1e-12
+
+
+def test_lsnmf_ignores_zero_weight_entries(oracle, quickstart):
+    V, W0, H0 = quickstart
+    gen = np.random.default_rng(3)
+    S = (gen.random(V.shape) > 0.1).astype(float)
+    V2 = V.copy()
+    V2[S == 0] = 1e3  # held-out entries may hold anything
+    a = oracle.nmf_method("lsnmf", V, W0, H0, 20, weight=S)
+    b = oracle.nmf_method("lsnmf", V2, W0, H0, 20, weight=S)
+    np.testing.assert_array_equal(a["W"], b["W"])
+    np.testing.assert_array_equal(a["H"], b["H"])
+
+
+def test_lsnmf_stationary_trace(oracle, quickstart):
+    V, W0, H0 = quickstart
+    S = np.random.default_rng(5).uniform(0.2, 1.5, V.shape)
+    res = oracle.nmf_method("lsnmf", V, W0, H0, 30, weight=S, stop="stationary",
+                            check_interval=5, check_niter=2)
+    d = res["deviances"]
+    assert d.size == res["n_iter"] + 1
+    assert d[-1] == oracle.weighted_distance(V, S, res["W"], res["H"])
+    assert d[-1] < d[0]
+    with pytest.raises(ValueError, match="weight"):
+        oracle.nmf_method("lsnmf", V, W0, H0, 3)
