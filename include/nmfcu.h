@@ -229,6 +229,52 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *ctx, int32_t trans, int64_t n
                                     int64_t l, const double *dV, int64_t ldv, const double *dX,
                                     int64_t ldx, double *dOut, int64_t ldo, void *stream);
 
+/*
+ * Column shards -- one solve over several GPUs, one process a GPU.  The
+ * reference has no multi-device path; this splits its loop (nmf_run_lee
+ * lib.rs:1589-1647, nmf_run_brunet :1529-1586, nmf_run_hals :638-688,
+ * nmf_run_dnmf :827-906) by columns of V.  Each rank holds V[:, c0:c1], its
+ * H columns and a copy of W.  The H update is local; the W update needs
+ * the W contraction (V H^T, or the ratio form for brunet), H H^T and
+ * rowSums(H) summed over ranks: the caller all-reduces (sums) the reduce
+ * buffer between the two halves of an iteration, and the objective scalar
+ * between NMFCU_SHARD_OBJECTIVE and NMFCU_SHARD_STOP.  Every rank applies
+ * the same W update to its copy, so the copies stay identical.
+ *
+ * One iteration:  HALF_STEP, all-reduce(reduce buffer), W_UPDATE
+ *                 [stationary: OBJECTIVE, all-reduce(objective), STOP,
+ *                  nmfcu_shard_status -> stop when `stopped`]
+ * Before the first iteration with stop stationary: OBJECTIVE, all-reduce,
+ * STOP.  Methods brunet, lee, hals, dnmf; all three precisions.
+ *
+ * nmfcu_shard_reduce_len(n, r): doubles in the reduce buffer.
+ * nmfcu_shard_create: dV (n x p_local, pitch ldv, 16-byte aligned rows),
+ *   dW0 (n x r) and dH0 (r x p_local) are device pointers; dReduce
+ *   (reduce_len doubles) and dObjective (1 double) are the caller's device
+ *   buffers that its collective sums.  The shard uses `ctx` until destroyed.
+ * nmfcu_shard_status: synchronises `stream`; iterations done and the stop.
+ * nmfcu_shard_result: W (n x r), this shard's H (r x p_local) and the
+ *   deviances (n_iter + 1 with stop stationary) into device buffers.
+ */
+typedef struct nmfcu_shard nmfcu_shard;
+enum {
+    NMFCU_SHARD_HALF_STEP = 0,
+    NMFCU_SHARD_W_UPDATE = 1,
+    NMFCU_SHARD_OBJECTIVE = 2,
+    NMFCU_SHARD_STOP = 3
+};
+int64_t nmfcu_shard_reduce_len(int64_t n, int64_t r);
+nmfcu_status nmfcu_shard_create(nmfcu_context *ctx, const nmfcu_options *opt, int64_t n,
+                                int64_t p_local, int64_t r, const double *dV, int64_t ldv,
+                                const double *dW0, const double *dH0, double *dReduce,
+                                double *dObjective, nmfcu_shard **shard, void *stream);
+nmfcu_status nmfcu_shard_step(nmfcu_shard *shard, int32_t phase, void *stream);
+nmfcu_status nmfcu_shard_status(nmfcu_shard *shard, int64_t *n_iter, int32_t *stopped,
+                                void *stream);
+nmfcu_status nmfcu_shard_result(nmfcu_shard *shard, double *dW, double *dH, double *d_dev,
+                                int64_t *n_deviances, int64_t *n_iter, void *stream);
+void nmfcu_shard_destroy(nmfcu_shard *shard);
+
 /* Per-kernel CUDA-event timing inside nmfcu_run_device (off by default).
  * Kernel classes: 0 = H-step V contraction, 1 = W-step V contraction,
  * 2 = objective V pass, 3 = everything else (grams, epilogues, stop),

@@ -822,6 +822,44 @@ struct StopParams {
     double scale;         // 0.5 for the Frobenius objective, 1 for KL
 };
 
+// Sum of B partials in objective_finalize's order, into out[0] (a column
+// shard's objective term, before the sum over shards).
+static __global__ void sum_partials(const double *__restrict__ part, int B,
+                                    double *__restrict__ out) {
+    __shared__ double red[kThreads];
+    const int tid = threadIdx.x;
+    double a = 0.0;
+    for (int b = tid; b < B; b += kThreads) a += part[b];
+    red[tid] = a;
+    __syncthreads();
+    for (int s = kThreads / 2; s > 0; s >>= 1) {
+        if (tid < s) red[tid] += red[tid + s];
+        __syncthreads();
+    }
+    if (tid == 0) out[0] = red[0];
+}
+
+// W update from a dense contraction num (n x RP) summed over column shards:
+// one thread a row, the update of w_update.
+template <int RP>
+__global__ void __launch_bounds__(kThreads)
+    w_apply_dense(double *__restrict__ W, int n, const double *__restrict__ num, EpiParams e,
+                  const RunState *st) {
+    if (run_stopped(st)) return;
+    const int i = blockIdx.x * kThreads + threadIdx.x;
+    if (i >= n) return;
+    double nm[RP], wr[RP];
+#pragma unroll
+    for (int k = 0; k < RP; k++) {
+        nm[k] = num[(size_t)i * RP + k];
+        wr[k] = W[(size_t)i * RP + k];
+    }
+    w_update<RP>(e, nm, wr);
+#pragma unroll
+    for (int k = 0; k < RP; k++)
+        if (k < e.r) W[(size_t)i * RP + k] = wr[k];
+}
+
 static __global__ void objective_finalize(const double *__restrict__ part, int B, double *__restrict__ dev,
                                    StopParams sp, RunState *st) {
     if (st->stopped) return;

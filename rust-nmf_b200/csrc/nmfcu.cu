@@ -103,6 +103,9 @@ struct Ops {
                            const double *H, int mode, int S2, int cols_per_split, double *obj,
                            const RunState *st, cudaStream_t s,
                            const double *roff = nullptr) const = 0;
+    // W update from a dense (summed) contraction num (n x RP)
+    virtual void w_apply(double *W, int n, const double *num, const EpiParams &e,
+                         const RunState *st, cudaStream_t s) const = 0;
     // lsNMF objective partials over V o S and S: one per block, nblocks blocks
     virtual void ls_objective(const double *Vs, const double *S, int64_t ld, int n, int p,
                               const double *W, const double *H, int nblocks, double *part,
@@ -145,6 +148,10 @@ struct OpsT final : Ops {
         else
             nmfcu::rowpass<double, double, RP, 3><<<grid, block, 0, s>>>(
                 V, ldv, n, p, W, H, cols_per_split, nullptr, obj, st, roff);
+    }
+    void w_apply(double *W, int n, const double *num, const EpiParams &e, const RunState *st,
+                 cudaStream_t s) const override {
+        if (n > 0) nmfcu::w_apply_dense<RP><<<cdiv(n, kThreads), kThreads, 0, s>>>(W, n, num, e, st);
     }
     void ls_objective(const double *Vs, const double *S, int64_t ld, int n, int p,
                       const double *W, const double *H, int nblocks, double *part,
@@ -630,10 +637,11 @@ struct RunArgs {
     double *NH = nullptr, *NW = nullptr;
     PassSet pden;
     bool weighted = false;  // h_step / w_step run the weighted passes
+    double *Wout = nullptr;  // w_step's epilogue target when not W (column shards)
 };
 
-nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
-                               cudaStream_t s) {
+// The objective's per-block partials over this V (c->obj, pl.obj_blocks).
+nmfcu_status enqueue_objective_partials(nmfcu_context *c, const RunArgs &a, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     const bool kl = (a.opt->method == NMFCU_BRUNET || a.opt->method == NMFCU_NSNMF);
@@ -653,18 +661,28 @@ nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long ite
                          pl.cols_per_split, c->obj.as<double>(), st, s,
                          a.opt->method == NMFCU_OFFSET ? a.off : nullptr);
     }
+    return NMFCU_OK;
+}
+
+StopParams stop_params(const nmfcu_options *o, long long iter) {
     StopParams sp;
     sp.stationary = 1;
     sp.iter = iter;
-    sp.check_interval = a.opt->check_interval;
-    sp.check_niter = a.opt->check_niter;
-    sp.threshold = a.opt->stationary_th;
-    sp.scale = kl ? 1.0 : 0.5;
-    {
-        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-        objective_finalize<<<1, kThreads, 0, s>>>(c->obj.as<double>(), pl.n > 0 ? pl.obj_blocks : 0,
-                                                  a.dev, sp, st);
-    }
+    sp.check_interval = o->check_interval;
+    sp.check_niter = o->check_niter;
+    sp.threshold = o->stationary_th;
+    sp.scale = (o->method == NMFCU_BRUNET || o->method == NMFCU_NSNMF) ? 1.0 : 0.5;
+    return sp;
+}
+
+// Objective of iteration `iter` into the deviances and the stationary stop.
+nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long iter,
+                               cudaStream_t s) {
+    NMF_TRY(enqueue_objective_partials(c, a, s));
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    objective_finalize<<<1, kThreads, 0, s>>>(c->obj.as<double>(),
+                                              a.pl.n > 0 ? a.pl.obj_blocks : 0, a.dev,
+                                              stop_params(a.opt, iter), c->state.as<RunState>());
     return NMFCU_OK;
 }
 
@@ -744,7 +762,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                                     c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-        ps.so->w_epi(a.W, pl.n, c->part.as<double>(), sk, kTcTile, e, st, s);
+        ps.so->w_epi(a.Wout ? a.Wout : a.W, pl.n, c->part.as<double>(), sk, kTcTile, e, st, s);
         return NMFCU_OK;
     }
     const int trows = ps.so->w_trows(ratio);
@@ -761,7 +779,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                                   c->part.as<double>(), st, sk.G, s));
     }
     nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-    ps.so->w_epi(a.W, pl.n, c->part.as<double>(), sk, trows, e, st, s);
+    ps.so->w_epi(a.Wout ? a.Wout : a.W, pl.n, c->part.as<double>(), sk, trows, e, st, s);
     return NMFCU_OK;
 }
 
@@ -1453,6 +1471,19 @@ nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop) {
 
 }  // extern "C"
 
+// One rank's column shard of a solve (nmfcu_shard_*): its context (used by
+// this shard alone while it lives), plan, passes and the caller's buffers.
+struct nmfcu_shard {
+    nmfcu_context *c = nullptr;
+    nmfcu_options opt{};
+    Plan pl{};
+    RunArgs a{};
+    double *R = nullptr;     // [W contraction n x RP | H H^T RP x RP | rowSums(H) RP]
+    double *Robj = nullptr;  // this shard's objective term, then the sum over shards
+    long long it = 0;        // iterations whose W update has been applied
+    long long refine_from = LLONG_MAX;
+};
+
 namespace {
 
 // Method state set up before the first iteration: nsNMF's W S / S H buffers;
@@ -1764,6 +1795,193 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     *n_iter = ni;
     return NMFCU_OK;
 }
+
+int64_t nmfcu_shard_reduce_len(int64_t n, int64_t r) {
+    const int RP = (r >= 1 && r <= NMFCU_MAX_RANK) ? bucket_for(r) : 0;
+    if (RP == 0 || n < 0) return 0;
+    return n * RP + (int64_t)RP * RP + RP;
+}
+
+nmfcu_status nmfcu_shard_create(nmfcu_context *c, const nmfcu_options *opt, int64_t n,
+                                int64_t p_local, int64_t r, const double *dV, int64_t ldv,
+                                const double *dW0, const double *dH0, double *dReduce,
+                                double *dObjective, nmfcu_shard **out, void *stream) {
+    if (!c || !out) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    *out = nullptr;
+    NMF_TRY(validate_options(opt, n, p_local, r));
+    switch (opt->method) {
+        case NMFCU_BRUNET: case NMFCU_LEE: case NMFCU_HALS: case NMFCU_DNMF: break;
+        default:
+            return fail(NMFCU_ERR_UNSUPPORTED,
+                        "column shards run brunet, lee, hals and dnmf");
+    }
+    if (!dW0 || !dReduce || !dObjective || (p_local > 0 && (!dV || !dH0)))
+        return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    if (ldv < p_local) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p_local");
+    if (p_local > 0 && !tma_layout_ok(dV, ldv, 8))
+        return fail(NMFCU_ERR_INVALID_ARG,
+                    "the shard's V must be 16-byte aligned with a 16-byte row pitch");
+    std::unique_ptr<nmfcu_shard> sh(new nmfcu_shard());
+    sh->c = c;
+    sh->opt = *opt;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const nmfcu_options *o = &sh->opt;
+    const Plan pl = make_plan(n, p_local, r, c->sms);
+    const bool f32 = f32_form(o), tc = tc_form(o);
+    const bool stat = o->stop == NMFCU_STOP_STATIONARY;
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, o->method));
+    if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(o->max_iter + 1)));
+    NMF_TRY(put_factors(c, pl, dW0, dH0, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
+    CUDA_TRY(cudaMemsetAsync(dReduce, 0, sizeof(double) * (size_t)nmfcu_shard_reduce_len(n, r), s));
+    RunArgs &a = sh->a;
+    a.opt = o;
+    a.pl = pl;
+    a.ops = ops_for(pl.RP);
+    const bool ratio = (o->method == NMFCU_BRUNET);
+    NMF_TRY(make_passset(c, pl, false, ratio, dV, ldv, &a.p64));
+    if (tc) {
+        NMF_TRY(make_tc_passset(c, pl, dV, ldv, s, &a.main));
+    } else if (f32) {
+        int64_t ld32 = 0;
+        NMF_TRY(make_f32(c, dV, ldv, n, p_local, &ld32, s));
+        NMF_TRY(make_passset(c, pl, true, ratio, c->V32.ptr, ld32, &a.main));
+    } else {
+        a.main = a.p64;
+    }
+    a.V64 = dV;
+    a.ldv64 = ldv;
+    a.W = c->W.as<double>();
+    a.H = c->H.as<double>();
+    a.dev = stat ? c->dev.as<double>() : nullptr;
+    sh->pl = pl;
+    sh->R = dReduce;
+    sh->Robj = dObjective;
+    sh->refine_from =
+        (o->precision != NMFCU_PREC_FP64) ? (long long)o->max_iter - o->refine_iters : LLONG_MAX;
+    CUDA_TRY(cudaGetLastError());
+    *out = sh.release();
+    return NMFCU_OK;
+}
+
+nmfcu_status nmfcu_shard_step(nmfcu_shard *sh, int32_t phase, void *stream) {
+    if (!sh) return fail(NMFCU_ERR_INVALID_ARG, "NULL shard");
+    nmfcu_context *c = sh->c;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    const nmfcu_options *o = &sh->opt;
+    const RunArgs &a = sh->a;
+    const Plan &pl = sh->pl;
+    RunState *st = c->state.as<RunState>();
+    double *Rnum = sh->R;
+    double *RG = Rnum + (size_t)pl.n * pl.RP;
+    double *Rs = RG + (size_t)pl.RP * pl.RP;
+    switch (phase) {
+        case NMFCU_SHARD_HALF_STEP: {
+            // The H update on this shard's columns (W replicated), then this
+            // shard's terms of H H^T / rowSums(H) and of the W contraction.
+            const long long itn = sh->it + 1;
+            if (itn > o->max_iter) return fail(NMFCU_ERR_INVALID_ARG, "max_iter reached");
+            const bool fp64 = (o->precision == NMFCU_PREC_FP64) || (itn > sh->refine_from);
+            const PassSet &ps = fp64 ? a.p64 : a.main;
+            const bool ratio = (o->method == NMFCU_BRUNET);
+            double *Gw = c->Gw.as<double>(), *sw = c->sw.as<double>();
+            gram_w_full(c, a, Gw, sw, s);
+            NMF_TRY(h_step(c, a, ps, epi(o, pl.r, Gw, sw, true), ratio, s));
+            gram_h_full(c, a, RG, Rs, s);
+            RunArgs aw = a;
+            aw.Wout = Rnum;
+            EpiParams ep = epi(o, pl.r, nullptr, nullptr, false);
+            ep.method = nmfcu::M_PRODUCT;
+            NMF_TRY(w_step(c, aw, ps, ep, ratio, s));
+            break;
+        }
+        case NMFCU_SHARD_W_UPDATE: {
+            // The W update from the contraction and Grams summed over shards;
+            // every shard applies it to its identical copy of W.
+            const long long itn = sh->it + 1;
+            {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->w_apply(a.W, pl.n, Rnum, epi(o, pl.r, RG, Rs, false), st, s);
+            }
+            if (o->method == NMFCU_BRUNET && itn % 10 == 0) {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->clamp(a.W, a.H, pl.n, pl.p, pl.r, DBL_EPSILON, st, s);
+            } else if (o->method == NMFCU_LEE && o->rescale) {
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
+                a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(),
+                              c->ps.as<double>(), st, s);
+                a.ops->rescale(a.W, pl.n, pl.r, c->ps.as<double>(), pl.Bw, st, s);
+            } else if (o->method == NMFCU_DNMF) {
+                gram_w_full(c, a, c->Gw2.as<double>(), c->sw2.as<double>(), s);
+                nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+                a.ops->dnmf_scale(a.W, a.H, pl.n, pl.p, pl.r, c->Gw2.as<double>(), RG, st, s);
+            }
+            sh->it = itn;
+            break;
+        }
+        case NMFCU_SHARD_OBJECTIVE: {
+            if (o->stop != NMFCU_STOP_STATIONARY)
+                return fail(NMFCU_ERR_INVALID_ARG, "the objective runs with stop stationary");
+            NMF_TRY(enqueue_objective_partials(c, a, s));
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            sum_partials<<<1, kThreads, 0, s>>>(c->obj.as<double>(),
+                                                pl.n > 0 ? pl.obj_blocks : 0, sh->Robj);
+            break;
+        }
+        case NMFCU_SHARD_STOP: {
+            if (o->stop != NMFCU_STOP_STATIONARY)
+                return fail(NMFCU_ERR_INVALID_ARG, "the stop test runs with stop stationary");
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            objective_finalize<<<1, kThreads, 0, s>>>(sh->Robj, 1, a.dev,
+                                                      stop_params(o, sh->it), st);
+            break;
+        }
+        default: return fail(NMFCU_ERR_INVALID_ARG, "unknown shard phase");
+    }
+    CUDA_TRY(cudaGetLastError());
+    return NMFCU_OK;
+}
+
+nmfcu_status nmfcu_shard_status(nmfcu_shard *sh, int64_t *n_iter, int32_t *stopped, void *stream) {
+    if (!sh || !n_iter || !stopped) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    nmfcu_context *c = sh->c;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    NMF_TRY(finish_checked(c, (cudaStream_t)stream));
+    const RunState &hs = *c->h_state;
+    if (hs.error == 1)
+        return fail(NMFCU_ERR_INVALID_ARG,
+                    "check_interval must be > 0 (the stationary stop evaluates iter % check_interval)");
+    *stopped = hs.stopped ? 1 : 0;
+    *n_iter = hs.stopped ? hs.n_iter : sh->it;
+    return NMFCU_OK;
+}
+
+nmfcu_status nmfcu_shard_result(nmfcu_shard *sh, double *dW, double *dH, double *d_dev,
+                                int64_t *n_deviances, int64_t *n_iter, void *stream) {
+    if (!sh || !dW || !n_deviances || !n_iter || (sh->pl.p > 0 && !dH))
+        return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    int32_t stopped = 0;
+    NMF_TRY(nmfcu_shard_status(sh, n_iter, &stopped, stream));
+    nmfcu_context *c = sh->c;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    cudaStream_t s = (cudaStream_t)stream;
+    NMF_TRY(get_factors(c, sh->pl, dW, dH, cudaMemcpyDeviceToDevice, s));
+    const bool stat = sh->opt.stop == NMFCU_STOP_STATIONARY;
+    *n_deviances = stat ? *n_iter + 1 : 0;
+    if (stat && d_dev && *n_deviances > 0)
+        CUDA_TRY(cudaMemcpyAsync(d_dev, c->dev.ptr, sizeof(double) * (size_t)*n_deviances,
+                                 cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return NMFCU_OK;
+}
+
+void nmfcu_shard_destroy(nmfcu_shard *sh) { delete sh; }
 
 nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, int64_t p,
                                     int64_t l, const double *dV, int64_t ldv, const double *dX,
