@@ -724,7 +724,8 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     }
     const int tcols = ps.so->h_tcols(ratio);
     const StreamK sk = plan_h(ps.so, ratio, pl.n, pl.p, c->sms);
-    const int kclass = (&ps == &a.p64 && a.opt->precision != NMFCU_PREC_FP64)
+    // An f64 pass in a reduced-precision run is a refinement iteration.
+    const int kclass = (!ps.f32 && a.opt->precision != NMFCU_PREC_FP64)
                            ? NMFCU_KCLASS_HSTEP_REFINE : NMFCU_KCLASS_HSTEP;
     if (ps.f32 && pl.n > 0) {
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -767,7 +768,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     }
     const int trows = ps.so->w_trows(ratio);
     const StreamK sk = plan_w(ps.so, ratio, pl.n, pl.p, c->sms);
-    const int kclass = (&ps == &a.p64 && a.opt->precision != NMFCU_PREC_FP64)
+    const int kclass = (!ps.f32 && a.opt->precision != NMFCU_PREC_FP64)
                            ? NMFCU_KCLASS_WSTEP_REFINE : NMFCU_KCLASS_WSTEP;
     if (sk.G > 0) {
         nmfcu_context::Scope sc(c, s, kclass);
