@@ -330,6 +330,22 @@ nmfcu_status nmfcu_consensus_device(nmfcu_context *ctx, int64_t p, int32_t nsolv
                                     const int32_t *ranks, const double *dH, int32_t nsel,
                                     const int32_t *sel, float *d_out, void *stream);
 
+/*
+ * nmfcu_consensus_stats_device -- the two summaries of a consensus matrix in
+ * the reference's consensus workflow (examples/build_scaling_notebook.py
+ * :126-141), computed on the device from C (p x p f32, pitch ldc, device):
+ *   *cophenetic -- Brunet et al. (2004): the correlation over the pairs
+ *     i < j between the distances 1 - C_ij and their cophenetic distances in
+ *     the average-linkage tree of 1 - C (the tree scipy's linkage builds,
+ *     ties included); 1 when either has no spread.
+ *   *dispersion -- Kim & Park (2007): mean over all p^2 entries of
+ *     4 (C_ij - 0.5)^2 (diagonal taken as 1).
+ * Uses p^2 doubles of context scratch; returns once both are on the host.
+ */
+nmfcu_status nmfcu_consensus_stats_device(nmfcu_context *ctx, int64_t p, const float *dC,
+                                          int64_t ldc, double *cophenetic, double *dispersion,
+                                          void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Serving: continuous batching of independent factorisations              */
 /* ---------------------------------------------------------------------- */

@@ -99,6 +99,9 @@ SIGNATURES = {
                                 ctypes.c_void_p, _i32, _i64, ctypes.c_void_p, _i64,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64p, _i64p,
                                 ctypes.c_void_p]),
+    "nmfcu_consensus_stats_device": (_i32, [ctypes.c_void_p, _i64, ctypes.c_void_p, _i64,
+                                            ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
     "nmfcu_shard_reduce_len": (_i64, [_i64, _i64]),
     "nmfcu_shard_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64, _i64,
                                   ctypes.c_void_p, _i64, ctypes.c_void_p, ctypes.c_void_p,

@@ -32,6 +32,7 @@ __all__ = [
     "connectivity_matrix",
     "cophenetic_correlation",
     "dispersion_coefficient",
+    "consensus_stats",
 ]
 
 
@@ -47,20 +48,49 @@ def connectivity_matrix(H: np.ndarray) -> np.ndarray:
 
 def cophenetic_correlation(consensus: np.ndarray) -> float:
     """Correlation between 1 - C and the cophenetic distances of an
-    average-linkage tree built on 1 - C (Brunet et al. 2004)."""
+    average-linkage tree built on 1 - C (Brunet et al. 2004), on the host
+    with scipy; 1 when either has no spread.
+
+    The notebook helper this follows (build_scaling_notebook.py:126-137)
+    takes element 0 of ``cophenet(Z, cond)`` -- the coefficient itself --
+    as the cophenetic distances and then returns 1.0 because a scalar has no
+    spread, so it reports 1.0 for every matrix; this returns the
+    coefficient.  ``consensus_stats`` computes the same on the GPU."""
     from scipy.cluster.hierarchy import cophenet, linkage
     from scipy.spatial.distance import squareform
 
     c = np.array(consensus, dtype=np.float64, copy=True)
     np.fill_diagonal(c, 1.0)
     cond = squareform(1.0 - c, checks=False)
-    Z = linkage(cond, method="average")
-    coph = cophenet(Z, cond)
-    if isinstance(coph, tuple):
-        coph = coph[0]
-    if cond.std() == 0 or coph.std() == 0:
+    if cond.size < 2 or cond.std() == 0:
         return 1.0
-    return float(np.corrcoef(cond, coph)[0, 1])
+    coef, coph = cophenet(linkage(cond, method="average"), cond)
+    if coph.std() == 0:
+        return 1.0
+    return float(coef)
+
+
+def consensus_stats(C, ctx=None) -> tuple[float, float]:
+    """(cophenetic correlation, dispersion coefficient) of a consensus
+    matrix held on the GPU (f32 torch tensor, p x p, unit column stride),
+    computed there (``nmfcu_consensus_stats_device``: average linkage by the
+    nearest-neighbour chain, the same tree as scipy's)."""
+    import torch
+
+    if C.device.type != "cuda" or C.dtype != torch.float32 or C.stride(1) != 1:
+        raise ValueError("C must be an f32 CUDA tensor with unit column stride")
+    own = ctx is None
+    ctx = ctx or _native.Context(C.device.index or 0)
+    coph, disp = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    try:
+        _native.check(_native.load().nmfcu_consensus_stats_device(
+            ctx.handle, C.shape[0], ctypes.c_void_p(C.data_ptr()), C.stride(0),
+            ctypes.byref(coph), ctypes.byref(disp),
+            ctypes.c_void_p(torch.cuda.current_stream(C.device).cuda_stream)))
+    finally:
+        if own:
+            ctx.close()
+    return float(coph.value), float(disp.value)
 
 
 def dispersion_coefficient(consensus: np.ndarray) -> float:
@@ -131,7 +161,9 @@ def consensus_sweep(V: np.ndarray, ranks: Iterable[int] = range(2, 11), n_runs: 
 
     Returns ``{"per_rank": {k: {"consensus", "cophenetic", "dispersion"}},
     "W", "H", "ranks", "solve_seconds", "consensus_seconds"}`` with the
-    stacked factors of all solves (rank-major, run-minor)."""
+    stacked factors of all solves (rank-major, run-minor).  The consensus
+    matrices and, with ``metrics``, their cophenetic correlation and
+    dispersion are computed on the GPU (``consensus_seconds``)."""
     import torch
 
     ranks = [int(k) for k in ranks]
@@ -177,21 +209,22 @@ def consensus_sweep(V: np.ndarray, ranks: Iterable[int] = range(2, 11), n_runs: 
     out = {"per_rank": {}, "solve_seconds": time.perf_counter() - t0}
     cons = torch.empty((p, p), dtype=torch.float32, device=dev)
     t1 = time.perf_counter()
-    mats = {}
+    mats, stats = {}, {}
     for ci, k in enumerate(ranks):
         sel = np.arange(ci * n_runs, (ci + 1) * n_runs, dtype=np.int32)
         _native.check(lib.nmfcu_consensus_device(
             ctx.handle, p, len(rk), _ranks_ptr(rk), ctypes.c_void_p(dH.data_ptr()), len(sel),
             _ranks_ptr(sel), ctypes.c_void_p(cons.data_ptr()),
             ctypes.c_void_p(stream.cuda_stream)))
+        if metrics:
+            stats[k] = consensus_stats(cons, ctx)
         mats[k] = cons.cpu().numpy()
     torch.cuda.synchronize(dev)
     out["consensus_seconds"] = time.perf_counter() - t1
     for k in ranks:
         entry = {"consensus": mats[k]}
         if metrics:
-            entry["cophenetic"] = cophenetic_correlation(mats[k])
-            entry["dispersion"] = dispersion_coefficient(mats[k])
+            entry["cophenetic"], entry["dispersion"] = stats[k]
         out["per_rank"][k] = entry
     out["W"] = dW.cpu().numpy()
     out["H"] = dH.cpu().numpy()

@@ -138,3 +138,47 @@ def test_consensus_sweep_batched_equals_one_by_one():
         np.testing.assert_allclose(ca, _numpy_consensus(Hs), rtol=0, atol=1e-7)
         assert -1.0 <= a["per_rank"][k]["cophenetic"] <= 1.0
         assert 0.0 <= a["per_rank"][k]["dispersion"] <= 1.0
+        host = consensus.cophenetic_correlation(a["per_rank"][k]["consensus"])
+        assert a["per_rank"][k]["cophenetic"] == pytest.approx(host, abs=1e-10)
+
+
+# ---------------------------------------------------------------------------
+# Consensus statistics on the device (nmfcu_consensus_stats_device)
+# ---------------------------------------------------------------------------
+
+def _tied_consensus(p, runs, k, seed, noise):
+    gen = np.random.default_rng(seed)
+    truth = gen.integers(0, k, p)
+    C = np.zeros((p, p))
+    for _ in range(runs):
+        lab = np.where(gen.random(p) < noise, gen.integers(0, k, p), truth)
+        C += lab[:, None] == lab[None, :]
+    return (C / runs).astype(np.float32)
+
+
+@pytest.mark.parametrize("p,runs,k,seed,noise", [(60, 8, 3, 0, 0.3), (300, 64, 5, 1, 0.4),
+                                                 (1500, 64, 6, 2, 0.25), (2, 4, 2, 3, 0.5),
+                                                 (1, 4, 2, 4, 0.5)])
+def test_consensus_stats_match_scipy(p, runs, k, seed, noise):
+    import torch
+
+    from nmf_rs import consensus
+
+    C = _tied_consensus(p, runs, k, seed, noise)
+    coph, disp = consensus.consensus_stats(torch.from_numpy(C).cuda())
+    assert coph == pytest.approx(consensus.cophenetic_correlation(C), abs=1e-10)
+    assert disp == pytest.approx(consensus.dispersion_coefficient(
+        np.where(np.eye(p, dtype=bool), 1.0, C.astype(np.float64))), abs=1e-12)
+
+
+def test_consensus_stats_pitched_input():
+    import torch
+
+    from nmf_rs import consensus
+
+    C = _tied_consensus(200, 16, 4, 7, 0.3)
+    buf = torch.zeros((200, 256), dtype=torch.float32, device="cuda")
+    buf[:, :200] = torch.from_numpy(C)
+    a = consensus.consensus_stats(buf[:, :200])
+    b = consensus.consensus_stats(torch.from_numpy(C).cuda())
+    assert a == b

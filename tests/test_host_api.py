@@ -230,3 +230,21 @@ def test_server_needs_a_device_and_checks_its_arguments():
     if _native.device_count() == 0:
         with pytest.raises(RuntimeError):
             serve.Server(slots=2)
+
+
+def test_cophenetic_is_the_coefficient_not_the_notebook_constant():
+    from scipy.cluster.hierarchy import cophenet, linkage
+    from scipy.spatial.distance import squareform
+
+    from nmf_rs import consensus
+
+    gen = np.random.default_rng(0)
+    C = np.zeros((30, 30))
+    for _ in range(10):
+        lab = gen.integers(0, 3, 30)
+        C += lab[:, None] == lab[None, :]
+    C /= 10
+    cond = squareform(1.0 - C, checks=False)
+    expected = cophenet(linkage(cond, method="average"), cond)[0]
+    assert consensus.cophenetic_correlation(C) == pytest.approx(expected, abs=1e-15)
+    assert expected < 0.99
