@@ -41,8 +41,9 @@ of the whole problem per second.
 --form consensus measures the batching form instead: a consensus sweep of
 64 brunet restarts x ranks 2..10 (576 solves x 200 iterations) on a
 2000 x 5000 V, one step = one whole sweep through nmfcu_run_batch_device
-plus the nine consensus matrices, against the same solves run one by one
-through the single-solve engine.
+plus the nine consensus matrices and their cophenetic correlation and
+dispersion (nmfcu_consensus_stats_device), against the same solves run one
+by one through the single-solve engine.
 """
 from __future__ import annotations
 
@@ -608,9 +609,28 @@ def consensus_inputs(runs, seed=7):
     return V, starts
 
 
+def host_linkage_seconds(p, runs=64, k=6, seed=0):
+    """One cophenetic correlation on the host the way the reference workflow
+    computes it (scipy average linkage + cophenet on 1 - C, p x p)."""
+    from nmf_rs import consensus
+
+    gen = np.random.default_rng(seed)
+    truth = gen.integers(0, k, p)
+    C = np.zeros((p, p), dtype=np.float32)
+    for _ in range(runs):
+        lab = np.where(gen.random(p) < 0.3, gen.integers(0, k, p), truth)
+        C += lab[:, None] == lab[None, :]
+    C /= runs
+    t0 = time.perf_counter()
+    consensus.cophenetic_correlation(C)
+    consensus.dispersion_coefficient(C)
+    return time.perf_counter() - t0
+
+
 def consensus_cpu_baseline(V, runs, seconds, iters=200):
     """The oracle's brunet iteration per rank on a column slice,
-    extrapolated to runs x 200 iterations per rank over the full V."""
+    extrapolated to runs x 200 iterations per rank over the full V, plus
+    each rank's cophenetic correlation and dispersion on the host."""
     from nmf_rs import consensus
 
     c = CONSENSUS
@@ -624,11 +644,15 @@ def consensus_cpu_baseline(V, runs, seconds, iters=200):
         b = cpu_baseline(fn, c["n"], c["p"], r, "brunet", seconds / len(c["ranks"]))
         total += runs * iters / b["value"]
         samples.append(b["sample"].split(" took ")[1].split(";")[0])
+    t_link = host_linkage_seconds(c["p"])
+    total += len(c["ranks"]) * t_link
     return {"value": runs * len(c["ranks"]) / total, "unit": "solves/s",
             "cores": os.cpu_count() or 1, "kind": "port",
             "sample": ("1 brunet iteration of the CPU restatement (oracle/, OpenMP) per rank "
                        "2..10 on a column slice of V (" + ", ".join(samples) + "), "
-                       f"extrapolated to {runs} restarts x {iters} iterations on 2000x5000")}
+                       f"extrapolated to {runs} restarts x {iters} iterations on 2000x5000; "
+                       f"plus 9 x {t_link:.2f} s of scipy average linkage + cophenet + "
+                       f"dispersion on a {c['p']}x{c['p']} consensus matrix")}
 
 
 def run_consensus_reference(args, world, rank):
@@ -702,6 +726,7 @@ def run_consensus(args, world, rank, local):
                 ctx.handle, p, nsolves, rp, ctypes.c_void_p(dH.data_ptr()), runs,
                 sel.ctypes.data_as(i32p), ctypes.c_void_p(cons.data_ptr()),
                 ctypes.c_void_p(stream.cuda_stream)))
+            consensus.consensus_stats(cons, ctx)  # cophenetic + dispersion, on the GPU
 
     warm = max(3, args.warmup)
     steps = args.steps or 3
@@ -758,8 +783,15 @@ def run_consensus(args, world, rank, local):
     # End to end: host V in, stacked factors and consensus matrices out.
     t0 = time.perf_counter()
     consensus.consensus_sweep(V, c["ranks"], runs, iters, precision=args.precision,
-                              device=local, metrics=False)
+                              device=local, metrics=True)
     t_e2e = time.perf_counter() - t0
+    # The consensus statistics alone: device vs the host (scipy) path.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        consensus.consensus_stats(cons, ctx)
+    stats_ms = (time.perf_counter() - t0) / 3 * 1000.0
+    host_stats_ms = host_linkage_seconds(p) * 1000.0
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = consensus_cpu_baseline(V, runs, args.cpu_seconds, iters)
@@ -781,12 +813,14 @@ def run_consensus(args, world, rank, local):
             "batched_over_one_by_one": value / seq_value if seq_value else None,
             "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled",
             "max_rel_dH_batched_vs_single": dh_rel,
+            "consensus_stats_ms_per_rank": stats_ms,
+            "host_scipy_stats_ms_per_rank": host_stats_ms,
             "cpu_baseline": cpu,
             "e2e": {"value": world * nsolves / t_e2e, "unit": "solves/s",
                     "h2d_bytes_per_step": V.nbytes + W0.nbytes + H0.nbytes,
                     "d2h_bytes_per_step": W0.nbytes + H0.nbytes + len(c["ranks"]) * p * p * 4,
-                    "note": "consensus_sweep: host V/starts in, stacked W/H and 9 consensus "
-                            "matrices out; cophenetic/dispersion (host scipy) not timed"},
+                    "note": "consensus_sweep: host V/starts in, stacked W/H, 9 consensus "
+                            "matrices and their cophenetic/dispersion (on the GPU) out"},
         }), flush=True)
     ctx.close()
 
