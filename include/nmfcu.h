@@ -307,7 +307,8 @@ int64_t nmfcu_context_launch_count(nmfcu_context *ctx);
  * with off_s = ranks[0] + ... + ranks[s-1].  Every solve runs exactly
  * max_iter iterations.  method must be NMFCU_BRUNET (others:
  * NMFCU_ERR_UNSUPPORTED).  precision FP64 gives each solve's single-solve
- * result to rounding; FP32 computes in f32 from an f32 copy of V.
+ * result to rounding; FP32 (and BF16X3, which runs brunet as FP32, as the
+ * single solve does) computes in f32 from an f32 copy of V.
  */
 nmfcu_status nmfcu_run_batch(int32_t method, int32_t precision, int64_t max_iter, int64_t n,
                              int64_t p, const double *V, int32_t nsolves, const int32_t *ranks,

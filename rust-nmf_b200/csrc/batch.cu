@@ -571,7 +571,10 @@ nmfcu_status validate_batch(int32_t method, int32_t precision, int64_t max_iter,
                             int64_t p, int32_t nsolves, const int32_t *ranks) {
     if (method != NMFCU_BRUNET)
         return fail(NMFCU_ERR_UNSUPPORTED, "batched solves are built for brunet only");
-    if (precision != NMFCU_PREC_FP64 && precision != NMFCU_PREC_FP32)
+    // BF16X3 runs brunet (whose ratio is formed per element) as FP32, as the
+    // single solve does.
+    if (precision != NMFCU_PREC_FP64 && precision != NMFCU_PREC_FP32 &&
+        precision != NMFCU_PREC_BF16X3)
         return fail(NMFCU_ERR_INVALID_ARG, "unknown precision id");
     if (max_iter < 0) return fail(NMFCU_ERR_INVALID_ARG, "max_iter must be >= 0");
     if (n < 1 || p < 1 || n > INT32_MAX || p > INT32_MAX)
