@@ -714,6 +714,15 @@ def run_consensus(args, world, rank, local):
     cons = torch.empty((p, p), dtype=torch.float32, device=dev)
     sels = [np.arange(ci * runs, (ci + 1) * runs, dtype=np.int32) for ci in range(len(c["ranks"]))]
 
+    def post():
+        """The nine consensus matrices and their statistics (dH: all solves)."""
+        for sel in sels:
+            _native.check(lib.nmfcu_consensus_device(
+                ctx.handle, p, nsolves, rp, ctypes.c_void_p(dH.data_ptr()), runs,
+                sel.ctypes.data_as(i32p), ctypes.c_void_p(cons.data_ptr()),
+                ctypes.c_void_p(stream.cuda_stream)))
+            consensus.consensus_stats(cons, ctx)  # cophenetic + dispersion, on the GPU
+
     def batched_sweep():
         dW.copy_(dW0)
         dH.copy_(dH0)
@@ -721,12 +730,7 @@ def run_consensus(args, world, rank, local):
             ctx.handle, _native.parse_method("brunet"), prec, iters, n, p,
             ctypes.c_void_p(dV.data_ptr()), p, nsolves, rp, ctypes.c_void_p(dW.data_ptr()),
             ctypes.c_void_p(dH.data_ptr()), ctypes.c_void_p(stream.cuda_stream)))
-        for sel in sels:
-            _native.check(lib.nmfcu_consensus_device(
-                ctx.handle, p, nsolves, rp, ctypes.c_void_p(dH.data_ptr()), runs,
-                sel.ctypes.data_as(i32p), ctypes.c_void_p(cons.data_ptr()),
-                ctypes.c_void_p(stream.cuda_stream)))
-            consensus.consensus_stats(cons, ctx)  # cophenetic + dispersion, on the GPU
+        post()
 
     warm = max(3, args.warmup)
     steps = args.steps or 3
@@ -776,6 +780,11 @@ def run_consensus(args, world, rank, local):
             h = one(s_)
         torch.cuda.synchronize()
         t_seq = (time.perf_counter() - t0) * runs / seq_runs
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        post()  # the same consensus matrices and statistics as the batched step
+        torch.cuda.synchronize()
+        t_seq += time.perf_counter() - t0
         seq_value = nsolves / t_seq
         a, r = int(offs[pick[-1]]), int(ranks[pick[-1]])
         dh_rel = float((h - dH[a:a + r]).abs().max() / h.abs().max())
@@ -801,7 +810,7 @@ def run_consensus(args, world, rank, local):
                       f"{iters} iterations, 2000x5000)",
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": steps, "warmup": warm,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "dtype": "f64" if args.precision == "fp64" else "f32",
             "data": "synthetic (seeded single-cell-like generator)",
             "config": {"workload": "consensus-sweep", "n": n, "p": p, "ranks": "2..10",
                        "restarts": runs, "iters": iters, "solves": nsolves, "sum_rank": rtot,
@@ -811,7 +820,8 @@ def run_consensus(args, world, rank, local):
             "clocks": clocks,
             "one_by_one_solves_per_s": seq_value,
             "batched_over_one_by_one": value / seq_value if seq_value else None,
-            "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled",
+            "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled; plus "
+                                 "the same consensus matrices and statistics",
             "max_rel_dH_batched_vs_single": dh_rel,
             "consensus_stats_ms_per_rank": stats_ms,
             "host_scipy_stats_ms_per_rank": host_stats_ms,
