@@ -665,6 +665,319 @@ __global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
 }
 
 // ---------------------------------------------------------------------------
+// FP64 plain passes on the FP64 tensor cores (lee / hals / dnmf / offset,
+// the lsNMF numerators and the NNDSVD products in the plain method)
+// ---------------------------------------------------------------------------
+// mma.sync.m8n8k4 with f64 operands: D (8 x 8) += A (8 x 4) B (4 x 8), one
+// A and one B element and two D elements a thread (A[g][q], B[q][g],
+// D[g][2q + e] with g = lane / 4, q = lane % 4).  One instruction does 256
+// FMAs, where the CUDA-core passes issue one DFMA (and its operand loads)
+// per 32; the ring, stream-K split and partial layouts are the CUDA-core
+// passes' own, so the epilogues are shared.
+__device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d[0]), "+d"(d[1])
+                 : "d"(a), "d"(b));
+}
+
+// H pass: A[k][j] = sum_u W[u][k] V[u][j] with M = k (rank tiles of 8), N = j
+// (4 column tiles of 8 a warp), K = u (4 rows a k-step, 2 k-steps a unit).
+template <int RP>
+struct DHCfg {
+    static constexpr int MT = (RP + 7) / 8;
+    // 16 warps of at most 128 registers; ranks above 24 (four rank tiles of
+    // accumulators) take 8 warps and their 255 registers.
+    static constexpr int kWarps = MT >= 4 ? 8 : 16;
+    static constexpr int NT = 4;
+    static constexpr int WCOLS = NT * 8;
+    static constexpr int TCOLS = kWarps * WCOLS;  // 512 columns a tile
+    static constexpr int BOXC = 256;
+    static constexpr int NBOX = TCOLS / BOXC;
+    static constexpr int BROWS = 8;
+    static constexpr int SEGU = kSegSpan / BROWS;
+    static constexpr int RPS = RankPad<double, RP>::RPS;
+    static constexpr int VBYTES = BROWS * TCOLS * 8;
+    static constexpr int WBYTES = BROWS * RPS * 8;
+    static constexpr int STAGE = (VBYTES + WBYTES + 1023) / 1024 * 1024;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
+    static constexpr int STAGES = STAGES_FIT > 10 ? 10 : STAGES_FIT;
+    static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
+    static_assert(WCOLS <= BOXC && BOXC % WCOLS == 0, "a warp's columns lie in one box");
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
+};
+
+template <int RP>
+__global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
+    hpass_dmma(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmW,
+               int n, int p, StreamK sk, double *__restrict__ part, RunState *st) {
+    using C = DHCfg<RP>;
+    if (run_stopped(st)) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = (threadIdx.x == 0);
+    const int b = blockIdx.x;
+    const long long u0 = sk.start(b), u1 = sk.start(b + 1);
+    const long long nunits = u1 - u0;
+
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int rb = c.along(sk);
+#pragma unroll
+        for (int q = 0; q < C::NBOX; q++)
+            tma_load_2d(stg + q * C::BROWS * C::BOXC * 8, &tmV, bar,
+                        c.major * C::TCOLS + q * C::BOXC, rb * C::BROWS);
+        tma_load_2d(stg + C::VBYTES, &tmW, bar, 0, rb * C::BROWS);
+    };
+    UnitCursor ahead;
+    ahead.init(sk, u0);
+    if (producer) {
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            arrivals[s] = 0;
+        }
+        fence_mbar_init();
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::WBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
+    }
+    __syncthreads();
+
+    const int g = lane >> 2, q4 = lane & 3;
+    const int wc0 = warp * C::WCOLS;  // this warp's first column in the tile
+    const int vbox = wc0 / C::BOXC, voff = wc0 % C::BOXC;
+    double acc[C::MT][C::NT][2];
+    int cur = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
+    bool ok = true;
+
+    auto flush = [&](int t) {
+        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS;
+#pragma unroll
+        for (int mt = 0; mt < C::MT; mt++) {
+            const int k = mt * 8 + g;
+            if (k < RP) {
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) {
+                    double *d = dst + (size_t)k * C::TCOLS + wc0 + nt * 8 + 2 * q4;
+                    d[0] = acc[mt][nt][0];
+                    d[1] = acc[mt][nt][1];
+                }
+            }
+        }
+    };
+
+    for (long long i = 0; i < nunits; ++i) {
+        const int t = uc.t;
+        if (t != cur) {
+            if (cur >= 0) flush(cur);
+            cur = t;
+#pragma unroll
+            for (int mt = 0; mt < C::MT; mt++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+        }
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
+            record_timeout(st, TIMEOUT_FULL);
+            ok = false;
+            break;
+        }
+        const unsigned char *stg = smem + s * C::STAGE;
+        const double *sv =
+            reinterpret_cast<const double *>(stg) + vbox * C::BROWS * C::BOXC + voff + g;
+        const double *sw = reinterpret_cast<const double *>(stg + C::VBYTES);
+#pragma unroll
+        for (int ks = 0; ks < C::BROWS / 4; ks++) {
+            const int r = ks * 4 + q4;
+            double a[C::MT], bv[C::NT];
+#pragma unroll
+            for (int mt = 0; mt < C::MT; mt++) {
+                const int k = mt * 8 + g;
+                a[mt] = (k < RP) ? sw[r * C::RPS + k] : 0.0;
+            }
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) bv[nt] = sv[r * C::BOXC + nt * 8];
+#pragma unroll
+            for (int mt = 0; mt < C::MT; mt++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) dmma_8x8x4(acc[mt][nt], a[mt], bv[nt]);
+        }
+        __syncwarp();
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::WBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
+        }
+        uc.next(sk);
+    }
+    if (ok && cur >= 0) flush(cur);
+}
+
+// W pass: B[i][k] = sum_j V[i][j] H[k][j] with M = i (4 row tiles of 8 a
+// warp), N = k (rank tiles of 8), K = j (4 columns a k-step, 4 k-steps a
+// unit of 16 columns read from a 128B-swizzled V box).
+template <int RP>
+struct DWCfg {
+    static constexpr int NT = (RP + 7) / 8;
+    static constexpr int kWarps = NT >= 4 ? 8 : 16;
+    static constexpr int MW = 4;
+    static constexpr int WROWS = MW * 8;
+    static constexpr int TROWS = kWarps * WROWS;  // 512 rows a tile
+    static constexpr int BOXR = 256;
+    static constexpr int NBOX = TROWS / BOXR;
+    static constexpr int ROWB = 128;  // one 128-byte swizzle span of a row a unit
+    static constexpr int BCOLS = ROWB / 8;
+    static constexpr int SEGU = kSegSpan / BCOLS;
+    static constexpr int RPS = RankPad<double, RP>::RPS;
+    static constexpr int VBYTES = TROWS * ROWB;
+    static constexpr int HBYTES = BCOLS * RPS * 8;
+    static constexpr int STAGE = (VBYTES + HBYTES + 1023) / 1024 * 1024;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
+    static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
+    static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
+    static_assert(TROWS % BOXR == 0 && BOXR % 8 == 0, "whole boxes of whole swizzle groups");
+};
+
+template <int RP>
+__global__ void __launch_bounds__(DWCfg<RP>::kWarps * 32, 1)
+    wpass_dmma(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmH,
+               int n, int p, StreamK sk, double *__restrict__ part, RunState *st) {
+    using C = DWCfg<RP>;
+    if (run_stopped(st)) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = (threadIdx.x == 0);
+    const int b = blockIdx.x;
+    const long long u0 = sk.start(b), u1 = sk.start(b + 1);
+    const long long nunits = u1 - u0;
+
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int cb = c.along(sk);
+#pragma unroll
+        for (int q = 0; q < C::NBOX; q++)
+            tma_load_2d(stg + q * C::BOXR * C::ROWB, &tmV, bar, cb * C::BCOLS,
+                        c.major * C::TROWS + q * C::BOXR);
+        tma_load_2d(stg + C::VBYTES, &tmH, bar, 0, cb * C::BCOLS);
+    };
+    UnitCursor ahead;
+    ahead.init(sk, u0);
+    if (producer) {
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            arrivals[s] = 0;
+        }
+        fence_mbar_init();
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::HBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
+    }
+    __syncthreads();
+
+    const int g = lane >> 2, q4 = lane & 3;
+    // Row of A fragment mw: warp * 32 + mw * 8 + g (its swizzle key is g, the
+    // row mod 8); its byte offset within the stage, before the chunk.
+    const int rbase = warp * C::WROWS + g;
+    double acc[C::MW][C::NT][2];
+    int cur = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
+    bool ok = true;
+
+    auto flush = [&](int t) {
+        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP;
+#pragma unroll
+        for (int mw = 0; mw < C::MW; mw++) {
+            const int row = rbase + mw * 8;
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) {
+                const int k = nt * 8 + 2 * q4;
+                if (k < RP) {  // RP is even: k + 1 < RP too
+                    double *d = dst + (size_t)row * RP + k;
+                    d[0] = acc[mw][nt][0];
+                    d[1] = acc[mw][nt][1];
+                }
+            }
+        }
+    };
+
+    for (long long i = 0; i < nunits; ++i) {
+        const int t = uc.t;
+        if (t != cur) {
+            if (cur >= 0) flush(cur);
+            cur = t;
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) acc[mw][nt][0] = acc[mw][nt][1] = 0.0;
+        }
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
+            record_timeout(st, TIMEOUT_FULL);
+            ok = false;
+            break;
+        }
+        const unsigned char *stg = smem + s * C::STAGE;
+        const double *sh = reinterpret_cast<const double *>(stg + C::VBYTES);
+#pragma unroll
+        for (int ks = 0; ks < C::BCOLS / 4; ks++) {
+            const int j = ks * 4 + q4;              // column within the unit
+            const int chunk = j >> 1, within = j & 1;
+            double a[C::MW], bh[C::NT];
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++) {
+                const int row = rbase + mw * 8;     // row & 7 == g
+                a[mw] = *reinterpret_cast<const double *>(
+                    stg + row * C::ROWB + (((chunk ^ g) << 4) | (within << 3)));
+            }
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) {
+                const int k = nt * 8 + g;
+                bh[nt] = (k < RP) ? sh[j * C::RPS + k] : 0.0;
+            }
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) dmma_8x8x4(acc[mw][nt], a[mw], bh[nt]);
+        }
+        __syncwarp();
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::HBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
+        }
+        uc.next(sk);
+    }
+    if (ok && cur >= 0) flush(cur);
+}
+
+// ---------------------------------------------------------------------------
 // Epilogues for the stream-K partials
 // ---------------------------------------------------------------------------
 

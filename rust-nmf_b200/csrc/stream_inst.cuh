@@ -12,31 +12,38 @@ template <int RP>
 struct StreamOpsT final : StreamOps {
     using T = STREAM_T;
     static constexpr int RPS = RankPad<T, RP>::RPS;
+    // The f64 plain passes run on the FP64 tensor cores (hpass_dmma /
+    // wpass_dmma); the ratio passes and every f32 pass on the CUDA cores.
+    static constexpr bool kDmma = sizeof(T) == 8;
+    using HP = HCfg<T, RP, false>;
+    using WP = WCfg<T, RP, false>;
+    static_assert(!kDmma || (DHCfg<RP>::BROWS == HP::BROWS && DHCfg<RP>::SEGU == HP::SEGU),
+                  "one W box and one segment length for every H pass");
 
     int elem_bytes() const override { return (int)sizeof(T); }
     int rps() const override { return RPS; }
     int h_tcols(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::TCOLS : HCfg<T, RP, false>::TCOLS;
+        return ratio ? HCfg<T, RP, true>::TCOLS : (kDmma ? DHCfg<RP>::TCOLS : HP::TCOLS);
     }
-    int h_brows() const override { return HCfg<T, RP, false>::BROWS; }
+    int h_brows() const override { return HP::BROWS; }
     int h_boxc(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::BOXC : HCfg<T, RP, false>::BOXC;
+        return ratio ? HCfg<T, RP, true>::BOXC : (kDmma ? DHCfg<RP>::BOXC : HP::BOXC);
     }
-    int h_segu() const override { return HCfg<T, RP, false>::SEGU; }
+    int h_segu() const override { return HP::SEGU; }
     int w_trows(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::TROWS : WCfg<T, RP, false>::TROWS;
+        return ratio ? WCfg<T, RP, true>::TROWS : (kDmma ? DWCfg<RP>::TROWS : WP::TROWS);
     }
     int w_bcols(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::BCOLS : WCfg<T, RP, false>::BCOLS;
+        return ratio ? WCfg<T, RP, true>::BCOLS : (kDmma ? DWCfg<RP>::BCOLS : WP::BCOLS);
     }
     int w_segu(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::SEGU : WCfg<T, RP, false>::SEGU;
+        return ratio ? WCfg<T, RP, true>::SEGU : (kDmma ? DWCfg<RP>::SEGU : WP::SEGU);
     }
     int w_rowb(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::ROWB : WCfg<T, RP, false>::ROWB;
+        return ratio ? WCfg<T, RP, true>::ROWB : (kDmma ? DWCfg<RP>::ROWB : WP::ROWB);
     }
     int w_boxr(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::BOXR : WCfg<T, RP, false>::BOXR;
+        return ratio ? WCfg<T, RP, true>::BOXR : (kDmma ? DWCfg<RP>::BOXR : WP::BOXR);
     }
 
     template <bool RATIO, bool WEIGHTED = false>
@@ -69,14 +76,36 @@ struct StreamOpsT final : StreamOps {
     cudaError_t hpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmW,
                       const double *H, int n, int p, const StreamK &sk, double *part,
                       RunState *st, int grid, cudaStream_t s) const override {
-        return ratio ? launch_h<true>(tmV, tmW, H, n, p, sk, part, st, grid, s)
-                     : launch_h<false>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+        if (ratio) return launch_h<true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+        if constexpr (kDmma) {
+            using C = DHCfg<RP>;
+            cudaError_t e = cudaFuncSetAttribute(nmfcu::hpass_dmma<RP>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 C::SMEM);
+            if (e != cudaSuccess) return e;
+            nmfcu::hpass_dmma<RP><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmW, n, p, sk, part,
+                                                                        st);
+            return cudaGetLastError();
+        } else {
+            return launch_h<false>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+        }
     }
     cudaError_t wpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmH,
                       const double *W, int n, int p, const StreamK &sk, double *part,
                       RunState *st, int grid, cudaStream_t s) const override {
-        return ratio ? launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s)
-                     : launch_w<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+        if (ratio) return launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+        if constexpr (kDmma) {
+            using C = DWCfg<RP>;
+            cudaError_t e = cudaFuncSetAttribute(nmfcu::wpass_dmma<RP>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 C::SMEM);
+            if (e != cudaSuccess) return e;
+            nmfcu::wpass_dmma<RP><<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmH, n, p, sk, part,
+                                                                        st);
+            return cudaGetLastError();
+        } else {
+            return launch_w<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+        }
     }
     cudaError_t hpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
                                int n, int p, const StreamK &sk, double *part, RunState *st,
