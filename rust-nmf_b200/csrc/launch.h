@@ -19,7 +19,6 @@ struct StreamOps {
     virtual int rps() const = 0;                 // padded rank of the W / H^T copies
     virtual int h_tcols(bool ratio) const = 0;   // H pass tile width (columns)
     virtual int h_brows() const = 0;             // H pass rows per unit
-    virtual int h_vswizzle(bool ratio) const = 0; // H pass V box swizzle span (0 or 128 bytes)
     virtual int h_boxc(bool ratio) const = 0;    // H pass V box width
     virtual int h_segu() const = 0;              // H pass max units per segment
     virtual int w_trows(bool ratio) const = 0;   // W pass tile height (rows)

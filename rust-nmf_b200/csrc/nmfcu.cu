@@ -562,10 +562,7 @@ nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio
     const CUtensorMapSwizzle wsw = rowb == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
                                    : rowb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
                                                 : CU_TENSOR_MAP_SWIZZLE_128B;
-    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(ratio),
-                      ps->so->h_brows(),
-                      ps->so->h_vswizzle(ratio) ? CU_TENSOR_MAP_SWIZZLE_128B
-                                                : CU_TENSOR_MAP_SWIZZLE_NONE));
+    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(ratio), ps->so->h_brows()));
     NMF_TRY(encode_2d(&ps->tmVw, V, f32, pl.n, pl.p, ldv, ps->so->w_bcols(ratio),
                       ps->so->w_boxr(ratio), wsw));
     if (f32)

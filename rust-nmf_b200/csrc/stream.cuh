@@ -681,11 +681,7 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 }
 
 // H pass: A[k][j] = sum_u W[u][k] V[u][j] with M = k (rank tiles of 8), N = j
-// (4 column tiles of 8 a warp), K = u (4 rows a k-step, 2 k-steps a unit:
-// rows 0, 2, 4, 6, then 1, 3, 5, 7).  V arrives as 128B-swizzled boxes of 8
-// rows x 16 columns (1 KB each): 16-byte chunk c of row r sits at chunk
-// c ^ r, so the four rows of a B fragment fall on all eight chunks and a
-// half-warp's 8-byte loads hit every bank once.
+// (4 column tiles of 8 a warp), K = u (4 rows a k-step, 2 k-steps a unit).
 template <int RP>
 struct DHCfg {
     static constexpr int MT = (RP + 7) / 8;
@@ -695,19 +691,18 @@ struct DHCfg {
     static constexpr int NT = 4;
     static constexpr int WCOLS = NT * 8;
     static constexpr int TCOLS = kWarps * WCOLS;  // 512 columns a tile
-    static constexpr int BOXC = 16;                // one 128-byte swizzle span
+    static constexpr int BOXC = 256;
     static constexpr int NBOX = TCOLS / BOXC;
     static constexpr int BROWS = 8;
-    static constexpr int BOXB = BROWS * BOXC * 8;  // 1024 bytes a box
     static constexpr int SEGU = kSegSpan / BROWS;
     static constexpr int RPS = RankPad<double, RP>::RPS;
-    static constexpr int VBYTES = NBOX * BOXB;
+    static constexpr int VBYTES = BROWS * TCOLS * 8;
     static constexpr int WBYTES = BROWS * RPS * 8;
     static constexpr int STAGE = (VBYTES + WBYTES + 1023) / 1024 * 1024;
     static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
     static constexpr int STAGES = STAGES_FIT > 10 ? 10 : STAGES_FIT;
     static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
-    static_assert(WCOLS % BOXC == 0 && BOXB == 1024, "whole 1 KB boxes a warp");
+    static_assert(WCOLS <= BOXC && BOXC % WCOLS == 0, "a warp's columns lie in one box");
     static_assert(STAGES >= 3, "a ring needs stages in flight");
 };
 
@@ -729,10 +724,10 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
 
     auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
         const int rb = c.along(sk);
-#pragma unroll 4
+#pragma unroll
         for (int q = 0; q < C::NBOX; q++)
-            tma_load_2d(stg + q * C::BOXB, &tmV, bar, c.major * C::TCOLS + q * C::BOXC,
-                        rb * C::BROWS);
+            tma_load_2d(stg + q * C::BROWS * C::BOXC * 8, &tmV, bar,
+                        c.major * C::TCOLS + q * C::BOXC, rb * C::BROWS);
         tma_load_2d(stg + C::VBYTES, &tmW, bar, 0, rb * C::BROWS);
     };
     UnitCursor ahead;
@@ -757,15 +752,7 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
 
     const int g = lane >> 2, q4 = lane & 3;
     const int wc0 = warp * C::WCOLS;  // this warp's first column in the tile
-    // Byte offset of B element (row 0, column wc0 + nt * 8 + g) before the
-    // row's swizzle: its box, and its 16-byte chunk / half within the row.
-    int bbox[C::NT], bchunk[C::NT];
-#pragma unroll
-    for (int nt = 0; nt < C::NT; nt++) {
-        const int c = wc0 + nt * 8 + g;
-        bbox[nt] = (c / C::BOXC) * C::BOXB + ((c & 1) << 3);
-        bchunk[nt] = (c % C::BOXC) >> 1;
-    }
+    const int vbox = wc0 / C::BOXC, voff = wc0 % C::BOXC;
     double acc[C::MT][C::NT][2];
     int cur = -1;
     UnitCursor uc;
@@ -806,10 +793,12 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
             break;
         }
         const unsigned char *stg = smem + s * C::STAGE;
+        const double *sv =
+            reinterpret_cast<const double *>(stg) + vbox * C::BROWS * C::BOXC + voff + g;
         const double *sw = reinterpret_cast<const double *>(stg + C::VBYTES);
 #pragma unroll
         for (int ks = 0; ks < C::BROWS / 4; ks++) {
-            const int r = 2 * q4 + ks;  // the k-step's K index q4 is row r
+            const int r = ks * 4 + q4;
             double a[C::MT], bv[C::NT];
 #pragma unroll
             for (int mt = 0; mt < C::MT; mt++) {
@@ -817,9 +806,7 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
                 a[mt] = (k < RP) ? sw[r * C::RPS + k] : 0.0;
             }
 #pragma unroll
-            for (int nt = 0; nt < C::NT; nt++)
-                bv[nt] = *reinterpret_cast<const double *>(
-                    stg + bbox[nt] + r * (C::BOXC * 8) + ((bchunk[nt] ^ r) << 4));
+            for (int nt = 0; nt < C::NT; nt++) bv[nt] = sv[r * C::BOXC + nt * 8];
 #pragma unroll
             for (int mt = 0; mt < C::MT; mt++)
 #pragma unroll

@@ -26,9 +26,6 @@ struct StreamOpsT final : StreamOps {
         return ratio ? HCfg<T, RP, true>::TCOLS : (kDmma ? DHCfg<RP>::TCOLS : HP::TCOLS);
     }
     int h_brows() const override { return HP::BROWS; }
-    int h_vswizzle(bool ratio) const override {
-        return (ratio || !kDmma) ? 0 : 128;  // hpass_dmma reads 128B-swizzled V boxes
-    }
     int h_boxc(bool ratio) const override {
         return ratio ? HCfg<T, RP, true>::BOXC : (kDmma ? DHCfg<RP>::BOXC : HP::BOXC);
     }
