@@ -18,9 +18,9 @@ struct StreamOps {
     virtual int elem_bytes() const = 0;          // 4 or 8
     virtual int rps() const = 0;                 // padded rank of the W / H^T copies
     virtual int h_tcols(bool ratio) const = 0;   // H pass tile width (columns)
-    virtual int h_brows() const = 0;             // H pass rows per unit
+    virtual int h_brows(bool ratio) const = 0;   // H pass rows per unit
     virtual int h_boxc(bool ratio) const = 0;    // H pass V box width
-    virtual int h_segu() const = 0;              // H pass max units per segment
+    virtual int h_segu(bool ratio) const = 0;    // H pass max units per segment
     virtual int w_trows(bool ratio) const = 0;   // W pass tile height (rows)
     virtual int w_bcols(bool ratio) const = 0;   // W pass columns per unit
     virtual int w_segu(bool ratio) const = 0;    // W pass max units per segment

@@ -384,7 +384,8 @@ StreamK plan_sk(int64_t majors, int64_t units, int64_t segu, int sms) {
 
 StreamK plan_h(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
     const int tcols = so->h_tcols(ratio);
-    return plan_sk((p + tcols - 1) / tcols, (n + so->h_brows() - 1) / so->h_brows(), so->h_segu(),
+    return plan_sk((p + tcols - 1) / tcols, (n + so->h_brows(ratio) - 1) / so->h_brows(ratio),
+                   so->h_segu(ratio),
                    sms);
 }
 StreamK plan_w(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
@@ -562,14 +563,16 @@ nmfcu_status make_passset(nmfcu_context *c, const Plan &pl, bool f32, bool ratio
     const CUtensorMapSwizzle wsw = rowb == 32   ? CU_TENSOR_MAP_SWIZZLE_32B
                                    : rowb == 64 ? CU_TENSOR_MAP_SWIZZLE_64B
                                                 : CU_TENSOR_MAP_SWIZZLE_128B;
-    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(ratio), ps->so->h_brows()));
+    NMF_TRY(encode_2d(&ps->tmVh, V, f32, pl.n, pl.p, ldv, ps->so->h_boxc(ratio),
+                      ps->so->h_brows(ratio)));
     NMF_TRY(encode_2d(&ps->tmVw, V, f32, pl.n, pl.p, ldv, ps->so->w_bcols(ratio),
                       ps->so->w_boxr(ratio), wsw));
     if (f32)
-        NMF_TRY(encode_2d(&ps->tmW, c->Wf32.ptr, true, pl.n, rps, rps, rps, ps->so->h_brows()));
+        NMF_TRY(encode_2d(&ps->tmW, c->Wf32.ptr, true, pl.n, rps, rps, rps,
+                          ps->so->h_brows(ratio)));
     else
         NMF_TRY(encode_2d(&ps->tmW, wsrc ? wsrc : c->W.as<double>(), false, pl.n, pl.RP, pl.RP,
-                          pl.RP, ps->so->h_brows()));
+                          pl.RP, ps->so->h_brows(ratio)));
     NMF_TRY(encode_2d(&ps->tmHt, ps->Ht, f32, pl.p, rps, rps, rps, ps->so->w_bcols(ratio)));
     return NMFCU_OK;
 }

@@ -681,7 +681,8 @@ __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
 }
 
 // H pass: A[k][j] = sum_u W[u][k] V[u][j] with M = k (rank tiles of 8), N = j
-// (4 column tiles of 8 a warp), K = u (4 rows a k-step, 2 k-steps a unit).
+// (4 column tiles of 8 a warp), K = u (4 rows a k-step, 4 k-steps a unit of
+// 16 rows, so that a stage's wait and release serve 4 k-steps).
 template <int RP>
 struct DHCfg {
     static constexpr int MT = (RP + 7) / 8;
@@ -693,7 +694,7 @@ struct DHCfg {
     static constexpr int TCOLS = kWarps * WCOLS;  // 512 columns a tile
     static constexpr int BOXC = 256;
     static constexpr int NBOX = TCOLS / BOXC;
-    static constexpr int BROWS = 8;
+    static constexpr int BROWS = 16;
     static constexpr int SEGU = kSegSpan / BROWS;
     static constexpr int RPS = RankPad<double, RP>::RPS;
     static constexpr int VBYTES = BROWS * TCOLS * 8;

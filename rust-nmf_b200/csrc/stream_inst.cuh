@@ -17,19 +17,21 @@ struct StreamOpsT final : StreamOps {
     static constexpr bool kDmma = sizeof(T) == 8;
     using HP = HCfg<T, RP, false>;
     using WP = WCfg<T, RP, false>;
-    static_assert(!kDmma || (DHCfg<RP>::BROWS == HP::BROWS && DHCfg<RP>::SEGU == HP::SEGU),
-                  "one W box and one segment length for every H pass");
 
     int elem_bytes() const override { return (int)sizeof(T); }
     int rps() const override { return RPS; }
     int h_tcols(bool ratio) const override {
         return ratio ? HCfg<T, RP, true>::TCOLS : (kDmma ? DHCfg<RP>::TCOLS : HP::TCOLS);
     }
-    int h_brows() const override { return HP::BROWS; }
+    int h_brows(bool ratio) const override {
+        return ratio ? HCfg<T, RP, true>::BROWS : (kDmma ? DHCfg<RP>::BROWS : HP::BROWS);
+    }
     int h_boxc(bool ratio) const override {
         return ratio ? HCfg<T, RP, true>::BOXC : (kDmma ? DHCfg<RP>::BOXC : HP::BOXC);
     }
-    int h_segu() const override { return HP::SEGU; }
+    int h_segu(bool ratio) const override {
+        return ratio ? HCfg<T, RP, true>::SEGU : (kDmma ? DHCfg<RP>::SEGU : HP::SEGU);
+    }
     int w_trows(bool ratio) const override {
         return ratio ? WCfg<T, RP, true>::TROWS : (kDmma ? DWCfg<RP>::TROWS : WP::TROWS);
     }
