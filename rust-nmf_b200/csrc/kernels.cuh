@@ -58,9 +58,24 @@ __device__ __forceinline__ bool run_stopped(const RunState *st) {
 // Arithmetic helpers
 // ---------------------------------------------------------------------------
 
-// x / y for the ratio V / (WH): IEEE division in f64 (parity path); in f32
-// the fast reciprocal-multiply form (the FP32 form is tolerance-checked).
-__device__ __forceinline__ double ratio_div(double x, double y) { return x / y; }
+// x / y for the ratio V / (WH), y != 0.  f64: x (1 / y) with the reciprocal
+// from the hardware approximation (rcp.approx.ftz.f64) refined by two
+// Newton-Raphson steps r <- r + r (1 - y r), each of which doubles the
+// correct bits, so the quotient is within about an ulp of the IEEE one (the
+// tests hold the loop to 1e-10 of the oracle's IEEE divisions); |y| outside
+// [2^-1000, 2^1000] and NaN take the IEEE division.  f32: the fast
+// reciprocal-multiply form (the FP32 form is tolerance-checked).
+__device__ __forceinline__ double ratio_div(double x, double y) {
+    const double a = fabs(y);
+    if (!(a > 0x1p-1000 && a < 0x1p1000)) return x / y;
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(y));
+    double e = fma(-y, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-y, r, 1.0);
+    r = fma(r, e, r);
+    return x * r;
+}
 __device__ __forceinline__ float ratio_div(float x, float y) { return __fdividef(x, y); }
 
 // Epilogue arithmetic without FMA contraction, so that the update formulas
