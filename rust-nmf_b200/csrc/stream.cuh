@@ -979,6 +979,374 @@ __global__ void __launch_bounds__(DWCfg<RP>::kWarps * 32, 1)
 }
 
 // ---------------------------------------------------------------------------
+// FP64 ratio passes on the FP64 tensor cores (brunet / nsNMF; lsNMF's
+// weighted denominators with WEIGHTED)
+// ---------------------------------------------------------------------------
+// Per 8 x 8 tile of (rows i, columns j) two MMA chains:
+//   1. WH: D1[g][2q + e] = sum_k (W H) over the rank (K = k in steps of 4);
+//   2. the contraction, K = the tile's 8 rows (H pass) or columns (W pass)
+//      taken as two k-steps (2q and 2q + 1): the B (H pass) or A (W pass)
+//      operand a thread needs there is exactly its own D1[e], turned into
+//      q = V / WH (0 where WH == 0, lib.rs:93-99) or q = S WH (WEIGHTED).
+// Accumulators and partial layouts are the plain DMMA passes'.
+
+// H pass: A[k][j] = sum_i W[i][k] q[i][j].  MMA 1: M = j, N = i, K = k (A = H
+// columns, held in registers for the whole column tile; B = W rows).  MMA 2:
+// M = k, N = j, K = i.
+template <int RP>
+struct DHRCfg {
+    static constexpr int KST = (RP + 3) / 4;  // k-steps of the WH chain
+    static constexpr int MT = (RP + 7) / 8;
+    static constexpr int kWarps = MT >= 4 ? 8 : 16;
+    static constexpr int NT = 2;  // column tiles of 8 a warp
+    static constexpr int WCOLS = NT * 8;
+    static constexpr int TCOLS = kWarps * WCOLS;
+    static constexpr int BOXC = TCOLS;
+    static constexpr int BROWS = 16;  // two 8-row tiles a unit
+    static constexpr int SEGU = kSegSpan / BROWS;
+    static constexpr int RPS = RankPad<double, RP>::RPS;
+    static constexpr int VBYTES = BROWS * TCOLS * 8;
+    static constexpr int WBYTES = BROWS * RPS * 8;
+    static constexpr int STAGE = (VBYTES + WBYTES + 1023) / 1024 * 1024;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
+    static constexpr int STAGES = STAGES_FIT > 10 ? 10 : STAGES_FIT;
+    static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
+    static_assert(BOXC <= 256, "one V box a unit");
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
+};
+
+template <int RP, bool WEIGHTED>
+__global__ void __launch_bounds__(DHRCfg<RP>::kWarps * 32, 1)
+    hpass_dmma_ratio(const __grid_constant__ CUtensorMap tmV,
+                     const __grid_constant__ CUtensorMap tmW, const double *__restrict__ H, int n,
+                     int p, StreamK sk, double *__restrict__ part, RunState *st) {
+    using C = DHRCfg<RP>;
+    if (run_stopped(st)) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = (threadIdx.x == 0);
+    const int b = blockIdx.x;
+    const long long u0 = sk.start(b), u1 = sk.start(b + 1);
+    const long long nunits = u1 - u0;
+
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int rb = c.along(sk);
+        tma_load_2d(stg, &tmV, bar, c.major * C::TCOLS, rb * C::BROWS);
+        tma_load_2d(stg + C::VBYTES, &tmW, bar, 0, rb * C::BROWS);
+    };
+    UnitCursor ahead;
+    ahead.init(sk, u0);
+    if (producer) {
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            arrivals[s] = 0;
+        }
+        fence_mbar_init();
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::WBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
+    }
+    __syncthreads();
+
+    const int g = lane >> 2, q4 = lane & 3;
+    const int wc0 = warp * C::WCOLS;
+    double acc[C::MT][C::NT][2];
+    double hreg[C::NT][C::KST];  // MMA 1's A: H[ks * 4 + q4][column of row g]
+    int cur = -1, cur_major = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
+    bool ok = true;
+
+    auto flush = [&](int t) {
+        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS;
+#pragma unroll
+        for (int mt = 0; mt < C::MT; mt++) {
+            const int k = mt * 8 + g;
+            if (k < RP) {
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) {
+                    double *d = dst + (size_t)k * C::TCOLS + wc0 + nt * 8 + 2 * q4;
+                    d[0] = acc[mt][nt][0];
+                    d[1] = acc[mt][nt][1];
+                }
+            }
+        }
+    };
+
+    for (long long i = 0; i < nunits; ++i) {
+        const int t = uc.t;
+        if (t != cur) {
+            if (cur >= 0) flush(cur);
+            cur = t;
+#pragma unroll
+            for (int mt = 0; mt < C::MT; mt++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+            if (uc.major != cur_major) {
+                cur_major = uc.major;
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) {
+                    const int j = uc.major * C::TCOLS + wc0 + nt * 8 + g;
+#pragma unroll
+                    for (int ks = 0; ks < C::KST; ks++) {
+                        const int k = ks * 4 + q4;
+                        hreg[nt][ks] = (k < RP && j < p) ? H[(size_t)k * p + j] : 0.0;
+                    }
+                }
+            }
+        }
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
+            record_timeout(st, TIMEOUT_FULL);
+            ok = false;
+            break;
+        }
+        const unsigned char *stg = smem + s * C::STAGE;
+        const double *sv = reinterpret_cast<const double *>(stg) + wc0 + g;
+        const double *sw = reinterpret_cast<const double *>(stg + C::VBYTES);
+#pragma unroll
+        for (int rt = 0; rt < C::BROWS / 8; rt++) {
+            const int r0 = rt * 8;
+            double b1[C::KST];  // MMA 1's B: W[r0 + g][ks * 4 + q4]
+#pragma unroll
+            for (int ks = 0; ks < C::KST; ks++) {
+                const int k = ks * 4 + q4;
+                b1[ks] = (k < RP) ? sw[(r0 + g) * C::RPS + k] : 0.0;
+            }
+            double a2[C::MT][2];  // MMA 2's A: W[r0 + 2 q4 + e][mt * 8 + g]
+#pragma unroll
+            for (int mt = 0; mt < C::MT; mt++) {
+                const int k = mt * 8 + g;
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    a2[mt][e] = (k < RP) ? sw[(r0 + 2 * q4 + e) * C::RPS + k] : 0.0;
+            }
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) {
+                double wh[2] = {0.0, 0.0};
+#pragma unroll
+                for (int ks = 0; ks < C::KST; ks++) dmma_8x8x4(wh, hreg[nt][ks], b1[ks]);
+                double qv[2];
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const double v = sv[(r0 + 2 * q4 + e) * C::BOXC + nt * 8];
+                    if constexpr (WEIGHTED)
+                        qv[e] = v * wh[e];
+                    else
+                        qv[e] = (wh[e] != 0.0) ? ratio_div(v, wh[e]) : 0.0;
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+#pragma unroll
+                    for (int mt = 0; mt < C::MT; mt++) dmma_8x8x4(acc[mt][nt], a2[mt][e], qv[e]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::WBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
+        }
+        uc.next(sk);
+    }
+    if (ok && cur >= 0) flush(cur);
+}
+
+// W pass: B[i][k] = sum_j q[i][j] H[k][j].  MMA 1: M = i, N = j, K = k (A = W
+// rows, held in registers for the whole row tile; B = H^T rows).  MMA 2:
+// M = i, N = k, K = j.
+template <int RP>
+struct DWRCfg {
+    static constexpr int KST = (RP + 3) / 4;
+    static constexpr int NT = (RP + 7) / 8;
+    static constexpr int kWarps = NT >= 4 ? 8 : 16;
+    static constexpr int MW = 2;  // row tiles of 8 a warp
+    static constexpr int WROWS = MW * 8;
+    static constexpr int TROWS = kWarps * WROWS;
+    static constexpr int BOXR = TROWS;
+    static constexpr int ROWB = 128;
+    static constexpr int BCOLS = ROWB / 8;  // two 8-column tiles a unit
+    static constexpr int SEGU = kSegSpan / BCOLS;
+    static constexpr int RPS = RankPad<double, RP>::RPS;
+    static constexpr int VBYTES = TROWS * ROWB;
+    static constexpr int HBYTES = BCOLS * RPS * 8;
+    static constexpr int STAGE = (VBYTES + HBYTES + 1023) / 1024 * 1024;
+    static constexpr int STAGES_FIT = (220 * 1024) / STAGE;
+    static constexpr int STAGES = STAGES_FIT > 8 ? 8 : STAGES_FIT;
+    static constexpr int SMEM = STAGES * STAGE + 2 * STAGES * 8 + 1024;
+    static_assert(BOXR <= 256 && BOXR % 8 == 0, "one V box of whole swizzle groups");
+    static_assert(STAGES >= 3, "a ring needs stages in flight");
+};
+
+template <int RP, bool WEIGHTED>
+__global__ void __launch_bounds__(DWRCfg<RP>::kWarps * 32, 1)
+    wpass_dmma_ratio(const __grid_constant__ CUtensorMap tmV,
+                     const __grid_constant__ CUtensorMap tmH, const double *__restrict__ W, int n,
+                     int p, StreamK sk, double *__restrict__ part, RunState *st) {
+    using C = DWRCfg<RP>;
+    if (run_stopped(st)) return;
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char *smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + C::STAGES * C::STAGE);
+    int *arrivals = reinterpret_cast<int *>(full + C::STAGES);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool producer = (threadIdx.x == 0);
+    const int b = blockIdx.x;
+    const long long u0 = sk.start(b), u1 = sk.start(b + 1);
+    const long long nunits = u1 - u0;
+
+    auto issue = [&](unsigned char *stg, uint64_t *bar, const UnitCursor &c) {
+        const int cb = c.along(sk);
+        tma_load_2d(stg, &tmV, bar, cb * C::BCOLS, c.major * C::TROWS);
+        tma_load_2d(stg + C::VBYTES, &tmH, bar, 0, cb * C::BCOLS);
+    };
+    UnitCursor ahead;
+    ahead.init(sk, u0);
+    if (producer) {
+        for (int s = 0; s < C::STAGES; s++) {
+            mbar_init(&full[s], 1);
+            arrivals[s] = 0;
+        }
+        fence_mbar_init();
+        for (int j = 0; j < C::STAGES; j++) {
+            if (j < nunits) {
+                mbar_expect_tx(&full[j], C::VBYTES + C::HBYTES);
+                issue(smem + j * C::STAGE, &full[j], ahead);
+            }
+            ahead.next(sk);
+        }
+    } else {
+        for (int j = 0; j < C::STAGES; j++) ahead.next(sk);
+    }
+    __syncthreads();
+
+    const int g = lane >> 2, q4 = lane & 3;
+    const int rbase = warp * C::WROWS + g;  // row of fragment mw: rbase + mw * 8 (row & 7 == g)
+    double acc[C::MW][C::NT][2];
+    double wreg[C::MW][C::KST];  // MMA 1's A: W[row][ks * 4 + q4]
+    int cur = -1, cur_major = -1;
+    UnitCursor uc;
+    uc.init(sk, u0);
+    const int tile0 = uc.t;
+    int s = 0, rnd = 0;
+    bool ok = true;
+
+    auto flush = [&](int t) {
+        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP;
+#pragma unroll
+        for (int mw = 0; mw < C::MW; mw++) {
+            const int row = rbase + mw * 8;
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) {
+                const int k = nt * 8 + 2 * q4;
+                if (k < RP) {
+                    double *d = dst + (size_t)row * RP + k;
+                    d[0] = acc[mw][nt][0];
+                    d[1] = acc[mw][nt][1];
+                }
+            }
+        }
+    };
+
+    for (long long i = 0; i < nunits; ++i) {
+        const int t = uc.t;
+        if (t != cur) {
+            if (cur >= 0) flush(cur);
+            cur = t;
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) acc[mw][nt][0] = acc[mw][nt][1] = 0.0;
+            if (uc.major != cur_major) {
+                cur_major = uc.major;
+#pragma unroll
+                for (int mw = 0; mw < C::MW; mw++) {
+                    const int row = uc.major * C::TROWS + rbase + mw * 8;
+#pragma unroll
+                    for (int ks = 0; ks < C::KST; ks++) {
+                        const int k = ks * 4 + q4;
+                        wreg[mw][ks] = (k < RP && row < n) ? W[(size_t)row * RP + k] : 0.0;
+                    }
+                }
+            }
+        }
+        if (!mbar_wait(&full[s], (uint32_t)(rnd & 1))) {
+            record_timeout(st, TIMEOUT_FULL);
+            ok = false;
+            break;
+        }
+        const unsigned char *stg = smem + s * C::STAGE;
+        const double *sh = reinterpret_cast<const double *>(stg + C::VBYTES);
+#pragma unroll
+        for (int jt = 0; jt < C::BCOLS / 8; jt++) {
+            const int j0 = jt * 8;
+            double b1[C::KST];  // MMA 1's B: H^T[j0 + g][ks * 4 + q4]
+#pragma unroll
+            for (int ks = 0; ks < C::KST; ks++) {
+                const int k = ks * 4 + q4;
+                b1[ks] = (k < RP) ? sh[(j0 + g) * C::RPS + k] : 0.0;
+            }
+            double b2[C::NT][2];  // MMA 2's B: H^T[j0 + 2 q4 + e][nt * 8 + g]
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++) {
+                const int k = nt * 8 + g;
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+                    b2[nt][e] = (k < RP) ? sh[(j0 + 2 * q4 + e) * C::RPS + k] : 0.0;
+            }
+            // V[row][j0 + 2 q4 + e], e = 0, 1: one 16-byte chunk of the row.
+            const int chunk = (j0 >> 1) + q4;
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++) {
+                const int row = rbase + mw * 8;
+                double wh[2] = {0.0, 0.0};
+#pragma unroll
+                for (int ks = 0; ks < C::KST; ks++) dmma_8x8x4(wh, wreg[mw][ks], b1[ks]);
+                const double2 v2 = *reinterpret_cast<const double2 *>(
+                    stg + row * C::ROWB + ((chunk ^ g) << 4));
+                double qv[2];
+                const double vv[2] = {v2.x, v2.y};
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    if constexpr (WEIGHTED)
+                        qv[e] = vv[e] * wh[e];
+                    else
+                        qv[e] = (wh[e] != 0.0) ? ratio_div(vv[e], wh[e]) : 0.0;
+                }
+#pragma unroll
+                for (int e = 0; e < 2; e++)
+#pragma unroll
+                    for (int nt = 0; nt < C::NT; nt++) dmma_8x8x4(acc[mw][nt], qv[e], b2[nt][e]);
+            }
+        }
+        __syncwarp();
+        if (lane == 0)
+            release_stage<C::STAGE, C::VBYTES + C::HBYTES>(smem, full, arrivals, s, C::kWarps,
+                                                           i + C::STAGES < nunits, ahead, issue);
+        ahead.next(sk);
+        if (++s == C::STAGES) {
+            s = 0;
+            ++rnd;
+        }
+        uc.next(sk);
+    }
+    if (ok && cur >= 0) flush(cur);
+}
+
+// ---------------------------------------------------------------------------
 // Epilogues for the stream-K partials
 // ---------------------------------------------------------------------------
 

@@ -12,40 +12,52 @@ template <int RP>
 struct StreamOpsT final : StreamOps {
     using T = STREAM_T;
     static constexpr int RPS = RankPad<T, RP>::RPS;
-    // The f64 plain passes run on the FP64 tensor cores (hpass_dmma /
-    // wpass_dmma); the ratio passes and every f32 pass on the CUDA cores.
+    // Every f64 pass runs on the FP64 tensor cores (hpass_dmma / wpass_dmma,
+    // and the *_dmma_ratio kernels for the ratio and weighted forms); the f32
+    // passes on the CUDA cores.
     static constexpr bool kDmma = sizeof(T) == 8;
     using HP = HCfg<T, RP, false>;
     using WP = WCfg<T, RP, false>;
+    using HR = HCfg<T, RP, true>;
+    using WR = WCfg<T, RP, true>;
 
     int elem_bytes() const override { return (int)sizeof(T); }
     int rps() const override { return RPS; }
     int h_tcols(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::TCOLS : (kDmma ? DHCfg<RP>::TCOLS : HP::TCOLS);
+        return ratio ? (kDmma ? DHRCfg<RP>::TCOLS : HR::TCOLS)
+                     : (kDmma ? DHCfg<RP>::TCOLS : HP::TCOLS);
     }
     int h_brows(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::BROWS : (kDmma ? DHCfg<RP>::BROWS : HP::BROWS);
+        return ratio ? (kDmma ? DHRCfg<RP>::BROWS : HR::BROWS)
+                     : (kDmma ? DHCfg<RP>::BROWS : HP::BROWS);
     }
     int h_boxc(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::BOXC : (kDmma ? DHCfg<RP>::BOXC : HP::BOXC);
+        return ratio ? (kDmma ? DHRCfg<RP>::BOXC : HR::BOXC)
+                     : (kDmma ? DHCfg<RP>::BOXC : HP::BOXC);
     }
     int h_segu(bool ratio) const override {
-        return ratio ? HCfg<T, RP, true>::SEGU : (kDmma ? DHCfg<RP>::SEGU : HP::SEGU);
+        return ratio ? (kDmma ? DHRCfg<RP>::SEGU : HR::SEGU)
+                     : (kDmma ? DHCfg<RP>::SEGU : HP::SEGU);
     }
     int w_trows(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::TROWS : (kDmma ? DWCfg<RP>::TROWS : WP::TROWS);
+        return ratio ? (kDmma ? DWRCfg<RP>::TROWS : WR::TROWS)
+                     : (kDmma ? DWCfg<RP>::TROWS : WP::TROWS);
     }
     int w_bcols(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::BCOLS : (kDmma ? DWCfg<RP>::BCOLS : WP::BCOLS);
+        return ratio ? (kDmma ? DWRCfg<RP>::BCOLS : WR::BCOLS)
+                     : (kDmma ? DWCfg<RP>::BCOLS : WP::BCOLS);
     }
     int w_segu(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::SEGU : (kDmma ? DWCfg<RP>::SEGU : WP::SEGU);
+        return ratio ? (kDmma ? DWRCfg<RP>::SEGU : WR::SEGU)
+                     : (kDmma ? DWCfg<RP>::SEGU : WP::SEGU);
     }
     int w_rowb(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::ROWB : (kDmma ? DWCfg<RP>::ROWB : WP::ROWB);
+        return ratio ? (kDmma ? DWRCfg<RP>::ROWB : WR::ROWB)
+                     : (kDmma ? DWCfg<RP>::ROWB : WP::ROWB);
     }
     int w_boxr(bool ratio) const override {
-        return ratio ? WCfg<T, RP, true>::BOXR : (kDmma ? DWCfg<RP>::BOXR : WP::BOXR);
+        return ratio ? (kDmma ? DWRCfg<RP>::BOXR : WR::BOXR)
+                     : (kDmma ? DWCfg<RP>::BOXR : WP::BOXR);
     }
 
     template <bool RATIO, bool WEIGHTED = false>
@@ -75,11 +87,37 @@ struct StreamOpsT final : StreamOps {
         return cudaGetLastError();
     }
 
+    // f64 ratio / weighted passes on the FP64 tensor cores.
+    template <bool WEIGHTED>
+    static cudaError_t launch_hr(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
+                                 int n, int p, const StreamK &sk, double *part, RunState *st,
+                                 int grid, cudaStream_t s) {
+        using C = DHRCfg<RP>;
+        auto *kern = nmfcu::hpass_dmma_ratio<RP, WEIGHTED>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmW, H, n, p, sk, part, st);
+        return cudaGetLastError();
+    }
+    template <bool WEIGHTED>
+    static cudaError_t launch_wr(const CUtensorMap &tmV, const CUtensorMap &tmH, const double *W,
+                                 int n, int p, const StreamK &sk, double *part, RunState *st,
+                                 int grid, cudaStream_t s) {
+        using C = DWRCfg<RP>;
+        auto *kern = nmfcu::wpass_dmma_ratio<RP, WEIGHTED>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             C::SMEM);
+        if (e != cudaSuccess) return e;
+        kern<<<grid, 32 * C::kWarps, C::SMEM, s>>>(tmV, tmH, W, n, p, sk, part, st);
+        return cudaGetLastError();
+    }
+
     cudaError_t hpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmW,
                       const double *H, int n, int p, const StreamK &sk, double *part,
                       RunState *st, int grid, cudaStream_t s) const override {
-        if (ratio) return launch_h<true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
         if constexpr (kDmma) {
+            if (ratio) return launch_hr<false>(tmV, tmW, H, n, p, sk, part, st, grid, s);
             using C = DHCfg<RP>;
             cudaError_t e = cudaFuncSetAttribute(nmfcu::hpass_dmma<RP>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -89,14 +127,15 @@ struct StreamOpsT final : StreamOps {
                                                                         st);
             return cudaGetLastError();
         } else {
+            if (ratio) return launch_h<true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
             return launch_h<false>(tmV, tmW, H, n, p, sk, part, st, grid, s);
         }
     }
     cudaError_t wpass(bool ratio, const CUtensorMap &tmV, const CUtensorMap &tmH,
                       const double *W, int n, int p, const StreamK &sk, double *part,
                       RunState *st, int grid, cudaStream_t s) const override {
-        if (ratio) return launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
         if constexpr (kDmma) {
+            if (ratio) return launch_wr<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
             using C = DWCfg<RP>;
             cudaError_t e = cudaFuncSetAttribute(nmfcu::wpass_dmma<RP>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -106,22 +145,23 @@ struct StreamOpsT final : StreamOps {
                                                                         st);
             return cudaGetLastError();
         } else {
+            if (ratio) return launch_w<true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
             return launch_w<false>(tmV, tmH, W, n, p, sk, part, st, grid, s);
         }
     }
     cudaError_t hpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmW, const double *H,
                                int n, int p, const StreamK &sk, double *part, RunState *st,
                                int grid, cudaStream_t s) const override {
-        if constexpr (sizeof(T) == 8)
-            return launch_h<true, true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
+        if constexpr (kDmma)
+            return launch_hr<true>(tmV, tmW, H, n, p, sk, part, st, grid, s);
         else
             return cudaErrorNotSupported;
     }
     cudaError_t wpass_weighted(const CUtensorMap &tmV, const CUtensorMap &tmH, const double *W,
                                int n, int p, const StreamK &sk, double *part, RunState *st,
                                int grid, cudaStream_t s) const override {
-        if constexpr (sizeof(T) == 8)
-            return launch_w<true, true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
+        if constexpr (kDmma)
+            return launch_wr<true>(tmV, tmH, W, n, p, sk, part, st, grid, s);
         else
             return cudaErrorNotSupported;
     }
