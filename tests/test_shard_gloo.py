@@ -70,17 +70,17 @@ def _worker(rank, world, port, method, kw, out_dir):
         dist.destroy_process_group()
 
 
-def _run(tmp_path, method, V, W0, H0, **kw):
+def _run(tmp_path, method, V, W0, H0, world=2, **kw):
     np.savez(tmp_path / "inputs.npz", V=V, W0=W0, H0=H0)
-    world = 2
     mp.start_processes(_worker, args=(world, _free_port(), method, kw, str(tmp_path)),
                        nprocs=world, join=True, start_method="spawn")
     parts = [np.load(tmp_path / f"rank{q}.npz") for q in range(world)]
     H = np.zeros_like(H0)
     for z in parts:
         H[:, int(z["c0"]):int(z["c1"])] = z["H"]
-    np.testing.assert_array_equal(parts[0]["W"], parts[1]["W"])  # identical copies of W
-    assert int(parts[0]["n_iter"]) == int(parts[1]["n_iter"])
+    for z in parts[1:]:
+        np.testing.assert_array_equal(parts[0]["W"], z["W"])  # identical copies of W
+        assert int(parts[0]["n_iter"]) == int(z["n_iter"])
     return parts[0]["W"], H, int(parts[0]["n_iter"]), parts[0]["dev"]
 
 
@@ -118,3 +118,12 @@ def test_two_gloo_ranks_stationary_stop(tmp_path, oracle, start, method):
     assert dev.size == ref["deviances"].size
     assert np.max(np.abs(dev - ref["deviances"]) / np.abs(ref["deviances"])) <= TOL
     assert rel_max(W, ref["W"]) <= TOL
+
+
+@pytest.mark.parametrize("method", ["lee", "brunet"])
+def test_three_gloo_ranks_uneven_blocks(tmp_path, oracle, start, method):
+    V, W0, H0, _, _ = start  # 60 columns: blocks of 16, 16 and 28
+    W, H, n_iter, _ = _run(tmp_path, method, V, W0, H0, world=3, max_iter=15)
+    ref = oracle.nmf_method(method, V, W0, H0, 15)
+    assert n_iter == 15
+    assert rel_max(W, ref["W"]) <= TOL and rel_max(H, ref["H"]) <= TOL
