@@ -89,7 +89,16 @@ def _load():
         ctypes.c_double, _i64, _i64, _dp, ctypes.POINTER(_i64), ctypes.POINTER(_i64),
         ctypes.c_int,
     ]
-    if lib.orc_version() < 3:
+    lib.orc_fcnnls.restype = None
+    lib.orc_fcnnls.argtypes = [ctypes.c_int, _i64, _dp, _dp, _i64, _i64, ctypes.c_double, _dp]
+    lib.orc_cholesky.restype = ctypes.c_int
+    lib.orc_cholesky.argtypes = [ctypes.c_int, _dp]
+    lib.orc_nmf_run_snmf.restype = ctypes.c_int
+    lib.orc_nmf_run_snmf.argtypes = [
+        ctypes.c_int, _i64, _i64, _i64, _dp, _dp, _dp, _i64, ctypes.c_double, ctypes.c_double,
+        ctypes.c_double, _dp, ctypes.c_int,
+    ]
+    if lib.orc_version() < 4:
         raise RuntimeError("liboracle.so is stale: rebuild it (make -C oracle)")
     _lib = lib
     return lib
@@ -219,6 +228,43 @@ def nmf_lsnmf(V, weight, W0, H0, max_iter: int, *, eps: float = 1e-9, stop: str 
     return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": dev[: nd.value].copy()}
 
 
+def fcnnls(ctc, cta, eps: float = 0.0):
+    """fcnnls (fcnnls.rs:297-470) on the normal equations ctc (l x l) and
+    cta (l x P); returns K (l x P)."""
+    lib = _load()
+    ctc, cta = _c(ctc), _c(cta)
+    l, P = cta.shape
+    K = np.zeros((P, l))
+    lib.orc_fcnnls(l, P, _ptr(ctc), _ptr(cta), P, 1, float(eps), _ptr(K))
+    return K.T.copy()
+
+
+def cholesky(a):
+    lib = _load()
+    f = _c(a).copy()
+    ok = lib.orc_cholesky(f.shape[0], _ptr(f))
+    return bool(ok), np.tril(f)
+
+
+def nmf_snmf(V, W0, H0, max_iter: int, *, left: bool, eta: float = -1.0, beta: float = 0.01,
+             eps: float = 1e-9, num_threads: int | None = None) -> dict:
+    """Oracle of py_nmf_run with method snmf/r (left False) or snmf/l (left
+    True): nmf_run_snmf_kim_park, lib.rs:1216-1320."""
+    lib = _load()
+    V = _c(V)
+    W = _c(W0).copy()
+    H = _c(H0).copy()
+    n, p = V.shape
+    k = W.shape[1]
+    dev = np.zeros(max(int(max_iter), 1))
+    rc = lib.orc_nmf_run_snmf(int(bool(left)), n, p, k, _ptr(V), _ptr(W), _ptr(H), int(max_iter),
+                              float(eta), float(beta), float(eps), _ptr(dev),
+                              int(num_threads or os.cpu_count() or 1))
+    if rc != 0:
+        raise ValueError("rank above 32")
+    return {"W": W, "H": H, "n_iter": int(max_iter), "deviances": dev[: int(max_iter)].copy()}
+
+
 def weighted_distance(V, weight, W, H) -> float:
     lib = _load()
     V, S, W, H = _c(V), _c(weight), _c(W), _c(H)
@@ -238,6 +284,12 @@ def nmf_method(method: str, V, W0, H0, max_iter: int, *, eps=1e-9, rescale=True,
         return nmf_nsnmf(V, W0, H0, max_iter, theta=theta, stop=stop, **kw)
     if m == "offset":
         return nmf_offset(V, W0, H0, max_iter, offset=offset, eps=eps, stop=stop, **kw)
+    if m in ("snmf/r", "snmf_r", "snmfr", "snmf/l", "snmf_l", "snmfl"):
+        left = m in ("snmf/l", "snmf_l", "snmfl")
+        # python/nmf_rs/__init__.py:528-538 -> lib.rs:2117-2148: snmf/r takes
+        # beta = sparsity (on H), eta = smoothness (on W); snmf/l the mirror.
+        return nmf_snmf(V, W0, H0, max_iter, left=left, eta=smoothness, beta=sparsity, eps=eps,
+                        **kw)
     if m in ("lsnmf", "ls-nmf"):
         if weight is None:
             raise ValueError("method='lsnmf' requires a `weight` matrix of the same shape as V")

@@ -869,5 +869,330 @@ int orc_nmf_run_lsnmf(i64 n, i64 p, i64 r, const double *v, const double *weight
     return status;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Kim-Park sparse NMF (snmf/r, snmf/l): ANLS with FCNNLS                    */
+/* ------------------------------------------------------------------------ */
+
+/* Cholesky factor in place (lower triangle of the m x m row-major a), in
+ * the order of fcnnls.rs:19-41; 0 when a pivot is not positive. */
+static int chol_inplace(double *a, int m) {
+    for (int j = 0; j < m; j++) {
+        double s = a[j * m + j];
+        for (int q = 0; q < j; q++) s -= a[j * m + q] * a[j * m + q];
+        if (s <= 0.0) return 0;
+        const double l = sqrt(s);
+        a[j * m + j] = l;
+        for (int i = j + 1; i < m; i++) {
+            double t = a[i * m + j];
+            for (int q = 0; q < j; q++) t -= a[i * m + q] * a[j * m + q];
+            a[i * m + j] = t / l;
+        }
+    }
+    return 1;
+}
+
+/* L L^T x = b in place (fcnnls.rs:44-60). */
+static void chol_solve(const double *l, int m, double *b) {
+    for (int i = 0; i < m; i++) {
+        double s = b[i];
+        for (int q = 0; q < i; q++) s -= l[i * m + q] * b[q];
+        b[i] = s / l[i * m + i];
+    }
+    for (int i = m - 1; i >= 0; i--) {
+        double s = b[i];
+        for (int q = i + 1; q < m; q++) s -= l[q * m + i] * b[q];
+        b[i] = s / l[i * m + i];
+    }
+}
+
+/* Solve a x = b (m x m), falling back as pseudoinv_solve does
+ * (fcnnls.rs:62-90): while the Cholesky fails, add eps to the diagonal
+ * (eps = 1e-12, then x10 each try, accumulating); zeros once eps > 1e6.
+ * work holds 2 m^2 doubles. */
+static void spd_solve(const double *a, int m, double *b, double *work) {
+    double *f = work, *areg = work + m * m;
+    memcpy(f, a, sizeof(double) * (size_t)(m * m));
+    if (chol_inplace(f, m)) {
+        chol_solve(f, m, b);
+        return;
+    }
+    memcpy(areg, a, sizeof(double) * (size_t)(m * m));
+    double eps = 1e-12;
+    for (;;) {
+        memcpy(f, areg, sizeof(double) * (size_t)(m * m));
+        if (chol_inplace(f, m)) {
+            chol_solve(f, m, b);
+            return;
+        }
+        for (int i = 0; i < m; i++) areg[i * m + i] += eps;
+        eps *= 10.0;
+        if (eps > 1e6) {
+            for (int i = 0; i < m; i++) b[i] = 0.0;
+            return;
+        }
+    }
+}
+
+/* One column of cssls (fcnnls.rs:93-290): the least-squares solution on the
+ * passive variables (pset, bit i = variable i), zero elsewhere.  ctc is
+ * l x l; rhs_i = cta[i * cs + j * js]; k receives l values. */
+static void cssls_col(int l, const double *ctc, const double *cta, i64 cs, i64 js, int j,
+                      unsigned pset, double *k, double *work) {
+    int act[32], m = 0;
+    for (int i = 0; i < l; i++) {
+        k[i] = 0.0;
+        if (pset >> i & 1u) act[m++] = i;
+    }
+    if (m == 0) return;
+    double *g = work, *b = work + 32 * 32, *w2 = b + 32;
+    for (int a = 0; a < m; a++) {
+        for (int c = 0; c < m; c++) g[a * m + c] = ctc[act[a] * l + act[c]];
+        b[a] = cta[act[a] * cs + (i64)j * js];
+    }
+    spd_solve(g, m, b, w2);
+    for (int a = 0; a < m; a++) k[act[a]] = b[a];
+}
+
+/*
+ * orc_fcnnls: fcnnls (fcnnls.rs:297-470) on precomputed normal equations:
+ * ctc (l x l, row-major), cta (l x P, element (i, j) at cta[i * cs + j * js]),
+ * eps; K (l x P, element (i, j) at K[j * l + i]).  Restated step by step,
+ * including its control flow: one iteration counter (cap 3 l) for all
+ * columns; the inner loop's set of columns recomputed over all P columns as
+ * "any value < eps" (which counts the zeros of inactive variables); a column
+ * of that set without a passive variable below eps takes the step with
+ * alpha = inf, as the reference does.  l <= 32.
+ */
+void orc_fcnnls(int l, i64 P, const double *ctc, const double *cta, i64 cs, i64 js, double eps,
+                double *K) {
+    const int max_iter = 3 * l;
+    int iter = 0;
+    unsigned *pset = (unsigned *)calloc((size_t)(P > 0 ? P : 1), sizeof(unsigned));
+    unsigned char *fset = (unsigned char *)calloc((size_t)(P > 0 ? P : 1), 1);
+    unsigned char *hset = (unsigned char *)calloc((size_t)(P > 0 ? P : 1), 1);
+    double *D = (double *)malloc(sizeof(double) * (size_t)(P * l > 0 ? P * l : 1));
+    double work[32 * 32 + 32 + 2 * 32 * 32];
+    /* Unconstrained start: cssls with every variable passive. */
+    const unsigned all = (l == 32) ? 0xffffffffu : ((1u << l) - 1u);
+    i64 nf = 0;
+    for (i64 j = 0; j < P; j++) {
+        double *kj = K + j * l;
+        cssls_col(l, ctc, cta, cs, js, (int)j, all, kj, work);
+        unsigned ps = 0;
+        for (int i = 0; i < l; i++) {
+            if (kj[i] > 0.0) ps |= 1u << i;
+            else kj[i] = 0.0;
+        }
+        pset[j] = ps;
+        memcpy(D + j * l, kj, sizeof(double) * (size_t)l);
+        fset[j] = (ps != all);
+        nf += fset[j];
+    }
+    while (nf > 0) {
+        i64 nh = 0;
+        for (i64 j = 0; j < P; j++) {
+            hset[j] = 0;
+            if (!fset[j]) continue;
+            cssls_col(l, ctc, cta, cs, js, (int)j, pset[j], K + j * l, work);
+        }
+        for (i64 j = 0; j < P; j++) {
+            if (!fset[j]) continue;
+            for (int i = 0; i < l; i++)
+                if (K[j * l + i] < eps) {
+                    hset[j] = 1;
+                    break;
+                }
+            nh += hset[j];
+        }
+        while (nh > 0 && iter < max_iter) {
+            iter++;
+            int any_ij = 0;
+            for (i64 j = 0; j < P && !any_ij; j++)
+                if (hset[j])
+                    for (int i = 0; i < l; i++)
+                        if ((pset[j] >> i & 1u) && K[j * l + i] < eps) {
+                            any_ij = 1;
+                            break;
+                        }
+            if (!any_ij) break;
+            for (i64 j = 0; j < P; j++) {
+                if (!hset[j]) continue;
+                double *dj = D + j * l;
+                const double *kj = K + j * l;
+                double amin = INFINITY;
+                int imin = 0;
+                for (int i = 0; i < l; i++) {
+                    double a = INFINITY;
+                    if ((pset[j] >> i & 1u) && kj[i] < eps) {
+                        const double den = dj[i] - kj[i];
+                        if (den != 0.0) a = dj[i] / den;
+                    }
+                    if (a < amin) {
+                        amin = a;
+                        imin = i;
+                    }
+                }
+                for (int i = 0; i < l; i++) dj[i] -= amin * (dj[i] - kj[i]);
+                dj[imin] = 0.0;
+                pset[j] &= ~(1u << imin);
+            }
+            for (i64 j = 0; j < P; j++)
+                if (hset[j]) cssls_col(l, ctc, cta, cs, js, (int)j, pset[j], K + j * l, work);
+            nh = 0;
+            for (i64 j = 0; j < P; j++) {
+                hset[j] = 0;
+                for (int i = 0; i < l; i++)
+                    if (K[j * l + i] < eps) {
+                        hset[j] = 1;
+                        break;
+                    }
+                nh += hset[j];
+            }
+        }
+        nf = 0;
+        for (i64 j = 0; j < P; j++) {
+            if (!fset[j]) continue;
+            const double *kj = K + j * l;
+            double best = -INFINITY;
+            int ib = 0;
+            for (int i = 0; i < l; i++) {
+                if (pset[j] >> i & 1u) continue;
+                double w = cta[i * cs + j * js];
+                double s = 0.0;
+                for (int q = 0; q < l; q++) s += ctc[i * l + q] * kj[q];
+                w -= s;
+                if (w > best) {
+                    best = w;
+                    ib = i;
+                }
+            }
+            fset[j] = 0;
+            if (best > eps) {
+                pset[j] |= 1u << ib;
+                memcpy(D + j * l, kj, sizeof(double) * (size_t)l);
+                fset[j] = 1;
+                nf++;
+            }
+        }
+        if (iter >= max_iter) break;
+    }
+    free(pset);
+    free(fset);
+    free(hset);
+    free(D);
+}
+
+/* Test hook: the Cholesky factor of an m x m matrix, in place; 0 on failure. */
+int orc_cholesky(int m, double *a) { return chol_inplace(a, m); }
+
+/* col_l2_normalize (lib.rs:1203-1213). */
+static void col_l2_normalize(i64 m, i64 k, double *w) {
+    for (i64 j = 0; j < k; j++) {
+        double s = 0.0;
+        for (i64 i = 0; i < m; i++) s += w[i * k + j] * w[i * k + j];
+        const double nrm = sqrt(s);
+        if (nrm > 0.0)
+            for (i64 i = 0; i < m; i++) w[i * k + j] /= nrm;
+    }
+}
+
+/*
+ * orc_nmf_run_snmf: nmf_run_snmf_kim_park (lib.rs:1216-1320).  snmf/r
+ * (is_left 0) works on A = V (n x p) with W (n x k), H (k x p); snmf/l on
+ * A = V^T with the roles swapped.  Per iteration: H from FCNNLS on
+ * [W; sqrt(beta) 1^T] against [A; 0], then W^T from FCNNLS on [H^T; eta I]
+ * against [A^T; 0]; eta < 0 means max(A); beta floors at 1e-30.  Records
+ * 0.5 ||A - W H||^2 every iteration (dev: max_iter doubles); runs max_iter
+ * iterations.  w, h hold the user's W0 / H0 on entry and W / H on exit.
+ */
+int orc_nmf_run_snmf(int is_left, i64 n, i64 p, i64 k, const double *v, double *w, double *h,
+                     i64 max_iter, double eta, double beta, double eps, double *dev, int nt) {
+    set_threads(nt);
+    if (k > 32) return -1;
+    /* Internal problem: A (m x q), Wi (m x k), Hi (k x q). */
+    const i64 m = is_left ? p : n, q = is_left ? n : p;
+    double *A = is_left ? transpose(v, n, p) : (double *)malloc(sizeof(double) * (size_t)(n * p > 0 ? n * p : 1));
+    if (!is_left) memcpy(A, v, sizeof(double) * (size_t)(n * p));
+    double *Wi = is_left ? transpose(h, k, p) : (double *)malloc(sizeof(double) * (size_t)(m * k > 0 ? m * k : 1));
+    double *Hi = is_left ? transpose(w, n, k) : (double *)malloc(sizeof(double) * (size_t)(k * q > 0 ? k * q : 1));
+    if (!is_left) {
+        memcpy(Wi, w, sizeof(double) * (size_t)(m * k));
+        memcpy(Hi, h, sizeof(double) * (size_t)(k * q));
+    }
+    double eta_eff = eta;
+    if (eta < 0.0) {
+        eta_eff = 0.0;
+        for (i64 t = 0; t < m * q; t++) eta_eff = (A[t] > eta_eff) ? A[t] : eta_eff;
+    }
+    const double beta_eff = beta > 1e-30 ? beta : 1e-30;
+    const double sb = sqrt(beta_eff);
+    col_l2_normalize(m, k, Wi);
+    double ctc[32 * 32];
+    double *cta = (double *)malloc(sizeof(double) * (size_t)(k * (m > q ? m : q) + 1));
+    double *K = (double *)malloc(sizeof(double) * (size_t)(k * (m > q ? m : q) + 1));
+    for (i64 it = 0; it < max_iter; it++) {
+        /* H: x = [Wi; sb 1^T] ((m + 1) x k), y = [A; 0]. */
+        for (i64 a = 0; a < k; a++)
+            for (i64 c = 0; c < k; c++) {
+                double s = 0.0;
+                for (i64 r = 0; r < m; r++) s += Wi[r * k + a] * Wi[r * k + c];
+                s += sb * sb;
+                ctc[a * k + c] = s;
+            }
+#pragma omp parallel for schedule(static)
+        for (i64 a = 0; a < k; a++)
+            for (i64 j = 0; j < q; j++) {
+                double s = 0.0;
+                for (i64 r = 0; r < m; r++) s += Wi[r * k + a] * A[r * q + j];
+                cta[a * q + j] = s;
+            }
+        orc_fcnnls((int)k, q, ctc, cta, q, 1, eps, K);
+        for (i64 a = 0; a < k; a++)
+            for (i64 j = 0; j < q; j++) Hi[a * q + j] = K[j * k + a];
+        /* W: x = [Hi^T; eta I] ((q + k) x k), y = [A^T; 0]. */
+        for (i64 a = 0; a < k; a++)
+            for (i64 c = 0; c < k; c++) {
+                double s = 0.0;
+                for (i64 r = 0; r < q; r++) s += Hi[a * q + r] * Hi[c * q + r];
+                if (a == c) s += eta_eff * eta_eff;
+                ctc[a * k + c] = s;
+            }
+#pragma omp parallel for schedule(static)
+        for (i64 a = 0; a < k; a++)
+            for (i64 i = 0; i < m; i++) {
+                double s = 0.0;
+                for (i64 r = 0; r < q; r++) s += Hi[a * q + r] * A[i * q + r];
+                cta[a * m + i] = s;
+            }
+        orc_fcnnls((int)k, m, ctc, cta, m, 1, eps, K);
+        for (i64 i = 0; i < m; i++)
+            for (i64 a = 0; a < k; a++) Wi[i * k + a] = K[i * k + a];
+        double s = 0.0;
+        for (i64 i = 0; i < m; i++)
+            for (i64 j = 0; j < q; j++) {
+                double r = 0.0;
+                for (i64 a = 0; a < k; a++) r += Wi[i * k + a] * Hi[a * q + j];
+                const double d = A[i * q + j] - r;
+                s += d * d;
+            }
+        dev[it] = 0.5 * s;
+    }
+    if (is_left) {  /* user W = Hi^T (n x k), user H = Wi^T (k x p) */
+        for (i64 i = 0; i < n; i++)
+            for (i64 a = 0; a < k; a++) w[i * k + a] = Hi[a * n + i];
+        for (i64 a = 0; a < k; a++)
+            for (i64 j = 0; j < p; j++) h[a * p + j] = Wi[j * k + a];
+    } else {
+        memcpy(w, Wi, sizeof(double) * (size_t)(n * k));
+        memcpy(h, Hi, sizeof(double) * (size_t)(k * p));
+    }
+    free(A);
+    free(Wi);
+    free(Hi);
+    free(cta);
+    free(K);
+    return 0;
+}
+
 /* Build identification so the Python side can tell a stale build apart. */
-int orc_version(void) { return 3; }
+int orc_version(void) { return 4; }

@@ -25,6 +25,7 @@
 #include "kernels.cuh"
 #include "launch.h"
 #include "stream.cuh"
+#include "fcnnls.cuh"
 
 using namespace nmfcu;
 
@@ -412,8 +413,11 @@ struct nmfcu_context {
     DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
     DevBuf Wprev, Hprev;     // ehals: the iterate before the last extrapolation
     DevBuf S64, NH, NW;      // lsNMF: weights (pitched like V), the numerator contractions
+                             // (snmf: the FCNNLS right-hand sides)
+    DevBuf fcK, fcD, fcP, fcF, fcC;  // snmf: FCNNLS solutions, steps, sets, flags, ctc + counter
     DevBuf extra[16];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
+    int *h_count = nullptr;       // pinned: the FCNNLS set sizes
 
     // Timing.
     bool timing = false;
@@ -437,6 +441,7 @@ struct nmfcu_context {
         }
         for (auto e : pool) cudaEventDestroy(e);
         if (h_state) cudaFreeHost(h_state);
+        if (h_count) cudaFreeHost(h_count);
         if (own_stream) cudaStreamDestroy(own_stream);
         cudaSetDevice(prev);
     }
@@ -997,9 +1002,17 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         v.push_back({&c->Wns, sizeof(double) * (size_t)pl.n * RP});
         v.push_back({&c->Hns, sizeof(double) * RP * (size_t)pl.p});
     }
-    if (method == NMFCU_LSNMF) {
+    if (method == NMFCU_LSNMF || method == NMFCU_SNMF_R || method == NMFCU_SNMF_L) {
         v.push_back({&c->NW, sizeof(double) * (size_t)pl.n * RP});
         v.push_back({&c->NH, sizeof(double) * RP * (size_t)pl.p});
+    }
+    if (method == NMFCU_SNMF_R || method == NMFCU_SNMF_L) {
+        const size_t P = (size_t)std::max(pl.n, pl.p);
+        v.push_back({&c->fcK, sizeof(double) * P * pl.r});
+        v.push_back({&c->fcD, sizeof(double) * P * pl.r});
+        v.push_back({&c->fcP, sizeof(unsigned) * P});
+        v.push_back({&c->fcF, 2 * P});
+        v.push_back({&c->fcC, sizeof(double) * (nmfcu::kFcMax * nmfcu::kFcMax + 4)});
     }
     if (method == NMFCU_EHALS) {
         v.push_back({&c->Wprev, sizeof(double) * (size_t)pl.n * RP});
@@ -1018,6 +1031,7 @@ nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32,
     for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc, method))
         NMF_TRY(w.buf->ensure(w.bytes));
     if (!c->h_state) CUDA_TRY(cudaMallocHost((void **)&c->h_state, sizeof(RunState)));
+    if (!c->h_count) CUDA_TRY(cudaMallocHost((void **)&c->h_count, sizeof(int)));
     return NMFCU_OK;
 }
 
@@ -1039,11 +1053,9 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
         case NMFCU_HALS:
         case NMFCU_EHALS:
         case NMFCU_LSNMF:
+        case NMFCU_SNMF_R:
+        case NMFCU_SNMF_L:
         case NMFCU_DNMF: break;
-        case NMFCU_SNMF_R: case NMFCU_SNMF_L:
-            return fail(NMFCU_ERR_UNSUPPORTED,
-                        "method is not built in the GPU engine (built: brunet, lee, offset, nsNMF, "
-                        "hals, ehals, dnmf, lsNMF)");
         default: return fail(NMFCU_ERR_INVALID_ARG, "unknown method id");
     }
     if (o->stop != NMFCU_STOP_MAX_ITER && o->stop != NMFCU_STOP_STATIONARY)
@@ -1054,6 +1066,9 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
     if (o->max_iter < 0) return fail(NMFCU_ERR_INVALID_ARG, "max_iter must be >= 0");
     if (o->method == NMFCU_LSNMF && o->precision != NMFCU_PREC_FP64)
         return fail(NMFCU_ERR_UNSUPPORTED, "lsNMF runs in FP64 only");
+    if ((o->method == NMFCU_SNMF_R || o->method == NMFCU_SNMF_L) &&
+        o->precision != NMFCU_PREC_FP64)
+        return fail(NMFCU_ERR_UNSUPPORTED, "snmf/r and snmf/l run in FP64 only");
     if (o->check_niter < 0 || o->check_interval < 0)
         return fail(NMFCU_ERR_INVALID_ARG, "check_interval / check_niter must be >= 0");
     if (o->refine_iters < 0) return fail(NMFCU_ERR_INVALID_ARG, "refine_iters must be >= 0");
@@ -1061,6 +1076,160 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
 }
 
 // Runs the loop on prepared device buffers; fills n_iter / n_dev.
+// Waits for the stream and reports a streaming kernel that gave up waiting
+// for its copies (the device state's timeout flag).
+nmfcu_status finish_checked(nmfcu_context *c, cudaStream_t s) {
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(c->h_state, c->state.ptr, sizeof(RunState), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (c->h_state->timeout != 0)
+        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies (code " +
+                                           std::to_string(c->h_state->timeout) + ")");
+    return NMFCU_OK;
+}
+
+// FCNNLS over P columns (fcnnls.rs:297-470): the kernels of fcnnls.cuh in
+// the reference's loop order, with its one iteration counter (cap 3 l) and
+// its tests for empty sets read back after each set update.
+nmfcu_status fcnnls_device(nmfcu_context *c, int l, int64_t P, const double *ctc,
+                           const double *cta, int64_t cs, int64_t js, double eps,
+                           cudaStream_t s) {
+    if (P <= 0) return NMFCU_OK;
+    nmfcu::FcState fs;
+    fs.K = c->fcK.as<double>();
+    fs.D = c->fcD.as<double>();
+    fs.pset = c->fcP.as<unsigned>();
+    fs.fflag = c->fcF.as<uint8_t>();
+    fs.hflag = fs.fflag + P;
+    fs.count = reinterpret_cast<int *>(c->fcC.as<double>() + nmfcu::kFcMax * nmfcu::kFcMax + 2);
+    constexpr int kT = 128;
+    const unsigned g = (unsigned)cdiv(P, kT);
+    int launches = 0;
+    auto counted = [&](auto &&launch) -> nmfcu_status {
+        CUDA_TRY(cudaMemsetAsync(fs.count, 0, sizeof(int), s));
+        launch();
+        launches++;
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(c->h_count, fs.count, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        return NMFCU_OK;
+    };
+    NMF_TRY(counted([&] { nmfcu::fc_start<<<g, kT, 0, s>>>(l, P, ctc, cta, cs, js, fs); }));
+    int nf = *c->h_count;
+    int iter = 0;
+    const int max_iter = 3 * l;
+    while (nf > 0) {
+        nmfcu::fc_solve<<<g, kT, 0, s>>>(l, P, ctc, cta, cs, js, fs, fs.fflag);
+        launches++;
+        NMF_TRY(counted([&] { nmfcu::fc_hset<<<g, kT, 0, s>>>(l, P, eps, fs, 1); }));
+        int nh = *c->h_count;
+        while (nh > 0 && iter < max_iter) {
+            iter++;
+            NMF_TRY(counted([&] { nmfcu::fc_any_ij<<<g, kT, 0, s>>>(l, P, eps, fs); }));
+            if (*c->h_count == 0) break;
+            nmfcu::fc_step<<<g, kT, 0, s>>>(l, P, eps, fs);
+            nmfcu::fc_solve<<<g, kT, 0, s>>>(l, P, ctc, cta, cs, js, fs, fs.hflag);
+            launches += 2;
+            NMF_TRY(counted([&] { nmfcu::fc_hset<<<g, kT, 0, s>>>(l, P, eps, fs, 0); }));
+            nh = *c->h_count;
+        }
+        NMF_TRY(counted([&] { nmfcu::fc_tail<<<g, kT, 0, s>>>(l, P, ctc, cta, cs, js, eps, fs); }));
+        nf = *c->h_count;
+        if (iter >= max_iter) break;
+    }
+    c->launch_total += launches;
+    return NMFCU_OK;
+}
+
+// Kim-Park sparse NMF (nmf_run_snmf_kim_park, lib.rs:1216-1320): ANLS with
+// FCNNLS.  snmf/r solves H from [W; sqrt(beta) 1^T] against [V; 0], then W
+// from [H^T; eta I] against [V^T; 0]; snmf/l works on V^T, so it solves W
+// first (normal equations H H^T + beta, right-hand sides V H^T) and then H
+// (W^T W + eta^2 I, W^T V).  The right-hand sides are the plain passes'
+// products; the Grams are the iteration's own.  Every iteration records
+// 0.5 ||V - W H||^2; there is no stop test (the reference runs max_iter).
+nmfcu_status run_snmf(nmfcu_context *c, RunArgs &a, cudaStream_t s, double *dev) {
+    const nmfcu_options *o = a.opt;
+    const Plan &pl = a.pl;
+    const bool left = (o->method == NMFCU_SNMF_L);
+    RunState *st = c->state.as<RunState>();
+    CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
+    // snmf/r: eta = smoothness_w, beta = sparsity_h; snmf/l: the mirror
+    // (lib.rs:2117-2148).
+    const double eta = left ? o->smoothness_h : o->smoothness_w;
+    const double beta = left ? o->sparsity_w : o->sparsity_h;
+    double *ctc = c->fcC.as<double>();
+    double *misc = ctc + nmfcu::kFcMax * nmfcu::kFcMax;  // [vmax, -, count]
+    double eta_eff = eta;
+    if (eta < 0.0) {  // max(V) (and 0), lib.rs:1252-1256
+        nmfcu::fc_vmax<<<1, 256, 0, s>>>(a.V64, a.ldv64, pl.n, pl.p, misc);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(&eta_eff, misc, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+    }
+    const double beta_eff = beta > 1e-30 ? beta : 1e-30;
+    const double sb = std::sqrt(beta_eff);
+    const int r = pl.r, RP = pl.RP;
+    double *Gw = c->Gw.as<double>(), *sw = c->sw.as<double>();
+    double *Gh = c->Gh.as<double>(), *sh = c->sh.as<double>();
+    double *NH = c->NH.as<double>(), *NW = c->NW.as<double>();
+    EpiParams ep = epi(o, r, nullptr, nullptr, true);
+    ep.method = nmfcu::M_PRODUCT;
+    // The factor normalised first: W's columns (snmf/r) or H's rows (snmf/l).
+    if (left)
+        nmfcu::fc_normalize<<<r, 256, 0, s>>>(a.H, pl.p, r, RP, 1);
+    else
+        nmfcu::fc_normalize<<<r, 256, 0, s>>>(a.W, pl.n, r, RP, 0);
+    CUDA_TRY(cudaGetLastError());
+    auto solve_h = [&](double add_all, double add_diag) -> nmfcu_status {
+        // ctc = W^T W + ..., right-hand sides W^T V (the H pass's product).
+        gram_w_full(c, a, Gw, sw, s);
+        nmfcu::fc_normal<<<1, r * r, 0, s>>>(Gw, RP, r, add_all, add_diag, ctc);
+        RunArgs an = a;
+        an.H = NH;
+        NMF_TRY(h_step(c, an, a.p64, ep, false, s));
+        NMF_TRY(fcnnls_device(c, r, pl.p, ctc, NH, pl.p, 1, o->eps, s));
+        if (pl.p > 0)
+            nmfcu::fc_scatter<<<grid_for((int64_t)pl.p * r), kThreads, 0, s>>>(
+                c->fcK.as<double>(), r, pl.p, RP, 1, a.H);
+        CUDA_TRY(cudaGetLastError());
+        return NMFCU_OK;
+    };
+    auto solve_w = [&](double add_all, double add_diag) -> nmfcu_status {
+        // ctc = H H^T + ..., right-hand sides V H^T (the W pass's product).
+        gram_h_full(c, a, Gh, sh, s);
+        nmfcu::fc_normal<<<1, r * r, 0, s>>>(Gh, RP, r, add_all, add_diag, ctc);
+        transpose_h(c, a, a.p64, s);
+        RunArgs aw = a;
+        aw.Wout = NW;
+        NMF_TRY(w_step(c, aw, a.p64, ep, false, s));
+        NMF_TRY(fcnnls_device(c, r, pl.n, ctc, NW, 1, RP, o->eps, s));
+        if (pl.n > 0)
+            nmfcu::fc_scatter<<<grid_for((int64_t)pl.n * r), kThreads, 0, s>>>(
+                c->fcK.as<double>(), r, pl.n, RP, 0, a.W);
+        CUDA_TRY(cudaGetLastError());
+        return NMFCU_OK;
+    };
+    StopParams sp{};
+    sp.stationary = 0;
+    sp.scale = 0.5;
+    for (long long it = 0; it < o->max_iter; it++) {
+        if (left) {
+            NMF_TRY(solve_w(sb * sb, 0.0));        // user W from [H^T; sqrt(beta) 1^T]
+            NMF_TRY(solve_h(0.0, eta_eff * eta_eff));  // user H from [W; eta I]
+        } else {
+            NMF_TRY(solve_h(sb * sb, 0.0));
+            NMF_TRY(solve_w(0.0, eta_eff * eta_eff));
+        }
+        NMF_TRY(enqueue_objective_partials(c, a, s));
+        sp.iter = it;
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        objective_finalize<<<1, kThreads, 0, s>>>(c->obj.as<double>(),
+                                                  pl.n > 0 ? pl.obj_blocks : 0, dev, sp, st);
+    }
+    return finish_checked(c, s);
+}
+
 nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_dev,
                       int64_t *n_iter) {
     const nmfcu_options *o = a.opt;
@@ -1203,18 +1372,6 @@ bool ieq(const char *a, const char *b) {
     for (; *a && *b; a++, b++)
         if (tolower((unsigned char)*a) != tolower((unsigned char)*b)) return false;
     return *a == 0 && *b == 0;
-}
-
-// Waits for the stream and reports a streaming kernel that gave up waiting
-// for its copies (the device state's timeout flag).
-nmfcu_status finish_checked(nmfcu_context *c, cudaStream_t s) {
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(c->h_state, c->state.ptr, sizeof(RunState), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    if (c->h_state->timeout != 0)
-        return fail(NMFCU_ERR_TIMEOUT, "a streaming kernel gave up waiting for its copies (code " +
-                                           std::to_string(c->h_state->timeout) + ")");
-    return NMFCU_OK;
 }
 
 // Columns [c0, c0 + kc) of X (rows x ldx) into out (rows x ld, zero padded).
@@ -1369,7 +1526,8 @@ size_t context_bytes(nmfcu_context *c) {
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
                             &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
                             &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
-                            &c->S64, &c->NH, &c->NW})
+                            &c->S64, &c->NH, &c->NW,
+                            &c->fcK, &c->fcD, &c->fcP, &c->fcF, &c->fcC})
         t += b->bytes;
     for (const DevBuf &b : c->extra) t += b.bytes;
     return t;
@@ -1402,7 +1560,8 @@ void context_release(nmfcu_context *c) {
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
                       &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
                             &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
-                            &c->S64, &c->NH, &c->NW})
+                            &c->S64, &c->NH, &c->NW,
+                            &c->fcK, &c->fcD, &c->fcP, &c->fcF, &c->fcC})
         b->release();
     for (DevBuf &b : c->extra) b.release();
 }
@@ -1538,6 +1697,10 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
     NMF_TRY(validate_options(opt, n, p, r));
     if (!V || !W0 || !H0 || !W || !H || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    const bool snmf = opt->method == NMFCU_SNMF_R || opt->method == NMFCU_SNMF_L;
+    if (snmf && (!deviances || deviances_cap < opt->max_iter))
+        return fail(NMFCU_ERR_INVALID_ARG,
+                    "snmf records a deviance every iteration: deviances must hold max_iter values");
     const bool ls = opt->method == NMFCU_LSNMF;
     if (ls && !weight)  // py_nmf_run, lib.rs:1967-1971
         return fail(NMFCU_ERR_INVALID_ARG,
@@ -1595,6 +1758,19 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
     }
     NMF_TRY(setup_method(c, pl, opt, a, offset0, true, s));
     int64_t nd = 0, ni = 0;
+    if (snmf) {
+        NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)std::max<int64_t>(1, opt->max_iter)));
+        NMF_TRY(run_snmf(c, a, s, c->dev.as<double>()));
+        ni = nd = opt->max_iter;
+        NMF_TRY(get_factors(c, pl, W, H, cudaMemcpyDeviceToHost, s));
+        if (nd > 0)
+            CUDA_TRY(cudaMemcpyAsync(deviances, c->dev.ptr, sizeof(double) * (size_t)nd,
+                                     cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaStreamSynchronize(s));
+        *n_deviances = nd;
+        *n_iter = ni;
+        return NMFCU_OK;
+    }
     NMF_TRY(run_loop(c, a, s, &nd, &ni));
     NMF_TRY(get_factors(c, pl, W, H, cudaMemcpyDeviceToHost, s));
     if (offset && opt->method == NMFCU_OFFSET && n > 0)
@@ -1717,6 +1893,8 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     if (opt->method == NMFCU_LSNMF)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
+    if (opt->method == NMFCU_SNMF_R || opt->method == NMFCU_SNMF_L)
+        return fail(NMFCU_ERR_UNSUPPORTED, "snmf/r and snmf/l run through nmfcu_run");
     if (!dV || !dW || !dH || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (v_dtype != NMFCU_F64 && v_dtype != NMFCU_F32)

@@ -336,6 +336,8 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
     if (opt->method == NMFCU_LSNMF)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
+    if (opt->method == NMFCU_SNMF_R || opt->method == NMFCU_SNMF_L)
+        return fail(NMFCU_ERR_UNSUPPORTED, "snmf/r and snmf/l run through nmfcu_run");
     if (!V || !W0 || !H0 || !W || !H) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
     if (dev_cap < 0 || (dev_cap > 0 && !deviances))

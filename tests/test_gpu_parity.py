@@ -273,8 +273,8 @@ def test_fp32_precision_form(oracle, method):
 
 def test_unsupported_method_and_rank(quickstart):
     V, W0, H0 = quickstart
-    with pytest.raises(NotImplementedError):
-        nmf_rs.nmf(V, 5, "snmf/r", W0=W0, H0=H0, max_iter=2)
+    with pytest.raises(NotImplementedError):  # snmf runs in FP64 only
+        nmf_rs.nmf(V, 5, "snmf/r", W0=W0, H0=H0, max_iter=2, precision="bf16x3")
     V2 = synthetic.counts_matrix(50, 60, 4, 0.3, seed=1)
     with pytest.raises(NotImplementedError, match="rank 33"):
         nmf_rs.nmf(V2, 33, "lee", max_iter=2, seed=0)

@@ -1,8 +1,6 @@
 """The reference's own behavioural tests of the methods this engine builds
 (tests/test_lsnmf_snmf.py of omicverse/rust-NMF: the lsNMF and alias checks),
-restated on the GPU path with the same inputs and thresholds.  The Kim-Park
-snmf/r and snmf/l are not built here; their checks become "raises
-NotImplementedError"."""
+restated on the GPU path with the same inputs and thresholds.""" 
 from __future__ import annotations
 
 import numpy as np
@@ -52,12 +50,14 @@ def test_lsnmf_requires_weight(synth):
         nmf_rs.nmf(V, rank=rank, method="lsnmf", W0=W0, H0=H0, max_iter=10, num_threads=1)
 
 
-@pytest.mark.parametrize("method", ["snmf/r", "snmf/l"])
-def test_kim_park_snmf_is_not_built(synth, method):
+@pytest.mark.parametrize("method,which", [("snmf/r", "H"), ("snmf/l", "W")])
+def test_snmf_makes_the_factor_sparser(synth, method, which):
     V, W0, H0, rank = synth["V"], synth["W0"], synth["H0"], synth["rank"]
-    with pytest.raises(NotImplementedError):
-        nmf_rs.nmf(V, rank=rank, method=method, sparsity=0.5, smoothness=-1.0, W0=W0, H0=H0,
-                   max_iter=20)
+    res_lee = nmf_rs.nmf(V, rank=rank, method="lee", W0=W0, H0=H0, max_iter=200, num_threads=2)
+    res_s = nmf_rs.nmf(V, rank=rank, method=method, sparsity=0.5, smoothness=-1.0, W0=W0,
+                       H0=H0, max_iter=20, num_threads=2)
+    dens = lambda M: float((M > 1e-6).mean())  # noqa: E731
+    assert dens(getattr(res_s, which)) < dens(getattr(res_lee, which))
 
 
 def test_method_aliases():
@@ -65,7 +65,8 @@ def test_method_aliases():
     W0, H0 = nmf_rs.random_init(V, 3, seed=0)
     pairs = [("ls-nmf", "lsnmf"), ("kl", "brunet"), ("frobenius", "lee"), ("euclidean", "lee"),
              ("ns", "nsnmf"), ("ns_nmf", "nsNMF"), ("e-hals", "ehals"), ("extrap_hals", "ehals"),
-             ("diag_nmf", "dnmf"), ("rcppml", "dnmf")]
+             ("diag_nmf", "dnmf"), ("rcppml", "dnmf"), ("snmf_r", "snmf/r"),
+             ("snmf_l", "snmf/l")]
     for a, b in pairs:
         kw = dict(W0=W0, H0=H0, max_iter=20, num_threads=1)
         if b == "lsnmf":

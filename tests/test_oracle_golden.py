@@ -199,3 +199,71 @@ def test_lsnmf_stationary_trace(oracle, quickstart):
     assert d[-1] < d[0]
     with pytest.raises(ValueError, match="weight"):
         oracle.nmf_method("lsnmf", V, W0, H0, 3)
+
+
+# ---------------------------------------------------------------------------
+# Kim-Park snmf/r, snmf/l (FCNNLS): the reference's own unit tests of its
+# FCNNLS (rust/src/fcnnls.rs tests) and behavioural tests
+# (tests/test_lsnmf_snmf.py), on the restatement.
+# ---------------------------------------------------------------------------
+
+def test_fcnnls_cholesky_identity(oracle):
+    ok, L = oracle.cholesky(np.array([[4.0, 12.0, -16.0], [12.0, 37.0, -43.0],
+                                      [-16.0, -43.0, 98.0]]))
+    assert ok
+    np.testing.assert_allclose(L, [[2, 0, 0], [6, 1, 0], [-8, 5, 3]], atol=1e-12)
+
+
+def test_fcnnls_unconstrained_active(oracle):
+    x = np.array([[1.0, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 0], [0, 1, 1]])
+    y = np.array([[2.0, 1.0], [3.0, 2.0], [4.0, 3.0], [4.5, 2.5], [6.5, 4.5]])
+    K = oracle.fcnnls(x.T @ x, x.T @ y, eps=0.0)
+    assert (K >= -1e-9).all()
+    assert ((x @ K - y) ** 2).sum() < 1.0
+
+
+def test_fcnnls_matches_scipy_nnls_when_well_posed(oracle):
+    from scipy.optimize import nnls
+
+    gen = np.random.default_rng(4)
+    x = gen.uniform(0, 1, (40, 6))
+    y = gen.uniform(-0.5, 1.5, (40, 25))
+    K = oracle.fcnnls(x.T @ x, x.T @ y, eps=0.0)
+    for j in range(y.shape[1]):
+        ref, _ = nnls(x, y[:, j])
+        assert np.abs(K[:, j] - ref).max() <= 1e-8
+
+
+@pytest.fixture(scope="module")
+def synth():
+    rng = np.random.default_rng(42)
+    n, p, rank = 120, 60, 6
+    V = rng.uniform(0.1, 1.5, (n, rank)) @ rng.uniform(0.1, 1.5, (rank, p)) + \
+        rng.uniform(0, 0.05, (n, p))
+    gen = np.random.default_rng(0)
+    W0 = gen.uniform(0, V.max(), (n, rank))
+    H0 = gen.uniform(0, V.max(), (rank, p))
+    return V, W0, H0
+
+
+@pytest.mark.parametrize("left", [False, True])
+def test_snmf_sparser_than_lee(oracle, synth, left):
+    V, W0, H0 = synth
+    lee = oracle.nmf_method("lee", V, W0, H0, 200)
+    res = oracle.nmf_method("snmf/l" if left else "snmf/r", V, W0, H0, 20, sparsity=0.5,
+                            smoothness=-1.0)
+    dens = lambda M: float((M > 1e-6).mean())  # noqa: E731
+    if left:
+        assert dens(res["W"]) < dens(lee["W"])
+    else:
+        assert dens(res["H"]) < dens(lee["H"])
+    assert res["n_iter"] == 20 and res["deviances"].size == 20
+    assert np.isfinite(res["W"]).all() and np.isfinite(res["H"]).all()
+
+
+def test_snmf_thread_count_independent(oracle, synth):
+    V, W0, H0 = synth
+    a = oracle.nmf_method("snmf/r", V, W0, H0, 5, sparsity=0.5, smoothness=-1.0, num_threads=1)
+    b = oracle.nmf_method("snmf/r", V, W0, H0, 5, sparsity=0.5, smoothness=-1.0, num_threads=4)
+    np.testing.assert_array_equal(a["W"], b["W"])
+    np.testing.assert_array_equal(a["H"], b["H"])
