@@ -53,8 +53,8 @@ enum {
     NMFCU_EHALS = 5,
     NMFCU_DNMF = 6,
     NMFCU_LSNMF = 7,  /* through nmfcu_run_weighted (FP64) */
-    NMFCU_SNMF_R = 8, /* not built */
-    NMFCU_SNMF_L = 9  /* not built */
+    NMFCU_SNMF_R = 8, /* FP64 */
+    NMFCU_SNMF_L = 9  /* FP64 */
 };
 
 /* Stop ids: the variants of `Stop` (lib.rs:1507-1513). */
@@ -110,7 +110,9 @@ nmfcu_status nmfcu_parse_stop(const char *name, int32_t *stop);
  * offset, nsNMF, hals, ehals and dnmf: the whole iteration loop
  * (nmf_run_brunet :1529-1586, nmf_run_lee :1589-1647, nmf_run_offset
  * :1650-1760, nmf_run_nsnmf :1762-1830, nmf_run_hals :638-688,
- * nmf_run_ehals :711-786, nmf_run_dnmf :827-906).
+ * nmf_run_ehals :711-786, nmf_run_dnmf :827-906) and the Kim-Park snmf/r,
+ * snmf/l (nmf_run_snmf_kim_park :1216-1320, FP64; deviances then hold one
+ * value an iteration whatever the stop, as the reference returns).
  * For offset it starts from rowMeans(V) and drops the final offsets; use
  * nmfcu_run_offset to pass and receive them.
  *

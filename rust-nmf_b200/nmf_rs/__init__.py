@@ -7,9 +7,10 @@ and ``set_num_threads``, with the iteration loop running as hand-written
 sm_100a CUDA kernels behind the C ABI of ``include/nmfcu.h``.
 
 Built methods: ``brunet`` (KL), ``lee`` (Frobenius), ``offset``, ``nsNMF``,
-``hals``, ``ehals``, ``dnmf`` and ``lsnmf`` (weighted, FP64), each with
-``stop='max_iter'`` or ``'stationary'``.  The Kim-Park ``snmf/r`` and
-``snmf/l`` raise ``NotImplementedError``.  There is no CPU fallback: without the CUDA library
+``hals``, ``ehals``, ``dnmf``, ``lsnmf`` (weighted) and the Kim-Park
+``snmf/r`` / ``snmf/l`` (FCNNLS), each with ``stop='max_iter'`` or
+``'stationary'`` (snmf runs max_iter iterations, as the reference does);
+lsnmf and snmf in FP64 only.  There is no CPU fallback: without the CUDA library
 or a GPU every compute call raises ``RuntimeError``.
 
 Engine extensions (keyword-only, defaults keep the reference's behaviour):
