@@ -311,8 +311,9 @@ def host_slice_fn(V64, p_full, rank, seed=0):
 PASS_DRAM_BYTES_PER_ELEMENT = {
     ("hpass", "fp32"): (1634701568 + 35060736) / 4e8,
     ("wpass", "fp32"): (1637906432 + 33353984) / 4e8,
-    ("hpass", "fp64"): (3232219392 + 31828224) / 4e8,
-    ("wpass", "fp64"): (3242305792 + 32467968) / 4e8,
+    # f64: the FP64 tensor-core passes (hpass_dmma / wpass_dmma)
+    ("hpass", "fp64"): (3233123072 + 32075008) / 4e8,
+    ("wpass", "fp64"): (3237119744 + 31909376) / 4e8,
     # split-bf16 form: the tensor-core passes (H pass streams the split V^T)
     ("hpass", "bf16x3"): (1614820000 + 7405568) / 4e8,
     ("wpass", "bf16x3"): (1614029000 + 9831936) / 4e8,
@@ -491,11 +492,17 @@ def run_ours(args, world, rank, local):
         if (args.workload in ("atlas", "atlas-slice") and r == 20 and
                 (kname, args.precision) in PASS_DRAM_BYTES_PER_ELEMENT):
             traffic = PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] * n * p  # per launch
+        hw = "H step" if dom == _native.KCLASS_HSTEP else "W step"
+        if args.precision == "bf16x3" and args.method != "brunet":
+            kernel = "tc_pass<H>" if dom == _native.KCLASS_HSTEP else "tc_pass<W>"
+        elif args.precision == "fp64":
+            kernel = ("h" if dom == _native.KCLASS_HSTEP else "w") + "pass_dmma" + (
+                "_ratio" if args.method == "brunet" else "") + f" ({hw}, FP64 tensor cores)"
+        else:
+            kernel = ("hpass" if dom == _native.KCLASS_HSTEP else "wpass") + f" ({hw})"
         roof = {
             "bound": "hbm",
-            "kernel": ((("tc_pass<H>" if dom == _native.KCLASS_HSTEP else "tc_pass<W>")
-                        if args.precision == "bf16x3" and args.method != "brunet" else
-                        ("hpass (H step)" if dom == _native.KCLASS_HSTEP else "wpass (W step)"))),
+            "kernel": kernel,
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
