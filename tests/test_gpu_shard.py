@@ -138,3 +138,13 @@ def test_shard_rejects_other_methods(quickstart):
     V, W0, H0 = quickstart
     with pytest.raises(NotImplementedError):
         shard.nmf_sharded(nndsvd.upload(V), 5, "offset", W0=W0, H0_local=H0, max_iter=2)
+
+
+@pytest.mark.parametrize("method", ["lee", "brunet"])
+def test_shards_with_empty_blocks(oracle, method):
+    # p = 40 over 5 shards: blocks of 0, 16, 0, 16 and 8 columns
+    V = synthetic.counts_matrix(90, 40, 4, 0.3, seed=12) + 0.01
+    W0, H0 = nmf_rs.random_init(V, 5, seed=1)
+    W, H, n_iter, _ = run_local(V, W0, H0, method, 5, 15)
+    ref = oracle.nmf_method(method, V, W0, H0, 15)
+    assert rel_max(W, ref["W"]) <= TOL and rel_max(H, ref["H"]) <= TOL

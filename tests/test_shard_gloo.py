@@ -127,3 +127,12 @@ def test_three_gloo_ranks_uneven_blocks(tmp_path, oracle, start, method):
     ref = oracle.nmf_method(method, V, W0, H0, 15)
     assert n_iter == 15
     assert rel_max(W, ref["W"]) <= TOL and rel_max(H, ref["H"]) <= TOL
+
+
+def test_gloo_rank_with_no_columns(tmp_path, oracle, start):
+    # 20 columns over 3 ranks: rank 0 holds none, yet takes every collective step
+    V, W0, H0, _, _ = start
+    V, H0 = V[:, :20].copy(), H0[:, :20].copy()
+    W, H, n_iter, _ = _run(tmp_path, "lee", V, W0, H0, world=3, max_iter=10)
+    ref = oracle.nmf_method("lee", V, W0, H0, 10)
+    assert rel_max(W, ref["W"]) <= TOL and rel_max(H, ref["H"]) <= TOL
