@@ -314,8 +314,10 @@ struct HCfg {
     static constexpr int W32 = (int)sizeof(T) / 4;  // 32-bit registers per T
     static constexpr int KB = RP / KS;               // k per thread
     static constexpr int LPK = 32 / KS;              // lanes per k-half
-    // Columns per thread: more where one column's arithmetic is cheap.
-    static constexpr int CPT = RATIO ? 1 : (sizeof(T) == 4 ? 4 : 2);
+    // Columns per thread: more where one column's arithmetic is cheap; two in
+    // the f32 ratio pass, whose per-column chain (dot, exchange, reciprocal,
+    // axpy) needs a second independent chain to hide its latency.
+    static constexpr int CPT = RATIO ? (sizeof(T) == 4 ? 2 : 1) : (sizeof(T) == 4 ? 4 : 2);
     static constexpr int REGS = W32 * (CPT * KB * (RATIO ? 2 : 1) + KB + CPT);
     static constexpr int kWarps = warps_for(REGS, reg_limit<T, RATIO>());
     static constexpr int TCOLS = LPK * CPT * kWarps;
