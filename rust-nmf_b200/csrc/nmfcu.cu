@@ -369,6 +369,7 @@ Plan make_plan(int64_t n, int64_t p, int64_t r, int sms) {
 // into segments of at most `segu` units, over at most `sms` CTAs.
 StreamK plan_sk(int64_t majors, int64_t units, int64_t segu, int sms) {
     StreamK sk;
+    sk.fold = 0;
     sk.nseg = (int)std::max<int64_t>(1, (units + segu - 1) / segu);
     sk.UPT = (int)std::max<int64_t>(1, (units + sk.nseg - 1) / sk.nseg);
     sk.U = (units > 0) ? majors * sk.nseg * (int64_t)sk.UPT : 0;
@@ -527,11 +528,22 @@ bool f32_form(const nmfcu_options *o) {
 }
 int64_t round8(int64_t x) { return std::max<int64_t>(8, (x + 7) / 8 * 8); }
 int tc_rpn(int RP) { return RP <= 16 ? 16 : 32; }
+// The tensor-core passes fold their partials: one slot per major tile a CTA
+// meets (at most ceil(units a CTA / units a major tile) + 1 of them).
+StreamK fold_sk(StreamK sk) {
+    if (sk.G <= 0) return sk;
+    sk.fold = 1;
+    const int64_t per = (sk.U + sk.G - 1) / sk.G, mu = (int64_t)sk.nseg * sk.UPT;
+    sk.slots = (int)((per + mu - 1) / mu + 1);
+    return sk;
+}
 StreamK plan_tc_h(int64_t n, int64_t p, int sms) {
-    return plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms);
+    return fold_sk(
+        plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms));
 }
 StreamK plan_tc_w(int64_t n, int64_t p, int sms) {
-    return plan_sk((n + kTcTile - 1) / kTcTile, (p + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms);
+    return fold_sk(
+        plan_sk((n + kTcTile - 1) / kTcTile, (p + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms));
 }
 size_t tc_partial_bytes(const Plan &pl, int sms) {
     const StreamK h = plan_tc_h(pl.n, pl.p, sms), w = plan_tc_w(pl.n, pl.p, sms);

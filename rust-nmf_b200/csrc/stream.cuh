@@ -120,15 +120,22 @@ struct StreamK {
     int UPT;      // units per tile (= per segment)
     int slots;    // partial slots per CTA
     int nseg;     // segments per major tile (tile t = major * nseg + segment)
+    // 0: one partial per (CTA, tile).  1: one per (CTA, major tile) -- the
+    // pass adds a CTA's segments of a major tile in f64 before writing it,
+    // and `slots` counts major tiles.
+    int fold;
     __host__ __device__ __forceinline__ long long start(int b) const {
         return (long long)b * U / G;
     }
+    // Units of a major tile.
+    __host__ __device__ __forceinline__ long long major_units() const {
+        return (long long)nseg * UPT;
+    }
 };
 
-// CTAs [lo, hi] whose unit range meets tile t.
-__device__ __forceinline__ void sk_range(const StreamK &sk, int t, int *lo, int *hi) {
-    const long long a = (long long)t * sk.UPT;
-    const long long e = min(a + sk.UPT, sk.U);
+// CTAs [lo, hi] whose unit range meets units [a, e) (a < e <= U).
+__device__ __forceinline__ void sk_range_units(const StreamK &sk, long long a, long long e,
+                                               int *lo, int *hi) {
     int l = 0, h = sk.G - 1;
     while (l < h) {  // first b with start(b + 1) > a
         const int m = (l + h) >> 1;
@@ -142,6 +149,23 @@ __device__ __forceinline__ void sk_range(const StreamK &sk, int t, int *lo, int 
         if (sk.start(m) < e) l = m; else h = m - 1;
     }
     *hi = l;
+}
+
+// CTAs [lo, hi] whose unit range meets tile t.
+__device__ __forceinline__ void sk_range(const StreamK &sk, int t, int *lo, int *hi) {
+    const long long a = (long long)t * sk.UPT;
+    sk_range_units(sk, a, min(a + sk.UPT, sk.U), lo, hi);
+}
+
+// CTAs [lo, hi] whose unit range meets major tile m (folded partials).
+__device__ __forceinline__ void sk_range_major(const StreamK &sk, int m, int *lo, int *hi) {
+    const long long a = (long long)m * sk.major_units();
+    sk_range_units(sk, a, min(a + sk.major_units(), sk.U), lo, hi);
+}
+
+// Slot of major tile m in CTA b's folded partials.
+__device__ __forceinline__ int fold_slot(const StreamK &sk, int b, int m) {
+    return m - (int)(sk.start(b) / sk.major_units());
 }
 
 // Position of a unit in the tile order, advanced one unit at a time so that
@@ -1362,6 +1386,17 @@ __device__ __forceinline__ void gather_partials(const double *__restrict__ part,
 #pragma unroll
     for (int k = 0; k < RP; k++) num[k] = 0.0;
     if (sk.G <= 0) return;  // no units at all: every sum is empty
+    if (sk.fold) {
+        int lo, hi;
+        sk_range_major(sk, mt, &lo, &hi);
+        for (int b = lo; b <= hi; b++) {
+            const double *src =
+                part + ((size_t)b * sk.slots + fold_slot(sk, b, mt)) * slot_elems + off;
+#pragma unroll
+            for (int k = 0; k < RP; k++) num[k] += src[(size_t)k * stride_k];
+        }
+        return;
+    }
     for (int seg = 0; seg < sk.nseg; seg++) {
         const int t = mt * sk.nseg + seg;
         int lo, hi;
@@ -1404,7 +1439,8 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // One warp per row: lane l adds the partials of segments l, l + 32, ...
-// (each over its CTAs in order), a fixed xor butterfly adds the lanes, and
+// (each over its CTAs in order; with folded partials, of CTAs l, l + 32, ...
+// of the row tile), a fixed xor butterfly adds the lanes, and
 // lane 0 applies the W update -- a long row (many column segments) is
 // gathered 32 segments at a time.  Deterministic.
 template <int RP>
@@ -1419,7 +1455,18 @@ __global__ void __launch_bounds__(kThreads)
     double num[RP];
 #pragma unroll
     for (int k = 0; k < RP; k++) num[k] = 0.0;
-    if (sk.G > 0) {
+    if (sk.G > 0 && sk.fold) {
+        // Folded partials: lane l adds CTAs lo + l, lo + l + 32, ...
+        const size_t slot_elems = (size_t)trows * RP;
+        int lo, hi;
+        sk_range_major(sk, rt, &lo, &hi);
+        for (int b = lo + lane; b <= hi; b += 32) {
+            const double *src = part + ((size_t)b * sk.slots + fold_slot(sk, b, rt)) * slot_elems +
+                                (size_t)rl * RP;
+#pragma unroll
+            for (int k = 0; k < RP; k++) num[k] += src[k];
+        }
+    } else if (sk.G > 0) {
         const size_t slot_elems = (size_t)trows * RP;
         for (int seg = lane; seg < sk.nseg; seg += 32) {
             const int t = rt * sk.nseg + seg;

@@ -25,9 +25,10 @@
 // (one thread), warps 2..5 move finished accumulators from tensor memory to
 // the stream-K partial buffer.  Work is split stream-K exactly like the
 // CUDA-core passes (stream.cuh): a unit is 64 streamed elements of one tile,
-// a segment of at most 32 units bounds every f32 sum to 2048 terms, and each
-// CTA writes one f64 partial per (tile, segment) it touches, in the layout
-// the CUDA-core epilogues read (H: [RP][128], W: [128][RP]).  Two
+// a segment of at most 32 units bounds every f32 sum to 2048 terms, the
+// epilogue warps add a CTA's segments of one tile in f64, and each CTA
+// writes one f64 partial per tile it touches (folded stream-K partials), in
+// the layout the CUDA-core epilogues read (H: [RP][128], W: [128][RP]).  Two
 // accumulators let the MMAs of the next segment run while the previous one
 // is drained.  Every wait is bounded; a CTA that gives up records a timeout
 // in RunState, waits (bounded) for its own loads and MMAs, frees its tensor
@@ -322,9 +323,15 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
         UnitCursor cur;
         cur.init(sk, u0);
         long long u = u0;
-        const long long tile0 = u0 / sk.UPT;
+        const int major0 = cur.major;
+        // The segments of one major tile are added here in f64, in segment
+        // order, and written once per (CTA, major tile) when the next unit
+        // starts another major tile or the CTA's range ends.
+        double sum[RPN];
+#pragma unroll
+        for (int i = 0; i < RPN; i++) sum[i] = 0.0;
         while (u < u1) {
-            const int t = cur.t;
+            const int t = cur.t, m = cur.major;
             bool any = false;
             for (; u < u1 && cur.t == t; ++u, cur.next(sk))
                 if ((long long)cur.along(sk) * kKC < kext) any = true;
@@ -355,14 +362,20 @@ __global__ void __launch_bounds__(kThreadsTC, 1)
             }
             tc_fence_before();
             mbar_arrive(&bars.acce[acc]);
-            double *dst = part + ((size_t)b * sk.slots + (size_t)(t - tile0)) * (size_t)kM * RP;
 #pragma unroll
-            for (int k = 0; k < RPN; k++) {
-                if (k < RP) {
-                    if (OUT_KM)
-                        dst[(size_t)k * kM + row] = (double)v[k];
-                    else
-                        dst[(size_t)row * RP + k] = (double)v[k];
+            for (int k = 0; k < RPN; k++) sum[k] += (double)v[k];
+            if (u >= u1 || cur.major != m) {
+                double *dst =
+                    part + ((size_t)b * sk.slots + (size_t)(m - major0)) * (size_t)kM * RP;
+#pragma unroll
+                for (int k = 0; k < RPN; k++) {
+                    if (k < RP) {
+                        if (OUT_KM)
+                            dst[(size_t)k * kM + row] = sum[k];
+                        else
+                            dst[(size_t)row * RP + k] = sum[k];
+                    }
+                    sum[k] = 0.0;
                 }
             }
             acc ^= 1;
