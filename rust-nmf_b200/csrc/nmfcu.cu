@@ -384,15 +384,26 @@ StreamK plan_sk(int64_t majors, int64_t units, int64_t segu, int sms) {
     return sk;
 }
 
+// Every pass folds its partials: one slot per major tile a CTA meets (at
+// most ceil(units a CTA / units a major tile) + 1 of them).
+StreamK fold_sk(StreamK sk) {
+    if (sk.G <= 0) return sk;
+    sk.fold = 1;
+    const int64_t per = (sk.U + sk.G - 1) / sk.G, mu = (int64_t)sk.nseg * sk.UPT;
+    sk.slots = (int)((per + mu - 1) / mu + 1);
+    return sk;
+}
+
 StreamK plan_h(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
     const int tcols = so->h_tcols(ratio);
-    return plan_sk((p + tcols - 1) / tcols, (n + so->h_brows(ratio) - 1) / so->h_brows(ratio),
-                   so->h_segu(ratio),
-                   sms);
+    return fold_sk(plan_sk((p + tcols - 1) / tcols,
+                           (n + so->h_brows(ratio) - 1) / so->h_brows(ratio), so->h_segu(ratio),
+                           sms));
 }
 StreamK plan_w(const StreamOps *so, bool ratio, int64_t n, int64_t p, int sms) {
     const int trows = so->w_trows(ratio), bcols = so->w_bcols(ratio);
-    return plan_sk((n + trows - 1) / trows, (p + bcols - 1) / bcols, so->w_segu(ratio), sms);
+    return fold_sk(
+        plan_sk((n + trows - 1) / trows, (p + bcols - 1) / bcols, so->w_segu(ratio), sms));
 }
 
 }  // namespace
@@ -528,15 +539,6 @@ bool f32_form(const nmfcu_options *o) {
 }
 int64_t round8(int64_t x) { return std::max<int64_t>(8, (x + 7) / 8 * 8); }
 int tc_rpn(int RP) { return RP <= 16 ? 16 : 32; }
-// The tensor-core passes fold their partials: one slot per major tile a CTA
-// meets (at most ceil(units a CTA / units a major tile) + 1 of them).
-StreamK fold_sk(StreamK sk) {
-    if (sk.G <= 0) return sk;
-    sk.fold = 1;
-    const int64_t per = (sk.U + sk.G - 1) / sk.G, mu = (int64_t)sk.nseg * sk.UPT;
-    sk.slots = (int)((per + mu - 1) / mu + 1);
-    return sk;
-}
 StreamK plan_tc_h(int64_t n, int64_t p, int sms) {
     return fold_sk(
         plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms));

@@ -168,6 +168,27 @@ __device__ __forceinline__ int fold_slot(const StreamK &sk, int b, int m) {
     return m - (int)(sk.start(b) / sk.major_units());
 }
 
+// Slot of tile t among the partials of a CTA whose first tile is tile0, and
+// whether the write adds to it: with folded partials a later segment of the
+// major tile written last adds to that slot.  Flushes come in tile order;
+// `last` is the major tile of the previous flush (-1 before the first).
+__device__ __forceinline__ size_t partial_slot(const StreamK &sk, int t, int tile0, int &last,
+                                               bool &add) {
+    if (!sk.fold) {
+        add = false;
+        return (size_t)(t - tile0);
+    }
+    const int m = t / sk.nseg;
+    add = (m == last);
+    last = m;
+    return (size_t)(m - tile0 / sk.nseg);
+}
+// Write (or, folding, add) one partial value.  Only the thread that wrote
+// an element adds to it later, so no other thread's write intervenes.
+__device__ __forceinline__ void put_partial(double *d, double v, bool add) {
+    *d = add ? *d + v : v;
+}
+
 // Position of a unit in the tile order, advanced one unit at a time so that
 // the loops do no integer division (a runtime 64-bit division per unit costs
 // more than the arithmetic of a small unit).
@@ -329,6 +350,9 @@ __host__ __device__ constexpr int reg_limit() {
 
 // Rows / columns a segment may span (bounds every f32 running sum).
 constexpr int kSegSpan = 2048;
+// Units a segment may span in the f64 passes: unbounded, so that a tile is
+// one segment and its running sums stay in registers until the tile ends.
+constexpr int kSegNone = 1 << 30;
 
 // ---------------------------------------------------------------------------
 // H pass
@@ -348,7 +372,7 @@ struct HCfg {
     static constexpr int BOXC = TCOLS < 256 ? TCOLS : 256;
     static constexpr int NBOX = TCOLS / BOXC;
     static constexpr int BROWS = 8;
-    static constexpr int SEGU = kSegSpan / BROWS;  // max units per segment
+    static constexpr int SEGU = sizeof(T) == 8 ? kSegNone : kSegSpan / BROWS;  // max units per segment
     static constexpr int RPS = RankPad<T, RP>::RPS;
     static constexpr int KALIGN = align_of_offset<T>(KB);
     static constexpr int VBYTES = BROWS * TCOLS * (int)sizeof(T);
@@ -424,16 +448,19 @@ __global__ void __launch_bounds__(HCfg<T, RP, RATIO>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS + colw;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * RP * C::TCOLS + colw;
 #pragma unroll
         for (int k = 0; k < KB; k++)
 #pragma unroll
             for (int c = 0; c < CPT; c++)
-                dst[(size_t)(k0 + k) * C::TCOLS + c] = (double)acc[c][k];
+                put_partial(&dst[(size_t)(k0 + k) * C::TCOLS + c], (double)acc[c][k], add);
     };
 
     int cur_major = -1;
@@ -522,7 +549,7 @@ struct WCfg {
     static constexpr int ROWB = 32768 / TROWS < 128 ? 32768 / TROWS : 128;
     static constexpr int BCOLS = ROWB / (int)sizeof(T);   // columns per unit
     static constexpr int CHUNKS = ROWB / 16;              // 16 B chunks per row
-    static constexpr int SEGU = kSegSpan / BCOLS;         // max units per segment
+    static constexpr int SEGU = sizeof(T) == 8 ? kSegNone : kSegSpan / BCOLS;  // max units per segment
     // TMA swizzle of span ROWB: logical chunk c of row r sits at physical
     // chunk c ^ ((r * ROWB >> 7) & (CHUNKS - 1)).
     static constexpr int RPS = RankPad<T, RP>::RPS;
@@ -607,15 +634,19 @@ __global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP + k0;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * C::TROWS * RP + k0;
 #pragma unroll
         for (int q = 0; q < RT; q++)
 #pragma unroll
-            for (int k = 0; k < KB; k++) dst[(size_t)rows[q] * RP + k] = (double)acc[q][k];
+            for (int k = 0; k < KB; k++)
+                put_partial(&dst[(size_t)rows[q] * RP + k], (double)acc[q][k], add);
     };
 
     int cur_major = -1;
@@ -721,7 +752,7 @@ struct DHCfg {
     static constexpr int BOXC = 256;
     static constexpr int NBOX = TCOLS / BOXC;
     static constexpr int BROWS = 16;
-    static constexpr int SEGU = kSegSpan / BROWS;
+    static constexpr int SEGU = kSegNone;  // f64 sums: one segment a tile
     static constexpr int RPS = RankPad<double, RP>::RPS;
     static constexpr int VBYTES = BROWS * TCOLS * 8;
     static constexpr int WBYTES = BROWS * RPS * 8;
@@ -785,11 +816,14 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * RP * C::TCOLS;
 #pragma unroll
         for (int mt = 0; mt < C::MT; mt++) {
             const int k = mt * 8 + g;
@@ -797,8 +831,8 @@ __global__ void __launch_bounds__(DHCfg<RP>::kWarps * 32, 1)
 #pragma unroll
                 for (int nt = 0; nt < C::NT; nt++) {
                     double *d = dst + (size_t)k * C::TCOLS + wc0 + nt * 8 + 2 * q4;
-                    d[0] = acc[mt][nt][0];
-                    d[1] = acc[mt][nt][1];
+                    put_partial(&d[0], acc[mt][nt][0], add);
+                    put_partial(&d[1], acc[mt][nt][1], add);
                 }
             }
         }
@@ -867,7 +901,7 @@ struct DWCfg {
     static constexpr int NBOX = TROWS / BOXR;
     static constexpr int ROWB = 128;  // one 128-byte swizzle span of a row a unit
     static constexpr int BCOLS = ROWB / 8;
-    static constexpr int SEGU = kSegSpan / BCOLS;
+    static constexpr int SEGU = kSegNone;  // f64 sums: one segment a tile
     static constexpr int RPS = RankPad<double, RP>::RPS;
     static constexpr int VBYTES = TROWS * ROWB;
     static constexpr int HBYTES = BCOLS * RPS * 8;
@@ -932,11 +966,14 @@ __global__ void __launch_bounds__(DWCfg<RP>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * C::TROWS * RP;
 #pragma unroll
         for (int mw = 0; mw < C::MW; mw++) {
             const int row = rbase + mw * 8;
@@ -945,8 +982,8 @@ __global__ void __launch_bounds__(DWCfg<RP>::kWarps * 32, 1)
                 const int k = nt * 8 + 2 * q4;
                 if (k < RP) {  // RP is even: k + 1 < RP too
                     double *d = dst + (size_t)row * RP + k;
-                    d[0] = acc[mw][nt][0];
-                    d[1] = acc[mw][nt][1];
+                    put_partial(&d[0], acc[mw][nt][0], add);
+                    put_partial(&d[1], acc[mw][nt][1], add);
                 }
             }
         }
@@ -1029,7 +1066,7 @@ struct DHRCfg {
     static constexpr int TCOLS = kWarps * WCOLS;
     static constexpr int BOXC = TCOLS;
     static constexpr int BROWS = 16;  // two 8-row tiles a unit
-    static constexpr int SEGU = kSegSpan / BROWS;
+    static constexpr int SEGU = kSegNone;  // f64 sums: one segment a tile
     static constexpr int RPS = RankPad<double, RP>::RPS;
     static constexpr int VBYTES = BROWS * TCOLS * 8;
     static constexpr int WBYTES = BROWS * RPS * 8;
@@ -1091,11 +1128,14 @@ __global__ void __launch_bounds__(DHRCfg<RP>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * RP * C::TCOLS;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * RP * C::TCOLS;
 #pragma unroll
         for (int mt = 0; mt < C::MT; mt++) {
             const int k = mt * 8 + g;
@@ -1103,8 +1143,8 @@ __global__ void __launch_bounds__(DHRCfg<RP>::kWarps * 32, 1)
 #pragma unroll
                 for (int nt = 0; nt < C::NT; nt++) {
                     double *d = dst + (size_t)k * C::TCOLS + wc0 + nt * 8 + 2 * q4;
-                    d[0] = acc[mt][nt][0];
-                    d[1] = acc[mt][nt][1];
+                    put_partial(&d[0], acc[mt][nt][0], add);
+                    put_partial(&d[1], acc[mt][nt][1], add);
                 }
             }
         }
@@ -1205,7 +1245,7 @@ struct DWRCfg {
     static constexpr int BOXR = TROWS;
     static constexpr int ROWB = 128;
     static constexpr int BCOLS = ROWB / 8;  // two 8-column tiles a unit
-    static constexpr int SEGU = kSegSpan / BCOLS;
+    static constexpr int SEGU = kSegNone;  // f64 sums: one segment a tile
     static constexpr int RPS = RankPad<double, RP>::RPS;
     static constexpr int VBYTES = TROWS * ROWB;
     static constexpr int HBYTES = BCOLS * RPS * 8;
@@ -1267,11 +1307,14 @@ __global__ void __launch_bounds__(DWRCfg<RP>::kWarps * 32, 1)
     UnitCursor uc;
     uc.init(sk, u0);
     const int tile0 = uc.t;
+    int flast = -1;  // major tile of the last flush
     int s = 0, rnd = 0;
     bool ok = true;
 
     auto flush = [&](int t) {
-        double *dst = part + ((size_t)b * sk.slots + (t - tile0)) * C::TROWS * RP;
+        bool add;
+        const size_t slot = partial_slot(sk, t, tile0, flast, add);
+        double *dst = part + ((size_t)b * sk.slots + slot) * C::TROWS * RP;
 #pragma unroll
         for (int mw = 0; mw < C::MW; mw++) {
             const int row = rbase + mw * 8;
@@ -1280,8 +1323,8 @@ __global__ void __launch_bounds__(DWRCfg<RP>::kWarps * 32, 1)
                 const int k = nt * 8 + 2 * q4;
                 if (k < RP) {
                     double *d = dst + (size_t)row * RP + k;
-                    d[0] = acc[mw][nt][0];
-                    d[1] = acc[mw][nt][1];
+                    put_partial(&d[0], acc[mw][nt][0], add);
+                    put_partial(&d[1], acc[mw][nt][1], add);
                 }
             }
         }
