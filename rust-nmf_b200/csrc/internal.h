@@ -40,10 +40,11 @@ void count_launches(nmfcu_context *c, int64_t launches);
 size_t context_bytes(nmfcu_context *c);
 // Bytes the context would add to run an n x p rank-r problem (f32: f32 main
 // passes, including the f32 copy of an f64 V; tc: the split-bf16 tensor-core
-// passes and their V / factor planes; method: the method's own buffers);
+// passes and their V / factor planes; method: the method's own buffers;
+// tcr: brunet's split-bf16 tensor-core passes and their factor planes);
 // 0 when its buffers suffice.
 size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32, bool tc,
-                      int method);
+                      int method, bool tcr = false);
 // Bytes scratch slot `slot` would add to hold `bytes`.
 size_t slot_growth(nmfcu_context *c, int slot, size_t bytes);
 // Frees every device buffer of the context (it regrows on the next run).

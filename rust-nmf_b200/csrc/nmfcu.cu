@@ -284,10 +284,11 @@ bool tma_layout_ok(const void *base, int64_t ld, size_t es) {
     return (reinterpret_cast<uintptr_t>(base) % 16 == 0) && ((ld * (int64_t)es) % 16 == 0);
 }
 
-// bf16 matrix (rows x cols, leading dimension ld elements) with a
-// 128-byte-swizzled box of box_cols x box_rows (box_cols * 2 <= 128).
+// bf16 matrix (rows x cols, leading dimension ld elements) with a swizzled
+// box of box_cols x box_rows (box_cols * 2 <= the swizzle span).
 nmfcu_status encode_2d_bf16(CUtensorMap *map, const void *base, int64_t rows, int64_t cols,
-                            int64_t ld, int box_cols, int box_rows) {
+                            int64_t ld, int box_cols, int box_rows,
+                            CUtensorMapSwizzle swizzle = CU_TENSOR_MAP_SWIZZLE_128B) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc) return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
@@ -295,7 +296,7 @@ nmfcu_status encode_2d_bf16(CUtensorMap *map, const void *base, int64_t rows, in
     cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims,
-                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swizzle,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS)
         return fail(NMFCU_ERR_CUDA, "cuTensorMapEncodeTiled (bf16) failed (code " +
@@ -373,6 +374,7 @@ StreamK plan_sk(int64_t majors, int64_t units, int64_t segu, int sms) {
     sk.nseg = (int)std::max<int64_t>(1, (units + segu - 1) / segu);
     sk.UPT = (int)std::max<int64_t>(1, (units + sk.nseg - 1) / sk.nseg);
     sk.U = (units > 0) ? majors * sk.nseg * (int64_t)sk.UPT : 0;
+    sk.valid = (int)std::max<int64_t>(units, 0);
     sk.G = (int)std::min<int64_t>(sms, sk.U);
     if (sk.G <= 0) {
         sk.G = 0;
@@ -421,6 +423,7 @@ struct nmfcu_context {
     DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
     DevBuf Wf32, Ht64, Ht32;
     DevBuf Vs, Fs;     // split-bf16 form: V hi/lo, the factor's three terms
+    DevBuf Xs;         // split-bf16 brunet: W and H as [3][xpad][32] bf16 terms
     DevBuf Wns, Hns;   // nsNMF: W S (n x RP), S H (RP x p)
     DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
     DevBuf Wprev, Hprev;     // ehals: the iterate before the last extrapolation
@@ -524,6 +527,13 @@ struct PassSet {
     int rpn = 0;
     int64_t ldw = 0, ldh = 0;  // leading dimensions of the W / H term planes
     CUtensorMap tmVhH, tmVlH, tmVhW, tmVlW, tmFw[3], tmFh[3];  // H: V^T planes; W: V planes
+    // brunet in the split-bf16 form (tensor-core ratio passes over the f32
+    // V): V maps of the H and W passes, the factors' [3][xpad][32] term
+    // planes as tile (box 128 rows) and chunk (box 64 rows) operands, and
+    // their [3][32][ld] planes (in Fs, one factor at a time).
+    bool tcr = false;
+    int64_t xpadW = 0, xpadH = 0;
+    CUtensorMap tmVrH, tmVrW, tmXwT, tmXwF, tmXhT, tmXhF, tmKw, tmKh;
 };
 
 // The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
@@ -537,8 +547,15 @@ bool tc_form(const nmfcu_options *o) {
 bool f32_form(const nmfcu_options *o) {
     return o->precision == NMFCU_PREC_FP32 || (o->precision == NMFCU_PREC_BF16X3 && !tc_form(o));
 }
+// brunet in the split-bf16 form runs its ratio passes on the tensor cores
+// (tcr.cuh) over the f32 V; its element type is still f32 (f32_form).
+bool tcr_form(const nmfcu_options *o) {
+    return o->precision == NMFCU_PREC_BF16X3 && o->method == NMFCU_BRUNET;
+}
 int64_t round8(int64_t x) { return std::max<int64_t>(8, (x + 7) / 8 * 8); }
+int64_t round128(int64_t x) { return std::max<int64_t>(128, (x + 127) / 128 * 128); }
 int tc_rpn(int RP) { return RP <= 16 ? 16 : 32; }
+constexpr int kTcrRank = 32;  // the tensor-core ratio passes pad the rank to 32
 StreamK plan_tc_h(int64_t n, int64_t p, int sms) {
     return fold_sk(
         plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms));
@@ -637,6 +654,33 @@ nmfcu_status make_tc_passset(nmfcu_context *c, const Plan &pl, const double *V64
     return NMFCU_OK;
 }
 
+// brunet's split-bf16 passes (tensor cores) over the f32 V (leading
+// dimension ld32): added to the f32 pass set `ps` made for that V.
+nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, int64_t ld32,
+                            PassSet *ps) {
+    ps->tcr = true;
+    ps->Ht = nullptr;  // no H^T copy: the W pass streams the split terms of H
+    ps->xpadW = round128(pl.n);
+    ps->xpadH = round128(pl.p);
+    ps->ldw = round8(pl.n);
+    ps->ldh = round8(pl.p);
+    if (pl.n <= 0 || pl.p <= 0) return NMFCU_OK;
+    if (pl.r > kTcrRank) return fail(NMFCU_ERR_UNSUPPORTED, "rank above 32");
+    NMF_TRY(encode_2d(&ps->tmVrH, V32, true, pl.n, pl.p, ld32, 128, 64));
+    NMF_TRY(encode_2d(&ps->tmVrW, V32, true, pl.n, pl.p, ld32, 32, 128,
+                      CU_TENSOR_MAP_SWIZZLE_128B));
+    unsigned char *xw = c->Xs.as<unsigned char>();
+    unsigned char *xh = xw + (size_t)3 * ps->xpadW * kTcrRank * 2;
+    const CUtensorMapSwizzle sw64 = CU_TENSOR_MAP_SWIZZLE_64B;
+    NMF_TRY(encode_2d_bf16(&ps->tmXwT, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 128, sw64));
+    NMF_TRY(encode_2d_bf16(&ps->tmXwF, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
+    NMF_TRY(encode_2d_bf16(&ps->tmXhT, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 128, sw64));
+    NMF_TRY(encode_2d_bf16(&ps->tmXhF, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
+    NMF_TRY(encode_2d_bf16(&ps->tmKw, c->Fs.ptr, 3 * kTcrRank, pl.n, ps->ldw, kTcUnit, kTcrRank));
+    NMF_TRY(encode_2d_bf16(&ps->tmKh, c->Fs.ptr, 3 * kTcrRank, pl.p, ps->ldh, kTcUnit, kTcrRank));
+    return NMFCU_OK;
+}
+
 // ===========================================================================
 // The iteration loop
 // ===========================================================================
@@ -728,6 +772,29 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                     bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
+    if (ps.tcr) {
+        // brunet, split-bf16 form: W's terms in both layouts (the chunk
+        // operand of both MMAs), H's x-row terms (the tile operand of WH);
+        // tensor-core ratio pass; update.
+        const StreamK sk = plan_tc_h(pl.n, pl.p, c->sms);
+        unsigned char *xw = c->Xs.as<unsigned char>();
+        unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
+        {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, c->Fs.ptr, kTcrRank, ps.ldw, xw,
+                             ps.xpadW, st, c->sms, s);
+            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, nullptr, kTcrRank, 0, xh, ps.xpadH, st,
+                             c->sms, s);
+        }
+        if (sk.G > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
+            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, ps.tmXhT, ps.tmXwF, ps.tmKw, (int)ps.xpadH,
+                                     (int)ps.xpadW, pl.n, pl.RP, sk, c->part.as<double>(), st, s));
+        }
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        ps.so->h_epi(a.H, nullptr, pl.p, c->part.as<double>(), sk, kTcTile, e, st, s);
+        return NMFCU_OK;
+    }
     if (ps.tc) {
         // W (n x RP f64) -> three bf16 terms of W^T; tensor-core pass; update.
         const StreamK sk = plan_tc_h(pl.n, pl.p, c->sms);
@@ -772,6 +839,29 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
                     bool ratio, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
+    if (ps.tcr) {
+        // brunet, split-bf16 form: H's terms in both layouts (the chunk
+        // operand), W's x-row terms (the tile operand); tensor-core ratio
+        // pass; update.
+        const StreamK sk = plan_tc_w(pl.n, pl.p, c->sms);
+        unsigned char *xw = c->Xs.as<unsigned char>();
+        unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
+        {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, c->Fs.ptr, kTcrRank, ps.ldh, xh,
+                             ps.xpadH, st, c->sms, s);
+            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, nullptr, kTcrRank, 0, xw, ps.xpadW, st,
+                             c->sms, s);
+        }
+        if (sk.G > 0) {
+            nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
+            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, ps.tmXwT, ps.tmXhF, ps.tmKh, (int)ps.xpadW,
+                                     (int)ps.xpadH, pl.p, pl.RP, sk, c->part.as<double>(), st, s));
+        }
+        nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+        ps.so->w_epi(a.Wout ? a.Wout : a.W, pl.n, c->part.as<double>(), sk, kTcTile, e, st, s);
+        return NMFCU_OK;
+    }
     if (ps.tc) {
         // H (RP x p f64) -> three bf16 terms; tensor-core pass; update.
         const StreamK sk = plan_tc_w(pl.n, pl.p, c->sms);
@@ -976,7 +1066,7 @@ struct WsNeed {
 };
 
 std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_f32,
-                                    bool need_tc, int method) {
+                                    bool need_tc, int method, bool need_tcr = false) {
     std::vector<WsNeed> v;
     const size_t RP = pl.RP;
     v.push_back({&c->W, sizeof(double) * (size_t)pl.n * RP});
@@ -987,14 +1077,18 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         part = std::max(part, pass_partial_bytes(stream_ops_f64(pl.RP), pl, rt, c->sms));
         if (need_f32) part = std::max(part, pass_partial_bytes(stream_ops_f32(pl.RP), pl, rt, c->sms));
     }
-    if (need_tc) part = std::max(part, tc_partial_bytes(pl, c->sms));
+    if (need_tc || need_tcr) part = std::max(part, tc_partial_bytes(pl, c->sms));
     v.push_back({&c->part, part});
-    if (need_tc) {
-        const size_t rpn = (size_t)tc_rpn(pl.RP);
-        v.push_back({&c->Vs, 2 * 2 * ((size_t)pl.n * (size_t)round8(pl.p) +
-                                      (size_t)pl.p * (size_t)round8(pl.n))});
+    if (need_tc || need_tcr) {
+        const size_t rpn = need_tcr ? (size_t)kTcrRank : (size_t)tc_rpn(pl.RP);
         v.push_back({&c->Fs, 3 * 2 * rpn * (size_t)std::max(round8(pl.n), round8(pl.p))});
     }
+    if (need_tc)
+        v.push_back({&c->Vs, 2 * 2 * ((size_t)pl.n * (size_t)round8(pl.p) +
+                                      (size_t)pl.p * (size_t)round8(pl.n))});
+    if (need_tcr)
+        v.push_back({&c->Xs, 3 * 2 * (size_t)kTcrRank *
+                                 (size_t)(round128(pl.n) + round128(pl.p))});
     v.push_back({&c->Ht64, sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()});
     if (need_f32) {
         const size_t rps = stream_ops_f32(pl.RP)->rps();
@@ -1041,8 +1135,8 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
 }
 
 nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32,
-                              bool need_tc = false, int method = -1) {
-    for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc, method))
+                              bool need_tc = false, int method = -1, bool need_tcr = false) {
+    for (const WsNeed &w : workspace_needs(c, pl, need_f32 || need_tc, need_tc, method, need_tcr))
         NMF_TRY(w.buf->ensure(w.bytes));
     if (!c->h_state) CUDA_TRY(cudaMallocHost((void **)&c->h_state, sizeof(RunState)));
     if (!c->h_count) CUDA_TRY(cudaMallocHost((void **)&c->h_count, sizeof(int)));
@@ -1538,7 +1632,7 @@ size_t context_bytes(nmfcu_context *c) {
     size_t t = 0;
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,
                             &c->sw, &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state,
-                            &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
+                            &c->Wf32, &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Xs, &c->Wns, &c->Hns,
                             &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
                             &c->S64, &c->NH, &c->NW,
                             &c->fcK, &c->fcD, &c->fcP, &c->fcF, &c->fcC})
@@ -1554,10 +1648,10 @@ static size_t grow_by(const DevBuf &b, size_t want) {
 }
 
 size_t context_growth(nmfcu_context *c, int64_t n, int64_t p, int64_t r, bool f32, bool tc,
-                      int method) {
+                      int method, bool tcr) {
     const Plan pl = make_plan(n, p, r, c->sms);
     size_t g = 0;
-    for (const WsNeed &w : workspace_needs(c, pl, f32 || tc, tc, method))
+    for (const WsNeed &w : workspace_needs(c, pl, f32 || tc, tc, method, tcr))
         g += grow_by(*w.buf, w.bytes);
     if (f32 && !tc) g += grow_by(c->V32, sizeof(float) * (size_t)n * std::max<int64_t>(32, round_up(p, 32)));
     return g;
@@ -1572,7 +1666,7 @@ void context_release(nmfcu_context *c) {
     DeviceGuard dg(c->device);
     for (DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw, &c->sw,
                       &c->Gh, &c->sh, &c->Gw2, &c->sw2, &c->obj, &c->dev, &c->state, &c->Wf32,
-                      &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Wns, &c->Hns,
+                      &c->Ht64, &c->Ht32, &c->Vs, &c->Fs, &c->Xs, &c->Wns, &c->Hns,
                             &c->off, &c->rsv, &c->addon, &c->Wprev, &c->Hprev,
                             &c->S64, &c->NH, &c->NW,
                             &c->fcK, &c->fcD, &c->fcP, &c->fcF, &c->fcC})
@@ -1730,7 +1824,7 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
     cudaStream_t s = c->own_stream;
     const Plan pl = make_plan(n, p, r, c->sms);
     const bool f32 = f32_form(opt), tc = tc_form(opt);
-    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method, tcr_form(opt)));
     if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(opt->max_iter + 1)));
     int64_t ldv = 0, ld32 = 0;
     NMF_TRY(upload_v(c, V, n, p, &ldv, s));
@@ -1749,6 +1843,7 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
         NMF_TRY(make_passset(c, pl, true, ratio, c->V32.ptr, ld32, &a.main));
     else
         a.main = a.p64;
+    if (tcr_form(opt)) NMF_TRY(add_tcr_passes(c, pl, c->V32.ptr, ld32, &a.main));
     a.V64 = c->V64.as<double>();
     a.ldv64 = ldv;
     a.W = c->W.as<double>();
@@ -1929,7 +2024,7 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     DeviceGuard dg(c->device);
     cudaStream_t s = (cudaStream_t)stream;
     const Plan pl = make_plan(n, p, r, c->sms);
-    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, opt->method, tcr_form(opt)));
     // The streaming passes read V through TMA, which needs a 16-byte aligned
     // base and row pitch; a V that is not laid out so is copied into the
     // context's pitched buffer first.
@@ -1972,6 +2067,7 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
         NMF_TRY(make_passset(c, pl, true, ratio, Vmain, ldmain, &a.main));
     else
         a.main = a.p64;
+    if (tcr_form(opt)) NMF_TRY(add_tcr_passes(c, pl, Vmain, ldmain, &a.main));
     if (f32 && !V64) {
         // No f64 V: no refinement iterations and no objective (checked above).
         a.p64 = a.main;
@@ -2027,7 +2123,7 @@ nmfcu_status nmfcu_shard_create(nmfcu_context *c, const nmfcu_options *opt, int6
     const Plan pl = make_plan(n, p_local, r, c->sms);
     const bool f32 = f32_form(o), tc = tc_form(o);
     const bool stat = o->stop == NMFCU_STOP_STATIONARY;
-    NMF_TRY(ensure_workspace(c, pl, f32, tc, o->method));
+    NMF_TRY(ensure_workspace(c, pl, f32, tc, o->method, tcr_form(o)));
     if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(o->max_iter + 1)));
     NMF_TRY(put_factors(c, pl, dW0, dH0, cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
@@ -2044,6 +2140,7 @@ nmfcu_status nmfcu_shard_create(nmfcu_context *c, const nmfcu_options *opt, int6
         int64_t ld32 = 0;
         NMF_TRY(make_f32(c, dV, ldv, n, p_local, &ld32, s));
         NMF_TRY(make_passset(c, pl, true, ratio, c->V32.ptr, ld32, &a.main));
+        if (tcr_form(o)) NMF_TRY(add_tcr_passes(c, pl, c->V32.ptr, ld32, &a.main));
     } else {
         a.main = a.p64;
     }

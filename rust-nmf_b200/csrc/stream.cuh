@@ -124,6 +124,10 @@ struct StreamK {
     // pass adds a CTA's segments of a major tile in f64 before writing it,
     // and `slots` counts major tiles.
     int fold;
+    // Units of a major tile that carry data: a prefix of its nseg * UPT (the
+    // rest pad its last segment).  A CTA that meets a major tile only in
+    // its padding may write no partial for it.
+    int valid;
     __host__ __device__ __forceinline__ long long start(int b) const {
         return (long long)b * U / G;
     }
@@ -157,10 +161,11 @@ __device__ __forceinline__ void sk_range(const StreamK &sk, int t, int *lo, int 
     sk_range_units(sk, a, min(a + sk.UPT, sk.U), lo, hi);
 }
 
-// CTAs [lo, hi] whose unit range meets major tile m (folded partials).
+// CTAs [lo, hi] whose unit range meets the units of major tile m that carry
+// data (folded partials).
 __device__ __forceinline__ void sk_range_major(const StreamK &sk, int m, int *lo, int *hi) {
     const long long a = (long long)m * sk.major_units();
-    sk_range_units(sk, a, min(a + sk.major_units(), sk.U), lo, hi);
+    sk_range_units(sk, a, min(a + (long long)sk.valid, sk.U), lo, hi);
 }
 
 // Slot of major tile m in CTA b's folded partials.

@@ -37,6 +37,21 @@ def test_one_iteration_matches_oracle(oracle, n, p, r):
     assert rel_max(got.W, ref["W"]) <= 5e-4, rel_max(got.W, ref["W"])
 
 
+# brunet's split-bf16 passes (tcr.cuh): W H and the contraction on the tensor
+# cores, the ratio in f32.  Shapes with ragged tiles (128 outputs), chunks
+# (64 elements) and segments (2048 terms), ranks 1..32.
+@pytest.mark.parametrize("n,p,r", [(1000, 1500, 20), (257, 3001, 3), (2000, 700, 32),
+                                   (130, 200, 16), (64, 64, 1), (4100, 129, 7)])
+def test_brunet_one_iteration_matches_oracle(oracle, n, p, r):
+    V = synthetic.counts_matrix(n, p, max(2, r // 2), 0.3, seed=n + p)
+    W0, H0 = nmf_rs.random_init(V, r, seed=3)
+    ref = oracle.nmf_method("brunet", V, W0, H0, 1)
+    got = nmf_rs.nmf(V, r, "brunet", W0=W0, H0=H0, max_iter=1, precision="bf16x3",
+                     refine_iters=0)
+    assert rel_max(got.H, ref["H"]) <= 5e-4, rel_max(got.H, ref["H"])
+    assert rel_max(got.W, ref["W"]) <= 5e-4, rel_max(got.W, ref["W"])
+
+
 @pytest.mark.parametrize("method", ["lee", "hals", "ehals", "dnmf", "brunet"])
 def test_split_bf16_form(oracle, method):
     V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
