@@ -489,11 +489,15 @@ def run_ours(args, world, rank, local):
         achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
         kname = "hpass" if dom == _native.KCLASS_HSTEP else "wpass"
         traffic = None
-        if (args.workload in ("atlas", "atlas-slice") and r == 20 and
+        tcr = args.precision == "bf16x3" and args.method == "brunet"
+        if (args.workload in ("atlas", "atlas-slice") and r == 20 and not tcr and
                 (kname, args.precision) in PASS_DRAM_BYTES_PER_ELEMENT):
             traffic = PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] * n * p  # per launch
         hw = "H step" if dom == _native.KCLASS_HSTEP else "W step"
-        if args.precision == "bf16x3" and args.method != "brunet":
+        if tcr:
+            kernel = ("tcr_pass<H>" if dom == _native.KCLASS_HSTEP else "tcr_pass<W>") + (
+                " (KL ratio pass on the tensor cores, f32 V)")
+        elif args.precision == "bf16x3":
             kernel = "tc_pass<H>" if dom == _native.KCLASS_HSTEP else "tc_pass<W>"
         elif args.precision == "fp64":
             kernel = ("h" if dom == _native.KCLASS_HSTEP else "w") + "pass_dmma" + (

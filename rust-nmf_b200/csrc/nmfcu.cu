@@ -528,12 +528,11 @@ struct PassSet {
     int64_t ldw = 0, ldh = 0;  // leading dimensions of the W / H term planes
     CUtensorMap tmVhH, tmVlH, tmVhW, tmVlW, tmFw[3], tmFh[3];  // H: V^T planes; W: V planes
     // brunet in the split-bf16 form (tensor-core ratio passes over the f32
-    // V): V maps of the H and W passes, the factors' [3][xpad][32] term
-    // planes as tile (box 128 rows) and chunk (box 64 rows) operands, and
-    // their [3][32][ld] planes (in Fs, one factor at a time).
+    // V): V maps of the H and W passes, and the factors' [3][xpad][32] term
+    // planes as tile (box 128 rows) and chunk (box 64 rows) operands.
     bool tcr = false;
     int64_t xpadW = 0, xpadH = 0;
-    CUtensorMap tmVrH, tmVrW, tmXwT, tmXwF, tmXhT, tmXhF, tmKw, tmKh;
+    CUtensorMap tmVrH, tmVrW, tmXwT, tmXwF, tmXhT, tmXhF;
 };
 
 // The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
@@ -676,8 +675,6 @@ nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, i
     NMF_TRY(encode_2d_bf16(&ps->tmXwF, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
     NMF_TRY(encode_2d_bf16(&ps->tmXhT, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 128, sw64));
     NMF_TRY(encode_2d_bf16(&ps->tmXhF, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
-    NMF_TRY(encode_2d_bf16(&ps->tmKw, c->Fs.ptr, 3 * kTcrRank, pl.n, ps->ldw, kTcUnit, kTcrRank));
-    NMF_TRY(encode_2d_bf16(&ps->tmKh, c->Fs.ptr, 3 * kTcrRank, pl.p, ps->ldh, kTcUnit, kTcrRank));
     return NMFCU_OK;
 }
 
@@ -773,22 +770,22 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     if (ps.tcr) {
-        // brunet, split-bf16 form: W's terms in both layouts (the chunk
-        // operand of both MMAs), H's x-row terms (the tile operand of WH);
-        // tensor-core ratio pass; update.
+        // brunet, split-bf16 form: the bf16 terms of W (the chunk operand of
+        // both MMAs) and of H (the tile operand of W H); tensor-core ratio
+        // pass; update.
         const StreamK sk = plan_tc_h(pl.n, pl.p, c->sms);
         unsigned char *xw = c->Xs.as<unsigned char>();
         unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
         {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, c->Fs.ptr, kTcrRank, ps.ldw, xw,
-                             ps.xpadW, st, c->sms, s);
+            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, nullptr, kTcrRank, 0, xw, ps.xpadW, st,
+                             c->sms, s);
             tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, nullptr, kTcrRank, 0, xh, ps.xpadH, st,
                              c->sms, s);
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
-            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, ps.tmXhT, ps.tmXwF, ps.tmKw, (int)ps.xpadH,
+            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, ps.tmXhT, ps.tmXwF, (int)ps.xpadH,
                                      (int)ps.xpadW, pl.n, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -840,22 +837,21 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     if (ps.tcr) {
-        // brunet, split-bf16 form: H's terms in both layouts (the chunk
-        // operand), W's x-row terms (the tile operand); tensor-core ratio
-        // pass; update.
+        // brunet, split-bf16 form: the bf16 terms of H (the chunk operand)
+        // and of W (the tile operand); tensor-core ratio pass; update.
         const StreamK sk = plan_tc_w(pl.n, pl.p, c->sms);
         unsigned char *xw = c->Xs.as<unsigned char>();
         unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
         {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, c->Fs.ptr, kTcrRank, ps.ldh, xh,
-                             ps.xpadH, st, c->sms, s);
+            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, nullptr, kTcrRank, 0, xh, ps.xpadH, st,
+                             c->sms, s);
             tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, nullptr, kTcrRank, 0, xw, ps.xpadW, st,
                              c->sms, s);
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
-            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, ps.tmXwT, ps.tmXhF, ps.tmKh, (int)ps.xpadW,
+            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, ps.tmXwT, ps.tmXhF, (int)ps.xpadW,
                                      (int)ps.xpadH, pl.p, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -1079,10 +1075,9 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
     }
     if (need_tc || need_tcr) part = std::max(part, tc_partial_bytes(pl, c->sms));
     v.push_back({&c->part, part});
-    if (need_tc || need_tcr) {
-        const size_t rpn = need_tcr ? (size_t)kTcrRank : (size_t)tc_rpn(pl.RP);
-        v.push_back({&c->Fs, 3 * 2 * rpn * (size_t)std::max(round8(pl.n), round8(pl.p))});
-    }
+    if (need_tc)
+        v.push_back({&c->Fs, 3 * 2 * (size_t)tc_rpn(pl.RP) *
+                                 (size_t)std::max(round8(pl.n), round8(pl.p))});
     if (need_tc)
         v.push_back({&c->Vs, 2 * 2 * ((size_t)pl.n * (size_t)round8(pl.p) +
                                       (size_t)pl.p * (size_t)round8(pl.n))});

@@ -44,8 +44,8 @@ __global__ void split_factor_both(const double *__restrict__ F, int64_t fk, int6
 
 template <bool HPASS>
 cudaError_t launch_one(const CUtensorMap &v, const CUtensorMap &t, const CUtensorMap &f1,
-                       const CUtensorMap &f2, int xpadT, int xpadF, int kext, int RP,
-                       const StreamK &sk, double *part, RunState *st, cudaStream_t s) {
+                       int xpadT, int xpadF, int kext, int RP, const StreamK &sk, double *part,
+                       RunState *st, cudaStream_t s) {
     static bool configured = false;  // per instantiation; the attribute is per device function
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(tcr_pass<HPASS>,
@@ -53,20 +53,18 @@ cudaError_t launch_one(const CUtensorMap &v, const CUtensorMap &t, const CUtenso
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, t, f1, f2, xpadT, xpadF, kext, RP, sk, part,
-                                                 st);
+    tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st);
     return cudaGetLastError();
 }
 
 }  // namespace tcr
 
 cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const CUtensorMap &t,
-                            const CUtensorMap &f1, const CUtensorMap &f2, int xpadT, int xpadF,
-                            int kext, int RP, const StreamK &sk, double *part, RunState *st,
-                            cudaStream_t s) {
+                            const CUtensorMap &f1, int xpadT, int xpadF, int kext, int RP,
+                            const StreamK &sk, double *part, RunState *st, cudaStream_t s) {
     if (sk.G <= 0) return cudaSuccess;
-    return hpass ? tcr::launch_one<true>(v, t, f1, f2, xpadT, xpadF, kext, RP, sk, part, st, s)
-                 : tcr::launch_one<false>(v, t, f1, f2, xpadT, xpadF, kext, RP, sk, part, st, s);
+    return hpass ? tcr::launch_one<true>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st, s)
+                 : tcr::launch_one<false>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st, s);
 }
 
 void tcr_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *kx, int RPN,
