@@ -142,10 +142,26 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
         : "r"(taddr));
 }
 
+// Bounded wait that lets the thread sleep: each try suspends it until the
+// phase completes or 1 us has passed, so waiting warps leave their issue
+// slots to the working ones; at most 2^21 tries (about 2 s).
+__device__ __forceinline__ bool mbar_sleep_wait(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < (1u << 21); ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+            " selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(ok)
+            : "r"(smem_u32(bar)), "r"(parity), "r"(1000u)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
 // Bounded wait taken by a whole warp, with one outcome for all its lanes (the
 // epilogue warps arrive once a warp, after a __syncwarp).
 __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
-    return __all_sync(0xffffffffu, mbar_wait(bar, parity)) != 0;
+    return __all_sync(0xffffffffu, mbar_sleep_wait(bar, parity)) != 0;
 }
 
 // Walks the valid chunks of a CTA's stream-K range in order (units past the
@@ -265,7 +281,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         while (w.ok && !*abort_flag) {
             const int major = w.cur.major, along = w.cur.along(sk);
             const int s = (int)(ci % kVStages);
-            if (!mbar_wait(&bars.vempty[s], (uint32_t)(((ci / kVStages) & 1) ^ 1))) {
+            if (!mbar_sleep_wait(&bars.vempty[s], (uint32_t)(((ci / kVStages) & 1) ^ 1))) {
                 give_up();
                 break;
             }
@@ -285,7 +301,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (*abort_flag) {
             // Let this thread's own loads land before the CTA exits.
             for (int i = 0; i < kVStages; i++)
-                if (issued[i] > 0) mbar_wait(&bars.vfull[i], (uint32_t)((issued[i] - 1) & 1));
+                if (issued[i] > 0) mbar_sleep_wait(&bars.vfull[i], (uint32_t)((issued[i] - 1) & 1));
         }
     } else if (warp == kFProdWarp && lane == 0) {
         // ---- TMA producer of the factor terms (L2-resident) ------------------
@@ -300,7 +316,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (major != cur_major) {
                 // The tile operand is reloaded once the last MMA1 of the
                 // previous tile has read it.
-                if (tloads > 0 && !mbar_wait(&bars.tempty, (uint32_t)((tloads - 1) & 1))) {
+                if (tloads > 0 && !mbar_sleep_wait(&bars.tempty, (uint32_t)((tloads - 1) & 1))) {
                     give_up();
                     break;
                 }
@@ -312,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 cur_major = major;
             }
             const int s = (int)(ci % kFStages);
-            if (!mbar_wait(&bars.fempty[s], (uint32_t)(((ci / kFStages) & 1) ^ 1))) {
+            if (!mbar_sleep_wait(&bars.fempty[s], (uint32_t)(((ci / kFStages) & 1) ^ 1))) {
                 give_up();
                 break;
             }
@@ -327,8 +343,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         if (*abort_flag) {
             for (int i = 0; i < kFStages; i++)
-                if (issued[i] > 0) mbar_wait(&bars.ffull[i], (uint32_t)((issued[i] - 1) & 1));
-            if (tloads > 0) mbar_wait(&bars.tfull, (uint32_t)((tloads - 1) & 1));
+                if (issued[i] > 0) mbar_sleep_wait(&bars.ffull[i], (uint32_t)((issued[i] - 1) & 1));
+            if (tloads > 0) mbar_sleep_wait(&bars.tfull, (uint32_t)((tloads - 1) & 1));
         }
     } else if ((warp == kMma1Warp || warp == kMma2Warp) && lane == 0) {
         // ---- MMA issuers ------------------------------------------------------
@@ -354,12 +370,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t fB = sbase + OFF_F + s * F_SLOT;
             if (first) {
                 // MMA1 of chunk ci into WH accumulator ci & 1.
-                if (!mbar_wait(&bars.ffull[s], (uint32_t)((ci / kFStages) & 1))) {
+                if (!mbar_sleep_wait(&bars.ffull[s], (uint32_t)((ci / kFStages) & 1))) {
                     ok = false;
                     break;
                 }
                 if (c.major != prev_major) {
-                    if (!mbar_wait(&bars.tfull, (uint32_t)(tcount & 1))) {
+                    if (!mbar_sleep_wait(&bars.tfull, (uint32_t)(tcount & 1))) {
                         ok = false;
                         break;
                     }
@@ -367,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     prev_major = c.major;
                 }
                 const int db = (int)(ci & 1);
-                if (!mbar_wait(&bars.d1empty[db], (uint32_t)(((ci >> 1) & 1) ^ 1))) {
+                if (!mbar_sleep_wait(&bars.d1empty[db], (uint32_t)(((ci >> 1) & 1) ^ 1))) {
                     ok = false;
                     break;
                 }
@@ -389,11 +405,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 // factor slot landed before MMA1 of this chunk, which the
                 // ratio step waited for.
                 if (c.first_seg && segs > 0 &&
-                    !mbar_wait(&bars.d2empty, (uint32_t)((segs - 1) & 1))) {
+                    !mbar_sleep_wait(&bars.d2empty, (uint32_t)((segs - 1) & 1))) {
                     ok = false;
                     break;
                 }
-                if (!mbar_wait(&bars.qfull, (uint32_t)(ci & 1))) {
+                if (!mbar_sleep_wait(&bars.qfull, (uint32_t)(ci & 1))) {
                     ok = false;
                     break;
                 }
@@ -420,7 +436,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (*abort_flag) {
             uint64_t *dr = first ? &bars.drain[0] : &bars.drain[1];
             tc::umma_commit(dr);
-            mbar_wait(dr, 0);
+            mbar_sleep_wait(dr, 0);
         }
     } else if (warp >= kEpiWarp0) {
         // ---- epilogue: WH -> Q, and the contraction -> f64 partials --------
