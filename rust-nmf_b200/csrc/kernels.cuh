@@ -630,6 +630,37 @@ __device__ __forceinline__ void w_update(const EpiParams &e, const double *num, 
     }
 }
 
+// Whether w_update's new W[i][j] depends on row i's old values and num only
+// through column j's own formula (every method but the sequential HALS /
+// dnmf sweeps), so that its columns can be computed by different threads.
+__device__ __forceinline__ bool w_update_by_column(int method) {
+    return method == M_LEE || method == M_OFFSET || method == M_BRUNET ||
+           method == M_NSNMF || method == M_LSNMF || method == M_PRODUCT;
+}
+// Column j (< e.r) of w_update for those methods, with the same operations
+// in the same order (so the same bits).  numj = num[j], wrj = wr[j].
+template <int RP>
+__device__ __forceinline__ double w_update_column(const EpiParams &e, double numj, double wrj,
+                                                  const double (&wr)[RP], int j,
+                                                  double ro = 0.0,
+                                                  const double *ax = nullptr) {
+    if (e.method == M_LSNMF) {
+        const double temp = mul(wrj, ax[j]);
+        return (temp > e.eps ? temp : e.eps) / add(numj, e.eps);
+    }
+    if (e.method == M_PRODUCT) return numj;
+    if (e.method == M_LEE || e.method == M_OFFSET) {
+        double den = 0.0;
+#pragma unroll
+        for (int l = RP - 1; l >= 0; l--)
+            if (l < e.r) den = add(den, mul(wr[l], e.G[l * RP + j]));
+        if (e.method == M_OFFSET) den = add(den, mul(ro, e.sums[j]));
+        const double temp = mul(wrj, numj);
+        return (temp < e.eps ? e.eps : temp) / add(den, e.eps);
+    }
+    return mul(wrj, numj) / e.sums[j];  // M_BRUNET, M_NSNMF
+}
+
 // H epilogue: one thread per column; sums the S split partials in order.
 template <int RP>
 __global__ void __launch_bounds__(kThreads)

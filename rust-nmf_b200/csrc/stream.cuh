@@ -1532,14 +1532,34 @@ __global__ void __launch_bounds__(kThreads)
     for (int k = 0; k < RP; k++)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) num[k] += __shfl_xor_sync(0xffffffffu, num[k], o);
-    if (lane != 0) return;
-    double wr[RP], ax[RP];
+    // Every lane now holds the row's sums.  Methods whose columns update
+    // independently take one lane a column; the HALS / dnmf sweeps, which
+    // run over the columns in order, lane 0.
+    double wr[RP];
 #pragma unroll
-    for (int k = 0; k < RP; k++) {
-        wr[k] = W[(size_t)i * RP + k];
-        ax[k] = e.aux != nullptr ? e.aux[(size_t)i * RP + k] : 0.0;
+    for (int k = 0; k < RP; k++) wr[k] = W[(size_t)i * RP + k];
+    const double ro = e.roff ? e.roff[i] : 0.0;
+    if (w_update_by_column(e.method)) {
+        if (lane >= e.r || lane >= RP) return;
+        double numj = 0.0, wrj = 0.0;
+#pragma unroll
+        for (int k = 0; k < RP; k++)
+            if (k == lane) {
+                numj = num[k];
+                wrj = wr[k];
+            }
+        const double *ax = e.aux != nullptr ? e.aux + (size_t)i * RP : nullptr;
+        const double out = w_update_column<RP>(e, numj, wrj, wr, lane, ro, ax);
+        // All lanes have read the row before any writes it.
+        __syncwarp(__activemask());
+        W[(size_t)i * RP + lane] = out;
+        return;
     }
-    w_update<RP>(e, num, wr, e.roff ? e.roff[i] : 0.0, ax);
+    if (lane != 0) return;
+    double ax[RP];
+#pragma unroll
+    for (int k = 0; k < RP; k++) ax[k] = e.aux != nullptr ? e.aux[(size_t)i * RP + k] : 0.0;
+    w_update<RP>(e, num, wr, ro, ax);
 #pragma unroll
     for (int k = 0; k < RP; k++)
         if (k < e.r) W[(size_t)i * RP + k] = wr[k];
