@@ -69,10 +69,10 @@ enum { NMFCU_STOP_MAX_ITER = 0, NMFCU_STOP_STATIONARY = 1 };
  *   BF16X3 -- lee / offset / hals / ehals / dnmf: V stored as two bf16 terms (hi + lo, 4 bytes
  *             an element), the factor of each contraction split into three
  *             bf16 terms, products on the tensor cores with f32 sums of at
- *             most 2048 terms; everything else as FP32.  brunet: W H and the
- *             contraction on the tensor cores (three bf16 terms per factor),
- *             the ratio V / (W H) in f32 over the f32 V, written as bf16
- *             hi + lo.  nsNMF runs as FP32.  Needs the f64 V. */
+ *             most 2048 terms; everything else as FP32.  brunet / nsNMF:
+ *             W H and the contraction on the tensor cores (three bf16 terms
+ *             per factor), the ratio V / (W H) in f32 over the f32 V, written
+ *             as bf16 hi + lo.  Needs the f64 V. */
 enum { NMFCU_PREC_FP64 = 0, NMFCU_PREC_FP32 = 1, NMFCU_PREC_BF16X3 = 2 };
 
 /* Keyword arguments of py_nmf_run (lib.rs:1912-1933), plus engine knobs. */

@@ -546,10 +546,12 @@ bool tc_form(const nmfcu_options *o) {
 bool f32_form(const nmfcu_options *o) {
     return o->precision == NMFCU_PREC_FP32 || (o->precision == NMFCU_PREC_BF16X3 && !tc_form(o));
 }
-// brunet in the split-bf16 form runs its ratio passes on the tensor cores
-// (tcr.cuh) over the f32 V; its element type is still f32 (f32_form).
+// brunet and nsNMF in the split-bf16 form run their ratio passes on the
+// tensor cores (tcr.cuh) over the f32 V; their element type is still f32
+// (f32_form).
 bool tcr_form(const nmfcu_options *o) {
-    return o->precision == NMFCU_PREC_BF16X3 && o->method == NMFCU_BRUNET;
+    return o->precision == NMFCU_PREC_BF16X3 &&
+           (o->method == NMFCU_BRUNET || o->method == NMFCU_NSNMF);
 }
 int64_t round8(int64_t x) { return std::max<int64_t>(8, (x + 7) / 8 * 8); }
 int64_t round128(int64_t x) { return std::max<int64_t>(128, (x + 127) / 128 * 128); }
@@ -971,9 +973,11 @@ nmfcu_status enqueue_iteration(nmfcu_context *c, const RunArgs &a, long long it,
                 nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
                 a.ops->ns_left(a.H, pl.p, pl.r, o->theta, a.Hns, st, s);
             }
-            transpose_h(c, ah, ps, s);      // the W pass streams (S H)^T
+            // The W pass streams (S H)^T (the tensor-core passes split S H
+            // themselves).
+            if (!ps.tcr) transpose_h(c, ah, ps, s);
             gram_h_full(c, ah, Gh, sh, s);  // rowsum(S H)
-            NMF_TRY(w_step(c, a, ps, epi(o, pl.r, Gh, sh, false), true, s));
+            NMF_TRY(w_step(c, ah, ps, epi(o, pl.r, Gh, sh, false), true, s));
             {
                 nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
                 a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(),

@@ -82,7 +82,8 @@ size_t growth_on(nmfcu_context *c, const Request &q) {
     const bool tc = q.opt.precision == NMFCU_PREC_BF16X3 && q.opt.method != NMFCU_BRUNET &&
                     q.opt.method != NMFCU_NSNMF;
     const bool f32 = q.opt.precision == NMFCU_PREC_FP32 || (q.opt.precision == NMFCU_PREC_BF16X3 && !tc);
-    const bool tcr = q.opt.precision == NMFCU_PREC_BF16X3 && q.opt.method == NMFCU_BRUNET;
+    const bool tcr = q.opt.precision == NMFCU_PREC_BF16X3 &&
+                     (q.opt.method == NMFCU_BRUNET || q.opt.method == NMFCU_NSNMF);
     return nmfcu_internal::context_growth(c, q.n, q.p, q.r, f32, tc, q.opt.method, tcr) +
            nmfcu_internal::slot_growth(c, kSlotV, v_bytes(q)) +
            nmfcu_internal::slot_growth(c, kSlotW, sizeof(double) * (size_t)(q.n * q.r)) +

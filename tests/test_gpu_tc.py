@@ -52,6 +52,18 @@ def test_brunet_one_iteration_matches_oracle(oracle, n, p, r):
     assert rel_max(got.W, ref["W"]) <= 5e-4, rel_max(got.W, ref["W"])
 
 
+# nsNMF's split-bf16 form runs the same passes on W S (H pass) and S H (W pass).
+@pytest.mark.parametrize("n,p,r", [(700, 900, 8), (257, 1301, 3)])
+def test_nsnmf_one_iteration_matches_oracle(oracle, n, p, r):
+    V = synthetic.counts_matrix(n, p, max(2, r // 2), 0.3, seed=n + p) + 0.01
+    W0, H0 = nmf_rs.random_init(V, r, seed=3)
+    ref = oracle.nmf_method("nsNMF", V, W0, H0, 1)
+    got = nmf_rs.nmf(V, r, "nsNMF", W0=W0, H0=H0, max_iter=1, precision="bf16x3",
+                     refine_iters=0)
+    assert rel_max(got.H, ref["H"]) <= 5e-4, rel_max(got.H, ref["H"])
+    assert rel_max(got.W, ref["W"]) <= 5e-4, rel_max(got.W, ref["W"])
+
+
 @pytest.mark.parametrize("method", ["lee", "hals", "ehals", "dnmf", "brunet"])
 def test_split_bf16_form(oracle, method):
     V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
