@@ -839,6 +839,9 @@ def run_consensus(args, world, rank, local):
             "one_by_one_sample": f"{seq_runs} of {runs} restarts per rank timed, scaled; plus "
                                  "the same consensus matrices and statistics",
             "max_rel_dH_batched_vs_single": dh_rel,
+            "batch_shape": {"chosen": consensus.last_batch_shape(),
+                            "candidates": consensus.batch_shape_count(),
+                            "how": "autotuned: each shape timed on the first run, fastest kept"},
             "consensus_stats_ms_per_rank": stats_ms,
             "host_scipy_stats_ms_per_rank": host_stats_ms,
             "cpu_baseline": cpu,

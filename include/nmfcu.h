@@ -324,6 +324,22 @@ nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t 
                                     int64_t ldv, int32_t nsolves, const int32_t *ranks,
                                     double *dW, double *dH, void *stream);
 
+/* Shape of the batched kernel: how many solves a CTA carries (and so how many
+ * solves each V element it loads serves) and how many CTAs a multiprocessor
+ * keeps resident.  With NMFCU_BATCH_SHAPE_AUTO (the default) the first
+ * batched run of a problem -- device, precision, n, p and the multiset of
+ * ranks -- with max_iter >= 20 times each candidate shape for a few
+ * iterations on copies of its starting factors and keeps the fastest for
+ * later runs of that problem; shorter runs take shape 0.  A shape changes
+ * which solves share a CTA, not the arithmetic of a solve: every shape gives
+ * the same results.  Process-wide. */
+#define NMFCU_BATCH_SHAPE_AUTO (-1)
+/* Selects NMFCU_BATCH_SHAPE_AUTO or forces shape 0 .. nmfcu_batch_shape_count() - 1. */
+nmfcu_status nmfcu_batch_set_shape(int32_t shape);
+int32_t nmfcu_batch_shape_count(void);
+/* The shape the last batched run used (-1 before the first). */
+int32_t nmfcu_batch_last_shape(void);
+
 /* Consensus matrix of the selected solves `sel[0..nsel)` of a stacked H
  * (layout as above): C[j1][j2] = fraction of the selected solves that put
  * columns j1 and j2 in the same cluster, the cluster of column j being

@@ -41,29 +41,49 @@ constexpr int kPrefetch = 4;       // V rows in flight per thread (H step)
 // (W step) of V, held in one "lane pack" P.  f32 packs two (float2, one
 // FFMA2 updates both), so a W value times an H pair, or an H value times a
 // W pair, is one instruction and the per-element ratio is computed for two
-// elements at once; f64 owns one (DFMA).  kComponents bounds the rank
-// components (sum of the ranks of the solves) a CTA carries.
+// elements at once; f64 owns one (DFMA).
 template <typename T>
 struct BTraits;
 template <>
 struct BTraits<float> {
     using P = float2;
     static constexpr int CPT = 2;
-    static constexpr int kComponents = 12;
 };
 template <>
 struct BTraits<double> {
     using P = double;
     static constexpr int CPT = 1;
-    static constexpr int kComponents = 8;
 };
 
-template <typename T, int R>
+// Kernel shapes the autotuner chooses from (run_batch_t): `comp` bounds the
+// rank components (sum of the ranks of the solves) a CTA carries -- so a CTA
+// takes comp / R solves of rank R and each V element it loads serves them
+// all -- and `min_blocks` is the CTAs a multiprocessor keeps resident (the
+// register cap of __launch_bounds__).  Shape 0 is the one measured best at
+// the consensus shape during development; a shape changes which solves share
+// a CTA, never the arithmetic of a solve, so every shape gives the same bits.
+template <typename T>
+struct BShapes;
+template <>
+struct BShapes<float> {
+    static constexpr int kN = 3;
+    static constexpr int comp[kN] = {12, 8, 16};
+    static constexpr int min_blocks[kN] = {4, 5, 3};
+};
+template <>
+struct BShapes<double> {
+    static constexpr int kN = 3;
+    static constexpr int comp[kN] = {8, 4, 12};
+    static constexpr int min_blocks[kN] = {5, 6, 4};
+};
+constexpr int kShapesMax = 3;
+
+template <typename T, int R, int COMP>
 struct BCfg {
-    static constexpr int NS = BTraits<T>::kComponents / R > 0 ? BTraits<T>::kComponents / R : 1;
+    static constexpr int NS = COMP / R > 0 ? COMP / R : 1;
     static constexpr int ROW = NS * R;  // staged values per W row / H column
 };
-constexpr int kMaxRow = 16;             // >= ROW for every (T, R)
+constexpr int kMaxRow = 16;             // >= ROW for every (T, R, COMP)
 template <typename T>
 constexpr int kTile = kThreads * BTraits<T>::CPT;  // columns / rows per CTA
 
@@ -132,7 +152,7 @@ template <typename T>
 struct BSmem {
     using P = typename BTraits<T>::P;
     P S[kRowChunk][kMaxRow + 2];
-    int off[BTraits<T>::kComponents];  // stacked offset per solve (-1: none)
+    int off[kMaxRow];  // stacked offset per solve (-1: none)
 };
 
 // One unit of a step: NS solves of rank R (offsets at goff[0..NS)) on one
@@ -150,15 +170,15 @@ struct BItem {
 // aligned, and A must be zero in columns [cols, round_up(cols, CPT)).
 // kComponentFast: the staged factor is contiguous along components (W in
 // the H step) -- staging loads walk components; otherwise (H^T) they walk rows.
-template <typename T, int R, bool kComponentFast>
+template <typename T, int R, int COMP, bool kComponentFast>
 __device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
                                         const int *__restrict__ goff, int tile) {
-    using C = BCfg<T, R>;
+    using C = BCfg<T, R, COMP>;
     using P = typename BTraits<T>::P;
     constexpr int CPT = BTraits<T>::CPT;
     constexpr int NS = C::NS, ROW = C::ROW;
     constexpr int SPT = (kRowChunk * ROW + kThreads - 1) / kThreads;  // staged values per thread
-    static_assert(ROW <= kMaxRow && NS <= BTraits<T>::kComponents, "staging row too long");
+    static_assert(ROW <= kMaxRow && NS <= kMaxRow, "staging row too long");
     static_assert(kRowChunk % kPrefetch == 0, "row chunk must hold whole prefetch groups");
     if (threadIdx.x < NS) sm.off[threadIdx.x] = goff[threadIdx.x];
     __syncthreads();
@@ -272,27 +292,27 @@ __device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
 // Rank buckets: ranks 1..8 and 9..16 run as separate kernels, so the
 // register budget of one bucket is not set by the other's largest rank.
 // Within a bucket one launch covers every rank class: CTA b runs item b.
-// The register caps keep four (f32) or five (f64) CTAs resident per SM
-// (measured best; occupancy outweighs the spills of ranks 9..16).
+// Ranks form two buckets with a launch each, so that a launch's register
+// cap fits its ranks.
 constexpr int kBucketSplit = 8;  // largest rank of the low bucket
-template <typename T, int B>
+template <int B>
 struct BBucket {
     static constexpr int kLo = B == 0 ? 1 : kBucketSplit + 1;
     static constexpr int kHi = B == 0 ? kBucketSplit : kMaxBatchRank;
-    static constexpr int kMinBlocks = sizeof(T) == 4 ? 4 : 5;
 };
 constexpr int bucket_of(int R) { return R <= kBucketSplit ? 0 : 1; }
 
-template <typename T, int B, bool kComponentFast>
-__global__ void __launch_bounds__(kThreads, (BBucket<T, B>::kMinBlocks))
+template <typename T, int B, int SHAPE, bool kComponentFast>
+__global__ void __launch_bounds__(kThreads, (BShapes<T>::min_blocks[SHAPE]))
     batch_mu(MuArgs<T> a, const int *__restrict__ off, const BItem *__restrict__ items) {
     __shared__ __align__(16) BSmem<T> sm;
     const BItem it = items[blockIdx.x];
+    constexpr int COMP = BShapes<T>::comp[SHAPE];
     switch (it.R) {
 #define MU_CASE(r)                                                                     \
     case r:                                                                            \
-        if constexpr (r >= BBucket<T, B>::kLo && r <= BBucket<T, B>::kHi)              \
-            mu_item<T, r, kComponentFast>(sm, a, off + it.goff, it.tile);              \
+        if constexpr (r >= BBucket<B>::kLo && r <= BBucket<B>::kHi)                    \
+            mu_item<T, r, COMP, kComponentFast>(sm, a, off + it.goff, it.tile);        \
         break;
         BATCH_RANK_CASES(MU_CASE)
 #undef MU_CASE
@@ -405,15 +425,8 @@ __global__ void batch_consensus(const unsigned char *__restrict__ lab, int p, in
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-template <typename T>
-int ns_for(int R) {
-    switch (R) {
-#define NS_CASE(r) case r: return BCfg<T, r>::NS;
-        BATCH_RANK_CASES(NS_CASE)
-#undef NS_CASE
-    }
-    return 1;
-}
+// Solves of rank R a CTA of shape `comp` carries (BCfg::NS).
+int ns_for(int R, int comp) { return comp / R > 0 ? comp / R : 1; }
 
 struct BatchPlan {
     int rtot = 0;
@@ -425,7 +438,7 @@ struct BatchPlan {
 // Solves of one rank form a class; a class is cut into groups of NS solves;
 // every (group, tile) pair is one CTA of its bucket's launch.
 template <typename T>
-BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
+BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks, int comp) {
     BatchPlan bp;
     std::vector<int> offsets(nsolves);
     std::map<int, std::vector<int>> by_rank;
@@ -441,7 +454,7 @@ BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks) {
             const int R = it->first;
             if (bucket_of(R) != b) continue;
             const auto &members = it->second;
-            const int ns = ns_for<T>(R);
+            const int ns = ns_for(R, comp);
             const int groups = (int)((members.size() + ns - 1) / ns);
             for (int g = 0; g < groups; g++) {
                 const int at = (int)bp.group_off.size();
@@ -469,19 +482,25 @@ struct BatchSteps {
     MuArgs<T> h, w;  // the H step streams V, the W step streams V^T
 };
 
-// Enqueue iterations [it0, it1] of the batched brunet loop.
-template <typename T>
-void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, const BatchDev &d,
-                         const BatchSteps<T> &st, int n, int p, T *W, T *H, T *sw, T *sh,
-                         cudaStream_t s, int64_t *launches) {
+// Enqueue iterations [it0, it1] of the batched brunet loop with shape SHAPE.
+template <typename T, int SHAPE>
+void enqueue_batch_iters_s(long long it0, long long it1, const BatchPlan &bp, const BatchDev &d,
+                           const BatchSteps<T> &st, int n, int p, T *W, T *H, T *sw, T *sh,
+                           cudaStream_t s, int64_t *launches) {
     const int rtot = bp.rtot;
     for (long long it = it0; it <= it1; it++) {
         batch_colsum<T><<<(rtot + 127) / 128, 128, 0, s>>>(W, n, rtot, rtot, sw);
-        if (bp.nh[0]) batch_mu<T, 0, true><<<bp.nh[0], kThreads, 0, s>>>(st.h, d.off, d.hitems);
-        if (bp.nh[1]) batch_mu<T, 1, true><<<bp.nh[1], kThreads, 0, s>>>(st.h, d.off, d.hitems + bp.nh[0]);
+        if (bp.nh[0])
+            batch_mu<T, 0, SHAPE, true><<<bp.nh[0], kThreads, 0, s>>>(st.h, d.off, d.hitems);
+        if (bp.nh[1])
+            batch_mu<T, 1, SHAPE, true><<<bp.nh[1], kThreads, 0, s>>>(st.h, d.off,
+                                                                     d.hitems + bp.nh[0]);
         batch_rowsum<T><<<(rtot + 7) / 8, 256, 0, s>>>(H, p, rtot, sh);
-        if (bp.nw[0]) batch_mu<T, 0, false><<<bp.nw[0], kThreads, 0, s>>>(st.w, d.off, d.witems);
-        if (bp.nw[1]) batch_mu<T, 1, false><<<bp.nw[1], kThreads, 0, s>>>(st.w, d.off, d.witems + bp.nw[0]);
+        if (bp.nw[0])
+            batch_mu<T, 0, SHAPE, false><<<bp.nw[0], kThreads, 0, s>>>(st.w, d.off, d.witems);
+        if (bp.nw[1])
+            batch_mu<T, 1, SHAPE, false><<<bp.nw[1], kThreads, 0, s>>>(st.w, d.off,
+                                                                      d.witems + bp.nw[0]);
         *launches += 2 + (bp.nh[0] > 0) + (bp.nh[1] > 0) + (bp.nw[0] > 0) + (bp.nw[1] > 0);
         if (it % 10 == 0) {
             batch_clamp<T><<<592, 256, 0, s>>>(W, (int64_t)n * rtot, H, (int64_t)rtot * p,
@@ -491,14 +510,44 @@ void enqueue_batch_iters(long long it0, long long it1, const BatchPlan &bp, cons
     }
 }
 
-// V (n x p, leading dimension ldv; for f32 zero in columns [p, ldv) with
-// ldv a multiple of 4) is streamed by the H step; the W step streams V^T,
-// built here once per call in context slot 12 (zero-padded the same way).
 template <typename T>
-nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const T *V,
-                         int64_t ldv, int nsolves, const int32_t *ranks, T *W, T *H,
-                         cudaStream_t s) {
-    const BatchPlan bp = plan_batch<T>(n, p, nsolves, ranks);
+void enqueue_batch_iters(int shape, long long it0, long long it1, const BatchPlan &bp,
+                         const BatchDev &d, const BatchSteps<T> &st, int n, int p, T *W, T *H,
+                         T *sw, T *sh, cudaStream_t s, int64_t *launches) {
+    static_assert(BShapes<T>::kN == 3, "one case per shape");
+    switch (shape) {
+        case 1:
+            enqueue_batch_iters_s<T, 1>(it0, it1, bp, d, st, n, p, W, H, sw, sh, s, launches);
+            break;
+        case 2:
+            enqueue_batch_iters_s<T, 2>(it0, it1, bp, d, st, n, p, W, H, sw, sh, s, launches);
+            break;
+        default:
+            enqueue_batch_iters_s<T, 0>(it0, it1, bp, d, st, n, p, W, H, sw, sh, s, launches);
+    }
+}
+
+// The autotuner's state, process-wide: the shape chosen per problem
+// signature, a forced shape (nmfcu_batch_set_shape) and the last one used.
+std::mutex g_shape_mu;
+std::map<std::string, int> g_shape_cache;
+int g_forced_shape = NMFCU_BATCH_SHAPE_AUTO;
+int g_last_shape = -1;
+constexpr long long kTuneMinIters = 20;  // shorter runs take shape 0 untimed
+constexpr int kTuneIters = 3;            // timed iterations per candidate shape
+
+std::string shape_key(int device, size_t es, int n, int p, int nsolves, const int32_t *ranks) {
+    int hist[kMaxBatchRank + 1] = {0};
+    for (int s = 0; s < nsolves; s++) hist[ranks[s]]++;
+    std::string k = std::to_string(device) + "/" + std::to_string(es) + "/" + std::to_string(n) +
+                    "x" + std::to_string(p);
+    for (int r = 1; r <= kMaxBatchRank; r++) k += "," + std::to_string(hist[r]);
+    return k;
+}
+
+// Uploads a plan's group offsets and items (context slot 0) and points `d`
+// at them.
+nmfcu_status upload_plan(nmfcu_context *c, const BatchPlan &bp, cudaStream_t s, BatchDev *d) {
     // One upload: group offsets, then H items, then W items (16-byte aligned).
     const size_t off_bytes = (sizeof(int) * bp.group_off.size() + 15) / 16 * 16;
     const size_t item_bytes = sizeof(BItem) * (bp.hitems.size() + bp.witems.size());
@@ -507,28 +556,123 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
     std::memcpy(table.data() + off_bytes, bp.hitems.data(), sizeof(BItem) * bp.hitems.size());
     std::memcpy(table.data() + off_bytes + sizeof(BItem) * bp.hitems.size(), bp.witems.data(),
                 sizeof(BItem) * bp.witems.size());
-    void *p_tab = nullptr, *p_sw = nullptr, *p_sh = nullptr, *p_vt = nullptr;
+    void *p_tab = nullptr;
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 0, table.size(), &p_tab));
-    NMFCU_TRY(nmfcu_internal::context_buffer(c, 1, sizeof(T) * (size_t)bp.rtot, &p_sw));
-    NMFCU_TRY(nmfcu_internal::context_buffer(c, 2, sizeof(T) * (size_t)bp.rtot, &p_sh));
+    // A pageable host source is staged before cudaMemcpyAsync returns, so the
+    // table may go out of scope; the kernels read it in stream order.
+    NMFCU_CUDA_TRY(cudaMemcpyAsync(p_tab, table.data(), table.size(), cudaMemcpyHostToDevice, s));
+    d->off = static_cast<const int *>(p_tab);
+    d->hitems = reinterpret_cast<const BItem *>(static_cast<unsigned char *>(p_tab) + off_bytes);
+    d->witems = d->hitems + bp.hitems.size();
+    return NMFCU_OK;
+}
+
+// The shape for this problem: the forced one, the cached choice, or the
+// fastest of the candidates timed over kTuneIters iterations (after one
+// untimed) on copies of the starting factors (context slots 16, 17), so
+// that the caller's run itself is unchanged.  Blocks until the timing ends.
+template <typename T>
+nmfcu_status pick_shape(nmfcu_context *c, int64_t max_iter, int n, int p, const T *V,
+                        int64_t ldv, const T *Vt, int64_t ldvt, int nsolves,
+                        const int32_t *ranks, const T *W, const T *H, T *sw, T *sh,
+                        cudaStream_t s, int64_t *launches, int *shape) {
+    const std::string key = shape_key(nmfcu_internal::context_device(c), sizeof(T), n, p,
+                                      nsolves, ranks);
+    {
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        if (g_forced_shape >= 0) {
+            *shape = g_forced_shape;
+            return NMFCU_OK;
+        }
+        auto it = g_shape_cache.find(key);
+        if (it != g_shape_cache.end()) {
+            *shape = it->second;
+            return NMFCU_OK;
+        }
+    }
+    *shape = 0;
+    if (max_iter < kTuneMinIters) return NMFCU_OK;
+    int64_t rtot = 0;
+    for (int i = 0; i < nsolves; i++) rtot += ranks[i];
+    void *p_w = nullptr, *p_h = nullptr;
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 16, sizeof(T) * (size_t)n * rtot, &p_w));
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 17, sizeof(T) * (size_t)rtot * p, &p_h));
+    T *W2 = static_cast<T *>(p_w), *H2 = static_cast<T *>(p_h);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    NMFCU_CUDA_TRY(cudaEventCreate(&e0));
+    cudaError_t ce = cudaEventCreate(&e1);
+    float best = 0.f;
+    for (int v = 0; ce == cudaSuccess && v < BShapes<T>::kN; v++) {
+        const BatchPlan bp = plan_batch<T>(n, p, nsolves, ranks, BShapes<T>::comp[v]);
+        BatchDev d;
+        const nmfcu_status ps = upload_plan(c, bp, s, &d);
+        if (ps != NMFCU_OK) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return ps;
+        }
+        ce = cudaMemcpyAsync(W2, W, sizeof(T) * (size_t)n * rtot, cudaMemcpyDeviceToDevice, s);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(H2, H, sizeof(T) * (size_t)rtot * p, cudaMemcpyDeviceToDevice, s);
+        if (ce != cudaSuccess) break;
+        BatchSteps<T> st;
+        st.h = MuArgs<T>{V, ldv, n, p, W2, (int64_t)bp.rtot, 1, H2, (int64_t)p, 1, sw};
+        st.w = MuArgs<T>{Vt, ldvt, p, n, H2, 1, (int64_t)p, W2, 1, (int64_t)bp.rtot, sh};
+        enqueue_batch_iters<T>(v, 1, 1, bp, d, st, n, p, W2, H2, sw, sh, s, launches);
+        ce = cudaEventRecord(e0, s);
+        if (ce != cudaSuccess) break;
+        enqueue_batch_iters<T>(v, 2, 1 + kTuneIters, bp, d, st, n, p, W2, H2, sw, sh, s,
+                               launches);
+        ce = cudaEventRecord(e1, s);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        float ms = 0.f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce == cudaSuccess && (v == 0 || ms < best)) {
+            best = ms;
+            *shape = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (ce != cudaSuccess) return nmfcu_internal::cuda_fail(ce, "batched shape timing");
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    g_shape_cache[key] = *shape;
+    return NMFCU_OK;
+}
+
+// V (n x p, leading dimension ldv; for f32 zero in columns [p, ldv) with
+// ldv a multiple of 4) is streamed by the H step; the W step streams V^T,
+// built here once per call in context slot 12 (zero-padded the same way).
+template <typename T>
+nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const T *V,
+                         int64_t ldv, int nsolves, const int32_t *ranks, T *W, T *H,
+                         cudaStream_t s) {
+    int64_t rtot = 0;
+    for (int i = 0; i < nsolves; i++) rtot += ranks[i];
+    void *p_sw = nullptr, *p_sh = nullptr, *p_vt = nullptr;
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 1, sizeof(T) * (size_t)rtot, &p_sw));
+    NMFCU_TRY(nmfcu_internal::context_buffer(c, 2, sizeof(T) * (size_t)rtot, &p_sh));
     const int64_t ldvt = sizeof(T) == 4 ? ((int64_t)n + 3) / 4 * 4 : (int64_t)n;
     NMFCU_TRY(nmfcu_internal::context_buffer(c, 12, sizeof(T) * (size_t)p * ldvt, &p_vt));
     T *sw = static_cast<T *>(p_sw), *sh = static_cast<T *>(p_sh), *Vt = static_cast<T *>(p_vt);
-    // A pageable host source is staged before cudaMemcpyAsync returns, so the
-    // table may go out of scope; the kernels below read it in stream order.
-    NMFCU_CUDA_TRY(cudaMemcpyAsync(p_tab, table.data(), table.size(), cudaMemcpyHostToDevice, s));
     {
         const dim3 tg((unsigned)((p + 31) / 32), (unsigned)((ldvt + 31) / 32));
         transpose_2d<T, T><<<tg, 256, 0, s>>>(V, ldv, Vt, ldvt, n, p);
     }
+    int64_t launches = 1;
+    int shape = 0;
+    NMFCU_TRY(pick_shape<T>(c, max_iter, n, p, V, ldv, Vt, ldvt, nsolves, ranks, W, H, sw, sh, s,
+                            &launches, &shape));
+    {
+        std::lock_guard<std::mutex> lk(g_shape_mu);
+        g_last_shape = shape;
+    }
+    const BatchPlan bp = plan_batch<T>(n, p, nsolves, ranks, BShapes<T>::comp[shape]);
     BatchDev d;
-    d.off = static_cast<const int *>(p_tab);
-    d.hitems = reinterpret_cast<const BItem *>(static_cast<unsigned char *>(p_tab) + off_bytes);
-    d.witems = d.hitems + bp.hitems.size();
+    NMFCU_TRY(upload_plan(c, bp, s, &d));
     BatchSteps<T> st;
     st.h = MuArgs<T>{V, ldv, n, p, W, (int64_t)bp.rtot, 1, H, (int64_t)p, 1, sw};
     st.w = MuArgs<T>{Vt, ldvt, p, n, H, 1, (int64_t)p, W, 1, (int64_t)bp.rtot, sh};
-    int64_t launches = 1;
     // The loop in blocks of 10 iterations (the clamp period), captured once
     // as a CUDA graph and replayed; the remainder is launched directly.
     const long long blocks = max_iter / 10;
@@ -544,7 +688,8 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (e == cudaSuccess) e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             int64_t cap_launches = 0;
-            enqueue_batch_iters<T>(1, 10, bp, d, st, n, p, W, H, sw, sh, cs, &cap_launches);
+            enqueue_batch_iters<T>(shape, 1, 10, bp, d, st, n, p, W, H, sw, sh, cs,
+                                   &cap_launches);
             e = cudaStreamEndCapture(cs, &graph);
             if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
             for (long long b = 0; e == cudaSuccess && b < blocks; b++) {
@@ -561,7 +706,8 @@ nmfcu_status run_batch_t(nmfcu_context *c, int64_t max_iter, int n, int p, const
         if (ready) cudaEventDestroy(ready);
         if (e != cudaSuccess) return nmfcu_internal::cuda_fail(e, "batched iteration graph");
     }
-    enqueue_batch_iters<T>(blocks * 10 + 1, max_iter, bp, d, st, n, p, W, H, sw, sh, s, &launches);
+    enqueue_batch_iters<T>(shape, blocks * 10 + 1, max_iter, bp, d, st, n, p, W, H, sw, sh, s,
+                           &launches);
     NMFCU_CUDA_TRY(cudaGetLastError());
     nmfcu_internal::count_launches(c, launches);
     return NMFCU_OK;
@@ -593,6 +739,21 @@ nmfcu_status validate_batch(int32_t method, int32_t precision, int64_t max_iter,
 }  // namespace
 
 extern "C" {
+
+nmfcu_status nmfcu_batch_set_shape(int32_t shape) {
+    if (shape != NMFCU_BATCH_SHAPE_AUTO && (shape < 0 || shape >= kShapesMax))
+        return fail(NMFCU_ERR_INVALID_ARG, "shape must be NMFCU_BATCH_SHAPE_AUTO or 0..count-1");
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    g_forced_shape = shape;
+    return NMFCU_OK;
+}
+
+int32_t nmfcu_batch_shape_count(void) { return kShapesMax; }
+
+int32_t nmfcu_batch_last_shape(void) {
+    std::lock_guard<std::mutex> lk(g_shape_mu);
+    return g_last_shape;
+}
 
 nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t precision,
                                     int64_t max_iter, int64_t n, int64_t p, const double *dV,

@@ -25,8 +25,8 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
 nmfcu_status default_context(int device, nmfcu_context **out);
 
 // A scratch buffer of the context that grows to at least `bytes` (slot
-// 0..15, one owner per slot; the contents survive between calls).
-constexpr int kContextSlots = 16;
+// 0..17, one owner per slot; the contents survive between calls).
+constexpr int kContextSlots = 18;
 nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out);
 
 cudaStream_t context_stream(nmfcu_context *c);

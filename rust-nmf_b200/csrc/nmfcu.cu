@@ -430,7 +430,7 @@ struct nmfcu_context {
     DevBuf S64, NH, NW;      // lsNMF: weights (pitched like V), the numerator contractions
                              // (snmf: the FCNNLS right-hand sides)
     DevBuf fcK, fcD, fcP, fcF, fcC;  // snmf: FCNNLS solutions, steps, sets, flags, ctc + counter
-    DevBuf extra[16];  // scratch slots of the other translation units
+    DevBuf extra[nmfcu_internal::kContextSlots];  // scratch slots of the other translation units
     RunState *h_state = nullptr;  // pinned
     int *h_count = nullptr;       // pinned: the FCNNLS set sizes
 

@@ -126,6 +126,9 @@ SIGNATURES = {
     "nmfcu_run_batch_device": (_i32, [ctypes.c_void_p, _i32, _i32, _i64, _i64, _i64,
                                       ctypes.c_void_p, _i64, _i32, ctypes.POINTER(_i32),
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "nmfcu_batch_set_shape": (_i32, [_i32]),
+    "nmfcu_batch_shape_count": (_i32, []),
+    "nmfcu_batch_last_shape": (_i32, []),
     "nmfcu_consensus_device": (_i32, [ctypes.c_void_p, _i64, _i32, ctypes.POINTER(_i32),
                                       ctypes.c_void_p, _i32, ctypes.POINTER(_i32),
                                       ctypes.c_void_p, ctypes.c_void_p]),

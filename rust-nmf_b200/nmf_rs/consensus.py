@@ -136,6 +136,27 @@ def _ranks_ptr(ranks: np.ndarray):
     return ranks.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
 
 
+def set_batch_shape(shape="auto") -> None:
+    """Shape of the batched kernel (solves a CTA carries, CTAs resident per
+    multiprocessor): ``"auto"`` -- the default -- times the candidate shapes on
+    the first batched run of each problem (device, precision, n, p, ranks;
+    runs of 20 or more iterations) and keeps the fastest; an int in
+    ``range(batch_shape_count())`` forces one.  Every shape gives the same
+    results.  Process-wide."""
+    lib = _native.load()
+    code = -1 if shape == "auto" else int(shape)
+    _native.check(lib.nmfcu_batch_set_shape(code))
+
+
+def batch_shape_count() -> int:
+    return int(_native.load().nmfcu_batch_shape_count())
+
+
+def last_batch_shape() -> int:
+    """The shape the last batched run used (-1 before the first)."""
+    return int(_native.load().nmfcu_batch_last_shape())
+
+
 def run_batch(V: np.ndarray, starts, max_iter: int, *, method: str = "brunet",
               precision: str = "fp64", device: int = 0):
     """Run every (W0, H0) in ``starts`` on V as one batch and return a list

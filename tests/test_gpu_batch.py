@@ -182,3 +182,29 @@ def test_consensus_stats_pitched_input():
     a = consensus.consensus_stats(buf[:, :200])
     b = consensus.consensus_stats(torch.from_numpy(C).cuda())
     assert a == b
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_batch_shapes_agree_and_autotune(precision):
+    # The kernel shapes the autotuner picks from regroup solves per CTA; a
+    # solve's arithmetic is the same in every shape, so the results agree bit
+    # for bit, and the tuned run (which times the shapes on copies of the
+    # starting factors) leaves the caller's result unchanged too.
+    V = _counts(260, 530, 3)
+    ranks = [2, 3, 3, 5, 9, 12, 1, 16]
+    starts = _starts(V, ranks, 8)
+    got = []
+    try:
+        for shape in range(consensus.batch_shape_count()):
+            consensus.set_batch_shape(shape)
+            got.append(consensus.run_batch(V, starts, 24, precision=precision))
+            assert consensus.last_batch_shape() == shape
+        consensus.set_batch_shape("auto")
+        tuned = consensus.run_batch(V, starts, 24, precision=precision)
+        assert 0 <= consensus.last_batch_shape() < consensus.batch_shape_count()
+    finally:
+        consensus.set_batch_shape("auto")
+    for other in got[1:] + [tuned]:
+        for (W, H), (W2, H2) in zip(got[0], other):
+            np.testing.assert_array_equal(W, W2)
+            np.testing.assert_array_equal(H, H2)

@@ -248,3 +248,17 @@ def test_cophenetic_is_the_coefficient_not_the_notebook_constant():
     expected = cophenet(linkage(cond, method="average"), cond)[0]
     assert consensus.cophenetic_correlation(C) == pytest.approx(expected, abs=1e-15)
     assert expected < 0.99
+
+
+def test_batch_shape_setting_needs_no_gpu():
+    # Selecting the batched kernel's shape is host state: it loads and
+    # validates without a device.
+    from nmf_rs import consensus
+    n = consensus.batch_shape_count()
+    assert n >= 1
+    with pytest.raises(ValueError):
+        consensus.set_batch_shape(n)
+    with pytest.raises(ValueError):
+        consensus.set_batch_shape(-2)
+    consensus.set_batch_shape(0)
+    consensus.set_batch_shape("auto")
