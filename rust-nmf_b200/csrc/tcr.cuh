@@ -2,7 +2,8 @@
 // split-bf16 precision form.
 //
 // The KL multiplicative update contracts the element-wise ratio V / (W H)
-// with a factor (rust/src/lib.rs:1474-1519, the brunet H and W updates):
+// with a factor (rust/src/lib.rs:74-115 divergence_update_h_inner, 151-204
+// divergence_update_w_impl; the loop nmf_run_brunet, 1529-1586):
 //   H pass  N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j]
 //   W pass  N[i][k] = sum_j H[k][j] V[i][j] / (W H)[i][j]
 // Per tile of 128 outputs (columns j for the H pass, rows i for the W pass)
