@@ -8,6 +8,8 @@
 namespace nmfcu {
 namespace tc {
 
+constexpr int kAttrDevices = 64;  // devices whose launch attributes are cached
+
 // One read of V, both split copies: V hi/lo (n x ldb) and V^T hi/lo (p x ldbt),
 // through 64 x 64 tiles: 16-byte reads of V rows, 4-byte (bf16 pair) writes
 // of both copies.  Grid: x over 64-column tiles up to ldb, y over 64-row
@@ -85,12 +87,17 @@ cudaError_t launch_one(const CUtensorMap &ah, const CUtensorMap &al, const CUten
                        int kext, int RP, const StreamK &sk, double *part, RunState *st,
                        cudaStream_t s) {
     constexpr int smem = tc_smem_bytes<RPN>();
-    static bool configured = false;  // per instantiation; the attribute is per device function
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(tc_pass<RPN, A_MN, OUT_KM>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    // The attribute lives in each device's context: set it once per device
+    // and instantiation.
+    static bool configured[kAttrDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kAttrDevices || !configured[dev]) {
+        e = cudaFuncSetAttribute(tc_pass<RPN, A_MN, OUT_KM>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        if (dev >= 0 && dev < kAttrDevices) configured[dev] = true;
     }
     tc_pass<RPN, A_MN, OUT_KM><<<sk.G, kThreadsTC, smem, s>>>(ah, al, b3[0], b3[1], b3[2], kext,
                                                                RP, sk, part, st);
@@ -123,7 +130,8 @@ void tc_split_v(const double *V, int64_t ldv, void *Vh, void *Vl, int64_t ldb, v
 void tc_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *out, int RPN,
                      int64_t ldk, const RunState *st, int sms, cudaStream_t s) {
     const int64_t plane = (int64_t)RPN * ldk;
-    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((plane + 255) / 256, (int64_t)sms * 8));
+    const unsigned blocks = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>((plane + 255) / 256, (int64_t)sms * 8));
     tc::split_factor<<<blocks, 256, 0, s>>>(F, fk, fx, R, K, static_cast<__nv_bfloat16 *>(out),
                                             RPN, ldk, st);
 }

@@ -8,6 +8,8 @@
 namespace nmfcu {
 namespace tcr {
 
+constexpr int kAttrDevices = 64;  // devices whose launch attributes are cached
+
 // Three bf16 terms of f: h = bf16(f), m = bf16(f - h), l = bf16(f - h - m).
 __device__ __forceinline__ void split3(double f, __nv_bfloat16 &h, __nv_bfloat16 &m,
                                        __nv_bfloat16 &l) {
@@ -46,12 +48,17 @@ template <bool HPASS>
 cudaError_t launch_one(const CUtensorMap &v, const CUtensorMap &t, const CUtensorMap &f1,
                        int xpadT, int xpadF, int kext, int RP, const StreamK &sk, double *part,
                        RunState *st, cudaStream_t s) {
-    static bool configured = false;  // per instantiation; the attribute is per device function
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(tcr_pass<HPASS>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+    // The attribute lives in each device's context: set it once per device
+    // and instantiation.
+    static bool configured[kAttrDevices] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kAttrDevices || !configured[dev]) {
+        e = cudaFuncSetAttribute(tcr_pass<HPASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SMEM);
         if (e != cudaSuccess) return e;
-        configured = true;
+        if (dev >= 0 && dev < kAttrDevices) configured[dev] = true;
     }
     tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st);
     return cudaGetLastError();
