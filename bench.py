@@ -2,9 +2,11 @@
 """Benchmark of the NMF iteration loop on B200.
 
 A step is one NMF iteration (H update + W update) over the whole V.  The
-default is the split-bf16 precision form (V as bf16 hi + lo, products on the
-tensor cores, f64 elsewhere, 2 trailing f64 iterations); --precision fp32
-(CUDA-core f32 products) and fp64 (the plain method) measure the others.
+default is the plain method in f64 (the precision the reference computes
+in), lee on the atlas shape 20000 x 200000 rank 20; beside it, as extra keys,
+the precision forms (split-bf16 on the tensor cores, f32 on the CUDA cores)
+with their relative objective and max|dW| against the f64 run, and brunet
+(f64 and split-bf16) at the same shape.
 
   value    iterations/s with V, W, H already in HBM (nmfcu_run_device),
            K timed iterations in one call, CUDA events on the launch stream,
@@ -13,11 +15,15 @@ tensor cores, f64 elsewhere, 2 trailing f64 iterations); --precision fp32
            behind nmf_rs.nmf): host->device copy of V, W0, H0, the K
            iterations and the device->host copy of W, H, all timed.
   roofline achieved HBM GB/s of the dominant V-streaming kernel class,
-           algorithmic bytes (one read of V per launch) / summed launch time
-           from the library's CUDA-event hooks, against MEASURED_PEAKS.json.
+           algorithmic bytes (one read of V per launch) / average launch time
+           from the library's CUDA-event hooks, against MEASURED_PEAKS.json;
+           for brunet in f64 also the FP64 TFLOP/s of the ratio pass against
+           a cuBLAS f64 GEMM measured in the same run.
   cpu_baseline  the CPU restatement of the reference loop (oracle/, the
-           Rust reference cannot be built here) on a bounded column slice of
-           the same V, extrapolated linearly in the column count.
+           Rust reference cannot be built here; -march=native, OpenMP on all
+           host cores) on a column slice of the same V: the difference of a
+           3- and a 1-iteration call (so the per-run set-up is not counted as
+           iteration time), extrapolated linearly in the column count.
 
 --impl reference times that CPU restatement as the reference arm.
 
@@ -85,7 +91,7 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="atlas")
     ap.add_argument("--method", choices=["lee", "brunet", "hals", "dnmf"], default="lee")
-    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp64"], default="bf16x3")
+    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp64"], default="fp64")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
@@ -146,36 +152,9 @@ def max_over_ranks(x: float, world: int) -> float:
 # ---------------------------------------------------------------------------
 
 def device_workload(n, p, k, alpha, rank, seed, device):
-    import torch
+    from nmf_rs import synthetic
 
-    g = torch.Generator(device=device)
-    g.manual_seed(seed)
-    f64 = torch.float64
-    w_true = torch._standard_gamma(torch.full((n, k), 0.5, dtype=f64, device=device),
-                                   generator=g)
-    w_true[torch.rand((n, k), generator=g, device=device, dtype=f64) < 0.7] = 0.0
-    ld64 = (p + 15) // 16 * 16
-    ld32 = (p + 31) // 32 * 32
-    V64 = torch.zeros((n, ld64), dtype=f64, device=device)
-    chunk = 8192
-    for c0 in range(0, p, chunk):
-        c = min(chunk, p - c0)
-        h = torch._standard_gamma(torch.full((k, c), float(alpha), dtype=f64, device=device),
-                                  generator=g)
-        h = h / h.sum(0, keepdim=True).clamp_min(1e-300)
-        lib = torch.empty(c, dtype=f64, device=device).log_normal_(7.0, 0.5, generator=g)
-        lam = (w_true @ h) * lib[None, :]
-        counts = torch.poisson(lam, generator=g)
-        col = counts.sum(0, keepdim=True)
-        scale = torch.where(col > 0, 1e4 / col.clamp_min(1e-300), torch.zeros_like(col))
-        V64[:, c0:c0 + c] = torch.log1p(counts * scale)
-        del h, lam, counts
-    V32 = torch.zeros((n, ld32), dtype=torch.float32, device=device)
-    V32[:, :p] = V64[:, :p].float()
-    vmax = float(V64[:, :p].max())
-    W0 = torch.rand((n, rank), generator=g, device=device, dtype=f64) * vmax
-    H0 = torch.rand((rank, p), generator=g, device=device, dtype=f64) * vmax
-    return V64, ld64, V32, ld32, W0, H0
+    return synthetic.device_workload(n, p, k, alpha, rank, seed, device)
 
 
 def objective_torch(V64, p, W, H, method):
@@ -261,33 +240,65 @@ class Clocks:
 # CPU baseline: the oracle (CPU restatement of the reference loop)
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(V_host_fn, n, p, rank, method, seconds, seed=0):
+def _oracle_native():
+    """The oracle built -march=native on this host (same bits as the generic
+    build; see oracle/Makefile)."""
     import oracle
 
-    oracle.build()
-    threads = os.cpu_count() or 1
-    p_s = 256
-    rate = None
-    sample = None
-    for _ in range(6):
+    oracle.use_native()
+    return oracle
+
+
+def oracle_iteration_seconds(method, V, W0, H0, iters, threads):
+    """Seconds per iteration of the CPU restatement on V: one call of 1 + iters
+    iterations minus one call of 1 iteration, so the per-run set-up that the
+    reference also pays once per run (its V^T copy, lib.rs:1606, and the
+    buffers) is not counted as iteration time."""
+    oracle = _oracle_native()
+    t0 = time.perf_counter()
+    oracle.nmf_method(method, V, W0, H0, 1, num_threads=threads)
+    t1 = time.perf_counter()
+    oracle.nmf_method(method, V, W0, H0, 1 + iters, num_threads=threads)
+    t2 = time.perf_counter()
+    return max((t2 - t1) - (t1 - t0), 1e-9) / iters, (t1 - t0), (t2 - t1)
+
+
+def pick_slice(V_host_fn, p, method, seconds, threads):
+    """Column count whose single iteration takes about `seconds` / 4."""
+    oracle = _oracle_native()
+    p_s = min(p, 512)
+    while True:
         V_s, W0, H0 = V_host_fn(p_s)
         t0 = time.perf_counter()
         oracle.nmf_method(method, V_s, W0, H0, 1, num_threads=threads)
         dt = time.perf_counter() - t0
-        rate = dt / p_s  # seconds per iteration per column
-        sample = (p_s, dt)
-        if dt > seconds / 4 or p_s >= p:
+        if dt > seconds / 16 or p_s >= p:
             break
-        p_s = int(min(p, max(p_s * 2, p_s * (seconds / 2) / max(dt, 1e-3))))
-    t_full = rate * p
+        p_s = int(min(p, max(p_s * 2, p_s * (seconds / 4) / max(dt, 1e-3))))
+    target = int(min(p, max(64, p_s * (seconds / 4) / max(dt, 1e-3))))
+    return (target + 15) // 16 * 16 if target < p else p
+
+
+def cpu_baseline(V_host_fn, n, p, rank, method, seconds, seed=0):
+    """The CPU restatement of the reference loop (oracle/, -march=native,
+    OpenMP on all host cores) on a column slice of the workload: 2 timed
+    iterations beyond a 1-iteration call, extrapolated linearly in columns
+    (every part of an iteration is linear in p)."""
+    threads = os.cpu_count() or 1
+    p_s = pick_slice(V_host_fn, p, method, seconds, threads)
+    V_s, W0, H0 = V_host_fn(p_s)
+    per_iter, t_one, t_three = oracle_iteration_seconds(method, V_s, W0, H0, 2, threads)
+    t_full = per_iter * p / p_s
     return {
         "value": 1.0 / t_full,
         "unit": "iters/s",
         "cores": threads,
         "kind": "port",
-        "sample": (f"1 {method} iteration of the CPU restatement (oracle/, OpenMP) on all "
-                   f"{n} rows x {sample[0]} of {p} columns took {sample[1]:.2f} s; "
-                   f"extrapolated linearly in columns to the full V"),
+        "sample": (f"{method} on the CPU restatement (oracle/, -march=native, OpenMP, "
+                   f"{threads} threads) on all {n} rows x {p_s} of {p} columns: a 1-iteration "
+                   f"call took {t_one:.2f} s and a 3-iteration call {t_three:.2f} s; their "
+                   f"difference / 2 = {per_iter:.3f} s an iteration, extrapolated linearly "
+                   f"in columns to the full V"),
     }
 
 
@@ -333,48 +344,75 @@ def measured_peaks():
 # Reference arm
 # ---------------------------------------------------------------------------
 
+def iterate_metric(method, workload):
+    """The metric string both arms of the iterate form print."""
+    n, p, _, _, r, _ = WORKLOADS[workload]
+    return f"{method} iterations/s, {workload} {n}x{p} rank {r}"
+
+
 def run_reference(args, world, rank):
+    """The reference arm: the CPU restatement of the reference loop on the
+    host cores.  A step is one iteration over a column slice of the workload
+    (the full f64 V would need ~96 GB of host memory and minutes a step);
+    exactly `steps` slice iterations are timed after `warmup` untimed ones,
+    in one call (so the per-run V^T copy and buffers are paid once, as in
+    the reference), and `value` is full-V iterations per second, the slice
+    time scaled by p / slice columns."""
     if rank != 0:
         return
     n, p, k, alpha, r, iters = WORKLOADS[args.workload]
     steps = args.steps or iters
+    warm = max(1, args.warmup)
+    threads = os.cpu_count() or 1
     from nmf_rs import synthetic
 
-    # A bounded column slice of the workload, generated on the host.
     def V_host_fn(p_s):
         V = synthetic.counts_matrix(n, p_s, k, alpha, seed=0)
         W0, H0 = synthetic.starting_point(V, r, seed=0)
         return V, W0, H0
 
-    vals = []
-    base = None
-    for _ in range(max(1, args.warmup)):
-        base = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds / 3)
-    for _ in range(max(1, min(steps, 3))):
-        base = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds / 3)
-        vals.append(base["value"])
-    value = statistics.median(vals)
+    # Slice sized so one iteration takes about cpu_seconds / 8 (the whole
+    # arm, warm-up and calibration included, stays within a few minutes).
+    budget = args.cpu_seconds * max(1.0, 20.0 / max(steps, 1))
+    p_s = pick_slice(V_host_fn, p, args.method, budget / 2, threads)
+    V_s, W0, H0 = V_host_fn(p_s)
+    oracle = _oracle_native()
+    t0 = time.perf_counter()
+    oracle.nmf_method(args.method, V_s, W0, H0, warm, num_threads=threads)
+    t1 = time.perf_counter()
+    oracle.nmf_method(args.method, V_s, W0, H0, warm + steps, num_threads=threads)
+    t2 = time.perf_counter()
+    timed_s = max((t2 - t1) - (t1 - t0), 1e-9)
+    ms_step = 1000.0 * timed_s / steps
+    value = steps * p_s / p / timed_s
+    sample = (f"{steps} {args.method} iterations of the CPU restatement (oracle/, -march=native, "
+              f"OpenMP, {threads} threads) on all {n} rows x {p_s} of {p} columns: "
+              f"{timed_s:.2f} s beyond a {warm}-iteration call ({t1 - t0:.2f} s); "
+              f"value = iterations of the full V per second, scaled by {p}/{p_s} columns")
     line = {
         "impl": "reference",
-        "metric": f"{args.method} iterations/s, {args.workload} {n}x{p} rank {r}",
+        "metric": iterate_metric(args.method, args.workload),
         "value": value,
         "unit": "iters/s",
         "n_gpus": args.gpus,
         "steps": steps,
-        "warmup": args.warmup,
-        "ms_per_step": 1000.0 / value,
+        "warmup": warm,
+        "ms_per_step": ms_step,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded generator, column slice)",
+        "data": f"synthetic (seeded generator), {n}x{p_s} column slice of the workload",
         "config": {"workload": args.workload, "n": n, "p": p, "rank": r,
-                   "method": args.method},
-        "cpu_baseline": {**base, "value": value},
+                   "method": args.method, "precision": "fp64", "slice_columns": p_s,
+                   "step": f"one iteration over the {n}x{p_s} slice"},
+        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "port",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "note": ("the Rust reference cannot be built in this image (no cargo/rustc); "
-                 "this arm times the C restatement of its loop (oracle/) on host cores"),
+                 "this arm times the C restatement of its loop (oracle/) on host cores; "
+                 "ms_per_step is one slice iteration"),
     }
     print(json.dumps(line), flush=True)
 
@@ -383,7 +421,33 @@ def run_reference(args, world, rank):
 # Our arm
 # ---------------------------------------------------------------------------
 
+def measure_fp64_gemm_tflops(dev):
+    """FP64 throughput of cuBLAS (torch.matmul, 8192^3 f64, best of 5, CUDA
+    events): the measured FP64 denominator of the ratio passes' FLOP
+    roofline."""
+    import torch
+
+    a = torch.rand((8192, 8192), dtype=torch.float64, device=dev)
+    b = torch.rand((8192, 8192), dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * 8192 ** 3 / (best / 1000.0) / 1e12
+
+
 def run_ours(args, world, rank, local):
+    """The iterate form.  The headline is the precision the reference
+    computes in (f64, the plain method); the mixed-precision forms and, at the
+    atlas shape, brunet are measured beside it as extra keys."""
     import torch
 
     from nmf_rs import _native
@@ -394,9 +458,10 @@ def run_ours(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     V64, ld64, V32, ld32, W0, H0 = device_workload(n, p, k, alpha, r, 1234 + rank, dev)
-    if args.workload in ATLAS_WORKLOADS:
-        # The precision form starts from an NNDSVD start computed in f64 (on
-        # the device, outside the timed region); the small workloads from the
+    atlas = args.workload in ATLAS_WORKLOADS
+    if atlas:
+        # The atlas shape starts from an NNDSVD start computed in f64 (on the
+        # device, outside the timed region); the small workloads from the
         # seeded uniform start above.
         from nmf_rs import nndsvd
         W0, H0 = nndsvd.nndsvd_device(V64[:, :p], r, fill="mean", seed=0)
@@ -404,10 +469,14 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     ctx = _native.Context(local)
     stream = torch.cuda.current_stream(dev)
+    KCLASSES = (("hstep", _native.KCLASS_HSTEP), ("wstep", _native.KCLASS_WSTEP),
+                ("objective", _native.KCLASS_OBJECTIVE), ("other", _native.KCLASS_OTHER),
+                ("hstep_refine", _native.KCLASS_HSTEP_REFINE),
+                ("wstep_refine", _native.KCLASS_WSTEP_REFINE))
 
-    def options(precision, iters_, refine=2):
+    def options(method, precision, iters_, refine=2):
         o = _native.default_options()
-        o.method = _native.parse_method(args.method)
+        o.method = _native.parse_method(method)
         o.stop = 0
         o.precision = _native.PRECISIONS[precision]
         o.max_iter = iters_
@@ -415,121 +484,151 @@ def run_ours(args, world, rank, local):
         o.device = local
         return o
 
-    def device_run(precision, iters_, W, H):
-        o = options(precision, iters_)
-        if precision == "bf16x3":
-            return ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(),
-                           H.data_ptr(), stream=stream.cuda_stream)
+    def device_run(method, precision, iters_, W, H):
+        o = options(method, precision, iters_)
         if precision == "fp32":
-            return ctx.run(o, n, p, r, V32.data_ptr(), _native.F32, ld32, W.data_ptr(), H.data_ptr(), v64_ptr=V64.data_ptr(), ldv64=ld64,
+            return ctx.run(o, n, p, r, V32.data_ptr(), _native.F32, ld32, W.data_ptr(),
+                           H.data_ptr(), v64_ptr=V64.data_ptr(), ldv64=ld64,
                            stream=stream.cuda_stream)
-        return ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(), H.data_ptr(),
-                       stream=stream.cuda_stream)
+        return ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(),
+                       H.data_ptr(), stream=stream.cuda_stream)
 
-    def timed(precision, kernel_timing):
+    def timed(method, precision):
         W = W0.clone()
         H = H0.clone()
-        device_run(precision, warm, W, H)  # warm-up iterations (untimed)
+        device_run(method, precision, warm, W, H)  # warm-up iterations (untimed)
         W = W0.clone()
         H = H0.clone()
         torch.cuda.synchronize()
         ctx.reset_timing()
-        ctx.set_timing(kernel_timing)
+        ctx.set_timing(True)
         barrier(world)
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        device_run(precision, steps, W, H)
+        device_run(method, precision, steps, W, H)
         e1.record(stream)
         torch.cuda.synchronize()
         barrier(world)
         ms = e0.elapsed_time(e1)
         launches = ctx.launch_count()
-        classes = {}
-        if kernel_timing:
-            for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP, _native.KCLASS_OBJECTIVE,
-                       _native.KCLASS_OTHER, _native.KCLASS_HSTEP_REFINE,
-                       _native.KCLASS_WSTEP_REFINE):
-                classes[kc] = ctx.kernel_time(kc)
+        classes = {name: ctx.kernel_time(kc) for name, kc in KCLASSES}
         ctx.set_timing(False)
         return ms, launches, classes, W, H
 
-    # Headline: the requested precision, with the clock sampler running.
-    with Clocks(local) as clk:
-        ms, launches, classes, W, H = timed(args.precision, True)
-    clocks = clk.summary()
-    ms_max = max_over_ranks(ms, world)
-    value = world * steps / (ms_max / 1000.0)
+    def rate(ms):
+        return world * steps / (max_over_ranks(ms, world) / 1000.0)
 
-    extra = {}
-    if args.precision != "fp64" and not args.no_fp64_compare:
-        ms64, _, _, W64, H64 = timed("fp64", False)
-        ms64_max = max_over_ranks(ms64, world)
-        fp64_value = world * steps / (ms64_max / 1000.0)
-        o_mixed = objective_torch(V64, p, W[:, :], H, args.method)
-        o_plain = objective_torch(V64, p, W64, H64, args.method)
-        extra = {}
-        if args.precision == "bf16x3":
-            ms32, _, _, _, _ = timed("fp32", False)
-            extra["fp32_form_iters_per_s"] = world * steps / (max_over_ranks(ms32, world) / 1000.0)
-        extra.update({
-            "fp64_iters_per_s": fp64_value,
-            "mixed_over_fp64": value / fp64_value,
-            "rel_objective_vs_fp64": abs(o_mixed - o_plain) / abs(o_plain),
-            "max_rel_dW_vs_fp64": float((W - W64).abs().max() / W64.abs().max()),
-        })
-
-    # Roofline of the dominant V-streaming class.
     peak, peak_kind = measured_peaks()
-    s_main = 8 if args.precision == "fp64" else 4  # f32 V, or bf16 hi + lo
-    refine = 0 if args.precision == "fp64" else 2
-    main_iters = max(0, steps - refine)
-    fp64_iters = steps - main_iters
-    # The dominant class's launches are the main-form passes only (the FP64
-    # refinement passes are timed in their own classes).
-    bytes_per_class = n * p * main_iters * s_main
-    roof = None
-    if classes:
-        cand = {kc: classes[kc] for kc in (_native.KCLASS_HSTEP, _native.KCLASS_WSTEP)}
-        dom = max(cand, key=lambda kc: cand[kc][1])
-        nl, tot_ms = cand[dom]
-        achieved = bytes_per_class / (tot_ms / 1000.0) / 1e9
-        kname = "hpass" if dom == _native.KCLASS_HSTEP else "wpass"
+    fp64_tflops = measure_fp64_gemm_tflops(dev) if args.method == "brunet" or atlas else None
+
+    def kernel_name(method, precision, dom):
+        hw = "H step" if dom == "hstep" else "W step"
+        ratio = method == "brunet"
+        if precision == "bf16x3":
+            return (("tcr_pass" if ratio else "tc_pass") + ("<H>" if dom == "hstep" else "<W>") +
+                    (" (KL ratio pass, tensor cores, f32 V)" if ratio else
+                     " (split-bf16 pass, tensor cores)"))
+        if precision == "fp64":
+            return (("h" if dom == "hstep" else "w") + "pass_dmma" + ("_ratio" if ratio else "") +
+                    f" ({hw}, FP64 tensor cores)")
+        return ("hpass" if dom == "hstep" else "wpass") + f" ({hw}, f32 CUDA cores)"
+
+    def roofline(method, precision, classes):
+        """Achieved HBM GB/s (and, for the KL ratio passes, FP64 TFLOP/s) of
+        the dominant V-streaming pass: algorithmic bytes (one read of V) per
+        launch / its average launch time (library CUDA events)."""
+        s_main = 8 if precision == "fp64" else 4  # f64 V; f32 V or bf16 hi + lo
+        main_iters = steps if precision == "fp64" else max(0, steps - 2)
+        dom = max(("hstep", "wstep"), key=lambda name: classes[name][1])
+        nl, tot_ms = classes[dom]
+        bytes_per_launch = n * p * s_main
+        avg_ms = tot_ms / max(nl, 1)
+        achieved = bytes_per_launch / (avg_ms / 1000.0) / 1e9
+        kname = "hpass" if dom == "hstep" else "wpass"
         traffic = None
-        tcr = args.precision == "bf16x3" and args.method == "brunet"
-        if (args.workload in ("atlas", "atlas-slice") and r == 20 and not tcr and
-                (kname, args.precision) in PASS_DRAM_BYTES_PER_ELEMENT):
-            traffic = PASS_DRAM_BYTES_PER_ELEMENT[(kname, args.precision)] * n * p  # per launch
-        hw = "H step" if dom == _native.KCLASS_HSTEP else "W step"
-        if tcr:
-            kernel = ("tcr_pass<H>" if dom == _native.KCLASS_HSTEP else "tcr_pass<W>") + (
-                " (KL ratio pass on the tensor cores, f32 V)")
-        elif args.precision == "bf16x3":
-            kernel = "tc_pass<H>" if dom == _native.KCLASS_HSTEP else "tc_pass<W>"
-        elif args.precision == "fp64":
-            kernel = ("h" if dom == _native.KCLASS_HSTEP else "w") + "pass_dmma" + (
-                "_ratio" if args.method == "brunet" else "") + f" ({hw}, FP64 tensor cores)"
-        else:
-            kernel = ("hpass" if dom == _native.KCLASS_HSTEP else "wpass") + f" ({hw})"
+        if (atlas and r == 20 and method != "brunet" and
+                (kname, precision) in PASS_DRAM_BYTES_PER_ELEMENT):
+            traffic = PASS_DRAM_BYTES_PER_ELEMENT[(kname, precision)] * n * p  # per launch
         roof = {
             "bound": "hbm",
-            "kernel": kernel,
+            "kernel": kernel_name(method, precision, dom),
             "achieved": achieved,
             "peak": peak,
             "unit": "GB/s",
             "frac": achieved / peak,
             "peak_kind": peak_kind,
             "launches": nl,
-            "avg_launch_ms": tot_ms / max(nl, 1),
+            "main_form_iterations": main_iters,
+            "avg_launch_ms": avg_ms,
             "traffic": traffic,
             "traffic_note": ("ncu DRAM bytes per launch, measured on the 20000x20000 slice and "
                              "scaled by V elements") if traffic else None,
-            "algorithmic_bytes_per_launch": bytes_per_class / max(nl, 1),
-            "class_ms": {name: classes[kc][1] for name, kc in
-                         (("hstep", 0), ("wstep", 1), ("objective", 2), ("other", 3),
-                          ("hstep_refine", 4), ("wstep_refine", 5))},
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+            "class_ms": {name: classes[name][1] for name, _ in KCLASSES},
         }
+        if method == "brunet" and precision == "fp64" and fp64_tflops:
+            # A ratio pass recomputes WH (2 n p r) and contracts (2 n p r).
+            flops = 4.0 * n * p * r
+            tf = flops / (avg_ms / 1000.0) / 1e12
+            roof["fp64_flops"] = {"achieved": tf, "peak": fp64_tflops, "unit": "TFLOP/s",
+                                  "frac": tf / fp64_tflops,
+                                  "peak_kind": "measured cuBLAS f64 GEMM 8192^3, same run",
+                                  "flops_per_launch": flops}
+        if n * p * 8 <= 126e6:
+            roof["regime"] = ("V (f64) fits in the 126 MB L2: the GB/s figure is L2 and HBM "
+                              "traffic together, not an HBM roofline")
+        return roof
+
+    # Headline: the requested precision (f64 by default), clocks sampled.
+    with Clocks(local) as clk:
+        ms, launches, classes, W, H = timed(args.method, args.precision)
+    clocks = clk.summary()
+    ms_max = max_over_ranks(ms, world)
+    value = world * steps / (ms_max / 1000.0)
+    roof = roofline(args.method, args.precision, classes)
+
+    extra = {}
+    if not args.no_fp64_compare:
+        # The mixed-precision forms against the f64 run of the same inputs.
+        def compare(method, W64, H64, ms64, precisions):
+            out = {}
+            o_plain = objective_torch(V64, p, W64, H64, method)
+            fp64_rate = rate(ms64)
+            for prec in precisions:
+                ms_m, _, cls_m, Wm, Hm = timed(method, prec)
+                o_m = objective_torch(V64, p, Wm, Hm, method)
+                rf = roofline(method, prec, cls_m)
+                out[prec] = {
+                    "iters_per_s": rate(ms_m),
+                    "over_fp64": rate(ms_m) / fp64_rate,
+                    "rel_objective_vs_fp64": abs(o_m - o_plain) / abs(o_plain),
+                    "max_rel_dW_vs_fp64": float((Wm - W64).abs().max() / W64.abs().max()),
+                    "dominant_pass": {"kernel": rf["kernel"], "avg_launch_ms": rf["avg_launch_ms"],
+                                      "achieved_gbs": rf["achieved"], "frac": rf["frac"]},
+                }
+            return out
+
+        if args.precision == "fp64":
+            extra["mixed"] = {args.method: {"fp64_iters_per_s": value,
+                                            **compare(args.method, W, H, ms, ("bf16x3", "fp32"))}}
+            if atlas and args.method == "lee":
+                # brunet (KL) at the same shape: the plain f64 ratio passes and
+                # the split-bf16 tensor-core ratio passes.
+                ms_b, _, cls_b, Wb, Hb = timed("brunet", "fp64")
+                extra["mixed"]["brunet"] = {
+                    "fp64_iters_per_s": rate(ms_b),
+                    "fp64_roofline": roofline("brunet", "fp64", cls_b),
+                    **compare("brunet", Wb, Hb, ms_b, ("bf16x3",))}
+        else:
+            ms64, _, _, W64, H64 = timed(args.method, "fp64")
+            o_plain = objective_torch(V64, p, W64, H64, args.method)
+            o_m = objective_torch(V64, p, W, H, args.method)
+            extra["fp64_iters_per_s"] = rate(ms64)
+            extra["mixed_over_fp64"] = value / rate(ms64)
+            extra["rel_objective_vs_fp64"] = abs(o_m - o_plain) / abs(o_plain)
+            extra["max_rel_dW_vs_fp64"] = float((W - W64).abs().max() / W64.abs().max())
 
     # End to end through the host-pointer C ABI.
     e2e = None
@@ -546,11 +645,11 @@ def run_ours(args, world, rank, local):
         import ctypes
 
         lib = _native.load()
-        o = options(args.precision, steps)
+        o = options(args.method, args.precision, steps)
         nd, ni = ctypes.c_int64(0), ctypes.c_int64(0)
         dp = _native._ptr
         # warm-up (allocates the library's workspace)
-        ow = options(args.precision, 1)
+        ow = options(args.method, args.precision, 1)
         _native.check(lib.nmfcu_run(ctypes.byref(ow), n, p, r, dp(Vh), dp(W0h), dp(H0h), dp(Wout),
                                     dp(Hout), None, 0, ctypes.byref(nd), ctypes.byref(ni)))
         barrier(world)
@@ -562,7 +661,8 @@ def run_ours(args, world, rank, local):
         e2e = {"value": world * steps / t_e2e, "unit": "iters/s",
                "h2d_bytes_per_step": (n * p + n * r + r * p) * 8 / steps,
                "d2h_bytes_per_step": (n * r + r * p) * 8 / steps,
-               "note": "one nmfcu_run call per K steps: V, W0, H0 uploaded once, W, H read back once"}
+               "note": ("one nmfcu_run call per K steps (the call behind nmf_rs.nmf): V, W0, "
+                        "H0 uploaded from pinned host memory once, W, H read back once")}
         del V_host
     else:
         del V64, V32
@@ -580,8 +680,7 @@ def run_ours(args, world, rank, local):
 
     if rank == 0:
         line = {
-            "metric": f"{args.method} iterations/s, {args.workload} {n}x{p} rank {r}, "
-                      f"{args.precision} form",
+            "metric": iterate_metric(args.method, args.workload),
             "value": value,
             "unit": "iters/s",
             "n_gpus": world,
@@ -591,15 +690,17 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": {"fp32": "f32", "bf16x3": "bf16x3 (split bf16, f32 accumulation)",
+            "dtype": {"fp32": "f32 products, f64 epilogues/objective",
+                      "bf16x3": "bf16x3 (split bf16, f32 accumulation), f64 epilogues",
                       "fp64": "f64"}[args.precision],
             "data": "synthetic (seeded single-cell-like generator on the device)",
             "config": {"workload": args.workload, "n": n, "p": p, "rank": r,
                        "method": args.method, "precision": args.precision,
                        "start": ("NNDSVD (mean fill), f64, on the device"
-                                 if args.workload in ATLAS_WORKLOADS else "seeded uniform"),
+                                 if atlas else "seeded uniform"),
                        "parallelism": f"replicas x{world}",
-                       "l2": "V is larger than L2 (no flush needed)"},
+                       "l2": ("V is larger than L2 (no flush needed)" if n * p * 8 > 126e6 else
+                              "V fits in L2 (126 MB): L2-resident regime, no flush")},
             "gpu_launches": launches,
             "clocks": clocks,
             "roofline": roof,
@@ -649,12 +750,16 @@ def host_linkage_seconds(p, runs=64, k=6, seed=0):
 
 
 def consensus_cpu_baseline(V, runs, seconds, iters=200):
-    """The oracle's brunet iteration per rank on a column slice,
-    extrapolated to runs x 200 iterations per rank over the full V, plus
-    each rank's cophenetic correlation and dispersion on the host."""
+    """The reference workflow on the CPU restatement: per rank, one solve's
+    set-up (a 1-iteration call minus an iteration) plus `iters` iterations
+    (the difference of a 3- and a 1-iteration call, / 2), on a column slice of
+    V and scaled to the full V, times `runs` restarts (each restart is its own
+    nmf() call in the reference, so each pays the set-up); plus each rank's
+    cophenetic correlation and dispersion on the host."""
     from nmf_rs import consensus
 
     c = CONSENSUS
+    threads = os.cpu_count() or 1
     total = 0.0
     samples = []
     for r in c["ranks"]:
@@ -662,16 +767,19 @@ def consensus_cpu_baseline(V, runs, seconds, iters=200):
             v = np.ascontiguousarray(V[:, :p_s])
             W0, H0 = consensus.restart_starts(v, r, 1)[0]
             return v, W0, H0
-        b = cpu_baseline(fn, c["n"], c["p"], r, "brunet", seconds / len(c["ranks"]))
-        total += runs * iters / b["value"]
-        samples.append(b["sample"].split(" took ")[1].split(";")[0])
+        p_s = pick_slice(fn, c["p"], "brunet", seconds / len(c["ranks"]), threads)
+        v, W0, H0 = fn(p_s)
+        per_iter, t_one, _ = oracle_iteration_seconds("brunet", v, W0, H0, 2, threads)
+        setup = max(t_one - per_iter, 0.0)
+        total += runs * (setup + iters * per_iter) * c["p"] / p_s
+        samples.append(f"k={r}: {p_s} cols, {1000 * per_iter:.1f} ms/it + {1000 * setup:.1f} ms")
     t_link = host_linkage_seconds(c["p"])
     total += len(c["ranks"]) * t_link
     return {"value": runs * len(c["ranks"]) / total, "unit": "solves/s",
-            "cores": os.cpu_count() or 1, "kind": "port",
-            "sample": ("1 brunet iteration of the CPU restatement (oracle/, OpenMP) per rank "
-                       "2..10 on a column slice of V (" + ", ".join(samples) + "), "
-                       f"extrapolated to {runs} restarts x {iters} iterations on 2000x5000; "
+            "cores": threads, "kind": "port",
+            "sample": ("brunet on the CPU restatement (oracle/, -march=native, OpenMP) per rank "
+                       "2..10 on a column slice of V (" + "; ".join(samples) + "), "
+                       f"scaled to {runs} restarts x {iters} iterations on 2000x5000; "
                        f"plus 9 x {t_link:.2f} s of scipy average linkage + cophenet + "
                        f"dispersion on a {c['p']}x{c['p']} consensus matrix")}
 

@@ -436,11 +436,16 @@ nmfcu_status nmfcu_server_reset_stats(nmfcu_server *srv);
  * Its scratch is a fixed 512 KB array compiled into the library (one f64 per
  * 8 rows), which every GPU that loads the library holds until the process
  * exits; n above NMFCU_NOALLOC_MAX_ROWS is rejected (NMFCU_ERR_INVALID_ARG).
- * It runs on the caller's current device.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the one array: calls whose
- * work overlaps on the GPU (different streams, or other host threads) race
- * and may return wrong values, so serialise them. */
+ * It runs on the caller's current device.  The first call in a CUDA context
+ * (the device's primary context, or one the caller created) looks up the
+ * array's device address (cudaGetSymbolAddress) and caches it for that
+ * context; make that first call before any stream capture.  The cache does
+ * not survive cudaDeviceReset: a caller that resets the device must not call
+ * this entry point again in the same process.  An empty V (n == 0 or
+ * p == 0) writes 0 and reads none of dV, dW, dH (they may be NULL).  All
+ * calls share the one array: calls whose work overlaps on the GPU
+ * (different streams, or other host threads) race and may return wrong
+ * values, so serialise them. */
 #define NMFCU_NOALLOC_MAX_ROWS 524288
 enum { NMFCU_OBJECTIVE_KL = 0, NMFCU_OBJECTIVE_FROBENIUS = 1 };
 nmfcu_status nmfcu_objective_noalloc(int32_t kind, int64_t n, int64_t p, int64_t r,

@@ -42,6 +42,37 @@ def build(force: bool = False) -> Path:
     return _LIB_PATH
 
 
+def _cpu_fingerprint() -> str:
+    """A short hash of this host's CPU model and feature flags."""
+    import hashlib
+
+    txt = ""
+    try:
+        for ln in Path("/proc/cpuinfo").read_text().splitlines():
+            if ln.startswith(("model name", "flags")):
+                txt += ln
+                if ln.startswith("flags"):
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(txt.encode()).hexdigest()[:12]
+
+
+def use_native() -> Path:
+    """Build (once per CPU model) and load a -march=native copy of the oracle
+    for the CPU-baseline timing.  It computes the same values as the generic
+    build: -ffp-contract=off and no fast-math hold in both."""
+    global _lib, _LIB_PATH
+    path = _HERE / f"liboracle_native_{_cpu_fingerprint()}.so"
+    if not path.exists() or path.stat().st_mtime < (_HERE / "nmf_oracle.c").stat().st_mtime:
+        subprocess.run(["make", "-s", "-C", str(_HERE), "native", f"NATIVE_OUT={path}"],
+                       check=True)
+    _LIB_PATH = path
+    _lib = None
+    _load()
+    return path
+
+
 def _load():
     global _lib
     if _lib is not None:

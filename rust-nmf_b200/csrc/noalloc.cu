@@ -45,7 +45,7 @@ __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, 
 // be cleared between calls).
 template <int RP, bool KL>
 __global__ void __launch_bounds__(256)
-    noalloc_objective_partial(const double *__restrict__ V, int64_t ldv, int n, int p, int r,
+    noalloc_objective_partial(const double *__restrict__ V, int64_t ldv, int n, int64_t p, int r,
                               const double *__restrict__ W, const double *__restrict__ H,
                               double *__restrict__ partials) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -56,11 +56,12 @@ __global__ void __launch_bounds__(256)
 #pragma unroll
         for (int k = 0; k < RP; k++) w[k] = (k < r) ? W[(int64_t)i * r + k] : 0.0;
         const double *vrow = V + (int64_t)i * ldv;
-        for (int j = lane; j < p; j += 32) {
+        // 64-bit column index: j + 32 cannot wrap for any p the entry accepts.
+        for (int64_t j = lane; j < p; j += 32) {
             double wh = 0.0;
 #pragma unroll
             for (int k = 0; k < RP; k++)
-                if (k < r) wh = fma(w[k], H[(int64_t)k * p + j], wh);
+                if (k < r) wh = fma(w[k], H[k * p + j], wh);
             const double v = vrow[j];
             if (KL) {
                 // kl_divergence term, lib.rs:1418-1427
@@ -102,34 +103,65 @@ __global__ void noalloc_objective_finalize(const double *__restrict__ partials, 
     if (threadIdx.x == 0) *out = red[0] * scale;
 }
 
-// Device address of the scratch, looked up once per device with that device
-// current (the caller's current device when the entry point is called).
+// Device address of the scratch, looked up with the caller's device current
+// the first time a call runs in a CUDA context, and cached per (device,
+// context): a caller that runs in a context of its own (cuCtxCreate) rather
+// than the device's primary context gets that context's copy of the array.
 std::mutex g_scratch_mu;
 constexpr int kMaxDevices = 64;
-double *g_scratch_ptr[kMaxDevices] = {nullptr};
+struct ScratchSlot {
+    void *ctx;
+    double *ptr;
+};
+ScratchSlot g_scratch[kMaxDevices] = {};
+
+typedef int (*CtxGetCurrentFn)(void **);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            return reinterpret_cast<CtxGetCurrentFn>(p);
+        cudaGetLastError();
+        return static_cast<CtxGetCurrentFn>(nullptr);
+    }();
+    return fn;
+}
 
 nmfcu_status noalloc_scratch(int device, double **out) {
     if (device < 0 || device >= kMaxDevices)
         return nmfcu_internal::fail(NMFCU_ERR_UNSUPPORTED, "device ordinal beyond 63");
+    CtxGetCurrentFn get = ctx_get_current();
+    void *ctx = nullptr;
+    if (get) get(&ctx);
     std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_ptr[device]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return nmfcu_internal::fail(
-                NMFCU_ERR_CUDA,
-                std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
-        }
-        g_scratch_ptr[device] = static_cast<double *>(ptr);
+    ScratchSlot &slot = g_scratch[device];
+    if (ctx && slot.ptr && slot.ctx == ctx) {
+        *out = slot.ptr;
+        return NMFCU_OK;
     }
-    *out = g_scratch_ptr[device];
+    // First call in this context (or no context is current yet: the lookup
+    // makes the device's primary context current, and the context is read
+    // again after it).
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return nmfcu_internal::fail(
+            NMFCU_ERR_CUDA,
+            std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
+    }
+    if (!ctx && get) get(&ctx);
+    slot.ctx = ctx;
+    slot.ptr = static_cast<double *>(ptr);
+    *out = slot.ptr;
     return NMFCU_OK;
 }
 
 template <int RP>
 void launch_partial(bool kl, unsigned blocks, cudaStream_t s, const double *V, int64_t ldv,
-                    int n, int p, int r, const double *W, const double *H, double *part) {
+                    int n, int64_t p, int r, const double *W, const double *H, double *part) {
     if (kl)
         noalloc_objective_partial<RP, true><<<blocks, 256, 0, s>>>(V, ldv, n, p, r, W, H, part);
     else
@@ -170,9 +202,14 @@ extern "C" nmfcu_status nmfcu_objective_noalloc(int32_t kind, int64_t n, int64_t
     if (st != NMFCU_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const bool kl = (kind == NMFCU_OBJECTIVE_KL);
-    const unsigned blocks = (unsigned)((n + kRowsPerBlock - 1) / kRowsPerBlock);
+    // An empty V (n == 0 or p == 0) has objective 0: no partial block runs
+    // (so NULL factor pointers are never read) and the finalize step sums
+    // zero partials.
+    const unsigned blocks =
+        (n > 0 && p > 0) ? (unsigned)((n + kRowsPerBlock - 1) / kRowsPerBlock) : 0u;
     if (blocks > 0) {
-        const int ni = (int)n, pi = (int)p, ri = (int)r;
+        const int ni = (int)n, ri = (int)r;
+        const int64_t pi = p;
         if (r <= 8)
             launch_partial<8>(kl, blocks, s, dV, ldv, ni, pi, ri, dW, dH, part);
         else if (r <= 16)

@@ -1,5 +1,6 @@
 // stream_tc.cu -- instantiation and launch of the tensor-core passes, and
 // the bf16 split kernels of the split-bf16 precision form.
+#include <atomic>
 #include <algorithm>
 
 #include "launch.h"
@@ -88,16 +89,17 @@ cudaError_t launch_one(const CUtensorMap &ah, const CUtensorMap &al, const CUten
                        cudaStream_t s) {
     constexpr int smem = tc_smem_bytes<RPN>();
     // The attribute lives in each device's context: set it once per device
-    // and instantiation.
-    static bool configured[kAttrDevices] = {};
+    // and instantiation.  Serving worker threads launch these passes
+    // concurrently, so the flags are atomics (a repeated set is harmless).
+    static std::atomic<bool> configured[kAttrDevices] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kAttrDevices || !configured[dev]) {
+    if (dev < 0 || dev >= kAttrDevices || !configured[dev].load(std::memory_order_acquire)) {
         e = cudaFuncSetAttribute(tc_pass<RPN, A_MN, OUT_KM>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < kAttrDevices) configured[dev] = true;
+        if (dev >= 0 && dev < kAttrDevices) configured[dev].store(true, std::memory_order_release);
     }
     tc_pass<RPN, A_MN, OUT_KM><<<sk.G, kThreadsTC, smem, s>>>(ah, al, b3[0], b3[1], b3[2], kext,
                                                                RP, sk, part, st);

@@ -1,5 +1,6 @@
 // stream_tcr.cu -- launch of brunet's tensor-core passes (tcr.cuh) and the
 // split of a factor into the two bf16 term layouts they read.
+#include <atomic>
 #include <algorithm>
 
 #include "launch.h"
@@ -49,16 +50,17 @@ cudaError_t launch_one(const CUtensorMap &v, const CUtensorMap &t, const CUtenso
                        int xpadT, int xpadF, int kext, int RP, const StreamK &sk, double *part,
                        RunState *st, cudaStream_t s) {
     // The attribute lives in each device's context: set it once per device
-    // and instantiation.
-    static bool configured[kAttrDevices] = {};
+    // and instantiation.  Serving worker threads launch these passes
+    // concurrently, so the flags are atomics (a repeated set is harmless).
+    static std::atomic<bool> configured[kAttrDevices] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kAttrDevices || !configured[dev]) {
+    if (dev < 0 || dev >= kAttrDevices || !configured[dev].load(std::memory_order_acquire)) {
         e = cudaFuncSetAttribute(tcr_pass<HPASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  SMEM);
         if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < kAttrDevices) configured[dev] = true;
+        if (dev >= 0 && dev < kAttrDevices) configured[dev].store(true, std::memory_order_release);
     }
     tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st);
     return cudaGetLastError();

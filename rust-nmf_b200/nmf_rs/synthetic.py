@@ -68,3 +68,41 @@ def make(w: Workload) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     V = counts_matrix(w.n, w.p, w.k, w.alpha, w.seed)
     W0, H0 = starting_point(V, w.rank, w.seed)
     return V, W0, H0
+
+
+def device_workload(n: int, p: int, k: int, alpha: float, rank: int, seed: int, device):
+    """The same generator on the device (torch's RNG, so not the same draws
+    as :func:`counts_matrix`), for shapes too large to build on the host in
+    reasonable time.  Returns (V64, ld64, V32, ld32, W0, H0): V in f64 with
+    its leading dimension padded to 16 elements and in f32 padded to 32
+    (zeros in the padding), and a U(0, max V) start."""
+    import torch
+
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    f64 = torch.float64
+    w_true = torch._standard_gamma(torch.full((n, k), 0.5, dtype=f64, device=device),
+                                   generator=g)
+    w_true[torch.rand((n, k), generator=g, device=device, dtype=f64) < 0.7] = 0.0
+    ld64 = (p + 15) // 16 * 16
+    ld32 = (p + 31) // 32 * 32
+    V64 = torch.zeros((n, ld64), dtype=f64, device=device)
+    chunk = 8192
+    for c0 in range(0, p, chunk):
+        c = min(chunk, p - c0)
+        h = torch._standard_gamma(torch.full((k, c), float(alpha), dtype=f64, device=device),
+                                  generator=g)
+        h = h / h.sum(0, keepdim=True).clamp_min(1e-300)
+        lib = torch.empty(c, dtype=f64, device=device).log_normal_(7.0, 0.5, generator=g)
+        lam = (w_true @ h) * lib[None, :]
+        counts = torch.poisson(lam, generator=g)
+        col = counts.sum(0, keepdim=True)
+        scale = torch.where(col > 0, 1e4 / col.clamp_min(1e-300), torch.zeros_like(col))
+        V64[:, c0:c0 + c] = torch.log1p(counts * scale)
+        del h, lam, counts
+    V32 = torch.zeros((n, ld32), dtype=torch.float32, device=device)
+    V32[:, :p] = V64[:, :p].float()
+    vmax = float(V64[:, :p].max())
+    W0 = torch.rand((n, rank), generator=g, device=device, dtype=f64) * vmax
+    H0 = torch.rand((rank, p), generator=g, device=device, dtype=f64) * vmax
+    return V64, ld64, V32, ld32, W0, H0

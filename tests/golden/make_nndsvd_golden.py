@@ -67,4 +67,6 @@ def main(reference: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_nndsvd_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -186,9 +186,10 @@ def test_pbmc_subset_lee_full(oracle):
 
 @pytest.mark.parametrize("method", ["brunet", "hals"])
 def test_pbmc8k_shape(oracle, method):
-    """brunet and hals on the 2000 x 7750 rank-10 workload (30 iterations)."""
+    """brunet and hals on the 2000 x 7750 rank-10 workload at its stated 100
+    iterations, from its seeded uniform start."""
     V, W0, H0 = synthetic.make(synthetic.PBMC8K_SHAPE)
-    _check(oracle, method, V, W0, H0, 30)
+    _check(oracle, method, V, W0, H0, 100)
 
 
 @pytest.mark.parametrize("method", METHODS)

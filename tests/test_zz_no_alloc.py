@@ -27,20 +27,28 @@ pytestmark = pytest.mark.gpu
 OBJ_TOL = 1e-12
 
 
-def _noalloc(kind, V, W, H):
-    """One call on device copies of V, W, H; returns the device result."""
+def _noalloc(kind, V, W, H, pad=0, side_stream=False):
+    """One call on device copies of V, W, H; returns the device result.
+
+    pad > 0 embeds V in a wider device buffer (leading dimension p + pad);
+    side_stream runs the call on a fresh stream instead of the current one."""
     import torch
 
     lib = _native.load()
-    dV = torch.from_numpy(np.ascontiguousarray(V)).cuda()
+    n, p = V.shape
+    r = W.shape[1]
+    ldv = p + pad
+    Vbuf = np.full((n, ldv), np.nan)  # the padding must never be read
+    Vbuf[:, :p] = V
+    dV = torch.from_numpy(Vbuf).cuda()
     dW = torch.from_numpy(np.ascontiguousarray(W)).cuda()
     dH = torch.from_numpy(np.ascontiguousarray(H)).cuda()
     out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
-    n, p = V.shape
-    r = W.shape[1]
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream() if side_stream else torch.cuda.current_stream()
+    if side_stream:
+        stream.wait_stream(torch.cuda.current_stream())
     _native.check(lib.nmfcu_objective_noalloc(
-        kind, n, p, r, ctypes.c_void_p(dV.data_ptr()), p, ctypes.c_void_p(dW.data_ptr()),
+        kind, n, p, r, ctypes.c_void_p(dV.data_ptr()), ldv, ctypes.c_void_p(dW.data_ptr()),
         ctypes.c_void_p(dH.data_ptr()), ctypes.c_void_p(out.data_ptr()),
         ctypes.c_void_p(stream.cuda_stream)))
     stream.synchronize()
@@ -68,3 +76,31 @@ def test_noalloc_rejects_rows_beyond_scratch():
         _native.check(lib.nmfcu_objective_noalloc(
             _native.OBJECTIVE_KL, _native.NOALLOC_MAX_ROWS + 1, 4, 2, None, 4, None, None,
             ctypes.addressof(out), None))
+
+
+def test_noalloc_padded_rows_and_side_stream():
+    """V inside a wider buffer (ldv > p; the padding holds NaN, so reading it
+    would show), on a stream other than the current one."""
+    V = synthetic.counts_matrix(333, 250, 4, 0.3, seed=8)
+    W, H = nmf_rs.random_init(V, 9, seed=3)
+    for kind, ref in ((_native.OBJECTIVE_KL, _native.divergence(V, W, H)),
+                      (_native.OBJECTIVE_FROBENIUS, _native.distance(V, W, H))):
+        assert rel(_noalloc(kind, V, W, H, pad=13), ref) <= OBJ_TOL
+        assert rel(_noalloc(kind, V, W, H, pad=6, side_stream=True), ref) <= OBJ_TOL
+
+
+def test_noalloc_empty_inputs_write_zero_without_reading_factors():
+    """n == 0 or p == 0: the objective is 0 and the (NULL) V, W, H are not
+    read.  The output starts as NaN, so a skipped write would show."""
+    import torch
+
+    lib = _native.load()
+    out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    for n, p in ((0, 40), (25, 0), (0, 0)):
+        for kind in (_native.OBJECTIVE_KL, _native.OBJECTIVE_FROBENIUS):
+            out.fill_(float("nan"))
+            _native.check(lib.nmfcu_objective_noalloc(
+                kind, n, p, 3, None, max(p, 0), None, None, ctypes.c_void_p(out.data_ptr()),
+                ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+            torch.cuda.synchronize()
+            assert float(out.item()) == 0.0
