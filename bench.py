@@ -91,12 +91,15 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="atlas")
     ap.add_argument("--method", choices=["lee", "brunet", "hals", "dnmf"], default="lee")
-    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["fp32", "bf16x3", "fp64"], default=None,
+                    help="default: fp64 (the reference's precision); fp32 for the consensus "
+                         "form (its batched FP32 form)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-compare", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--form", choices=["iterate", "consensus", "serve", "nndsvd", "shard"],
+    ap.add_argument("--form", choices=["iterate", "consensus", "serve", "nndsvd", "shard",
+                                       "sparse"],
                     default="iterate")
     ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="serve: server slots")
@@ -106,7 +109,12 @@ def parse():
     ap.add_argument("--seq-runs", type=int, default=None,
                     help="consensus: restarts per rank timed one by one (default: all; 0: skip)")
     ap.add_argument("--iters", type=int, default=200, help="consensus: iterations per solve")
-    return ap.parse_args()
+    ap.add_argument("--density", type=float, default=0.1,
+                    help="sparse: fraction of V's entries stored")
+    args = ap.parse_args()
+    if args.precision is None:
+        args.precision = "fp32" if args.form == "consensus" else "fp64"
+    return args
 
 
 # ---------------------------------------------------------------------------
@@ -840,17 +848,18 @@ def run_consensus(args, world, rank, local):
     prec = _native.PRECISIONS[args.precision]
     i32p = ctypes.POINTER(ctypes.c_int32)
     rp = ranks.ctypes.data_as(i32p)
-    cons = torch.empty((p, p), dtype=torch.float32, device=dev)
+    cons = torch.empty((len(c["ranks"]), p, p), dtype=torch.float32, device=dev)
     sels = [np.arange(ci * runs, (ci + 1) * runs, dtype=np.int32) for ci in range(len(c["ranks"]))]
 
     def post():
-        """The nine consensus matrices and their statistics (dH: all solves)."""
-        for sel in sels:
+        """The nine consensus matrices and their statistics (dH: all solves),
+        the nine average-linkage trees built concurrently."""
+        for ci, sel in enumerate(sels):
             _native.check(lib.nmfcu_consensus_device(
                 ctx.handle, p, nsolves, rp, ctypes.c_void_p(dH.data_ptr()), runs,
-                sel.ctypes.data_as(i32p), ctypes.c_void_p(cons.data_ptr()),
+                sel.ctypes.data_as(i32p), ctypes.c_void_p(cons[ci].data_ptr()),
                 ctypes.c_void_p(stream.cuda_stream)))
-            consensus.consensus_stats(cons, ctx)  # cophenetic + dispersion, on the GPU
+        consensus.consensus_stats_batch(cons, ctx)  # cophenetic + dispersion, on the GPU
 
     def batched_sweep():
         dW.copy_(dW0)
@@ -929,8 +938,12 @@ def run_consensus(args, world, rank, local):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(3):
-        consensus.consensus_stats(cons, ctx)
+        consensus.consensus_stats(cons[0], ctx)
     stats_ms = (time.perf_counter() - t0) / 3 * 1000.0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    consensus.consensus_stats_batch(cons, ctx)
+    batch_stats_ms = (time.perf_counter() - t0) * 1000.0
     host_stats_ms = host_linkage_seconds(p) * 1000.0
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -961,6 +974,7 @@ def run_consensus(args, world, rank, local):
                             "candidates": consensus.batch_shape_count(),
                             "how": "autotuned: each shape timed on the first run, fastest kept"},
             "consensus_stats_ms_per_rank": stats_ms,
+            "consensus_stats_ms_all_ranks_concurrent": batch_stats_ms,
             "host_scipy_stats_ms_per_rank": host_stats_ms,
             "cpu_baseline": cpu,
             "e2e": {"value": world * nsolves / t_e2e, "unit": "solves/s",
@@ -1423,6 +1437,178 @@ def run_shard_bench(args, world, rank, local):
         }), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Sparse form: V as CSR
+# ---------------------------------------------------------------------------
+
+def device_sparse_workload(n, p, k, alpha, rank, density, seed, device):
+    """The workload's V with all but about `density` of its entries set to
+    zero (a seeded mask), as a device CSR: (indptr int64, indices int32,
+    data f64, W0, H0), built 2048 rows at a time."""
+    import torch
+
+    V64, ld64, V32, _, W0, H0 = device_workload(n, p, k, alpha, rank, seed, device)
+    del V32
+    g = torch.Generator(device=device)
+    g.manual_seed(seed + 1)
+    nz_frac = float((V64[: min(n, 512), :p] > 0).double().mean())
+    keep = min(1.0, density / max(nz_frac, 1e-9))
+    counts, cols, vals = [], [], []
+    for r0 in range(0, n, 2048):
+        blk = V64[r0:r0 + 2048, :p]
+        blk = torch.where(torch.rand(blk.shape, generator=g, device=device, dtype=torch.float32)
+                          < keep, blk, torch.zeros_like(blk))
+        csr = blk.to_sparse_csr()
+        counts.append(csr.crow_indices().diff())
+        cols.append(csr.col_indices().to(torch.int32))
+        vals.append(csr.values())
+        del blk, csr
+    del V64
+    torch.cuda.empty_cache()
+    indptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    indptr[1:] = torch.cumsum(torch.cat(counts), 0)
+    return indptr, torch.cat(cols), torch.cat(vals), W0, H0
+
+
+def run_sparse(args, world, rank, local):
+    """One solve on a sparse V through nmfcu_run_csr_device (value) and
+    nmfcu_run_csr with host arrays (e2e).  The roofline counts the CSR bytes
+    a pass streams (12 per stored entry: the f64 value and the int32 index)
+    against HBM; the factor rows each stored entry gathers come from L2."""
+    import ctypes
+
+    import torch
+
+    from nmf_rs import _native
+
+    n, p, k, alpha, r, iters = WORKLOADS[args.workload]
+    steps = args.steps or iters
+    warm = max(3, args.warmup)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    indptr, indices, data, W0, H0 = device_sparse_workload(n, p, k, alpha, r, args.density,
+                                                           1234 + rank, dev)
+    nnz = int(data.numel())
+    torch.cuda.synchronize()
+    ctx = _native.Context(local)
+    stream = torch.cuda.current_stream(dev)
+    lib = _native.load()
+
+    def opts(iters_):
+        o = _native.default_options()
+        o.method = _native.parse_method(args.method)
+        o.max_iter = iters_
+        o.device = local
+        return o
+
+    def device_run(iters_, W, H):
+        nd, ni = ctypes.c_int64(0), ctypes.c_int64(0)
+        _native.check(lib.nmfcu_run_csr_device(
+            ctx.handle, ctypes.byref(opts(iters_)), n, p, r, nnz,
+            ctypes.c_void_p(indptr.data_ptr()), ctypes.c_void_p(indices.data_ptr()),
+            ctypes.c_void_p(data.data_ptr()), ctypes.c_void_p(W.data_ptr()),
+            ctypes.c_void_p(H.data_ptr()), None, ctypes.byref(nd), ctypes.byref(ni),
+            ctypes.c_void_p(stream.cuda_stream)))
+
+    device_run(warm, W0.clone(), H0.clone())
+    W, H = W0.clone(), H0.clone()
+    torch.cuda.synchronize()
+    ctx.reset_timing()
+    ctx.set_timing(True)
+    barrier(world)
+    with Clocks(local) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        device_run(steps, W, H)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    launches = ctx.launch_count()
+    classes = {name: ctx.kernel_time(kc) for name, kc in
+               (("hstep", _native.KCLASS_HSTEP), ("wstep", _native.KCLASS_WSTEP),
+                ("other", _native.KCLASS_OTHER))}
+    ctx.set_timing(False)
+    value = world * steps / (ms / 1000.0)
+    peak, peak_kind = measured_peaks()
+    dom = max(("hstep", "wstep"), key=lambda c: classes[c][1])
+    nl, tot = classes[dom]
+    avg = tot / max(nl, 1)
+    csr_bytes = nnz * 12
+    achieved = csr_bytes / (avg / 1000.0) / 1e9
+    roof = {"bound": "hbm", "kernel": ("sparse_pass<H> (CSC columns)" if dom == "hstep"
+                                        else "sparse_pass<W> (CSR rows)"),
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_kind": peak_kind, "launches": nl, "avg_launch_ms": avg, "traffic": None,
+            "algorithmic_bytes_per_launch": csr_bytes,
+            "gathered_factor_bytes_per_launch": nnz * (r + r % 2) * 8,
+            "class_ms": {c: classes[c][1] for c in classes},
+            "note": ("algorithmic bytes = the CSR a pass streams (12 B a stored entry); each "
+                     "stored entry also gathers an f64 factor row from L2")}
+    # End to end: host CSR arrays through nmfcu_run_csr.
+    e2e = None
+    if not args.no_e2e:
+        hp = indptr.cpu().numpy()
+        hi = indices.cpu().numpy()
+        hd = data.cpu().numpy()
+        W0h, H0h = W0.cpu().numpy(), H0.cpu().numpy()
+        Wo, Ho = np.empty_like(W0h), np.empty_like(H0h)
+        nd, ni = ctypes.c_int64(0), ctypes.c_int64(0)
+
+        def host_run(iters_):
+            _native.check(lib.nmfcu_run_csr(
+                ctypes.byref(opts(iters_)), n, p, r, nnz, hp.ctypes.data_as(_native._i64p),
+                hi.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _native._ptr(hd),
+                _native._ptr(W0h), _native._ptr(H0h), _native._ptr(Wo), _native._ptr(Ho), None,
+                0, ctypes.byref(nd), ctypes.byref(ni)))
+
+        host_run(1)
+        barrier(world)
+        t0 = time.perf_counter()
+        host_run(steps)
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+        e2e = {"value": world * steps / t_e2e, "unit": "iters/s",
+               "h2d_bytes_per_step": (hp.nbytes + hi.nbytes + hd.nbytes + W0h.nbytes +
+                                      H0h.nbytes) / steps,
+               "d2h_bytes_per_step": (Wo.nbytes + Ho.nbytes) / steps,
+               "note": "one nmfcu_run_csr call per K steps (host CSR validated and uploaded)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        # The reference densifies V (python/nmf_rs/__init__.py:495) and runs
+        # the dense loop: the dense CPU restatement on slices of this V.
+        hp = indptr.cpu().numpy()
+        hi = indices.cpu().numpy()
+        hd = data.cpu().numpy()
+        import scipy.sparse as sps
+
+        Vs = sps.csr_matrix((hd, hi, hp), shape=(n, p))
+        W0h, H0h = W0.cpu().numpy(), H0.cpu().numpy()
+
+        def V_host_fn(p_s):
+            v = np.ascontiguousarray(Vs[:, :p_s].toarray())
+            return v, W0h, np.ascontiguousarray(H0h[:, :p_s])
+
+        cpu = cpu_baseline(V_host_fn, n, p, r, args.method, args.cpu_seconds)
+        cpu["sample"] = "the reference densifies V; " + cpu["sample"]
+    if rank == 0:
+        print(json.dumps({
+            "metric": f"{args.method} iterations/s, sparse {args.workload} {n}x{p} rank {r}, "
+                      f"{args.density:.0%} stored",
+            "value": value, "unit": "iters/s", "n_gpus": world, "steps": steps, "warmup": warm,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded generator on the device, seeded mask to the density)",
+            "config": {"workload": args.workload, "n": n, "p": p, "rank": r, "nnz": nnz,
+                       "density": nnz / (n * p), "method": args.method, "form": "sparse",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "the CSR is larger than L2 (no flush needed)"},
+            "gpu_launches": launches, "clocks": clk.summary(), "roofline": roof,
+            "cpu_baseline": cpu, "e2e": e2e,
+        }), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -1432,6 +1618,11 @@ def main():
                 run_reference(args, world, rank)
             else:
                 run_shard_bench(args, world, rank, local)
+        elif args.form == "sparse":
+            if args.impl == "reference":
+                run_reference(args, world, rank)
+            else:
+                run_sparse(args, world, rank, local)
         elif args.form == "nndsvd":
             if args.impl == "reference":
                 run_nndsvd_reference(args, world, rank)

@@ -218,6 +218,38 @@ nmfcu_status nmfcu_run_device(nmfcu_context *ctx, const nmfcu_options *opt, int6
                               void *stream);
 
 /*
+ * nmfcu_run_csr -- nmfcu_run on a sparse V in compressed sparse row form.
+ * No counterpart in the reference, whose nmf() densifies V first
+ * (python/nmf_rs/__init__.py:495, `_f64_c(V)`), so it replaces that call
+ * path for the sparse (AnnData CSR) inputs single-cell data arrives in: the
+ * same loop (py_nmf_run, lib.rs:1934-2169) with V's zeros never stored or
+ * read.  Methods lee, brunet, hals and dnmf (others: NMFCU_ERR_UNSUPPORTED),
+ * FP64 only.
+ *   indptr   n + 1 row offsets (indptr[0] = 0, non-decreasing, indptr[n] = nnz)
+ *   indices  nnz column indices in [0, p), data nnz values (f64, >= 0): the
+ *            canonical CSR of V -- no duplicate (row, column) pairs (a
+ *            duplicate would enter brunet's objective twice); the order of
+ *            a row's entries only changes rounding.
+ * W0, H0, W, H, deviances, n_deviances, n_iter as in nmfcu_run.  nnz is at
+ * most 2^31 - 1.  The library keeps a column-sorted (CSC) copy of V for the
+ * H step on the device for the run (12 bytes per stored entry).
+ */
+nmfcu_status nmfcu_run_csr(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                           int64_t nnz, const int64_t *indptr, const int32_t *indices,
+                           const double *data, const double *W0, const double *H0, double *W,
+                           double *H, double *deviances, int64_t deviances_cap,
+                           int64_t *n_deviances, int64_t *n_iter);
+/* nmfcu_run_csr on device pointers, enqueued on `stream`: the CSR arrays as
+ * above, dW (n x r) and dH (r x p) f64 hold W0 / H0 on entry and the result
+ * on exit, d_dev as in nmfcu_run_device.  The CSR's structure is checked on
+ * the device before use (a bad indptr or index: NMFCU_ERR_INVALID_ARG). */
+nmfcu_status nmfcu_run_csr_device(nmfcu_context *ctx, const nmfcu_options *opt, int64_t n,
+                                  int64_t p, int64_t r, int64_t nnz, const int64_t *d_indptr,
+                                  const int32_t *d_indices, const double *d_data, double *dW,
+                                  double *dH, double *d_dev, int64_t *n_deviances,
+                                  int64_t *n_iter, void *stream);
+
+/*
  * nmfcu_v_product_device -- one V contraction of the randomized range finder
  * behind nndsvd_init (python/nmf_rs/__init__.py:129-219, which calls
  * scikit-learn's randomized_svd at :172-174; its products A @ Q, A.T @ Q and
@@ -365,6 +397,16 @@ nmfcu_status nmfcu_consensus_device(nmfcu_context *ctx, int64_t p, int32_t nsolv
 nmfcu_status nmfcu_consensus_stats_device(nmfcu_context *ctx, int64_t p, const float *dC,
                                           int64_t ldc, double *cophenetic, double *dispersion,
                                           void *stream);
+/* The same for `count` consensus matrices at once (matrix m at dC + m *
+ * stride elements, pitch ldc; the consensus matrices of a rank sweep, one per
+ * rank): cophenetic[m], dispersion[m] (host arrays of `count`).  The
+ * average-linkage trees of all matrices are built in one launch, one block
+ * each, so they run concurrently.  Uses count * p^2 doubles of context
+ * scratch. */
+nmfcu_status nmfcu_consensus_stats_batch_device(nmfcu_context *ctx, int32_t count, int64_t p,
+                                                const float *dC, int64_t ldc, int64_t stride,
+                                                double *cophenetic, double *dispersion,
+                                                void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Serving: continuous batching of independent factorisations              */

@@ -25,8 +25,10 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
 nmfcu_status default_context(int device, nmfcu_context **out);
 
 // A scratch buffer of the context that grows to at least `bytes` (slot
-// 0..17, one owner per slot; the contents survive between calls).
-constexpr int kContextSlots = 18;
+// 0..25, one owner per slot; the contents survive between calls).  Owners:
+// 0..12, 16, 17 batch.cu; 13..15 linkage.cu; 18..23 sparse.cu (serve.cu
+// uses the slots of its own contexts).
+constexpr int kContextSlots = 26;
 nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out);
 
 cudaStream_t context_stream(nmfcu_context *c);
@@ -35,6 +37,23 @@ int context_device(nmfcu_context *c);
 std::mutex &context_mutex(nmfcu_context *c);
 // Adds `launches` kernel launches to nmfcu_context_launch_count.
 void count_launches(nmfcu_context *c, int64_t launches);
+
+// Brackets the launches of one scope made by another translation unit for
+// the context's timing hooks (the kernel classes of
+// nmfcu_context_kernel_time) and its launch count.  The caller holds the
+// context's mutex.
+struct TimedScope {
+    nmfcu_context *c;
+    cudaStream_t s;
+    int kclass;
+    void *a;
+    TimedScope(nmfcu_context *c, cudaStream_t s, int kclass, int launches = 1);
+    ~TimedScope();
+    TimedScope(const TimedScope &) = delete;
+    TimedScope &operator=(const TimedScope &) = delete;
+};
+// Folds the recorded scopes into the per-class totals (waits for them).
+void drain_timing(nmfcu_context *c);
 
 // Device bytes the context holds now.
 size_t context_bytes(nmfcu_context *c);

@@ -29,6 +29,8 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <vector>
+#include <algorithm>
 
 #include "internal.h"
 
@@ -142,11 +144,9 @@ __device__ VI block_argmin(VI mine, VI *red) {
 // nearest-neighbour chain, one block.  Writes each merge's height and pair
 // count n_a n_b.  Every loop below ends: each merge takes at most p chain
 // extensions (a chain holds distinct clusters), and there are p - 1 merges.
-__global__ void __launch_bounds__(kT) nn_chain_average(double *__restrict__ D, int p,
-                                                       int *__restrict__ size,
-                                                       int *__restrict__ chain,
-                                                       double *__restrict__ height,
-                                                       double *__restrict__ npair) {
+__device__ void nn_chain_tree(double *__restrict__ D, int p, int *__restrict__ size,
+                              int *__restrict__ chain, double *__restrict__ height,
+                              double *__restrict__ npair) {
     __shared__ VI red[33];
     __shared__ int s_len;
     const int tid = threadIdx.x;
@@ -212,6 +212,21 @@ __global__ void __launch_bounds__(kT) nn_chain_average(double *__restrict__ D, i
     }
 }
 
+// One tree per block: block m builds the tree of matrix m (its distances,
+// sizes and chain `dstride` / `istride` elements after matrix m - 1's, its
+// merges `hstride` after).  The trees of a batch build concurrently on
+// different multiprocessors.
+__global__ void __launch_bounds__(kT) nn_chain_average(double *__restrict__ D, int p,
+                                                       int64_t dstride, int *__restrict__ size,
+                                                       int *__restrict__ chain, int64_t istride,
+                                                       double *__restrict__ height,
+                                                       double *__restrict__ npair,
+                                                       int64_t hstride) {
+    const int64_t m = blockIdx.x;
+    nn_chain_tree(D + m * dstride, p, size + m * istride, chain + m * istride,
+                  height + m * hstride, npair + m * hstride);
+}
+
 // out[0] = the cophenetic correlation from the merges (height, npair), the
 // sum of the distances (dsum) and of their squared deviations (dvar); 1 when
 // either side has no spread (the reference's convention).
@@ -237,6 +252,69 @@ __global__ void __launch_bounds__(kR) cophenetic_from_merges(
     }
 }
 
+// The statistics of `count` consensus matrices (matrix m at dC + m * stride),
+// the per-pair and dispersion sums one matrix at a time, the trees of all
+// matrices in one launch (one block each).
+nmfcu_status consensus_stats(nmfcu_context *ctx, int count, int64_t p, const float *dC,
+                             int64_t ldc, int64_t stride, double *cophenetic, double *dispersion,
+                             cudaStream_t s) {
+    const int sms = nmfcu_internal::context_sms(ctx);
+    const int B = sms * 8;
+    const size_t pp = (size_t)p * (size_t)p;
+    const size_t nd = 2 * (size_t)p + B + 8;  // doubles of one matrix: height, npair, part, stat
+    void *pD = nullptr, *pi = nullptr, *pd = nullptr;
+    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 13, sizeof(double) * pp * count, &pD));
+    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 14, sizeof(int) * 2 * (size_t)p * count, &pi));
+    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 15, sizeof(double) * nd * count, &pd));
+    double *D0 = static_cast<double *>(pD);
+    int *size0 = static_cast<int *>(pi);
+    double *dbl0 = static_cast<double *>(pd);
+    const double npairs = (double)p * (double)(p - 1) / 2.0;
+    const unsigned g = (unsigned)std::min<int64_t>(((int64_t)p * p + kR - 1) / kR, 4096);
+    int launches = 0;
+    for (int m = 0; m < count; m++) {
+        const float *C = dC + (size_t)m * stride;
+        double *D = D0 + pp * m;
+        double *part = dbl0 + nd * m + 2 * (size_t)p;
+        double *stat = part + B;  // [sum d, mean d, sum (d - mean)^2, dispersion, cophenetic]
+        distances_from_consensus<<<g, kR, 0, s>>>(C, ldc, (int)p, D);
+        pair_sums<<<B, kR, 0, s>>>(D, (int)p, nullptr, part);
+        finish_sum<<<1, kR, 0, s>>>(part, B, 1.0, stat);
+        finish_sum<<<1, kR, 0, s>>>(part, B, npairs > 0 ? 1.0 / npairs : 0.0, stat + 1);
+        pair_sums<<<B, kR, 0, s>>>(D, (int)p, stat + 1, part);
+        finish_sum<<<1, kR, 0, s>>>(part, B, 1.0, stat + 2);
+        dispersion_sums<<<B, kR, 0, s>>>(C, ldc, (int)p, part);
+        finish_sum<<<1, kR, 0, s>>>(part, B, 1.0 / ((double)p * (double)p), stat + 3);
+        launches += 8;
+    }
+    if (p >= 2) {
+        nn_chain_average<<<count, kT, 0, s>>>(D0, (int)p, (int64_t)pp, size0, size0 + p,
+                                              2 * p, dbl0, dbl0 + p, (int64_t)nd);
+        launches += 1;
+        for (int m = 0; m < count; m++) {
+            double *h = dbl0 + nd * m;
+            double *stat = h + 2 * (size_t)p + B;
+            cophenetic_from_merges<<<1, kR, 0, s>>>(h, h + p, (int)p - 1, stat, stat + 2, npairs,
+                                                    stat + 4);
+        }
+        launches += count;
+    }
+    NMFCU_CUDA_TRY(cudaGetLastError());
+    nmfcu_internal::count_launches(ctx, launches);
+    std::vector<double> host(5 * (size_t)count, 0.0);
+    for (int m = 0; m < count; m++) {
+        const double *stat = dbl0 + nd * m + 2 * (size_t)p + B;
+        NMFCU_CUDA_TRY(cudaMemcpyAsync(host.data() + 5 * m, stat, sizeof(double) * (p >= 2 ? 5 : 4),
+                                       cudaMemcpyDeviceToHost, s));
+    }
+    NMFCU_CUDA_TRY(cudaStreamSynchronize(s));
+    for (int m = 0; m < count; m++) {
+        dispersion[m] = host[5 * m + 3];
+        cophenetic[m] = p >= 2 ? host[5 * m + 4] : 1.0;
+    }
+    return NMFCU_OK;
+}
+
 }  // namespace
 
 extern "C" nmfcu_status nmfcu_consensus_stats_device(nmfcu_context *ctx, int64_t p,
@@ -250,41 +328,25 @@ extern "C" nmfcu_status nmfcu_consensus_stats_device(nmfcu_context *ctx, int64_t
     if (ldc < p) return fail(NMFCU_ERR_INVALID_ARG, "ldc must be >= p");
     std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
     nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const int sms = nmfcu_internal::context_sms(ctx);
-    const int B = sms * 8;
-    void *pD = nullptr, *pi = nullptr, *pd = nullptr;
-    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 13, sizeof(double) * (size_t)p * p, &pD));
-    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 14, sizeof(int) * 2 * (size_t)p, &pi));
-    NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 15, sizeof(double) * (2 * (size_t)p + B + 8), &pd));
-    double *D = static_cast<double *>(pD);
-    int *size = static_cast<int *>(pi), *chain = size + p;
-    double *height = static_cast<double *>(pd), *npair = height + p, *part = npair + p;
-    double *stat = part + B;  // [sum d, mean d, sum (d - mean)^2, dispersion, cophenetic]
-    const double npairs = (double)p * (double)(p - 1) / 2.0;
-    const unsigned g = (unsigned)std::min<int64_t>(((int64_t)p * p + kR - 1) / kR, 4096);
-    distances_from_consensus<<<g, kR, 0, s>>>(dC, ldc, (int)p, D);
-    pair_sums<<<B, kR, 0, s>>>(D, (int)p, nullptr, part);
-    finish_sum<<<1, kR, 0, s>>>(part, B, 1.0, stat);
-    finish_sum<<<1, kR, 0, s>>>(part, B, npairs > 0 ? 1.0 / npairs : 0.0, stat + 1);
-    pair_sums<<<B, kR, 0, s>>>(D, (int)p, stat + 1, part);
-    finish_sum<<<1, kR, 0, s>>>(part, B, 1.0, stat + 2);
-    dispersion_sums<<<B, kR, 0, s>>>(dC, ldc, (int)p, part);
-    finish_sum<<<1, kR, 0, s>>>(part, B, 1.0 / ((double)p * (double)p), stat + 3);
-    int launches = 9;
-    if (p >= 2) {
-        nn_chain_average<<<1, kT, 0, s>>>(D, (int)p, size, chain, height, npair);
-        cophenetic_from_merges<<<1, kR, 0, s>>>(height, npair, (int)p - 1, stat, stat + 2, npairs,
-                                                stat + 4);
-        launches += 2;
-    }
-    NMFCU_CUDA_TRY(cudaGetLastError());
-    nmfcu_internal::count_launches(ctx, launches);
-    double host[5] = {0, 0, 0, 0, 1.0};
-    NMFCU_CUDA_TRY(cudaMemcpyAsync(host, stat, sizeof(double) * (p >= 2 ? 5 : 4),
-                                   cudaMemcpyDeviceToHost, s));
-    NMFCU_CUDA_TRY(cudaStreamSynchronize(s));
-    *dispersion = host[3];
-    *cophenetic = host[4];
-    return NMFCU_OK;
+    return consensus_stats(ctx, 1, p, dC, ldc, 0, cophenetic, dispersion,
+                           static_cast<cudaStream_t>(stream));
+}
+
+extern "C" nmfcu_status nmfcu_consensus_stats_batch_device(nmfcu_context *ctx, int32_t count,
+                                                           int64_t p, const float *dC,
+                                                           int64_t ldc, int64_t stride,
+                                                           double *cophenetic,
+                                                           double *dispersion, void *stream) {
+    using nmfcu_internal::fail;
+    if (!ctx || !dC || !cophenetic || !dispersion)
+        return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    if (count < 1) return fail(NMFCU_ERR_INVALID_ARG, "count must be >= 1");
+    if (p < 1 || p > 200000) return fail(NMFCU_ERR_INVALID_ARG, "p must be in [1, 200000]");
+    if (ldc < p) return fail(NMFCU_ERR_INVALID_ARG, "ldc must be >= p");
+    if (count > 1 && stride < ldc * p)
+        return fail(NMFCU_ERR_INVALID_ARG, "stride must be >= ldc * p");
+    std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
+    nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
+    return consensus_stats(ctx, count, p, dC, ldc, stride, cophenetic, dispersion,
+                           static_cast<cudaStream_t>(stream));
 }

@@ -1627,6 +1627,26 @@ int context_device(nmfcu_context *c) { return c->device; }
 std::mutex &context_mutex(nmfcu_context *c) { return c->mu; }
 void count_launches(nmfcu_context *c, int64_t launches) { c->launch_total += launches; }
 
+TimedScope::TimedScope(nmfcu_context *c_, cudaStream_t s_, int k, int launches)
+    : c(c_), s(s_), kclass(k), a(nullptr) {
+    c->launch_total += launches;
+    if (c->timing) {
+        cudaEvent_t e = c->get_event();
+        cudaEventRecord(e, s);
+        a = e;
+    }
+}
+TimedScope::~TimedScope() {
+    if (c->timing && a) {
+        cudaEvent_t b = c->get_event();
+        cudaEventRecord(b, s);
+        c->events.push_back({static_cast<cudaEvent_t>(a), b, kclass});
+    }
+}
+void drain_timing(nmfcu_context *c) {
+    if (c->timing) c->drain_timing();
+}
+
 size_t context_bytes(nmfcu_context *c) {
     size_t t = 0;
     for (const DevBuf *b : {&c->V64, &c->V32, &c->W, &c->H, &c->part, &c->pg, &c->ps, &c->Gw,

@@ -246,6 +246,18 @@ def _regularisation(method: str, sparsity: float, smoothness: float):
     return 0.0, 0.0, 0.0, 0.0
 
 
+# Methods that run on a sparse V (nmfcu_run_csr).
+_SPARSE_METHODS = {"lee", "brunet", "hals", "dnmf"}
+
+
+def _is_sparse(V) -> bool:
+    try:
+        import scipy.sparse as sp
+    except ImportError:  # pragma: no cover - scipy ships with the engine's deps
+        return False
+    return sp.issparse(V)
+
+
 def _prepare(V, rank, method, W0, H0, seed, offset, weight, sparsity, smoothness):
     """nmf()'s argument handling before the native call, in the reference's
     order (python/nmf_rs/__init__.py:487-538): method aliases, V >= 0, a
@@ -255,12 +267,27 @@ def _prepare(V, rank, method, W0, H0, seed, offset, weight, sparsity, smoothness
         raise ValueError(
             f"unknown method '{method}'. supported: brunet, lee, offset, nsNMF "
             "(plus aliases KL/Frobenius/ns).")
-    V_arr = _f64_c(V, "V")
-    if (V_arr < 0).any():
-        raise ValueError("V must be non-negative.")
+    if _is_sparse(V):
+        # Engine extension: a scipy.sparse V stays sparse (the stored entries
+        # are all the loop reads); the reference densifies it here.
+        if method_norm not in _SPARSE_METHODS:
+            raise NotImplementedError(
+                f"method '{method}' needs a dense V; a sparse V runs "
+                + ", ".join(sorted(_SPARSE_METHODS)))
+        V_arr = V.tocsr().astype(np.float64)
+        if V_arr.ndim != 2:
+            raise ValueError(f"V must be 2-D, got shape {V_arr.shape}")
+        if (V_arr.data < 0).any():
+            raise ValueError("V must be non-negative.")
+        vmax = float(V_arr.max()) if V_arr.shape[0] * V_arr.shape[1] else 1.0
+    else:
+        V_arr = _f64_c(V, "V")
+        if (V_arr < 0).any():
+            raise ValueError("V must be non-negative.")
+        vmax = None
     n, p = V_arr.shape
     if W0 is None or H0 is None:
-        W0_, H0_ = random_init(V_arr, rank, seed=seed)
+        W0_, H0_ = random_init(V_arr, rank, seed=seed, max_value=vmax)
         W0 = W0_ if W0 is None else W0
         H0 = H0_ if H0 is None else H0
     W0 = _f64_c(W0, "W0")
@@ -302,11 +329,14 @@ def nmf(V: np.ndarray, rank: int, method: str = "brunet", *, W0: Optional[np.nda
     Engine extensions: ``precision='fp32'`` stores V in f32 for the two V
     contractions (f32 products, f64 reductions, f64 updates/objective/stop)
     and runs the last ``refine_iters`` iterations in full f64; ``device``
-    selects the GPU.
+    selects the GPU.  A ``scipy.sparse`` V (any format; CSR is used) is
+    factorised without densifying it, for lee, brunet, hals and dnmf in FP64:
+    the passes read only its stored entries.
     """
     method_norm, V_arr, W0, H0, offset_arr, weight_arr, (sh, sw, gh, gw) = _prepare(
         V, rank, method, W0, H0, seed, offset, weight, sparsity, smoothness)
-    out = _native.py_nmf_run(
+    run = _native.py_nmf_run_csr if _is_sparse(V_arr) else _native.py_nmf_run
+    out = run(
         method_norm, V_arr, W0, H0, int(max_iter), eps=float(eps), rescale=bool(rescale),
         theta=float(theta), offset=offset_arr, weight=weight_arr, sparsity_h=sh,
         sparsity_w=sw, smoothness_h=gh, smoothness_w=gw, stop=stop,

@@ -102,6 +102,10 @@ SIGNATURES = {
     "nmfcu_consensus_stats_device": (_i32, [ctypes.c_void_p, _i64, ctypes.c_void_p, _i64,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
+    "nmfcu_consensus_stats_batch_device": (_i32, [ctypes.c_void_p, _i32, _i64, ctypes.c_void_p,
+                                                  _i64, _i64, ctypes.POINTER(ctypes.c_double),
+                                                  ctypes.POINTER(ctypes.c_double),
+                                                  ctypes.c_void_p]),
     "nmfcu_shard_reduce_len": (_i64, [_i64, _i64]),
     "nmfcu_shard_create": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64, _i64,
                                   ctypes.c_void_p, _i64, ctypes.c_void_p, ctypes.c_void_p,
@@ -141,6 +145,13 @@ SIGNATURES = {
     "nmfcu_server_cancel": (_i32, [ctypes.c_void_p, _i64]),
     "nmfcu_server_get_stats": (_i32, [ctypes.c_void_p, ctypes.POINTER(ServerStats)]),
     "nmfcu_server_reset_stats": (_i32, [ctypes.c_void_p]),
+    "nmfcu_run_csr": (_i32, [ctypes.POINTER(Options), _i64, _i64, _i64, _i64, _i64p,
+                             ctypes.POINTER(_i32), _dp, _dp, _dp, _dp, _dp, _dp, _i64, _i64p,
+                             _i64p]),
+    "nmfcu_run_csr_device": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64, _i64,
+                                    _i64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64p,
+                                    _i64p, ctypes.c_void_p]),
     "nmfcu_objective_noalloc": (_i32, [_i32, _i64, _i64, _i64, ctypes.c_void_p, _i64,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                        ctypes.c_void_p]),
@@ -231,13 +242,18 @@ def default_options() -> Options:
     return o
 
 
-def _shapes(v: np.ndarray, w: np.ndarray, h: np.ndarray) -> tuple[int, int, int]:
-    n, p = v.shape
+def _shapes_of(vshape: tuple, w: np.ndarray, h: np.ndarray) -> tuple[int, int, int]:
+    n, p = vshape
     r = w.shape[1]
     if w.shape[0] != n or h.shape != (r, p):
         raise ValueError(
-            f"shape mismatch: V {v.shape}, W {w.shape}, H {h.shape} (need n x r and r x p)")
-    return n, p, r
+            f"shape mismatch: V {tuple(vshape)}, W {w.shape}, H {h.shape} "
+            "(need n x r and r x p)")
+    return int(n), int(p), int(r)
+
+
+def _shapes(v: np.ndarray, w: np.ndarray, h: np.ndarray) -> tuple[int, int, int]:
+    return _shapes_of(v.shape, w, h)
 
 
 # ---------------------------------------------------------------------------
@@ -344,6 +360,40 @@ def py_nmf_run(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
     return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}
 
 
+def csr_arrays(V):
+    """(indptr int64, indices int32, data f64, (n, p)) of a scipy sparse V in
+    canonical CSR form (duplicates summed, indices sorted), C-contiguous."""
+    import scipy.sparse as sp
+
+    m = sp.csr_matrix(V, dtype=np.float64, copy=True)
+    m.sum_duplicates()
+    m.sort_indices()
+    if m.nnz > np.iinfo(np.int32).max:
+        raise NotImplementedError("a sparse V holds at most 2^31 - 1 stored entries")
+    return (np.ascontiguousarray(m.indptr, dtype=np.int64),
+            np.ascontiguousarray(m.indices, dtype=np.int32),
+            np.ascontiguousarray(m.data, dtype=np.float64), m.shape)
+
+
+def py_nmf_run_csr(algo: str, v, w0, h0, max_iter: int, **kw) -> dict:
+    """py_nmf_run for a sparse V (scipy.sparse, any format): the loop over its
+    stored entries (nmfcu_run_csr), lee / brunet / hals / dnmf in FP64.  Same
+    keywords and result as :func:`py_nmf_run`; the reference densifies V
+    instead (python/nmf_rs/__init__.py:495)."""
+    indptr, indices, data, (n, p) = csr_arrays(v)
+    o, _, w0, h0, n, p, r = build_run_options(algo, None, w0, h0, max_iter, shape=(n, p), **kw)
+    W = np.empty((n, r), dtype=np.float64)
+    H = np.empty((r, p), dtype=np.float64)
+    cap = o.max_iter + 1
+    dev = np.empty(cap, dtype=np.float64)
+    nd, ni = _i64(0), _i64(0)
+    check(load().nmfcu_run_csr(
+        ctypes.byref(o), n, p, r, int(data.size),
+        indptr.ctypes.data_as(_i64p), indices.ctypes.data_as(ctypes.POINTER(_i32)), _ptr(data),
+        _ptr(w0), _ptr(h0), _ptr(W), _ptr(H), _ptr(dev), cap, ctypes.byref(nd), ctypes.byref(ni)))
+    return {"W": W, "H": H, "n_iter": int(ni.value), "deviances": list(dev[: nd.value])}
+
+
 def build_run_options(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
                       rescale: bool = True, theta: float = 0.5, offset=None, weight=None,
                       sparsity_h: float = 0.0, sparsity_w: float = 0.0,
@@ -351,10 +401,12 @@ def build_run_options(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
                       stop: str = "max_iter", stationary_th: float = 2.220446049250313e-16,
                       check_interval: int = 50, check_niter: int = 10,
                       num_threads: Optional[int] = None, precision: str = "fp64",
-                      refine_iters: int = 2, device: int = 0):
+                      refine_iters: int = 2, device: int = 0, shape=None):
     """py_nmf_run's argument handling (lib.rs:1934-1971): the checks in the
     reference's order and the ``nmfcu_options`` they produce.  Returns
-    ``(options, V, W0, H0, n, p, r)`` with the arrays as C-contiguous f64."""
+    ``(options, V, W0, H0, n, p, r)`` with the arrays as C-contiguous f64.
+    With ``shape=(n, p)`` V is not given (a sparse V) and None is returned
+    in its place."""
     o = default_options()
     o.method = parse_method(algo)            # Algo::from_str, lib.rs:1956
     o.stop = parse_stop(stop)                # Stop::from_str, lib.rs:1957
@@ -362,8 +414,12 @@ def build_run_options(algo: str, v, w0, h0, max_iter: int, *, eps: float = 1e-9,
         raise ValueError("method='lsnmf' requires a `weight` matrix of the same shape as V")
     if num_threads is not None and int(num_threads) < 0:
         raise OverflowError("num_threads must be a non-negative integer")
-    v, w0, h0 = _f64(v, "V"), _f64(w0, "W0"), _f64(h0, "H0")
-    n, p, r = _shapes(v, w0, h0)
+    w0, h0 = _f64(w0, "W0"), _f64(h0, "H0")
+    if shape is None:
+        v = _f64(v, "V")
+        n, p, r = _shapes(v, w0, h0)
+    else:
+        n, p, r = _shapes_of(tuple(shape), w0, h0)
     try:
         o.precision = PRECISIONS[str(precision).lower()]
     except KeyError:

@@ -33,6 +33,7 @@ __all__ = [
     "cophenetic_correlation",
     "dispersion_coefficient",
     "consensus_stats",
+    "consensus_stats_batch",
 ]
 
 
@@ -91,6 +92,31 @@ def consensus_stats(C, ctx=None) -> tuple[float, float]:
         if own:
             ctx.close()
     return float(coph.value), float(disp.value)
+
+
+def consensus_stats_batch(C, ctx=None) -> list[tuple[float, float]]:
+    """``consensus_stats`` of every matrix of a stacked (count x p x p) f32
+    device tensor, with the average-linkage trees of all of them built
+    concurrently (``nmfcu_consensus_stats_batch_device``)."""
+    count, p, p2 = C.shape
+    if p != p2:
+        raise ValueError(f"consensus matrices must be square, got {tuple(C.shape)}")
+    C = C.contiguous()
+    own = ctx is None
+    if own:
+        ctx = _native.Context(C.device.index or 0)
+    coph = (ctypes.c_double * count)()
+    disp = (ctypes.c_double * count)()
+    try:
+        import torch
+
+        _native.check(_native.load().nmfcu_consensus_stats_batch_device(
+            ctx.handle, count, p, ctypes.c_void_p(C.data_ptr()), p, p * p, coph, disp,
+            ctypes.c_void_p(torch.cuda.current_stream(C.device).cuda_stream)))
+    finally:
+        if own:
+            ctx.close()
+    return [(float(coph[m]), float(disp[m])) for m in range(count)]
 
 
 def dispersion_coefficient(consensus: np.ndarray) -> float:
@@ -228,18 +254,20 @@ def consensus_sweep(V: np.ndarray, ranks: Iterable[int] = range(2, 11), n_runs: 
             off += r
     torch.cuda.synchronize(dev)
     out = {"per_rank": {}, "solve_seconds": time.perf_counter() - t0}
-    cons = torch.empty((p, p), dtype=torch.float32, device=dev)
+    cons = torch.empty((len(ranks), p, p), dtype=torch.float32, device=dev)
     t1 = time.perf_counter()
     mats, stats = {}, {}
     for ci, k in enumerate(ranks):
         sel = np.arange(ci * n_runs, (ci + 1) * n_runs, dtype=np.int32)
         _native.check(lib.nmfcu_consensus_device(
             ctx.handle, p, len(rk), _ranks_ptr(rk), ctypes.c_void_p(dH.data_ptr()), len(sel),
-            _ranks_ptr(sel), ctypes.c_void_p(cons.data_ptr()),
+            _ranks_ptr(sel), ctypes.c_void_p(cons[ci].data_ptr()),
             ctypes.c_void_p(stream.cuda_stream)))
-        if metrics:
-            stats[k] = consensus_stats(cons, ctx)
-        mats[k] = cons.cpu().numpy()
+    if metrics:
+        for k, st in zip(ranks, consensus_stats_batch(cons, ctx)):
+            stats[k] = st
+    for ci, k in enumerate(ranks):
+        mats[k] = cons[ci].cpu().numpy()
     torch.cuda.synchronize(dev)
     out["consensus_seconds"] = time.perf_counter() - t1
     for k in ranks:

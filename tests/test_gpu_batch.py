@@ -184,6 +184,21 @@ def test_consensus_stats_pitched_input():
     assert a == b
 
 
+def test_consensus_stats_batch_equals_one_at_a_time():
+    """Several matrices' trees built concurrently (one block each) give the
+    same bits as one matrix at a time, and match scipy."""
+    import torch
+
+    from nmf_rs import consensus
+
+    mats = [_tied_consensus(700, 32, k, 10 + k, 0.3) for k in (2, 3, 5, 8)]
+    stack = torch.from_numpy(np.stack(mats)).cuda()
+    got = consensus.consensus_stats_batch(stack)
+    for m, C in enumerate(mats):
+        assert got[m] == consensus.consensus_stats(torch.from_numpy(C).cuda())
+        assert got[m][0] == pytest.approx(consensus.cophenetic_correlation(C), abs=1e-10)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32"])
 def test_batch_shapes_agree_and_autotune(precision):
     # The kernel shapes the autotuner picks from regroup solves per CTA; a
