@@ -101,7 +101,7 @@ def parse():
     ap.add_argument("--form", choices=["iterate", "consensus", "serve", "nndsvd", "shard",
                                        "sparse"],
                     default="iterate")
-    ap.add_argument("--requests", type=int, default=400, help="serve: requests in the stream")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
     ap.add_argument("--slots", type=int, default=4, help="serve: server slots")
     ap.add_argument("--load", type=float, default=0.8,
                     help="serve: Poisson arrival rate as a fraction of the measured capacity")

@@ -30,6 +30,11 @@ extern "C" {
 #define NMFCU_ABI_VERSION 1
 /* Largest factorisation rank the GPU kernels are built for. */
 #define NMFCU_MAX_RANK 32
+/* Ranks above NMFCU_MAX_RANK, up to NMFCU_MAX_WIDE_RANK, run lee, brunet, hals
+ * and dnmf in FP64 through nmfcu_run / nmfcu_run_device: the V contractions
+ * as streaming passes over 32-rank chunks (one pass over V each), the rest in
+ * kernels with the rank as a run-time value. */
+#define NMFCU_MAX_WIDE_RANK 256
 
 typedef enum nmfcu_status {
     NMFCU_OK = 0,
@@ -227,9 +232,9 @@ nmfcu_status nmfcu_run_device(nmfcu_context *ctx, const nmfcu_options *opt, int6
  * FP64 only.
  *   indptr   n + 1 row offsets (indptr[0] = 0, non-decreasing, indptr[n] = nnz)
  *   indices  nnz column indices in [0, p), data nnz values (f64, >= 0): the
- *            canonical CSR of V -- no duplicate (row, column) pairs (a
- *            duplicate would enter brunet's objective twice); the order of
- *            a row's entries only changes rounding.
+ *            canonical CSR of V -- each row's column indices strictly
+ *            increasing (sorted, no duplicates); anything else is refused
+ *            with NMFCU_ERR_INVALID_ARG.
  * W0, H0, W, H, deviances, n_deviances, n_iter as in nmfcu_run.  nnz is at
  * most 2^31 - 1.  The library keeps a column-sorted (CSC) copy of V for the
  * H step on the device for the run (12 bytes per stored entry).
@@ -248,6 +253,22 @@ nmfcu_status nmfcu_run_csr_device(nmfcu_context *ctx, const nmfcu_options *opt, 
                                   const int32_t *d_indices, const double *d_data, double *dW,
                                   double *dH, double *d_dev, int64_t *n_deviances,
                                   int64_t *n_iter, void *stream);
+
+/*
+ * nmfcu_run_offset_device -- nmfcu_run_offset on device pointers, enqueued on
+ * `stream` (py_nmf_run with method "offset", lib.rs:2023-2037, 2163-2165):
+ * the arguments of nmfcu_run_device plus d_offset0 (n doubles on the device,
+ * the `offset` keyword; NULL: rowMeans(V), lib.rs:1667-1679) and d_offset (n
+ * doubles on the device, receives the final offsets, the result dict's
+ * "offset" entry).  opt->method must be NMFCU_OFFSET; the f64 V is needed
+ * (dV, or dV64 beside an f32 dV) for the row sums the offset update uses.
+ */
+nmfcu_status nmfcu_run_offset_device(nmfcu_context *ctx, const nmfcu_options *opt, int64_t n,
+                                     int64_t p, int64_t r, const void *dV, int32_t v_dtype,
+                                     int64_t ldv, const double *dV64, int64_t ldv64, double *dW,
+                                     double *dH, const double *d_offset0, double *d_offset,
+                                     double *d_dev, int64_t *n_deviances, int64_t *n_iter,
+                                     void *stream);
 
 /*
  * nmfcu_v_product_device -- one V contraction of the randomized range finder
@@ -447,6 +468,17 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
                                  int64_t p, int64_t r, const double *V, int64_t ldv,
                                  const double *W0, const double *H0, double *W, double *H,
                                  double *deviances, int64_t dev_cap, int64_t *request_id);
+/* nmfcu_server_submit for the offset method (opt->method NMFCU_OFFSET): the
+ * nmfcu_run_offset of a served request.  offset0 (n doubles, host; NULL:
+ * rowMeans(V)) is read when the request starts, offset (n doubles, host)
+ * receives the final row offsets; both stay owned by the caller until
+ * nmfcu_server_wait has returned for the request. */
+nmfcu_status nmfcu_server_submit_offset(nmfcu_server *srv, const nmfcu_options *opt, int64_t n,
+                                        int64_t p, int64_t r, const double *V, int64_t ldv,
+                                        const double *W0, const double *H0,
+                                        const double *offset0, double *W, double *H,
+                                        double *offset, double *deviances, int64_t dev_cap,
+                                        int64_t *request_id);
 /* state: 0 queued, 1 running, 2 done. */
 nmfcu_status nmfcu_server_poll(nmfcu_server *srv, int64_t request_id, int32_t *state);
 /* Waits up to timeout_ms (< 0: no limit) and returns the request's own

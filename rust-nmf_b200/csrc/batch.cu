@@ -38,20 +38,27 @@ constexpr int kRowChunk = 64;      // W rows staged per chunk (H step)
 constexpr int kPrefetch = 4;       // V rows in flight per thread (H step)
 
 // Per element type: a thread owns CPT adjacent columns (H step) or rows
-// (W step) of V, held in one "lane pack" P.  f32 packs two (float2, one
-// FFMA2 updates both), so a W value times an H pair, or an H value times a
-// W pair, is one instruction and the per-element ratio is computed for two
-// elements at once; f64 owns one (DFMA).
+// (W step) of V, held in one "lane pack" P.  f32 packs four as two float2
+// halves (one FFMA2 updates each half), so a staged factor value times an
+// H (or W) pack is two instructions that share the value's register pair;
+// the staged factor sits in shared memory as a duplicated pair (SV), so
+// one 128-bit load brings two values for eight columns' worth of FFMA2.
+// f64 owns one column (DFMA).
+struct F4 {
+    float2 a, b;  // columns 0, 1 and 2, 3
+};
 template <typename T>
 struct BTraits;
 template <>
 struct BTraits<float> {
-    using P = float2;
-    static constexpr int CPT = 2;
+    using P = F4;
+    using SV = float2;  // a staged value in shared memory
+    static constexpr int CPT = 4;
 };
 template <>
 struct BTraits<double> {
     using P = double;
+    using SV = double;
     static constexpr int CPT = 1;
 };
 
@@ -67,8 +74,8 @@ struct BShapes;
 template <>
 struct BShapes<float> {
     static constexpr int kN = 3;
-    static constexpr int comp[kN] = {12, 8, 16};
-    static constexpr int min_blocks[kN] = {4, 5, 3};
+    static constexpr int comp[kN] = {6, 4, 8};
+    static constexpr int min_blocks[kN] = {4, 4, 4};  // ranks 1..8; 9..16: min_blocks_for
 };
 template <>
 struct BShapes<double> {
@@ -87,13 +94,21 @@ constexpr int kMaxRow = 16;             // >= ROW for every (T, R, COMP)
 template <typename T>
 constexpr int kTile = kThreads * BTraits<T>::CPT;  // columns / rows per CTA
 
-__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// A staged value (SV) times a pack plus a pack.
+__device__ __forceinline__ F4 pfma(float2 s, F4 b, F4 c) {
+    return F4{__ffma2_rn(s, b.a, c.a), __ffma2_rn(s, b.b, c.b)};
+}
 __device__ __forceinline__ double pfma(double a, double b, double c) { return fma(a, b, c); }
-__device__ __forceinline__ float2 pdup(float x) { return make_float2(x, x); }
-__device__ __forceinline__ double pdup(double x) { return x; }
-__device__ __forceinline__ void pzero(float2 &x) { x = make_float2(0.f, 0.f); }
+__device__ __forceinline__ float2 sdup(float x) { return make_float2(x, x); }
+__device__ __forceinline__ double sdup(double x) { return x; }
+__device__ __forceinline__ void pzero(F4 &x) {
+    x.a = make_float2(0.f, 0.f);
+    x.b = make_float2(0.f, 0.f);
+}
 __device__ __forceinline__ void pzero(double &x) { x = 0.0; }
-__device__ __forceinline__ float &plane(float2 &a, int c) { return c ? a.y : a.x; }
+__device__ __forceinline__ float &plane(F4 &a, int c) {
+    return c == 0 ? a.a.x : c == 1 ? a.a.y : c == 2 ? a.b.x : a.b.y;
+}
 __device__ __forceinline__ double &plane(double &a, int) { return a; }
 
 // The brunet ratio V / (WH), 0 where WH == 0 (lib.rs:93-99).  f32 uses the
@@ -103,8 +118,9 @@ __device__ __forceinline__ float ratio1(float v, float wh) {
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(wh));
     return (wh != 0.f) ? v * r : 0.f;
 }
-__device__ __forceinline__ float2 ratio(float2 v, float2 wh) {
-    return make_float2(ratio1(v.x, wh.x), ratio1(v.y, wh.y));
+__device__ __forceinline__ F4 ratio(F4 v, F4 wh) {
+    return F4{make_float2(ratio1(v.a.x, wh.a.x), ratio1(v.a.y, wh.a.y)),
+              make_float2(ratio1(v.b.x, wh.b.x), ratio1(v.b.y, wh.b.y))};
 }
 // f64: v * (1 / wh) with the reciprocal from the hardware approximation
 // (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
@@ -150,8 +166,8 @@ struct MuArgs {
 // stores of the W step spread over the banks and rows stay 16-B aligned.
 template <typename T>
 struct BSmem {
-    using P = typename BTraits<T>::P;
-    P S[kRowChunk][kMaxRow + 2];
+    using SV = typename BTraits<T>::SV;
+    SV S[kRowChunk][kMaxRow + 2];
     int off[kMaxRow];  // stacked offset per solve (-1: none)
 };
 
@@ -234,7 +250,7 @@ __device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
             const int e = t * kThreads + threadIdx.x;
             int rr, c;
             stage_index(e, rr, c);
-            if (e < kRowChunk * ROW) sm.S[rr][c] = pdup(spre[t]);
+            if (e < kRowChunk * ROW) sm.S[rr][c] = sdup(spre[t]);
         }
         __syncthreads();
         if (base + kRowChunk < rows) load_s(base + kRowChunk);
@@ -256,7 +272,7 @@ __device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
             // Rows past the chunk's end read zero staged rows and a = 0: no-ops.
 #pragma unroll
             for (int q = 0; q < kPrefetch; q++) {
-                const P *sr = sm.S[r0 + q];
+                const typename BTraits<T>::SV *sr = sm.S[r0 + q];
 #pragma unroll
                 for (int s = 0; s < NS; s++) {
                     P d;
@@ -302,8 +318,18 @@ struct BBucket {
 };
 constexpr int bucket_of(int R) { return R <= kBucketSplit ? 0 : 1; }
 
+// CTAs a multiprocessor keeps resident (the register cap) for a bucket and
+// shape.  f32 carries four columns a thread: ranks 9..16 hold up to 16
+// components in x and acc (128 registers of packs) and get two CTAs; the
+// low bucket keeps four.
+template <typename T, int B, int SHAPE>
+constexpr int min_blocks_for() {
+    if constexpr (sizeof(T) == 4) return B == 0 ? 4 : 2;
+    return BShapes<T>::min_blocks[SHAPE];
+}
+
 template <typename T, int B, int SHAPE, bool kComponentFast>
-__global__ void __launch_bounds__(kThreads, (BShapes<T>::min_blocks[SHAPE]))
+__global__ void __launch_bounds__(kThreads, (min_blocks_for<T, B, SHAPE>()))
     batch_mu(MuArgs<T> a, const int *__restrict__ off, const BItem *__restrict__ items) {
     __shared__ __align__(16) BSmem<T> sm;
     const BItem it = items[blockIdx.x];

@@ -21,6 +21,22 @@ nmfcu_status cuda_fail(cudaError_t e, const char *what);
 // The option checks every run entry point applies (method, stop, sizes...).
 nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r);
 
+// validate_options with another rank limit.
+nmfcu_status validate_options_rank(const nmfcu_options *o, int64_t n, int64_t p, int64_t r,
+                                   int64_t max_rank);
+// Ranks above NMFCU_MAX_RANK (wide.cu): the option checks, and the FP64 loop
+// on a device V (16-byte aligned base and pitch) with the factors copied in
+// with `in_kind` and out with `out_kind`.  The caller holds the context's
+// mutex with its device current.
+nmfcu_status wide_validate(const nmfcu_options *o, int64_t n, int64_t p, int64_t r);
+nmfcu_status wide_run(nmfcu_context *c, const nmfcu_options *o, int64_t n, int64_t p, int64_t r,
+                      const double *V, int64_t ldv, const double *W0, const double *H0,
+                      double *W, double *H, cudaMemcpyKind in_kind, cudaMemcpyKind out_kind,
+                      double *d_dev, cudaStream_t s, int64_t *n_dev, int64_t *n_iter);
+// Allocates the streaming passes' workspace (and the run state) of an
+// n x p problem at the largest streaming rank.
+nmfcu_status context_prepare(nmfcu_context *c, int64_t n, int64_t p);
+
 // The per-device context behind the host-pointer API (created on first use).
 nmfcu_status default_context(int device, nmfcu_context **out);
 
@@ -54,6 +70,19 @@ struct TimedScope {
 };
 // Folds the recorded scopes into the per-class totals (waits for them).
 void drain_timing(nmfcu_context *c);
+
+// out = V X (trans 0) or V^T X (trans 1), V n x p f64 (pitch ldv), X with
+// `l` columns, by the FP64 streaming passes in column chunks of at most
+// NMFCU_MAX_RANK (one pass over V each).  The caller holds the context's
+// mutex with its device current.  reset_state: clear the context's run state
+// first; otherwise the passes do no work once the state says stopped.
+// sync: wait for the stream and report a pass that gave up waiting.
+nmfcu_status v_product_locked(nmfcu_context *c, int32_t trans, int64_t n, int64_t p, int64_t l,
+                              const double *dV, int64_t ldv, const double *dX, int64_t ldx,
+                              double *dOut, int64_t ldo, cudaStream_t s, bool reset_state,
+                              bool sync);
+// The context's device run state (an nmfcu::RunState).
+void *context_state(nmfcu_context *c);
 
 // Device bytes the context holds now.
 size_t context_bytes(nmfcu_context *c);

@@ -1142,16 +1142,17 @@ nmfcu_status ensure_workspace(nmfcu_context *c, const Plan &pl, bool need_f32,
     return NMFCU_OK;
 }
 
-nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r) {
+nmfcu_status validate_options_rank(const nmfcu_options *o, int64_t n, int64_t p, int64_t r,
+                                   int64_t max_rank) {
     if (!o) return fail(NMFCU_ERR_INVALID_ARG, "options pointer is NULL");
     if (n < 0 || p < 0) return fail(NMFCU_ERR_INVALID_ARG, "negative matrix dimension");
     if (r < 1) return fail(NMFCU_ERR_INVALID_ARG, "rank must be >= 1");
     if (n > INT32_MAX || p > INT32_MAX)
         return fail(NMFCU_ERR_UNSUPPORTED, "n and p must each fit in 32 bits");
-    if (r > NMFCU_MAX_RANK)
+    if (r > max_rank)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "rank " + std::to_string(r) + " exceeds the largest built rank (" +
-                        std::to_string(NMFCU_MAX_RANK) + ")");
+                        std::to_string(max_rank) + ")");
     switch (o->method) {
         case NMFCU_BRUNET:
         case NMFCU_LEE:
@@ -1180,6 +1181,10 @@ nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int6
         return fail(NMFCU_ERR_INVALID_ARG, "check_interval / check_niter must be >= 0");
     if (o->refine_iters < 0) return fail(NMFCU_ERR_INVALID_ARG, "refine_iters must be >= 0");
     return NMFCU_OK;
+}
+
+nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r) {
+    return validate_options_rank(o, n, p, r, NMFCU_MAX_RANK);
 }
 
 // Runs the loop on prepared device buffers; fills n_iter / n_dev.
@@ -1613,6 +1618,13 @@ nmfcu_status default_context(int device, nmfcu_context **out) { return ::default
 nmfcu_status validate_options(const nmfcu_options *o, int64_t n, int64_t p, int64_t r) {
     return ::validate_options(o, n, p, r);
 }
+nmfcu_status validate_options_rank(const nmfcu_options *o, int64_t n, int64_t p, int64_t r,
+                                   int64_t max_rank) {
+    return ::validate_options_rank(o, n, p, r, max_rank);
+}
+nmfcu_status context_prepare(nmfcu_context *c, int64_t n, int64_t p) {
+    return ensure_workspace(c, make_plan(n, p, NMFCU_MAX_RANK, c->sms), false);
+}
 
 nmfcu_status context_buffer(nmfcu_context *c, int slot, size_t bytes, void **out) {
     if (slot < 0 || slot >= kContextSlots) return fail(NMFCU_ERR_INVALID_ARG, "bad scratch slot");
@@ -1814,6 +1826,38 @@ nmfcu_status setup_method(nmfcu_context *c, const Plan &pl, const nmfcu_options 
     return NMFCU_OK;
 }
 
+// nmfcu_run for a rank above NMFCU_MAX_RANK (nmfcu_internal::wide_run).
+nmfcu_status run_host_wide(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                           const double *V, const double *W0, const double *H0, double *W,
+                           double *H, double *deviances, int64_t deviances_cap,
+                           int64_t *n_deviances, int64_t *n_iter) {
+    NMF_TRY(nmfcu_internal::wide_validate(opt, n, p, r));
+    if (!V || !W0 || !H0 || !W || !H || !n_deviances || !n_iter)
+        return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    const bool stat = opt->stop == NMFCU_STOP_STATIONARY;
+    if (stat && (!deviances || deviances_cap < opt->max_iter + 1))
+        return fail(NMFCU_ERR_INVALID_ARG, "deviances must hold max_iter + 1 values");
+    nmfcu_context *c = nullptr;
+    NMF_TRY(default_context(opt->device, &c));
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard dg(c->device);
+    cudaStream_t s = c->own_stream;
+    if (stat) NMF_TRY(c->dev.ensure(sizeof(double) * (size_t)(opt->max_iter + 1)));
+    int64_t ldv = 0;
+    NMF_TRY(upload_v(c, V, n, p, &ldv, s));
+    int64_t nd = 0, ni = 0;
+    NMF_TRY(nmfcu_internal::wide_run(c, opt, n, p, r, c->V64.as<double>(), ldv, W0, H0, W, H,
+                                     cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost,
+                                     stat ? c->dev.as<double>() : nullptr, s, &nd, &ni));
+    if (stat && nd > 0)
+        CUDA_TRY(cudaMemcpyAsync(deviances, c->dev.ptr, sizeof(double) * (size_t)nd,
+                                 cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    *n_deviances = nd;
+    *n_iter = ni;
+    return NMFCU_OK;
+}
+
 // The host-buffer run shared by nmfcu_run, nmfcu_run_offset and
 // nmfcu_run_weighted.
 nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
@@ -1821,6 +1865,9 @@ nmfcu_status run_host(const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
                       const double *H0, const double *offset0, double *W, double *H,
                       double *offset, double *deviances, int64_t deviances_cap,
                       int64_t *n_deviances, int64_t *n_iter) {
+    if (opt && r > NMFCU_MAX_RANK)
+        return run_host_wide(opt, n, p, r, V, W0, H0, W, H, deviances, deviances_cap,
+                             n_deviances, n_iter);
     NMF_TRY(validate_options(opt, n, p, r));
     if (!V || !W0 || !H0 || !W || !H || !n_deviances || !n_iter)
         return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
@@ -2008,16 +2055,51 @@ nmfcu_status nmfcu_context_create(int32_t device, nmfcu_context **ctx) {
 
 void nmfcu_context_destroy(nmfcu_context *ctx) { delete ctx; }
 
-nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_t n, int64_t p,
-                              int64_t r, const void *dV, int32_t v_dtype, int64_t ldv,
-                              const double *dV64, int64_t ldv64, double *dW, double *dH,
-                              double *d_dev, int64_t *n_deviances, int64_t *n_iter,
-                              void *stream) {
+}  // extern "C"
+
+namespace {
+// nmfcu_run_device, and with `d_off` the offset method's run on device
+// pointers (d_off0: the starting row offsets, or NULL for rowMeans(V);
+// d_off receives the final ones).
+nmfcu_status run_device_impl(nmfcu_context *c, const nmfcu_options *opt, int64_t n, int64_t p,
+                             int64_t r, const void *dV, int32_t v_dtype, int64_t ldv,
+                             const double *dV64, int64_t ldv64, double *dW, double *dH,
+                             const double *d_off0, double *d_off, double *d_dev,
+                             int64_t *n_deviances, int64_t *n_iter, void *stream) {
     if (!c) return fail(NMFCU_ERR_INVALID_ARG, "NULL context");
+    if (opt && r > NMFCU_MAX_RANK) {
+        // Ranks above the streaming passes' buckets: the FP64 wide loop.
+        NMF_TRY(nmfcu_internal::wide_validate(opt, n, p, r));
+        if (!dV || !dW || !dH || !n_deviances || !n_iter)
+            return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+        if (v_dtype != NMFCU_F64)
+            return fail(NMFCU_ERR_INVALID_ARG, "ranks above 32 run in FP64: pass an f64 V");
+        if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
+        const bool stat = opt->stop == NMFCU_STOP_STATIONARY;
+        if (stat && !d_dev) return fail(NMFCU_ERR_INVALID_ARG, "stationary stop needs d_dev");
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard dg(c->device);
+        cudaStream_t s = (cudaStream_t)stream;
+        const double *V64 = (const double *)dV;
+        int64_t ld64 = ldv;
+        if (!tma_layout_ok(V64, ld64, 8)) {
+            const int64_t ld = std::max<int64_t>(16, round_up(p, 16));
+            NMF_TRY(c->V64.ensure(sizeof(double) * (size_t)(n * ld)));
+            if (n > 0 && p > 0)
+                CUDA_TRY(cudaMemcpy2DAsync(c->V64.ptr, ld * 8, V64, ld64 * 8, p * 8, n,
+                                           cudaMemcpyDeviceToDevice, s));
+            V64 = c->V64.as<double>();
+            ld64 = ld;
+        }
+        return nmfcu_internal::wide_run(c, opt, n, p, r, V64, ld64, dW, dH, dW, dH,
+                                        cudaMemcpyDeviceToDevice, cudaMemcpyDeviceToDevice,
+                                        stat ? d_dev : nullptr, s, n_deviances, n_iter);
+    }
     NMF_TRY(validate_options(opt, n, p, r));
-    if (opt->method == NMFCU_OFFSET)
+    if (opt->method == NMFCU_OFFSET && !d_off)
         return fail(NMFCU_ERR_UNSUPPORTED,
-                    "the offset method returns its row offsets: run it through nmfcu_run_offset");
+                    "the offset method returns its row offsets: run it through "
+                    "nmfcu_run_offset or nmfcu_run_offset_device");
     if (opt->method == NMFCU_LSNMF)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
@@ -2097,14 +2179,45 @@ nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_
     a.H = c->H.as<double>();
     a.dev = stat ? d_dev : nullptr;
     if (stat && !d_dev) return fail(NMFCU_ERR_INVALID_ARG, "stationary stop needs d_dev");
-    NMF_TRY(setup_method(c, pl, opt, a, nullptr, false, s));
+    if (opt->method == NMFCU_OFFSET && !V64)
+        return fail(NMFCU_ERR_INVALID_ARG, "the offset method needs the f64 V (dV64)");
+    NMF_TRY(setup_method(c, pl, opt, a, d_off0, false, s));
     int64_t nd = 0, ni = 0;
     NMF_TRY(run_loop(c, a, s, &nd, &ni));
     NMF_TRY(get_factors(c, pl, dW, dH, cudaMemcpyDeviceToDevice, s));
+    if (opt->method == NMFCU_OFFSET && n > 0)
+        CUDA_TRY(cudaMemcpyAsync(d_off, a.off, sizeof(double) * (size_t)n,
+                                 cudaMemcpyDeviceToDevice, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     *n_deviances = nd;
     *n_iter = ni;
     return NMFCU_OK;
+}
+}  // namespace
+
+extern "C" {
+
+nmfcu_status nmfcu_run_device(nmfcu_context *c, const nmfcu_options *opt, int64_t n, int64_t p,
+                              int64_t r, const void *dV, int32_t v_dtype, int64_t ldv,
+                              const double *dV64, int64_t ldv64, double *dW, double *dH,
+                              double *d_dev, int64_t *n_deviances, int64_t *n_iter,
+                              void *stream) {
+    return run_device_impl(c, opt, n, p, r, dV, v_dtype, ldv, dV64, ldv64, dW, dH, nullptr,
+                           nullptr, d_dev, n_deviances, n_iter, stream);
+}
+
+nmfcu_status nmfcu_run_offset_device(nmfcu_context *c, const nmfcu_options *opt, int64_t n,
+                                     int64_t p, int64_t r, const void *dV, int32_t v_dtype,
+                                     int64_t ldv, const double *dV64, int64_t ldv64, double *dW,
+                                     double *dH, const double *d_offset0, double *d_offset,
+                                     double *d_dev, int64_t *n_deviances, int64_t *n_iter,
+                                     void *stream) {
+    if (!opt) return fail(NMFCU_ERR_INVALID_ARG, "NULL options");
+    if (opt->method != NMFCU_OFFSET)
+        return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_run_offset_device runs method NMFCU_OFFSET only");
+    if (!d_offset) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    return run_device_impl(c, opt, n, p, r, dV, v_dtype, ldv, dV64, ldv64, dW, dH, d_offset0,
+                           d_offset, d_dev, n_deviances, n_iter, stream);
 }
 
 int64_t nmfcu_shard_reduce_len(int64_t n, int64_t r) {
@@ -2295,6 +2408,22 @@ nmfcu_status nmfcu_shard_result(nmfcu_shard *sh, double *dW, double *dH, double 
 
 void nmfcu_shard_destroy(nmfcu_shard *sh) { delete sh; }
 
+extern "C++" {
+namespace nmfcu_internal {
+// out = V X (trans 0) or V^T X (trans 1) with the context locked and its
+// device current; see nmfcu_v_product_device.  `reset_state` clears the
+// context's run state first (a standalone product); a caller that keeps its
+// own loop's stop state there passes false, and the passes then do no work
+// once that loop has stopped.  `sync` waits for the stream and reports a
+// streaming kernel that gave up waiting.
+nmfcu_status v_product_locked(nmfcu_context *c, int32_t trans, int64_t n, int64_t p, int64_t l,
+                              const double *dV, int64_t ldv, const double *dX, int64_t ldx,
+                              double *dOut, int64_t ldo, cudaStream_t s, bool reset_state,
+                              bool sync);
+void *context_state(nmfcu_context *c) { return c->state.ptr; }
+}  // namespace nmfcu_internal
+}  // extern "C++"
+
 nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, int64_t p,
                                     int64_t l, const double *dV, int64_t ldv, const double *dX,
                                     int64_t ldx, double *dOut, int64_t ldo, void *stream) {
@@ -2310,10 +2439,20 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, 
     if (!dOut || (xrows > 0 && (!dV || !dX))) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     std::lock_guard<std::mutex> lk(c->mu);
     DeviceGuard dg(c->device);
-    cudaStream_t s = (cudaStream_t)stream;
+    return nmfcu_internal::v_product_locked(c, trans, n, p, l, dV, ldv, dX, ldx, dOut, ldo,
+                                            (cudaStream_t)stream, true, true);
+}
+
+extern "C++" nmfcu_status nmfcu_internal::v_product_locked(nmfcu_context *c, int32_t trans, int64_t n,
+                                              int64_t p, int64_t l, const double *dV, int64_t ldv,
+                                              const double *dX, int64_t ldx, double *dOut,
+                                              int64_t ldo, cudaStream_t s, bool reset_state,
+                                              bool sync) {
+    const int64_t xrows = trans ? n : p, orows = trans ? p : n;
+    if (l == 0 || orows == 0) return NMFCU_OK;
     if (xrows == 0) {  // an empty sum: the product is zero
         CUDA_TRY(cudaMemset2DAsync(dOut, ldo * 8, 0, l * 8, orows, s));
-        CUDA_TRY(cudaStreamSynchronize(s));
+        if (sync) CUDA_TRY(cudaStreamSynchronize(s));
         return NMFCU_OK;
     }
     // TMA needs a 16-byte aligned base and row pitch: otherwise V is copied
@@ -2334,7 +2473,7 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, 
         const int kc = (int)std::min<int64_t>(NMFCU_MAX_RANK, l - c0);
         const Plan pl = make_plan(n, p, kc, c->sms);
         NMF_TRY(ensure_workspace(c, pl, false));  // allocates the device state too
-        if (c0 == 0) CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
+        if (c0 == 0 && reset_state) CUDA_TRY(cudaMemsetAsync(c->state.ptr, 0, sizeof(RunState), s));
         RunArgs a;
         a.opt = &o;
         a.pl = pl;
@@ -2374,7 +2513,7 @@ nmfcu_status nmfcu_v_product_device(nmfcu_context *c, int32_t trans, int64_t n, 
                                        n, cudaMemcpyDeviceToDevice, s));
         }
     }
-    return finish_checked(c, s);
+    return sync ? finish_checked(c, s) : NMFCU_OK;
 }
 
 nmfcu_status nmfcu_context_set_timing(nmfcu_context *ctx, int32_t enabled) {

@@ -13,7 +13,7 @@
 //     the engine workspace of that shape, computed from the same list the
 //     engine allocates from) fit in the server's budget next to what every
 //     slot holds; requests that arrive while others run are admitted as
-//     slots and memory free up, first fit in arrival order, with a bypass
+//     slots and memory free up, smallest work first, with a bypass
 //     limit so a large request is not starved by small ones;
 //   * a slot keeps its buffers for the next request (no allocation on the
 //     common path) and releases them when the request at the head of the
@@ -47,8 +47,9 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// Scratch slots of a worker's context holding the request's device copies.
-constexpr int kSlotV = 12, kSlotW = 13, kSlotH = 14, kSlotDev = 15;
+// Scratch slots of a worker's context holding the request's device copies
+// (offset method: the row offsets in and out).
+constexpr int kSlotV = 12, kSlotW = 13, kSlotH = 14, kSlotDev = 15, kSlotOff = 16;
 // A queued request may be passed over this many times by later, smaller
 // ones; after that nothing behind it is admitted before it.
 constexpr int kMaxBypass = 8;
@@ -61,6 +62,8 @@ struct Request {
     int64_t n = 0, p = 0, r = 0, ldv = 0;
     const double *V = nullptr, *W0 = nullptr, *H0 = nullptr;
     double *W = nullptr, *H = nullptr, *dev = nullptr;
+    const double *off0 = nullptr;  // offset method: starting offsets (NULL: rowMeans)
+    double *off = nullptr;         // offset method: final offsets
     int64_t dev_cap = 0;
     int state = kQueued;
     int bypassed = 0;
@@ -88,7 +91,9 @@ size_t growth_on(nmfcu_context *c, const Request &q) {
            nmfcu_internal::slot_growth(c, kSlotV, v_bytes(q)) +
            nmfcu_internal::slot_growth(c, kSlotW, sizeof(double) * (size_t)(q.n * q.r)) +
            nmfcu_internal::slot_growth(c, kSlotH, sizeof(double) * (size_t)(q.r * q.p)) +
-           nmfcu_internal::slot_growth(c, kSlotDev, sizeof(double) * dev_slots(q));
+           nmfcu_internal::slot_growth(c, kSlotDev, sizeof(double) * dev_slots(q)) +
+           (q.off ? nmfcu_internal::slot_growth(c, kSlotOff, 2 * sizeof(double) * (size_t)q.n)
+                  : 0);
 }
 
 double ms_between(Clock::time_point a, Clock::time_point b) {
@@ -131,22 +136,44 @@ struct nmfcu_server {
     void run(int k, Request *q);
 };
 
-// The first queued request that fits next to what the slots hold, in
-// arrival order; a request passed over kMaxBypass times blocks the rest.
+// Work of a request for the shortest-first order: V elements x rank x
+// iterations (each iteration streams V twice at a cost that grows with the
+// rank).
+double work_of(const Request &q) {
+    return (double)q.n * (double)q.p * (double)q.r * (double)std::max<int64_t>(1, q.opt.max_iter);
+}
+
+// The queued request with the least work that fits next to what the slots
+// hold (ties: the earlier one), so small requests are not held behind large
+// ones.  A request passed over kMaxBypass times is taken first if it fits,
+// and while it does not fit nothing behind it starts, so no request waits
+// for ever.
 Request *nmfcu_server::pick(int k, size_t *growth) {
     Slot &sl = slots[k];
+    auto best = queue.end();
+    size_t best_g = 0;
     for (auto it = queue.begin(); it != queue.end(); ++it) {
         Request *q = *it;
         const size_t g = growth_on(sl.ctx, *q);
-        if (in_use + g <= budget) {
-            for (auto jt = queue.begin(); jt != it; ++jt) (*jt)->bypassed++;
-            queue.erase(it);
-            *growth = g;
-            return q;
+        const bool fits = in_use + g <= budget;
+        if (q->bypassed >= kMaxBypass) {
+            if (!fits) return nullptr;  // the starved request blocks the rest
+            best = it;
+            best_g = g;
+            break;
         }
-        if (q->bypassed >= kMaxBypass) break;
+        if (fits && (best == queue.end() || work_of(*q) < work_of(**best))) {
+            best = it;
+            best_g = g;
+        }
     }
-    return nullptr;
+    if (best == queue.end()) return nullptr;
+    // Every earlier request (the queue is in arrival order) was overtaken.
+    for (auto jt = queue.begin(); jt != best; ++jt) (*jt)->bypassed++;
+    Request *q = *best;
+    queue.erase(best);
+    *growth = best_g;
+    return q;
 }
 
 void nmfcu_server::worker(int k) {
@@ -237,11 +264,31 @@ void nmfcu_server::run(int k, Request *q) {
     }
     const bool stat = q->opt.stop == NMFCU_STOP_STATIONARY;
     int64_t nd = 0, ni = 0;
-    if (record(nmfcu_run_device(c, &q->opt, q->n, q->p, q->r, dV, NMFCU_F64, ld, nullptr, 0,
-                                (double *)dW, (double *)dH, stat ? (double *)dD : nullptr, &nd,
-                                &ni, s)) != NMFCU_OK)
+    if (q->off) {
+        // The offset method: the starting offsets in, the final ones out.
+        void *dO = nullptr;
+        if (record(nmfcu_internal::context_buffer(c, kSlotOff, 2 * sizeof(double) * (size_t)q->n, &dO)) != NMFCU_OK)
+            return;
+        double *d_off0 = static_cast<double *>(dO), *d_off = d_off0 + q->n;
+        if (q->off0 && q->n > 0)
+            e = cudaMemcpyAsync(d_off0, q->off0, sizeof(double) * q->n, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            record(nmfcu_internal::cuda_fail(e, "request upload"));
+            return;
+        }
+        if (record(nmfcu_run_offset_device(c, &q->opt, q->n, q->p, q->r, dV, NMFCU_F64, ld,
+                                           nullptr, 0, (double *)dW, (double *)dH,
+                                           q->off0 ? d_off0 : nullptr, d_off,
+                                           stat ? (double *)dD : nullptr, &nd, &ni, s)) != NMFCU_OK)
+            return;
+        if (q->n > 0)
+            e = cudaMemcpyAsync(q->off, d_off, sizeof(double) * q->n, cudaMemcpyDeviceToHost, s);
+    } else if (record(nmfcu_run_device(c, &q->opt, q->n, q->p, q->r, dV, NMFCU_F64, ld, nullptr,
+                                       0, (double *)dW, (double *)dH,
+                                       stat ? (double *)dD : nullptr, &nd, &ni, s)) != NMFCU_OK) {
         return;
-    if (q->n * q->r > 0)
+    }
+    if (e == cudaSuccess && q->n * q->r > 0)
         e = cudaMemcpyAsync(q->W, dW, sizeof(double) * q->n * q->r, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && q->r * q->p > 0)
         e = cudaMemcpyAsync(q->H, dH, sizeof(double) * q->r * q->p, cudaMemcpyDeviceToHost, s);
@@ -326,15 +373,19 @@ void nmfcu_server_destroy(nmfcu_server *srv) {
     delete srv;
 }
 
-nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, int64_t n,
-                                 int64_t p, int64_t r, const double *V, int64_t ldv,
-                                 const double *W0, const double *H0, double *W, double *H,
-                                 double *deviances, int64_t dev_cap, int64_t *request_id) {
+namespace {
+nmfcu_status submit(nmfcu_server *srv, const nmfcu_options *opt, int64_t n, int64_t p, int64_t r,
+                    const double *V, int64_t ldv, const double *W0, const double *H0, double *W,
+                    double *H, const double *off0, double *off, double *deviances,
+                    int64_t dev_cap, int64_t *request_id) {
     if (!srv || !opt || !request_id) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
     NMFCU_TRY(nmfcu_internal::validate_options(opt, n, p, r));
-    if (opt->method == NMFCU_OFFSET)
+    if (opt->method == NMFCU_OFFSET && !off)
         return fail(NMFCU_ERR_UNSUPPORTED,
-                    "the offset method returns its row offsets: run it through nmfcu_run_offset");
+                    "the offset method returns its row offsets: submit it through "
+                    "nmfcu_server_submit_offset");
+    if (opt->method != NMFCU_OFFSET && off)
+        return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_server_submit_offset takes method offset only");
     if (opt->method == NMFCU_LSNMF)
         return fail(NMFCU_ERR_UNSUPPORTED,
                     "lsNMF takes a weight matrix: run it through nmfcu_run_weighted");
@@ -358,6 +409,8 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
     q->H = H;
     q->dev = deviances;
     q->dev_cap = dev_cap;
+    q->off0 = off0;
+    q->off = off;
     // A request that cannot fit even on an empty server is refused now.
     const size_t need = growth_on(srv->probe, *q);
     if (need > srv->budget)
@@ -378,6 +431,28 @@ nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, in
     srv->reqs.emplace(q->id, std::move(q));
     srv->cv_work.notify_all();
     return NMFCU_OK;
+}
+}  // namespace
+
+nmfcu_status nmfcu_server_submit(nmfcu_server *srv, const nmfcu_options *opt, int64_t n,
+                                 int64_t p, int64_t r, const double *V, int64_t ldv,
+                                 const double *W0, const double *H0, double *W, double *H,
+                                 double *deviances, int64_t dev_cap, int64_t *request_id) {
+    return submit(srv, opt, n, p, r, V, ldv, W0, H0, W, H, nullptr, nullptr, deviances, dev_cap,
+                  request_id);
+}
+
+nmfcu_status nmfcu_server_submit_offset(nmfcu_server *srv, const nmfcu_options *opt, int64_t n,
+                                        int64_t p, int64_t r, const double *V, int64_t ldv,
+                                        const double *W0, const double *H0,
+                                        const double *offset0, double *W, double *H,
+                                        double *offset, double *deviances, int64_t dev_cap,
+                                        int64_t *request_id) {
+    if (!offset) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    if (opt && opt->method != NMFCU_OFFSET)
+        return fail(NMFCU_ERR_INVALID_ARG, "nmfcu_server_submit_offset takes method offset only");
+    return submit(srv, opt, n, p, r, V, ldv, W0, H0, W, H, offset0, offset, deviances, dev_cap,
+                  request_id);
 }
 
 nmfcu_status nmfcu_server_poll(nmfcu_server *srv, int64_t request_id, int32_t *state) {

@@ -99,6 +99,11 @@ SIGNATURES = {
                                 ctypes.c_void_p, _i32, _i64, ctypes.c_void_p, _i64,
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64p, _i64p,
                                 ctypes.c_void_p]),
+    "nmfcu_run_offset_device": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64,
+                                       _i64, ctypes.c_void_p, _i32, _i64, ctypes.c_void_p, _i64,
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                       ctypes.c_void_p, ctypes.c_void_p, _i64p, _i64p,
+                                       ctypes.c_void_p]),
     "nmfcu_consensus_stats_device": (_i32, [ctypes.c_void_p, _i64, ctypes.c_void_p, _i64,
                                             ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double), ctypes.c_void_p]),
@@ -140,6 +145,9 @@ SIGNATURES = {
     "nmfcu_server_destroy": (None, [ctypes.c_void_p]),
     "nmfcu_server_submit": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64, _i64,
                                    _dp, _i64, _dp, _dp, _dp, _dp, _dp, _i64, _i64p]),
+    "nmfcu_server_submit_offset": (_i32, [ctypes.c_void_p, ctypes.POINTER(Options), _i64, _i64,
+                                          _i64, _dp, _i64, _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                          _i64, _i64p]),
     "nmfcu_server_poll": (_i32, [ctypes.c_void_p, _i64, ctypes.POINTER(_i32)]),
     "nmfcu_server_wait": (_i32, [ctypes.c_void_p, _i64, _i64, _i64p, _i64p]),
     "nmfcu_server_cancel": (_i32, [ctypes.c_void_p, _i64]),

@@ -85,7 +85,7 @@ class Request:
         b = self._bufs
         self._result = NMFResult(W=b["W"], H=b["H"], n_iter=int(ni.value),
                                  deviances=np.array(b["dev"][: nd.value], dtype=np.float64),
-                                 method=self._method, offset=None)
+                                 method=self._method, offset=b.get("off"))
         self._bufs = None
         return self._result
 
@@ -131,10 +131,19 @@ class Server:
         dev = np.empty(cap, dtype=np.float64)
         rid = ctypes.c_int64(0)
         dp = _native._ptr
-        _native.check(self._lib.nmfcu_server_submit(
-            self._h, ctypes.byref(o), n, p, r, dp(v), p, dp(w0), dp(h0), dp(W), dp(H), dp(dev),
-            cap, ctypes.byref(rid)))
         bufs = {"V": v, "W0": w0, "H0": h0, "W": W, "H": H, "dev": dev, "opts": o}
+        if method_norm == "offset":
+            # The offset method also returns its row offsets (lib.rs:2161-2165).
+            off = np.empty(n, dtype=np.float64)
+            bufs.update(off=off, off0=offset_arr)
+            _native.check(self._lib.nmfcu_server_submit_offset(
+                self._h, ctypes.byref(o), n, p, r, dp(v), p, dp(w0), dp(h0),
+                dp(offset_arr) if offset_arr is not None else None, dp(W), dp(H), dp(off),
+                dp(dev), cap, ctypes.byref(rid)))
+        else:
+            _native.check(self._lib.nmfcu_server_submit(
+                self._h, ctypes.byref(o), n, p, r, dp(v), p, dp(w0), dp(h0), dp(W), dp(H),
+                dp(dev), cap, ctypes.byref(rid)))
         return Request(self, int(rid.value), method_norm, bufs)
 
     def stats(self) -> dict:

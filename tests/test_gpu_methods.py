@@ -124,14 +124,56 @@ def test_reduced_precision(oracle, method, precision):
     assert rel(o_got, o_ref) <= 1e-5, rel(o_got, o_ref)
 
 
-def test_offset_rejected_where_offsets_cannot_be_returned():
-    V = synthetic.counts_matrix(40, 50, 3, 0.3, seed=1)
-    W0, H0 = nmf_rs.random_init(V, 3, seed=1)
-    with nmf_rs.serve.Server(slots=1) as srv:
-        with pytest.raises(NotImplementedError, match="nmfcu_run_offset"):
-            srv.submit(V, 3, "offset", W0=W0, H0=H0, max_iter=5)
-        ok = srv.submit(V, 3, "nsNMF", W0=W0, H0=H0, max_iter=5).result(timeout=120)
-    assert ok.n_iter == 5
+def test_offset_through_the_server_and_the_device_entry(oracle):
+    """The offset method's row offsets come back from a served request
+    (nmfcu_server_submit_offset) and from the device-pointer entry
+    (nmfcu_run_offset_device): both equal nmf()'s run bit for bit, and the
+    oracle to the plain tolerance."""
+    import ctypes
+
+    import torch
+
+    V = synthetic.counts_matrix(140, 230, 3, 0.3, seed=1) + 0.01
+    W0, H0 = nmf_rs.random_init(V, 4, seed=1)
+    ref = oracle.nmf_method("offset", V, W0, H0, 30)
+    alone = nmf_rs.nmf(V, 4, "offset", W0=W0, H0=H0, max_iter=30)
+    assert rel_max(alone.offset, ref["offset"]) <= FACTOR_TOL
+    off0 = V.mean(axis=1) * 0.5
+    given = nmf_rs.nmf(V, 4, "offset", W0=W0, H0=H0, max_iter=30, offset=off0)
+    with nmf_rs.serve.Server(slots=2) as srv:
+        a = srv.submit(V, 4, "offset", W0=W0, H0=H0, max_iter=30)
+        b = srv.submit(V, 4, "offset", W0=W0, H0=H0, max_iter=30, offset=off0)
+        c = srv.submit(V, 4, "nsNMF", W0=W0, H0=H0, max_iter=5)
+        ra, rb = a.result(timeout=120), b.result(timeout=120)
+        assert c.result(timeout=120).offset is None
+    for got, want in ((ra, alone), (rb, given)):
+        np.testing.assert_array_equal(got.W, want.W)
+        np.testing.assert_array_equal(got.H, want.H)
+        np.testing.assert_array_equal(got.offset, want.offset)
+    # The device entry, V / factors / offsets as device tensors.
+    dV = torch.from_numpy(V).cuda()
+    dW = torch.from_numpy(W0.copy()).cuda()
+    dH = torch.from_numpy(H0.copy()).cuda()
+    dO = torch.empty(V.shape[0], dtype=torch.float64, device="cuda")
+    o = nmf_rs._native.default_options()
+    o.method = nmf_rs._native.parse_method("offset")
+    o.max_iter = 30
+    ctx = nmf_rs._native.Context(0)
+    nd, ni = ctypes.c_int64(0), ctypes.c_int64(0)
+    nmf_rs._native.check(nmf_rs._native.load().nmfcu_run_offset_device(
+        ctx.handle, ctypes.byref(o), V.shape[0], V.shape[1], 4, ctypes.c_void_p(dV.data_ptr()),
+        nmf_rs._native.F64, V.shape[1], None, 0, ctypes.c_void_p(dW.data_ptr()),
+        ctypes.c_void_p(dH.data_ptr()), None, ctypes.c_void_p(dO.data_ptr()), None,
+        ctypes.byref(nd), ctypes.byref(ni), None))
+    ctx.close()
+    np.testing.assert_array_equal(dO.cpu().numpy(), alone.offset)
+    np.testing.assert_array_equal(dW.cpu().numpy(), alone.W)
+    # The plain device entry still refuses offset (it has no slot for them).
+    ctx = nmf_rs._native.Context(0)
+    with pytest.raises(NotImplementedError, match="nmfcu_run_offset_device"):
+        ctx.run(o, V.shape[0], V.shape[1], 4, dV.data_ptr(), nmf_rs._native.F64, V.shape[1],
+                dW.data_ptr(), dH.data_ptr())
+    ctx.close()
 
 
 # ---------------------------------------------------------------------------

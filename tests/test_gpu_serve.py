@@ -129,8 +129,6 @@ def test_argument_errors_are_raised_at_submit():
     with serve.Server(slots=1) as srv:
         with pytest.raises(ValueError):
             srv.submit(V, 3, "nope", W0=W0, H0=H0, max_iter=5)
-        with pytest.raises(NotImplementedError):
-            srv.submit(V, 3, "offset", W0=W0, H0=H0, max_iter=5)
         with pytest.raises(ValueError):
             srv.submit(-V - 1, 3, "lee", W0=W0, H0=H0, max_iter=5)
         ok = srv.submit(V, 3, "lee", W0=W0, H0=H0, max_iter=5).result(timeout=60)

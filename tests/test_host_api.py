@@ -262,3 +262,19 @@ def test_batch_shape_setting_needs_no_gpu():
         consensus.set_batch_shape(-2)
     consensus.set_batch_shape(0)
     consensus.set_batch_shape("auto")
+
+
+def test_wide_rank_limits_checked_before_the_device():
+    """Ranks above 32 run lee / brunet / hals / dnmf in FP64 up to
+    NMFCU_MAX_WIDE_RANK; everything else is refused before any device work,
+    so these raise on a machine without a GPU too."""
+    V = np.ones((6, 7))
+    W0, H0 = np.ones((6, 300)), np.ones((300, 7))
+    with pytest.raises(NotImplementedError, match="largest supported rank"):
+        _native.py_nmf_run("lee", V, W0, H0, 1)
+    W0, H0 = np.ones((6, 40)), np.ones((40, 7))
+    with pytest.raises(NotImplementedError, match="FP64 only"):
+        _native.py_nmf_run("lee", V, W0, H0, 1, precision="fp32")
+    for method in ("nsNMF", "ehals", "snmf/r"):
+        with pytest.raises(NotImplementedError, match="run lee, brunet, hals and dnmf"):
+            _native.py_nmf_run(method, V, W0, H0, 1)
