@@ -76,9 +76,9 @@ void tc_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void
 // split-bf16 passes.  hpass: N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j];
 // otherwise N[i][k] = sum_j H[k][j] V[i][j] / (W H)[i][j].  v: the f32 V (H
 // pass box {128, 64}; W pass box {32, 128}, 128-B swizzle); t: the tile
-// factor's [3][xpadT][32] terms (box {32, 128}, 64-B swizzle); f1: the
-// chunk factor's [3][xpadF][32] terms (box {32, 64}, 64-B swizzle).
-cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const CUtensorMap &t,
+// factor's [3][xpadT][32] bf16 terms (device pointer, 16-byte aligned); f1:
+// the chunk factor's [3][xpadF][32] terms (box {32, 64}, 64-B swizzle).
+cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t,
                             const CUtensorMap &f1, int xpadT, int xpadF, int kext, int RP,
                             const StreamK &sk, double *part, RunState *st, cudaStream_t s);
 // F(k, x) = F[k * fk + x * fx] (R x K) -> three bf16 terms as [3][RPN][ldk]

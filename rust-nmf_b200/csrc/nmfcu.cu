@@ -532,7 +532,7 @@ struct PassSet {
     // planes as tile (box 128 rows) and chunk (box 64 rows) operands.
     bool tcr = false;
     int64_t xpadW = 0, xpadH = 0;
-    CUtensorMap tmVrH, tmVrW, tmXwT, tmXwF, tmXhT, tmXhF;
+    CUtensorMap tmVrH, tmVrW, tmXwF, tmXhF;
 };
 
 // The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
@@ -673,9 +673,7 @@ nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, i
     unsigned char *xw = c->Xs.as<unsigned char>();
     unsigned char *xh = xw + (size_t)3 * ps->xpadW * kTcrRank * 2;
     const CUtensorMapSwizzle sw64 = CU_TENSOR_MAP_SWIZZLE_64B;
-    NMF_TRY(encode_2d_bf16(&ps->tmXwT, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 128, sw64));
     NMF_TRY(encode_2d_bf16(&ps->tmXwF, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
-    NMF_TRY(encode_2d_bf16(&ps->tmXhT, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 128, sw64));
     NMF_TRY(encode_2d_bf16(&ps->tmXhF, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
     return NMFCU_OK;
 }
@@ -787,7 +785,7 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
-            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, ps.tmXhT, ps.tmXwF, (int)ps.xpadH,
+            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, xh, ps.tmXwF, (int)ps.xpadH,
                                      (int)ps.xpadW, pl.n, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -853,7 +851,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
-            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, ps.tmXwT, ps.tmXhF, (int)ps.xpadW,
+            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, xw, ps.tmXhF, (int)ps.xpadW,
                                      (int)ps.xpadH, pl.p, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);

@@ -13,32 +13,44 @@
 //                                               F: the chunk's factor rows
 //   ratio Q[o][e]  = V[o][e] / WH[o][e]         (0 where WH is 0), f32, on
 //                                               the CUDA cores, split into
-//                                               bf16 hi + lo in shared memory
-//   MMA2  N[o][k] += sum_e Q[o][e] F[e][k]      accumulated over a segment;
-//                                               F read from MMA1's tile of it,
-//                                               as an MN-major operand
+//                                               bf16 hi + lo
+//   MMA2  N[o][k] += sum_e Q[o][e] F[e][k]      accumulated over a segment
 // so W H is never written out.  V is read once, as f32 (4 bytes an element);
 // the factors are L2-resident.  Factor operands are three bf16 terms each
-// (Fh + Fm + Fl ~ F to about 2^-24); MMA1 keeps the six products down to
-// 2^-16 x 2^-8 (Th[Fh;Fm;Fl], Tm[Fh;Fm], Tl Fh as N = 192 / 128 / 64 into
-// one accumulator of three column groups), MMA2 the five of the split-bf16
-// lee passes (Qh [Fh;Fm;Fl] + Ql [Fh;Fm], N = 96 / 64).
+// (Fh + Fm + Fl ~ F to about 2^-24).
 //
-// One CTA per SM, twenty warps: warp 0 loads V into a ring of its own (a
-// slot is refilled as soon as the ratio step has read it), warp 1 the factor
-// terms (L2-resident), warp 2 owns the tensor memory and issues MMA1 of each
-// chunk as soon as a WH accumulator is free, warp 3 issues MMA2 behind the
-// ratio step (two issuers, so that MMA1 of later chunks never waits on a
-// contraction), warps 4..19 read WH from tensor memory, form Q and drain the
-// contraction: warp w reads TMEM lanes 32 (w mod 4) .. +31, and the four
-// warps of a lane quarter take 16 of the chunk's 64 elements each.  Tensor memory:
-// two WH accumulators (3 x 64 columns at 0 and 192), one contraction
-// accumulator (3 x 32 columns at 384).  The stream-K split, the 2048-term
-// segments of every f32 sum and the folded f64 partials (one per CTA and
-// tile, layout H: [RP][128], W: [128][RP]) are those of the split-bf16 lee
-// passes, so the CUDA-core brunet epilogues apply unchanged.  Every wait is
-// bounded; a CTA that gives up records a timeout, lets its own loads and
-// MMAs finish, frees its tensor memory and returns.
+// Tensor memory carries everything that is not streamed, so shared memory
+// holds only the two TMA rings (V and the chunk factor F) and its bandwidth
+// goes to the streams:
+//   * T, the tile operand of MMA1, sits in tensor memory for the whole tile
+//     (MMA1 reads A from tensor memory): its three terms, 16 columns each.
+//   * MMA1 adds the six products Th Fh, Th Fm, Th Fl, Tm Fh, Tm Fm, Tl Fh
+//     (products down to 2^-16 x 2^-8) into ONE 64-column accumulator per
+//     chunk, so the ratio step reads one value an element.
+//   * The ratio step writes Q back over the W H it has just read, as bf16
+//     pairs: for chunk elements 16g .. 16g + 15 the hi terms fill columns
+//     16g .. 16g + 7 and the lo terms 16g + 8 .. 16g + 15 of the same
+//     buffer, and MMA2 reads them as its A operand (K step g: Qh at 16g, Ql
+//     at 16g + 8).  Each epilogue warp reads and rewrites only its own 16
+//     columns.  MMA2 contracts Qh [Fh; Fm; Fl] + Ql [Fh; Fm] (N = 96 / 64,
+//     B = F read MN-major) into a segment accumulator of three column groups.
+//   * Four W H / Q buffers (a buffer is freed by the MMA2 that read its Q),
+//     two segment accumulators (drained one chunk late, so MMA2 of the next
+//     segment never waits on the drain).
+//
+// One CTA per SM, twenty warps: warp 0 loads V into its ring (a slot is
+// refilled as soon as the ratio step has read it), warp 1 the chunk factor
+// terms, warp 2 owns the tensor memory and issues MMA1 as soon as a buffer
+// is free, warp 3 issues MMA2 behind the ratio step, warps 4..19 form Q and
+// drain the contraction: warp w reads tensor-memory lanes 32 (w mod 4) ..
+// +31 and the four warps of a lane quarter take 16 of the chunk's 64
+// elements each (three of them also write the quarter's rows of T when a
+// tile starts).  The stream-K split, the 2048-term segments of every f32
+// sum and the folded f64 partials (one per CTA and tile, layout H:
+// [RP][128], W: [128][RP]) are those of the split-bf16 lee passes, so the
+// CUDA-core brunet epilogues apply unchanged.  Every wait is bounded; a CTA
+// that gives up records a timeout, lets its own loads and MMAs finish,
+// frees its tensor memory and returns.
 #pragma once
 
 #include "tc.cuh"
@@ -49,22 +61,31 @@ namespace tcr {
 constexpr int kM = 128;        // outputs per tile (TMEM lanes, MMA M)
 constexpr int kC = 64;         // streamed elements per chunk (one stream-K unit)
 constexpr int kR = 32;         // padded rank: MMA1's K, MMA2's N per factor term
-constexpr int kVStages = 4;   // V ring: freed as soon as the ratio step has read V
-constexpr int kFStages = 3;   // factor ring: freed when the chunk's MMA2 is done
+constexpr int kVStages = 5;    // V ring: freed as soon as the ratio step has read V
+constexpr int kFStages = 4;    // factor ring: freed when the chunk's MMA2 is done
+constexpr int kNB = 4;         // W H / Q buffers in tensor memory
 // Warp roles: V producer, factor producer, MMA1 issuer (and the tensor
 // memory's owner), MMA2 issuer, then the epilogue warps.
 constexpr int kVProdWarp = 0, kFProdWarp = 1, kMma1Warp = 2, kMma2Warp = 3, kEpiWarp0 = 4;
 constexpr int kEpiWarps = 16;
 constexpr int kParts = kEpiWarps / 4;       // epilogue warps per TMEM lane quarter
-constexpr int kPartElems = kC / kParts;    // chunk elements per epilogue warp
+constexpr int kPartElems = kC / kParts;    // chunk elements per epilogue warp (16)
 constexpr int kPartRanks = kR / kParts;    // contraction ranks per epilogue warp
+constexpr int kTWarps = 3;                 // warps of a lane quarter that write T
 constexpr int kWarps = kEpiWarp0 + kEpiWarps;
 constexpr int kThreads = kWarps * 32;
 constexpr int kSegUnits = 32;  // chunks per segment: 2048 terms per f32 sum
+static_assert(kPartElems == 16, "a warp's share of the chunk is one 16-element MMA2 K step");
+
+// Tensor-memory columns.
 constexpr int kTmemCols = 512;
-constexpr uint32_t kD1 = 0;    // WH accumulators at columns 0 and 192
-constexpr uint32_t kD1Cols = 192;
-constexpr uint32_t kD2 = 384;  // contraction accumulator (96 columns)
+constexpr uint32_t kQCols = kC;          // one W H / Q buffer
+constexpr uint32_t kTOff = kNB * kQCols;  // T: three terms of 16 columns
+constexpr uint32_t kTCols = 3 * (kR / 2);
+constexpr uint32_t kD2Off = 320;          // two segment accumulators of 96 columns
+constexpr uint32_t kD2Cols = 3 * kR;
+static_assert(kTOff + kTCols <= kD2Off && kD2Off + 2 * kD2Cols <= (uint32_t)kTmemCols,
+              "tensor memory budget");
 
 // Shared memory, from a 1 KB-aligned base.
 constexpr int V_BYTES = kC * kM * 4;      // the f32 V chunk (one V ring slot)
@@ -74,15 +95,10 @@ constexpr int V_BYTES = kC * kM * 4;      // the f32 V chunk (one V ring slot)
 // apart.
 constexpr int F1_TERM = kC * kR * 2;
 constexpr int F_SLOT = 3 * F1_TERM;       // one factor ring slot: the three terms
-constexpr int T_TERM = kM * kR * 2;       // MMA1's A term: 128 rows x 32 k, 64-B swizzle
-constexpr int Q_PLANE = kM * kC * 2;      // Q hi or lo: 128 x 64, 128-B swizzle
 constexpr int OFF_F = kVStages * V_BYTES;
-constexpr int OFF_T = OFF_F + kFStages * F_SLOT;
-constexpr int OFF_Q = OFF_T + 3 * T_TERM;
-constexpr int OFF_BARS = OFF_Q + 2 * Q_PLANE;
+constexpr int OFF_BARS = OFF_F + kFStages * F_SLOT;
 static_assert(V_BYTES % 1024 == 0 && F_SLOT % 1024 == 0 && OFF_F % 1024 == 0 &&
-                  OFF_T % 1024 == 0 && OFF_Q % 1024 == 0 && T_TERM % 1024 == 0 &&
-                  Q_PLANE % 1024 == 0 && F1_TERM % 512 == 0,
+                  F1_TERM % 512 == 0,
               "swizzle atoms need their alignment");
 
 struct Bars {
@@ -90,12 +106,12 @@ struct Bars {
     uint64_t vempty[kVStages];  // V slot read (one arrival per epilogue warp)
     uint64_t ffull[kFStages];   // factor slot loaded (TMA bytes)
     uint64_t fempty[kFStages];  // factor slot free (MMA2 of its chunk done)
-    uint64_t tfull, tempty;   // the tile operand loaded / free (last MMA1 of its tile done)
-    uint64_t d1full[2];       // WH accumulator b written (MMA1 commit)
-    uint64_t d1empty[2];      // WH accumulator b read (one arrival per epilogue warp)
-    uint64_t qfull, qempty;   // Q written (epilogue warps) / read (MMA2 commit)
-    uint64_t d2full, d2empty; // a segment's contraction done / drained (epilogue warps)
-    uint64_t drain[2];        // every MMA of an issuer done (abort path)
+    uint64_t tfull, tempty;     // T written (T-writing warps) / free (last MMA1 of its tile done)
+    uint64_t d1full[kNB];       // W H of buffer b written (MMA1 commit)
+    uint64_t qfull[kNB];        // Q of buffer b written (one arrival per epilogue warp)
+    uint64_t qempty[kNB];       // buffer b free again (MMA2 commit)
+    uint64_t d2full[2], d2empty[2];  // a segment's contraction done / drained
+    uint64_t drain[2];          // every MMA of an issuer done (abort path)
     uint32_t tmem_base;
     int abort;
 };
@@ -129,9 +145,16 @@ template <int N>
 __host__ __device__ constexpr uint32_t instr_desc_bmn() {
     return tc::instr_desc<N, false>() | (1u << 16);
 }
-// K-major, 128-byte swizzle (rows of 64 bf16): 8-row groups 1024 bytes apart.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
-    return tc::smem_desc(addr, 16, 1024);
+
+// MMA with A read from tensor memory (rows in lanes, two bf16 K elements a
+// 32-bit column) and B from a shared-memory descriptor.
+__device__ __forceinline__ void umma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b,
+                                        uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
 }
 
 // 8 consecutive 32-bit columns of this thread's tensor-memory lane.
@@ -141,6 +164,25 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
           "=r"(r[7])
         : "r"(taddr));
+}
+// Writes 16 consecutive 32-bit columns of this thread's lane and waits until
+// the writes are done.
+__device__ __forceinline__ void tmem_st16_wait(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+        "%11, %12, %13, %14, %15, %16};" ::"r"(taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+        "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+        "r"(r[15])
+        : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// 1 / y to about 1 ulp (approximate reciprocal, subnormals flushed).
+__device__ __forceinline__ float rcp_approx(float y) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(y));
+    return r;
 }
 
 // Bounded wait that lets the thread sleep: each try suspends it until the
@@ -164,6 +206,19 @@ __device__ __forceinline__ bool mbar_sleep_wait(uint64_t *bar, uint32_t parity) 
 __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
     return __all_sync(0xffffffffu, mbar_sleep_wait(bar, parity)) != 0;
 }
+
+// Slot and phase parity of a ring of N slots, advanced one use at a time.
+template <int N>
+struct RingPos {
+    int slot = 0;
+    uint32_t par = 0;
+    __device__ __forceinline__ void next() {
+        if (++slot == N) {
+            slot = 0;
+            par ^= 1u;
+        }
+    }
+};
 
 // Walks the valid chunks of a CTA's stream-K range in order (units past the
 // streamed extent, which pad the last segment of a tile, are skipped).
@@ -216,12 +271,12 @@ __device__ __forceinline__ ChunkInfo take(ChunkWalker &w, const StreamK &sk, int
 // chunk = 64 columns.
 //   tmV   the f32 V: HPASS box {128, 64}, no swizzle; else box {32, 128},
 //         128-B swizzle (two boxes a chunk)
-//   tmT   the tile factor's terms as [3][xpadT][32] bf16, box {32, 128}, 64-B swizzle
+//   xT    the tile factor's terms as [3][xpadT][32] bf16 (rows of 64 bytes)
 //   tmF1  the chunk factor's terms as [3][xpadF][32] bf16, box {32, 64}, 64-B swizzle
 //   kext  streamed extent (n for the H pass, p for the W pass)
 template <bool HPASS>
 __global__ void __launch_bounds__(kThreads, 1)
-    tcr_pass(const __grid_constant__ CUtensorMap tmV, const __grid_constant__ CUtensorMap tmT,
+    tcr_pass(const __grid_constant__ CUtensorMap tmV, const __nv_bfloat16 *__restrict__ xT,
              const __grid_constant__ CUtensorMap tmF1,
              int xpadT, int xpadF, int kext, int RP, StreamK sk, double *__restrict__ part,
              RunState *st) {
@@ -243,18 +298,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&bars.ffull[s], 1);
             mbar_init(&bars.fempty[s], 1);
         }
-        mbar_init(&bars.tfull, 1);
+        mbar_init(&bars.tfull, 4 * kTWarps);
         mbar_init(&bars.tempty, 1);
-        for (int a = 0; a < 2; a++) {
+        for (int a = 0; a < kNB; a++) {
             mbar_init(&bars.d1full[a], 1);
-            mbar_init(&bars.d1empty[a], kEpiWarps);
+            mbar_init(&bars.qfull[a], kEpiWarps);
+            mbar_init(&bars.qempty[a], 1);
         }
-        mbar_init(&bars.qfull, kEpiWarps);
-        mbar_init(&bars.qempty, 1);
-        mbar_init(&bars.d2full, 1);
-        mbar_init(&bars.d2empty, kEpiWarps);
-        mbar_init(&bars.drain[0], 1);
-        mbar_init(&bars.drain[1], 1);
+        for (int a = 0; a < 2; a++) {
+            mbar_init(&bars.d2full[a], 1);
+            mbar_init(&bars.d2empty[a], kEpiWarps);
+            mbar_init(&bars.drain[a], 1);
+        }
         bars.abort = 0;
         fence_mbar_init();
     }
@@ -278,11 +333,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         int issued[kVStages] = {0};
-        long long ci = 0;
+        RingPos<kVStages> vr;
         while (w.ok && !*abort_flag) {
             const int major = w.cur.major, along = w.cur.along(sk);
-            const int s = (int)(ci % kVStages);
-            if (!mbar_sleep_wait(&bars.vempty[s], (uint32_t)(((ci / kVStages) & 1) ^ 1))) {
+            const int s = vr.slot;
+            if (!mbar_sleep_wait(&bars.vempty[s], vr.par ^ 1u)) {
                 give_up();
                 break;
             }
@@ -296,7 +351,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                                  major * kM, pol_v);
             }
             issued[s]++;
-            ++ci;
+            vr.next();
             w.advance(sk, kext);
         }
         if (*abort_flag) {
@@ -305,31 +360,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (issued[i] > 0) mbar_sleep_wait(&bars.vfull[i], (uint32_t)((issued[i] - 1) & 1));
         }
     } else if (warp == kFProdWarp && lane == 0) {
-        // ---- TMA producer of the factor terms (L2-resident) ------------------
+        // ---- TMA producer of the chunk factor terms (L2-resident) -----------
         const uint64_t pol_f = l2_evict_last_policy();
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         int issued[kFStages] = {0};
-        int tloads = 0, cur_major = -1;
-        long long ci = 0;
+        RingPos<kFStages> fr;
         while (w.ok && !*abort_flag) {
-            const int major = w.cur.major, along = w.cur.along(sk);
-            if (major != cur_major) {
-                // The tile operand is reloaded once the last MMA1 of the
-                // previous tile has read it.
-                if (tloads > 0 && !mbar_sleep_wait(&bars.tempty, (uint32_t)((tloads - 1) & 1))) {
-                    give_up();
-                    break;
-                }
-                mbar_expect_tx(&bars.tfull, 3 * T_TERM);
-                for (int q = 0; q < 3; q++)
-                    tma_load_2d_hint(smem + OFF_T + q * T_TERM, &tmT, &bars.tfull, 0,
-                                     q * xpadT + major * kM, pol_f);
-                ++tloads;
-                cur_major = major;
-            }
-            const int s = (int)(ci % kFStages);
-            if (!mbar_sleep_wait(&bars.fempty[s], (uint32_t)(((ci / kFStages) & 1) ^ 1))) {
+            const int along = w.cur.along(sk);
+            const int s = fr.slot;
+            if (!mbar_sleep_wait(&bars.fempty[s], fr.par ^ 1u)) {
                 give_up();
                 break;
             }
@@ -339,21 +379,18 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tma_load_2d_hint(base + q * F1_TERM, &tmF1, &bars.ffull[s], 0,
                                  q * xpadF + along * kC, pol_f);
             issued[s]++;
-            ++ci;
+            fr.next();
             w.advance(sk, kext);
         }
         if (*abort_flag) {
             for (int i = 0; i < kFStages; i++)
                 if (issued[i] > 0) mbar_sleep_wait(&bars.ffull[i], (uint32_t)((issued[i] - 1) & 1));
-            if (tloads > 0) mbar_sleep_wait(&bars.tfull, (uint32_t)((tloads - 1) & 1));
         }
     } else if ((warp == kMma1Warp || warp == kMma2Warp) && lane == 0) {
         // ---- MMA issuers ------------------------------------------------------
-        // MMA1 (W H of a chunk) runs ahead, held back only by free WH
-        // accumulators and landed factor terms; MMA2 (the contraction)
+        // MMA1 (W H of a chunk) runs ahead, held back only by free buffers,
+        // the tile's T and landed factor terms; MMA2 (the contraction)
         // follows the ratio step.  Each commit covers its own thread's MMAs.
-        constexpr uint32_t id192 = tc::instr_desc<192, false>();
-        constexpr uint32_t id128 = tc::instr_desc<128, false>();
         constexpr uint32_t id64 = tc::instr_desc<64, false>();
         constexpr uint32_t id96m = instr_desc_bmn<96>();  // MMA2: B = F MN-major
         constexpr uint32_t id64m = instr_desc_bmn<64>();
@@ -362,211 +399,171 @@ __global__ void __launch_bounds__(kThreads, 1)
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         long long ci = 0;
-        int tcount = 0, segs = 0, prev_t = -1, prev_major = -1;
+        RingPos<kFStages> fr;
+        RingPos<kNB> qr, qlast;
+        int tiles = 0, segs = 0, prev_t = -1, prev_major = -1;
         bool ok = true;
         while (w.ok && !*abort_flag) {
             const ChunkInfo c = take(w, sk, kext, prev_t);
             prev_t = c.t;
-            const int s = (int)(ci % kFStages);
+            const int s = fr.slot;
+            const int qb = qr.slot;
+            const uint32_t qpar = qr.par;
             const uint32_t fB = sbase + OFF_F + s * F_SLOT;
+            const uint32_t qcol = tmem + (uint32_t)qb * kQCols;
             if (first) {
-                // MMA1 of chunk ci into WH accumulator ci & 1.
-                if (!mbar_sleep_wait(&bars.ffull[s], (uint32_t)((ci / kFStages) & 1))) {
+                // MMA1 of chunk ci into buffer qb.
+                if (!mbar_sleep_wait(&bars.ffull[s], fr.par)) {
                     ok = false;
                     break;
                 }
                 if (c.major != prev_major) {
-                    if (!mbar_sleep_wait(&bars.tfull, (uint32_t)(tcount & 1))) {
+                    if (!mbar_sleep_wait(&bars.tfull, (uint32_t)(tiles & 1))) {
                         ok = false;
                         break;
                     }
-                    ++tcount;
+                    ++tiles;
                     prev_major = c.major;
                 }
-                const int db = (int)(ci & 1);
-                if (!mbar_sleep_wait(&bars.d1empty[db], (uint32_t)(((ci >> 1) & 1) ^ 1))) {
+                if (!mbar_sleep_wait(&bars.qempty[qb], qpar ^ 1u)) {
                     ok = false;
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t d = tmem + kD1 + (uint32_t)db * kD1Cols;
-                const uint32_t tA = sbase + OFF_T;
+                // Products (T term, F term): hh, hm, hl, mh, mm, lh; two K
+                // steps of 16 ranks each.
+                constexpr int ta[6] = {0, 0, 0, 1, 1, 2};
+                constexpr int fa[6] = {0, 1, 2, 0, 1, 0};
 #pragma unroll
-                for (int ks = 0; ks < kR / 16; ks++) {
-                    const uint32_t ko = (uint32_t)ks * 32u;  // 16 bf16 along a 64-byte row
-                    const uint64_t bdesc = desc_sw64(fB + ko);
-                    tc::umma(d, desc_sw64(tA + ko), bdesc, id192, ks > 0 ? 1u : 0u);
-                    tc::umma(d, desc_sw64(tA + T_TERM + ko), bdesc, id128, 1u);
-                    tc::umma(d, desc_sw64(tA + 2 * T_TERM + ko), bdesc, id64, 1u);
+                for (int pr = 0; pr < 6; pr++) {
+#pragma unroll
+                    for (int ks = 0; ks < kR / 16; ks++) {
+                        const uint32_t a =
+                            tmem + kTOff + (uint32_t)(ta[pr] * (kR / 2) + ks * 8);
+                        const uint64_t bdesc =
+                            desc_sw64(fB + (uint32_t)(fa[pr] * F1_TERM) + (uint32_t)ks * 32u);
+                        umma_ts(qcol, a, bdesc, id64, (pr > 0 || ks > 0) ? 1u : 0u);
+                    }
                 }
-                tc::umma_commit(&bars.d1full[db]);
+                tc::umma_commit(&bars.d1full[qb]);
                 if (c.last_tile) tc::umma_commit(&bars.tempty);
             } else {
-                // MMA2 of chunk ci into the contraction accumulator.  The
+                // MMA2 of chunk ci into segment accumulator segs & 1.  The
                 // factor slot landed before MMA1 of this chunk, which the
                 // ratio step waited for.
-                if (c.first_seg && segs > 0 &&
-                    !mbar_sleep_wait(&bars.d2empty, (uint32_t)((segs - 1) & 1))) {
+                const int x = segs & 1;
+                if (c.first_seg &&
+                    !mbar_sleep_wait(&bars.d2empty[x], (uint32_t)(((segs >> 1) & 1) ^ 1))) {
                     ok = false;
                     break;
                 }
-                if (!mbar_sleep_wait(&bars.qfull, (uint32_t)(ci & 1))) {
+                if (!mbar_sleep_wait(&bars.qfull[qb], qpar)) {
                     ok = false;
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t qh = sbase + OFF_Q, ql = qh + Q_PLANE;
+                const uint32_t d2 = tmem + kD2Off + (uint32_t)x * kD2Cols;
 #pragma unroll
                 for (int ks = 0; ks < kC / 16; ks++) {
-                    // K step: 16 bf16 along a Q row; 16 rows (1 KB) down F.
+                    // K step: chunk elements 16 ks .. +15; 16 rows (1 KB) down F.
                     const uint64_t bdesc = desc_sw64_mn(fB + (uint32_t)ks * 1024u, F1_TERM);
-                    tc::umma(tmem + kD2, desc_sw128(qh + (uint32_t)ks * 32u), bdesc, id96m,
-                             (c.first_seg && ks == 0) ? 0u : 1u);
-                    tc::umma(tmem + kD2, desc_sw128(ql + (uint32_t)ks * 32u), bdesc, id64m, 1u);
+                    umma_ts(d2, qcol + (uint32_t)ks * 16u, bdesc, id96m,
+                            (c.first_seg && ks == 0) ? 0u : 1u);
+                    umma_ts(d2, qcol + (uint32_t)ks * 16u + 8u, bdesc, id64m, 1u);
                 }
-                tc::umma_commit(&bars.qempty);
+                tc::umma_commit(&bars.qempty[qb]);
                 tc::umma_commit(&bars.fempty[s]);
                 if (c.last_seg) {
-                    tc::umma_commit(&bars.d2full);
+                    tc::umma_commit(&bars.d2full[x]);
                     ++segs;
                 }
             }
+            qlast = qr;
+            fr.next();
+            qr.next();
             ++ci;
         }
         if (!ok) give_up();
+        if (!*abort_flag && ci > 0) {
+            // The arrivals of this thread's last commits land before the CTA
+            // exits.
+            if (first) {
+                mbar_sleep_wait(&bars.d1full[qlast.slot], qlast.par);
+                if (tiles > 0) mbar_sleep_wait(&bars.tempty, (uint32_t)((tiles - 1) & 1));
+            } else {
+                mbar_sleep_wait(&bars.qempty[qlast.slot], qlast.par);
+            }
+        }
         if (*abort_flag) {
             uint64_t *dr = first ? &bars.drain[0] : &bars.drain[1];
             tc::umma_commit(dr);
             mbar_sleep_wait(dr, 0);
         }
     } else if (warp >= kEpiWarp0) {
-        // ---- epilogue: WH -> Q, and the contraction -> f64 partials --------
-        const int q = warp & 3;                  // lane quarter this warp may read
+        // ---- epilogue: W H -> Q in place, T, and the contraction -> partials
+        const int q = warp & 3;                  // lane quarter this warp may access
         const int pw = (warp - kEpiWarp0) >> 2;  // its share of the chunk / the ranks
-        const int e0 = pw * kPartElems;        // first chunk element of this warp
+        const int e0 = pw * kPartElems;          // first chunk element of this warp
         const int o = q * 32 + lane;             // output (TMEM lane) within the tile
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        unsigned char *qrow0 = smem + OFF_Q + o * 128;  // this output's Q row (hi plane)
+        // This quarter's rows of T for the tile `major` (warps pw < 3, one
+        // term each), after the last MMA1 of the previous tile.
+        auto write_t = [&](int major, int tiles_done) -> bool {
+            if (pw >= kTWarps) return true;
+            if (tiles_done > 0 && !warp_wait(&bars.tempty, (uint32_t)((tiles_done - 1) & 1)))
+                return false;
+            tc::tc_fence_after();
+            const uint4 *src = reinterpret_cast<const uint4 *>(
+                xT + ((size_t)pw * xpadT + (size_t)major * kM + o) * kR);
+            uint32_t r[16];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint4 x = __ldg(src + i);
+                r[4 * i] = x.x;
+                r[4 * i + 1] = x.y;
+                r[4 * i + 2] = x.z;
+                r[4 * i + 3] = x.w;
+            }
+            tmem_st16_wait(tmem + lane_off + kTOff + (uint32_t)(pw * (kR / 2)), r);
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars.tfull);
+            return true;
+        };
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         const int major0 = (int)(u0 / sk.major_units());
-        long long ci = 0;
-        int segs = 0, prev_t = -1;
+        RingPos<kVStages> vr;
+        RingPos<kNB> qr;
+        int segs = 0, tiles = 0, prev_t = -1;
+        // A finished segment waiting to be drained (one chunk late).
+        bool pend = false, pend_last_tile = false;
+        int pend_x = 0, pend_major = 0;
+        uint32_t pend_par = 0;
         double sum[kPartRanks];
 #pragma unroll
         for (int i = 0; i < kPartRanks; i++) sum[i] = 0.0;
-        while (w.ok && !*abort_flag) {
-            const ChunkInfo c = take(w, sk, kext, prev_t);
-            prev_t = c.t;
-            const int s = (int)(ci % kVStages), db = (int)(ci & 1);
-            // V first: its slot is refilled as soon as every epilogue thread
-            // has read its 16 values.
-            if (!warp_wait(&bars.vfull[s], (uint32_t)((ci / kVStages) & 1))) {
-                give_up();
-                break;
-            }
-            const unsigned char *vs = smem + s * V_BYTES;
-            uint32_t packh[kPartElems / 2], packl[kPartElems / 2];  // Q hi / lo, bf16 pairs
-            {
-                // Elements e0 .. e0 + 15 of the chunk.
-                float v[16];
-                if (HPASS) {
-                    const float *vf = reinterpret_cast<const float *>(vs);
-#pragma unroll
-                    for (int i = 0; i < 16; i++) v[i] = vf[(e0 + i) * kM + o];
-                } else {
-                    // Box e0 / 32 holds columns (e0 / 32) * 32 .. +31 of rows
-                    // 0..127, 16-byte chunk ch of row o at (ch ^ (o & 7)).
-                    const unsigned char *row = vs + (e0 >> 5) * (V_BYTES / 2) + o * 128;
-#pragma unroll
-                    for (int c4 = 0; c4 < 4; c4++) {
-                        const int ch = ((e0 & 31) >> 2) + c4;
-                        const float4 x =
-                            *reinterpret_cast<const float4 *>(row + ((ch ^ (o & 7)) << 4));
-                        v[4 * c4] = x.x;
-                        v[4 * c4 + 1] = x.y;
-                        v[4 * c4 + 2] = x.z;
-                        v[4 * c4 + 3] = x.w;
-                    }
-                }
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars.vempty[s]);
-                // W H as the sum of the three column groups.
-                if (!warp_wait(&bars.d1full[db], (uint32_t)((ci >> 1) & 1))) {
-                    give_up();
-                    break;
-                }
-                tc::tc_fence_after();
-                float g0[16], g1[16], g2[16];
-                const uint32_t ta =
-                    tmem + lane_off + kD1 + (uint32_t)db * kD1Cols + (uint32_t)e0;
-                tc::tmem_ld16(ta, g0);
-                tc::tmem_ld16(ta + 64, g1);
-                tc::tmem_ld16(ta + 128, g2);
-                tc::tmem_wait_ld();
-#pragma unroll
-                for (int i = 0; i < 16; i += 2) {
-                    float qv[2];
-#pragma unroll
-                    for (int e = 0; e < 2; e++) {
-                        const float wh = g0[i + e] + g1[i + e] + g2[i + e];
-                        qv[e] = (wh != 0.f) ? ratio_div(v[i + e], wh) : 0.f;
-                    }
-                    const __nv_bfloat162 hi = __floats2bfloat162_rn(qv[0], qv[1]);
-                    const float2 hf = __bfloat1622float2(hi);
-                    const __nv_bfloat162 lo = __floats2bfloat162_rn(qv[0] - hf.x, qv[1] - hf.y);
-                    packh[i / 2] = *reinterpret_cast<const uint32_t *>(&hi);
-                    packl[i / 2] = *reinterpret_cast<const uint32_t *>(&lo);
-                }
-            }
+        auto drain = [&]() -> bool {
+            if (!warp_wait(&bars.d2full[pend_x], pend_par)) return false;
+            tc::tc_fence_after();
+            // Ranks pw * 8 .. +7 of the three groups (the products with Fh,
+            // Fm, Fl); their sum is the contraction.
+            uint32_t x0[8], x1[8], x2[8];
+            const uint32_t ta = tmem + lane_off + kD2Off + (uint32_t)pend_x * kD2Cols +
+                                (uint32_t)(pw * kPartRanks);
+            tmem_ld8(ta, x0);
+            tmem_ld8(ta + kR, x1);
+            tmem_ld8(ta + 2 * kR, x2);
+            tc::tmem_wait_ld();
             tc::tc_fence_before();
             __syncwarp();
-            if (lane == 0) mbar_arrive(&bars.d1empty[db]);
-            // Q of the previous chunk must have been read by its MMA2.
-            if (!warp_wait(&bars.qempty, (uint32_t)((ci & 1) ^ 1))) {
-                give_up();
-                break;
-            }
-            unsigned char *qrow = qrow0;
+            if (lane == 0) mbar_arrive(&bars.d2empty[pend_x]);
 #pragma unroll
-            for (int c2 = 0; c2 < 2; c2++) {
-                const int kc = (e0 >> 3) + c2;  // 16-byte chunk of the 128-byte Q row
-                const int pos = (kc ^ (o & 7)) << 4;
-                *reinterpret_cast<uint4 *>(qrow + pos) =
-                    make_uint4(packh[4 * c2], packh[4 * c2 + 1], packh[4 * c2 + 2],
-                               packh[4 * c2 + 3]);
-                *reinterpret_cast<uint4 *>(qrow + Q_PLANE + pos) =
-                    make_uint4(packl[4 * c2], packl[4 * c2 + 1], packl[4 * c2 + 2],
-                               packl[4 * c2 + 3]);
-            }
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars.qfull);
-            if (c.last_seg) {
-                if (!warp_wait(&bars.d2full, (uint32_t)(segs & 1))) {
-                    give_up();
-                    break;
-                }
-                tc::tc_fence_after();
-                // Ranks pw * 8 .. +7 of the three groups (the products with
-                // Fh, Fm, Fl); their sum is the contraction.
-                uint32_t x0[8], x1[8], x2[8];
-                const uint32_t ta = tmem + lane_off + kD2 + (uint32_t)(pw * kPartRanks);
-                tmem_ld8(ta, x0);
-                tmem_ld8(ta + kR, x1);
-                tmem_ld8(ta + 2 * kR, x2);
-                tc::tmem_wait_ld();
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) mbar_arrive(&bars.d2empty);
-#pragma unroll
-                for (int i = 0; i < kPartRanks; i++)
-                    sum[i] += (double)(__uint_as_float(x0[i]) + __uint_as_float(x1[i]) +
-                                       __uint_as_float(x2[i]));
-                ++segs;
-            }
-            if (c.last_tile) {
-                double *dst = part + ((size_t)b * sk.slots + (size_t)(c.major - major0)) *
+            for (int i = 0; i < kPartRanks; i++)
+                sum[i] += (double)(__uint_as_float(x0[i]) + __uint_as_float(x1[i]) +
+                                   __uint_as_float(x2[i]));
+            if (pend_last_tile) {
+                double *dst = part + ((size_t)b * sk.slots + (size_t)(pend_major - major0)) *
                                          (size_t)kM * RP;
 #pragma unroll
                 for (int i = 0; i < kPartRanks; i++) {
@@ -580,8 +577,108 @@ __global__ void __launch_bounds__(kThreads, 1)
                     sum[i] = 0.0;
                 }
             }
-            ++ci;
+            pend = false;
+            return true;
+        };
+        bool ok = true;
+        if (w.ok) {
+            ok = write_t(w.cur.major, 0);
+            tiles = 1;
         }
+        while (ok && w.ok && !*abort_flag) {
+            const ChunkInfo c = take(w, sk, kext, prev_t);
+            prev_t = c.t;
+            const int s = vr.slot;
+            const int qb = qr.slot;
+            const uint32_t qpar = qr.par;
+            // V first: its slot is refilled as soon as every epilogue warp
+            // has read it.
+            if (!warp_wait(&bars.vfull[s], vr.par)) {
+                ok = false;
+                break;
+            }
+            const unsigned char *vs = smem + s * V_BYTES;
+            float v[16];
+            if (HPASS) {
+                const float *vf = reinterpret_cast<const float *>(vs);
+#pragma unroll
+                for (int i = 0; i < 16; i++) v[i] = vf[(e0 + i) * kM + o];
+            } else {
+                // Box e0 / 32 holds columns (e0 / 32) * 32 .. +31 of rows
+                // 0..127, 16-byte chunk ch of row o at (ch ^ (o & 7)).
+                const unsigned char *row = vs + (e0 >> 5) * (V_BYTES / 2) + o * 128;
+#pragma unroll
+                for (int c4 = 0; c4 < 4; c4++) {
+                    const int ch = ((e0 & 31) >> 2) + c4;
+                    const float4 x = *reinterpret_cast<const float4 *>(row + ((ch ^ (o & 7)) << 4));
+                    v[4 * c4] = x.x;
+                    v[4 * c4 + 1] = x.y;
+                    v[4 * c4 + 2] = x.z;
+                    v[4 * c4 + 3] = x.w;
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars.vempty[s]);
+            // W H of this warp's 16 elements, then Q over it.
+            if (!warp_wait(&bars.d1full[qb], qpar)) {
+                ok = false;
+                break;
+            }
+            tc::tc_fence_after();
+            const uint32_t ta = tmem + lane_off + (uint32_t)qb * kQCols + (uint32_t)e0;
+            float wh[16];
+            tc::tmem_ld16(ta, wh);
+            tc::tmem_wait_ld();
+            uint32_t qp[16];  // [0, 8): hi pairs, [8, 16): lo pairs
+#pragma unroll
+            for (int i = 0; i < 16; i += 2) {
+                // q = v / wh as v times an approximate reciprocal (two
+                // elements a packed multiply), 0 where wh is 0.
+                float2 qv = __fmul2_rn(make_float2(v[i], v[i + 1]),
+                                       make_float2(rcp_approx(wh[i]), rcp_approx(wh[i + 1])));
+                qv.x = (wh[i] != 0.f) ? qv.x : 0.f;
+                qv.y = (wh[i + 1] != 0.f) ? qv.y : 0.f;
+                const __nv_bfloat162 hi = __float22bfloat162_rn(qv);
+                const uint32_t hb = *reinterpret_cast<const uint32_t *>(&hi);
+                const float2 hf = make_float2(__uint_as_float(hb << 16),
+                                              __uint_as_float(hb & 0xffff0000u));
+                // lo = bf16(q - hi); q - hi is exact in f32.
+                const __nv_bfloat162 lo =
+                    __float22bfloat162_rn(__ffma2_rn(hf, make_float2(-1.f, -1.f), qv));
+                qp[i / 2] = hb;
+                qp[8 + i / 2] = *reinterpret_cast<const uint32_t *>(&lo);
+            }
+            tmem_st16_wait(ta, qp);
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars.qfull[qb]);
+            // The segment finished one chunk ago (its MMA2 has had this
+            // chunk's ratio step to complete).
+            if (pend && !drain()) {
+                ok = false;
+                break;
+            }
+            if (c.last_seg) {
+                pend = true;
+                pend_x = segs & 1;
+                pend_par = (uint32_t)((segs >> 1) & 1);
+                pend_last_tile = c.last_tile;
+                pend_major = c.major;
+                ++segs;
+            }
+            // The next tile's T, once the last MMA1 of this one is done.
+            if (c.last_tile && w.ok) {
+                if (!write_t(w.cur.major, tiles)) {
+                    ok = false;
+                    break;
+                }
+                ++tiles;
+            }
+            vr.next();
+            qr.next();
+        }
+        if (ok && pend && !*abort_flag && !drain()) ok = false;
+        if (!ok) give_up();
     }
     tc::tc_fence_before();
     __syncthreads();

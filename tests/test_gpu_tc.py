@@ -44,9 +44,12 @@ def test_one_iteration_matches_oracle(oracle, n, p, r):
 
 # brunet's split-bf16 passes (tcr.cuh): W H and the contraction on the tensor
 # cores, the ratio in f32.  Shapes with ragged tiles (128 outputs), chunks
-# (64 elements) and segments (2048 terms), ranks 1..32.
+# (64 elements) and segments (2048 terms), ranks 1..32; the two flat shapes
+# give a CTA several short tiles in a row (the tile operand is reloaded in
+# tensor memory each time).
 @pytest.mark.parametrize("n,p,r", [(1000, 1500, 20), (257, 3001, 3), (2000, 700, 32),
-                                   (130, 200, 16), (64, 64, 1), (4100, 129, 7)])
+                                   (130, 200, 16), (64, 64, 1), (4100, 129, 7),
+                                   (100, 40000, 12), (40000, 100, 12)])
 def test_brunet_one_iteration_matches_oracle(oracle, n, p, r):
     V = synthetic.counts_matrix(n, p, max(2, r // 2), 0.3, seed=n + p)
     W0, H0 = nmf_rs.random_init(V, r, seed=3)
