@@ -58,6 +58,9 @@ const StreamOps *stream_ops_f64(int rp);
 // Tensor-core passes of the split-bf16 form (stream_tc.cu).  Tiles are 128
 // outputs wide, units 64 streamed elements, segments at most 32 units.
 constexpr int kTcTile = 128, kTcUnit = 64, kTcSegUnits = 32;
+// brunet's tensor-core passes (tcr.cuh) stream units of 128 elements,
+// segments of 16 units (the same 2048 terms per f32 sum).
+constexpr int kTcrUnit = 128, kTcrSegUnits = 16;
 // hpass: D[j][k] = sum_i V[i][j] W[i][k] (ah/al: the split V^T, p x n);
 // otherwise D[i][k] = sum_j V[i][j] H[k][j] (ah/al: the split V).  Maps of
 // A have box {64, 128}; b3: the factor's three bf16 terms (box {64, RPN});
@@ -76,10 +79,9 @@ void tc_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void
 // split-bf16 passes.  hpass: N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j];
 // otherwise N[i][k] = sum_j H[k][j] V[i][j] / (W H)[i][j].  v: the f32 V (H
 // pass box {128, 64}; W pass box {32, 128}, 128-B swizzle); t: the tile
-// factor's [3][xpadT][32] bf16 terms (device pointer, 16-byte aligned); f1:
-// the chunk factor's [3][xpadF][32] terms (box {32, 64}, 64-B swizzle).
-cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t,
-                            const CUtensorMap &f1, int xpadT, int xpadF, int kext, int RP,
+// factor's [3][xpadT][32] bf16 terms, f1: the chunk factor's [3][xpadF][32]
+// terms (device pointers, 16-byte aligned).
+cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t, const void *f1, int xpadT, int xpadF, int kext, int RP,
                             const StreamK &sk, double *part, RunState *st, cudaStream_t s);
 // F(k, x) = F[k * fk + x * fx] (R x K) -> three bf16 terms as [3][RPN][ldk]
 // (kx) and as [3][xpad][32] (xk); either may be null.

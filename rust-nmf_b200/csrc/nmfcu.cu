@@ -532,7 +532,7 @@ struct PassSet {
     // planes as tile (box 128 rows) and chunk (box 64 rows) operands.
     bool tcr = false;
     int64_t xpadW = 0, xpadH = 0;
-    CUtensorMap tmVrH, tmVrW, tmXwF, tmXhF;
+    CUtensorMap tmVrH, tmVrW;
 };
 
 // The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
@@ -565,10 +565,20 @@ StreamK plan_tc_w(int64_t n, int64_t p, int sms) {
     return fold_sk(
         plan_sk((n + kTcTile - 1) / kTcTile, (p + kTcUnit - 1) / kTcUnit, kTcSegUnits, sms));
 }
+StreamK plan_tcr_h(int64_t n, int64_t p, int sms) {
+    return fold_sk(plan_sk((p + kTcTile - 1) / kTcTile, (n + kTcrUnit - 1) / kTcrUnit,
+                           kTcrSegUnits, sms));
+}
+StreamK plan_tcr_w(int64_t n, int64_t p, int sms) {
+    return fold_sk(plan_sk((n + kTcTile - 1) / kTcTile, (p + kTcrUnit - 1) / kTcrUnit,
+                           kTcrSegUnits, sms));
+}
 size_t tc_partial_bytes(const Plan &pl, int sms) {
     const StreamK h = plan_tc_h(pl.n, pl.p, sms), w = plan_tc_w(pl.n, pl.p, sms);
+    const StreamK rh = plan_tcr_h(pl.n, pl.p, sms), rw = plan_tcr_w(pl.n, pl.p, sms);
     return sizeof(double) * (size_t)pl.RP * kTcTile *
-           std::max((size_t)h.G * h.slots, (size_t)w.G * w.slots);
+           std::max({(size_t)h.G * h.slots, (size_t)w.G * w.slots, (size_t)rh.G * rh.slots,
+                     (size_t)rw.G * rw.slots});
 }
 
 // Partial-sum bytes the two passes of `so` need for this shape.
@@ -670,11 +680,6 @@ nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, i
     NMF_TRY(encode_2d(&ps->tmVrH, V32, true, pl.n, pl.p, ld32, 128, 64));
     NMF_TRY(encode_2d(&ps->tmVrW, V32, true, pl.n, pl.p, ld32, 32, 128,
                       CU_TENSOR_MAP_SWIZZLE_128B));
-    unsigned char *xw = c->Xs.as<unsigned char>();
-    unsigned char *xh = xw + (size_t)3 * ps->xpadW * kTcrRank * 2;
-    const CUtensorMapSwizzle sw64 = CU_TENSOR_MAP_SWIZZLE_64B;
-    NMF_TRY(encode_2d_bf16(&ps->tmXwF, xw, 3 * ps->xpadW, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
-    NMF_TRY(encode_2d_bf16(&ps->tmXhF, xh, 3 * ps->xpadH, kTcrRank, kTcrRank, kTcrRank, 64, sw64));
     return NMFCU_OK;
 }
 
@@ -773,7 +778,7 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
         // brunet, split-bf16 form: the bf16 terms of W (the chunk operand of
         // both MMAs) and of H (the tile operand of W H); tensor-core ratio
         // pass; update.
-        const StreamK sk = plan_tc_h(pl.n, pl.p, c->sms);
+        const StreamK sk = plan_tcr_h(pl.n, pl.p, c->sms);
         unsigned char *xw = c->Xs.as<unsigned char>();
         unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
         {
@@ -785,7 +790,7 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
-            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, xh, ps.tmXwF, (int)ps.xpadH,
+            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, xh, xw, (int)ps.xpadH,
                                      (int)ps.xpadW, pl.n, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
@@ -839,7 +844,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     if (ps.tcr) {
         // brunet, split-bf16 form: the bf16 terms of H (the chunk operand)
         // and of W (the tile operand); tensor-core ratio pass; update.
-        const StreamK sk = plan_tc_w(pl.n, pl.p, c->sms);
+        const StreamK sk = plan_tcr_w(pl.n, pl.p, c->sms);
         unsigned char *xw = c->Xs.as<unsigned char>();
         unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
         {
@@ -851,7 +856,7 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
-            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, xw, ps.tmXhF, (int)ps.xpadW,
+            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, xw, xh, (int)ps.xpadW,
                                      (int)ps.xpadH, pl.p, pl.RP, sk, c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);

@@ -46,7 +46,7 @@ __global__ void split_factor_both(const double *__restrict__ F, int64_t fk, int6
 }
 
 template <bool HPASS>
-cudaError_t launch_one(const CUtensorMap &v, const void *t, const CUtensorMap &f1,
+cudaError_t launch_one(const CUtensorMap &v, const void *t, const void *f1,
                        int xpadT, int xpadF, int kext, int RP, const StreamK &sk, double *part,
                        RunState *st, cudaStream_t s) {
     // The attribute lives in each device's context: set it once per device
@@ -62,15 +62,15 @@ cudaError_t launch_one(const CUtensorMap &v, const void *t, const CUtensorMap &f
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < kAttrDevices) configured[dev].store(true, std::memory_order_release);
     }
-    tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, static_cast<const __nv_bfloat16 *>(t), f1,
-                                                  xpadT, xpadF, kext, RP, sk, part, st);
+    tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, static_cast<const __nv_bfloat16 *>(t),
+                                                  static_cast<const __nv_bfloat16 *>(f1), xpadT,
+                                                  xpadF, kext, RP, sk, part, st);
     return cudaGetLastError();
 }
 
 }  // namespace tcr
 
-cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t,
-                            const CUtensorMap &f1, int xpadT, int xpadF, int kext, int RP,
+cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t, const void *f1, int xpadT, int xpadF, int kext, int RP,
                             const StreamK &sk, double *part, RunState *st, cudaStream_t s) {
     if (sk.G <= 0) return cudaSuccess;
     return hpass ? tcr::launch_one<true>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st, s)

@@ -7,10 +7,10 @@
 //   H pass  N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j]
 //   W pass  N[i][k] = sum_j H[k][j] V[i][j] / (W H)[i][j]
 // Per tile of 128 outputs (columns j for the H pass, rows i for the W pass)
-// and chunk of 64 streamed elements (rows i, columns j) the pass runs two
+// and unit of 128 streamed elements (rows i, columns j) the pass runs two
 // MMAs with the element-wise step between them, like the FP64 ratio passes:
 //   MMA1  WH[o][e] = sum_k T[o][k] F[e][k]      T: the tile's factor rows,
-//                                               F: the chunk's factor rows
+//                                               F: the unit's factor rows
 //   ratio Q[o][e]  = V[o][e] / WH[o][e]         (0 where WH is 0), f32, on
 //                                               the CUDA cores, split into
 //                                               bf16 hi + lo
@@ -19,38 +19,44 @@
 // the factors are L2-resident.  Factor operands are three bf16 terms each
 // (Fh + Fm + Fl ~ F to about 2^-24).
 //
+// A tcgen05 MMA (M = 128, K = 16) costs about the same issue time for any N
+// up to 128, so the pass is shaped to issue few, wide MMAs: a 128-element
+// unit makes MMA1 N = 128 (12 MMAs a unit: six term products x two 16-rank
+// K steps), MMA2 is 8 K steps x 2 (Qh, Ql) with N = 96 / 64.
+//
 // Tensor memory carries everything that is not streamed, so shared memory
-// holds only the two TMA rings (V and the chunk factor F) and its bandwidth
-// goes to the streams:
+// holds only the two rings (V and the unit factor F) and its bandwidth goes
+// to the streams:
 //   * T, the tile operand of MMA1, sits in tensor memory for the whole tile
 //     (MMA1 reads A from tensor memory): its three terms, 16 columns each.
 //   * MMA1 adds the six products Th Fh, Th Fm, Th Fl, Tm Fh, Tm Fm, Tl Fh
-//     (products down to 2^-16 x 2^-8) into ONE 64-column accumulator per
-//     chunk, so the ratio step reads one value an element.
+//     (products down to 2^-16 x 2^-8) into ONE 128-column accumulator per
+//     unit, so the ratio step reads one value an element.
 //   * The ratio step writes Q back over the W H it has just read, as bf16
-//     pairs: for chunk elements 16g .. 16g + 15 the hi terms fill columns
+//     pairs: for unit elements 16g .. 16g + 15 the hi terms fill columns
 //     16g .. 16g + 7 and the lo terms 16g + 8 .. 16g + 15 of the same
 //     buffer, and MMA2 reads them as its A operand (K step g: Qh at 16g, Ql
-//     at 16g + 8).  Each epilogue warp reads and rewrites only its own 16
+//     at 16g + 8).  Each epilogue warp reads and rewrites only its own 32
 //     columns.  MMA2 contracts Qh [Fh; Fm; Fl] + Ql [Fh; Fm] (N = 96 / 64,
 //     B = F read MN-major) into a segment accumulator of three column groups.
-//   * Four W H / Q buffers (a buffer is freed by the MMA2 that read its Q),
-//     two segment accumulators (drained one chunk late, so MMA2 of the next
+//   * Two W H / Q buffers (a buffer is freed by the MMA2 that read its Q),
+//     two segment accumulators (drained one unit late, so MMA2 of the next
 //     segment never waits on the drain).
 //
-// One CTA per SM, twenty warps: warp 0 loads V into its ring (a slot is
-// refilled as soon as the ratio step has read it), warp 1 the chunk factor
-// terms, warp 2 owns the tensor memory and issues MMA1 as soon as a buffer
-// is free, warp 3 issues MMA2 behind the ratio step, warps 4..19 form Q and
-// drain the contraction: warp w reads tensor-memory lanes 32 (w mod 4) ..
-// +31 and the four warps of a lane quarter take 16 of the chunk's 64
-// elements each (three of them also write the quarter's rows of T when a
-// tile starts).  The stream-K split, the 2048-term segments of every f32
-// sum and the folded f64 partials (one per CTA and tile, layout H:
-// [RP][128], W: [128][RP]) are those of the split-bf16 lee passes, so the
+// One CTA per SM, twenty warps: warp 0 loads V by TMA into a ring of
+// half-unit slots (a slot is refilled as soon as the ratio step has read
+// it), warp 1 copies the unit factor terms with plain asynchronous copies,
+// warp 2 owns the tensor memory and issues MMA1 as soon as a buffer is free,
+// warp 3 issues MMA2 behind the ratio step, warps 4..19 form Q and drain the
+// contraction: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 and the
+// four warps of a lane quarter take 32 of the unit's 128 elements each
+// (three of them also write the quarter's rows of T when a tile starts).
+// The stream-K split folds a CTA's segments (16 units: 2048 terms per f32
+// sum) of one tile in f64 into one partial per CTA and tile (layout H:
+// [RP][128], W: [128][RP]), the layout of the split-bf16 lee passes, so the
 // CUDA-core brunet epilogues apply unchanged.  Every wait is bounded; a CTA
-// that gives up records a timeout, lets its own loads and MMAs finish,
-// frees its tensor memory and returns.
+// that gives up records a timeout, lets its own loads and MMAs finish, frees
+// its tensor memory and returns.
 #pragma once
 
 #include "tc.cuh"
@@ -59,27 +65,29 @@ namespace nmfcu {
 namespace tcr {
 
 constexpr int kM = 128;        // outputs per tile (TMEM lanes, MMA M)
-constexpr int kC = 64;         // streamed elements per chunk (one stream-K unit)
+constexpr int kU = 128;        // streamed elements per unit (one stream-K unit; MMA1's N)
+constexpr int kC = 64;         // streamed elements per V ring slot (half a unit)
 constexpr int kR = 32;         // padded rank: MMA1's K, MMA2's N per factor term
-constexpr int kVStages = 5;    // V ring: freed as soon as the ratio step has read V
-constexpr int kFStages = 4;    // factor ring: freed when the chunk's MMA2 is done
-constexpr int kNB = 4;         // W H / Q buffers in tensor memory
+constexpr int kVStages = 4;    // V ring (half units): freed as soon as the ratio step has read V
+constexpr int kFStages = 3;    // factor ring (units): freed when the unit's MMA2 is done
+constexpr int kNB = 2;         // W H / Q buffers (units) in tensor memory
 // Warp roles: V producer, factor producer, MMA1 issuer (and the tensor
 // memory's owner), MMA2 issuer, then the epilogue warps.
 constexpr int kVProdWarp = 0, kFProdWarp = 1, kMma1Warp = 2, kMma2Warp = 3, kEpiWarp0 = 4;
 constexpr int kEpiWarps = 16;
 constexpr int kParts = kEpiWarps / 4;       // epilogue warps per TMEM lane quarter
-constexpr int kPartElems = kC / kParts;    // chunk elements per epilogue warp (16)
+constexpr int kPartElems = kU / kParts;    // unit elements per epilogue warp (32)
 constexpr int kPartRanks = kR / kParts;    // contraction ranks per epilogue warp
 constexpr int kTWarps = 3;                 // warps of a lane quarter that write T
 constexpr int kWarps = kEpiWarp0 + kEpiWarps;
 constexpr int kThreads = kWarps * 32;
-constexpr int kSegUnits = 32;  // chunks per segment: 2048 terms per f32 sum
-static_assert(kPartElems == 16, "a warp's share of the chunk is one 16-element MMA2 K step");
+constexpr int kSegUnits = 16;  // units per segment: 2048 terms per f32 sum
+static_assert(kPartElems == 32 && kVStages == 4,
+              "a warp's share of a unit is two 16-element MMA2 K steps of one V slot");
 
 // Tensor-memory columns.
 constexpr int kTmemCols = 512;
-constexpr uint32_t kQCols = kC;          // one W H / Q buffer
+constexpr uint32_t kQCols = kU;          // one W H / Q buffer
 constexpr uint32_t kTOff = kNB * kQCols;  // T: three terms of 16 columns
 constexpr uint32_t kTCols = 3 * (kR / 2);
 constexpr uint32_t kD2Off = 320;          // two segment accumulators of 96 columns
@@ -88,13 +96,16 @@ static_assert(kTOff + kTCols <= kD2Off && kD2Off + 2 * kD2Cols <= (uint32_t)kTme
               "tensor memory budget");
 
 // Shared memory, from a 1 KB-aligned base.
-constexpr int V_BYTES = kC * kM * 4;      // the f32 V chunk (one V ring slot)
-// One factor term of a chunk: 64 rows x 32 k, 64-B swizzle.  MMA1 reads it
+constexpr int V_BYTES = kC * kM * 4;      // half a unit of f32 V (one V ring slot)
+// One factor term of a unit: 128 rows x 32 k, 64-B swizzle.  MMA1 reads it
 // K-major (B = F, K = k); MMA2 reads the same tile MN-major (B[k][e], N = k
 // along a row, K = e down the rows), the three terms one 32-wide N block
 // apart.
-constexpr int F1_TERM = kC * kR * 2;
+constexpr int F1_TERM = kU * kR * 2;
 constexpr int F_SLOT = 3 * F1_TERM;       // one factor ring slot: the three terms
+constexpr int kFPieces = F_SLOT / 16;      // 16-byte copies a factor slot takes
+constexpr int kFLag = 1;                   // factor slots in flight before one is announced
+static_assert(kFPieces % 32 == 0 && kFLag < kFStages, "factor producer shape");
 constexpr int OFF_F = kVStages * V_BYTES;
 constexpr int OFF_BARS = OFF_F + kFStages * F_SLOT;
 static_assert(V_BYTES % 1024 == 0 && F_SLOT % 1024 == 0 && OFF_F % 1024 == 0 &&
@@ -103,9 +114,9 @@ static_assert(V_BYTES % 1024 == 0 && F_SLOT % 1024 == 0 && OFF_F % 1024 == 0 &&
 
 struct Bars {
     uint64_t vfull[kVStages];   // V slot loaded (TMA bytes)
-    uint64_t vempty[kVStages];  // V slot read (one arrival per epilogue warp)
-    uint64_t ffull[kFStages];   // factor slot loaded (TMA bytes)
-    uint64_t fempty[kFStages];  // factor slot free (MMA2 of its chunk done)
+    uint64_t vempty[kVStages];  // V slot read (one arrival per epilogue warp that reads it)
+    uint64_t ffull[kFStages];   // factor slot landed (one arrival by the factor producer)
+    uint64_t fempty[kFStages];  // factor slot free (MMA2 of its unit done)
     uint64_t tfull, tempty;     // T written (T-writing warps) / free (last MMA1 of its tile done)
     uint64_t d1full[kNB];       // W H of buffer b written (MMA1 commit)
     uint64_t qfull[kNB];        // Q of buffer b written (one arrival per epilogue warp)
@@ -178,6 +189,18 @@ __device__ __forceinline__ void tmem_st16_wait(uint32_t taddr, const uint32_t (&
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// 16-byte asynchronous copy global -> shared (L2 only), and its groups.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // 1 / y to about 1 ulp (approximate reciprocal, subnormals flushed).
 __device__ __forceinline__ float rcp_approx(float y) {
     float r;
@@ -220,14 +243,14 @@ struct RingPos {
     }
 };
 
-// Walks the valid chunks of a CTA's stream-K range in order (units past the
+// Walks the valid units of a CTA's stream-K range in order (units past the
 // streamed extent, which pad the last segment of a tile, are skipped).
 struct ChunkWalker {
     UnitCursor cur;
     long long u, u1;
     bool ok;
     __device__ __forceinline__ void skip(const StreamK &sk, int kext) {
-        while (u < u1 && (long long)cur.along(sk) * kC >= kext) {
+        while (u < u1 && (long long)cur.along(sk) * kU >= kext) {
             ++u;
             cur.next(sk);
         }
@@ -246,13 +269,13 @@ struct ChunkWalker {
     }
 };
 
-// Position of one valid chunk in its tile and segment.
+// Position of one valid unit in its tile and segment.
 struct ChunkInfo {
     int t, major, along;
     bool first_seg, last_seg, last_tile;
 };
 
-// The chunk under `w`, given the tile-segment of the chunk before it (-1 for
+// The unit under `w`, given the tile-segment of the unit before it (-1 for
 // none); advances `w` past it.
 __device__ __forceinline__ ChunkInfo take(ChunkWalker &w, const StreamK &sk, int kext,
                                           int prev_t) {
@@ -267,17 +290,17 @@ __device__ __forceinline__ ChunkInfo take(ChunkWalker &w, const StreamK &sk, int
     return ci;
 }
 
-// HPASS: tile = 128 columns of V, chunk = 64 rows; else tile = 128 rows,
-// chunk = 64 columns.
+// HPASS: tile = 128 columns of V, unit = 128 rows; else tile = 128 rows,
+// unit = 128 columns.
 //   tmV   the f32 V: HPASS box {128, 64}, no swizzle; else box {32, 128},
-//         128-B swizzle (two boxes a chunk)
+//         128-B swizzle (two boxes a V slot)
 //   xT    the tile factor's terms as [3][xpadT][32] bf16 (rows of 64 bytes)
-//   tmF1  the chunk factor's terms as [3][xpadF][32] bf16, box {32, 64}, 64-B swizzle
+//   xF    the unit factor's terms as [3][xpadF][32] bf16 (rows of 64 bytes)
 //   kext  streamed extent (n for the H pass, p for the W pass)
 template <bool HPASS>
 __global__ void __launch_bounds__(kThreads, 1)
     tcr_pass(const __grid_constant__ CUtensorMap tmV, const __nv_bfloat16 *__restrict__ xT,
-             const __grid_constant__ CUtensorMap tmF1,
+             const __nv_bfloat16 *__restrict__ xF,
              int xpadT, int xpadF, int kext, int RP, StreamK sk, double *__restrict__ part,
              RunState *st) {
     extern __shared__ unsigned char tcr_smem_raw[];
@@ -292,7 +315,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (threadIdx.x == 0) {
         for (int s = 0; s < kVStages; s++) {
             mbar_init(&bars.vfull[s], 1);
-            mbar_init(&bars.vempty[s], kEpiWarps);
+            mbar_init(&bars.vempty[s], kEpiWarps / 2);
         }
         for (int s = 0; s < kFStages; s++) {
             mbar_init(&bars.ffull[s], 1);
@@ -333,25 +356,30 @@ __global__ void __launch_bounds__(kThreads, 1)
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         int issued[kVStages] = {0};
-        RingPos<kVStages> vr;
-        while (w.ok && !*abort_flag) {
+        RingPos<kVStages / 2> ur;  // a unit takes V slots 2 slot and 2 slot + 1
+        bool okv = true;
+        while (okv && w.ok && !*abort_flag) {
             const int major = w.cur.major, along = w.cur.along(sk);
-            const int s = vr.slot;
-            if (!mbar_sleep_wait(&bars.vempty[s], vr.par ^ 1u)) {
-                give_up();
-                break;
+            for (int h = 0; h < 2; h++) {
+                const int s = 2 * ur.slot + h;
+                if (!mbar_sleep_wait(&bars.vempty[s], ur.par ^ 1u)) {
+                    give_up();
+                    okv = false;
+                    break;
+                }
+                unsigned char *base = smem + s * V_BYTES;
+                const int e0 = along * kU + h * kC;  // first streamed element of the slot
+                mbar_expect_tx(&bars.vfull[s], V_BYTES);
+                if (HPASS) {
+                    tma_load_2d_hint(base, &tmV, &bars.vfull[s], major * kM, e0, pol_v);
+                } else {
+                    tma_load_2d_hint(base, &tmV, &bars.vfull[s], e0, major * kM, pol_v);
+                    tma_load_2d_hint(base + V_BYTES / 2, &tmV, &bars.vfull[s], e0 + kC / 2,
+                                     major * kM, pol_v);
+                }
+                issued[s]++;
             }
-            unsigned char *base = smem + s * V_BYTES;
-            mbar_expect_tx(&bars.vfull[s], V_BYTES);
-            if (HPASS) {
-                tma_load_2d_hint(base, &tmV, &bars.vfull[s], major * kM, along * kC, pol_v);
-            } else {
-                tma_load_2d_hint(base, &tmV, &bars.vfull[s], along * kC, major * kM, pol_v);
-                tma_load_2d_hint(base + V_BYTES / 2, &tmV, &bars.vfull[s], along * kC + kC / 2,
-                                 major * kM, pol_v);
-            }
-            issued[s]++;
-            vr.next();
+            ur.next();
             w.advance(sk, kext);
         }
         if (*abort_flag) {
@@ -359,39 +387,70 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int i = 0; i < kVStages; i++)
                 if (issued[i] > 0) mbar_sleep_wait(&bars.vfull[i], (uint32_t)((issued[i] - 1) & 1));
         }
-    } else if (warp == kFProdWarp && lane == 0) {
-        // ---- TMA producer of the chunk factor terms (L2-resident) -----------
-        const uint64_t pol_f = l2_evict_last_policy();
+    } else if (warp == kFProdWarp) {
+        // ---- producer of the unit factor terms (L2-resident) ----------------
+        // Plain 16-byte asynchronous copies by the whole warp, not TMA: the
+        // factor slot of a unit is needed by MMA1 long before its V, and TMA
+        // copies would queue behind the V stream's.  Each lane copies 48 of
+        // the slot's 1536 16-byte pieces into the 64-byte-swizzled layout the
+        // MMAs read (16-byte piece j of row r at r * 64 + ((j ^ (r / 2 % 4))
+        // * 16)).  A slot is announced once its copies have landed, kFLag
+        // units later or before the warp would wait for a free slot: wait
+        // for them, order them before the tensor cores' reads (proxy fence),
+        // then one arrival.
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
-        int issued[kFStages] = {0};
-        RingPos<kFStages> fr;
+        RingPos<kFStages> fr, sig;
+        int unsig = 0;
+        auto announce = [&]() {
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bars.ffull[sig.slot]);
+            sig.next();
+            --unsig;
+        };
         while (w.ok && !*abort_flag) {
             const int along = w.cur.along(sk);
-            const int s = fr.slot;
-            if (!mbar_sleep_wait(&bars.fempty[s], fr.par ^ 1u)) {
-                give_up();
+            // Never hold landed-but-unannounced slots while waiting for a
+            // free one: MMA1 may need them to make progress.
+            if (unsig > 0 &&
+                !__all_sync(0xffffffffu, mbar_try_wait(&bars.fempty[fr.slot], fr.par ^ 1u))) {
+                cp_async_wait<0>();
+                while (unsig > 0) announce();
+            }
+            if (!warp_wait(&bars.fempty[fr.slot], fr.par ^ 1u)) {
+                if (lane == 0) give_up();
                 break;
             }
-            unsigned char *base = smem + OFF_F + s * F_SLOT;
-            mbar_expect_tx(&bars.ffull[s], F_SLOT);
-            for (int q = 0; q < 3; q++)
-                tma_load_2d_hint(base + q * F1_TERM, &tmF1, &bars.ffull[s], 0,
-                                 q * xpadF + along * kC, pol_f);
-            issued[s]++;
+            const uint32_t dst0 = smem_u32(smem + OFF_F + fr.slot * F_SLOT);
+#pragma unroll
+            for (int i = 0; i < kFPieces / 32; i++) {
+                const int k = lane + 32 * i;
+                const int t = k / (kU * 4), r = (k >> 2) & (kU - 1), j = k & 3;
+                const __nv_bfloat16 *src =
+                    xF + (((size_t)t * xpadF + (size_t)along * kU + r) * kR + j * 8);
+                cp_async16(dst0 + (uint32_t)(t * F1_TERM + r * 64 + ((j ^ ((r >> 1) & 3)) << 4)),
+                           src);
+            }
+            cp_async_commit();
             fr.next();
+            ++unsig;
+            if (unsig > kFLag) {
+                cp_async_wait<kFLag>();
+                announce();
+            }
             w.advance(sk, kext);
         }
-        if (*abort_flag) {
-            for (int i = 0; i < kFStages; i++)
-                if (issued[i] > 0) mbar_sleep_wait(&bars.ffull[i], (uint32_t)((issued[i] - 1) & 1));
-        }
+        // The remaining slots (or, after a give-up, only this warp's own
+        // copies) land before the CTA exits.
+        cp_async_wait<0>();
+        while (unsig > 0 && !*abort_flag) announce();
     } else if ((warp == kMma1Warp || warp == kMma2Warp) && lane == 0) {
         // ---- MMA issuers ------------------------------------------------------
-        // MMA1 (W H of a chunk) runs ahead, held back only by free buffers,
+        // MMA1 (W H of a unit) runs ahead, held back only by free buffers,
         // the tile's T and landed factor terms; MMA2 (the contraction)
         // follows the ratio step.  Each commit covers its own thread's MMAs.
-        constexpr uint32_t id64 = tc::instr_desc<64, false>();
+        constexpr uint32_t id128 = tc::instr_desc<kU, false>();
         constexpr uint32_t id96m = instr_desc_bmn<96>();  // MMA2: B = F MN-major
         constexpr uint32_t id64m = instr_desc_bmn<64>();
         const uint32_t sbase = smem_u32(smem);
@@ -412,7 +471,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t fB = sbase + OFF_F + s * F_SLOT;
             const uint32_t qcol = tmem + (uint32_t)qb * kQCols;
             if (first) {
-                // MMA1 of chunk ci into buffer qb.
+                // MMA1 of unit ci into buffer qb (N = the unit's 128 elements).
                 if (!mbar_sleep_wait(&bars.ffull[s], fr.par)) {
                     ok = false;
                     break;
@@ -442,14 +501,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                             tmem + kTOff + (uint32_t)(ta[pr] * (kR / 2) + ks * 8);
                         const uint64_t bdesc =
                             desc_sw64(fB + (uint32_t)(fa[pr] * F1_TERM) + (uint32_t)ks * 32u);
-                        umma_ts(qcol, a, bdesc, id64, (pr > 0 || ks > 0) ? 1u : 0u);
+                        umma_ts(qcol, a, bdesc, id128, (pr > 0 || ks > 0) ? 1u : 0u);
                     }
                 }
                 tc::umma_commit(&bars.d1full[qb]);
                 if (c.last_tile) tc::umma_commit(&bars.tempty);
             } else {
-                // MMA2 of chunk ci into segment accumulator segs & 1.  The
-                // factor slot landed before MMA1 of this chunk, which the
+                // MMA2 of unit ci into segment accumulator segs & 1.  The
+                // factor slot landed before MMA1 of this unit, which the
                 // ratio step waited for.
                 const int x = segs & 1;
                 if (c.first_seg &&
@@ -464,8 +523,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::tc_fence_after();
                 const uint32_t d2 = tmem + kD2Off + (uint32_t)x * kD2Cols;
 #pragma unroll
-                for (int ks = 0; ks < kC / 16; ks++) {
-                    // K step: chunk elements 16 ks .. +15; 16 rows (1 KB) down F.
+                for (int ks = 0; ks < kU / 16; ks++) {
+                    // K step: unit elements 16 ks .. +15; 16 rows (1 KB) down F.
                     const uint64_t bdesc = desc_sw64_mn(fB + (uint32_t)ks * 1024u, F1_TERM);
                     umma_ts(d2, qcol + (uint32_t)ks * 16u, bdesc, id96m,
                             (c.first_seg && ks == 0) ? 0u : 1u);
@@ -502,8 +561,10 @@ __global__ void __launch_bounds__(kThreads, 1)
     } else if (warp >= kEpiWarp0) {
         // ---- epilogue: W H -> Q in place, T, and the contraction -> partials
         const int q = warp & 3;                  // lane quarter this warp may access
-        const int pw = (warp - kEpiWarp0) >> 2;  // its share of the chunk / the ranks
-        const int e0 = pw * kPartElems;          // first chunk element of this warp
+        const int pw = (warp - kEpiWarp0) >> 2;  // its share of the unit / the ranks
+        const int e0 = pw * kPartElems;          // first unit element of this warp
+        const int vh = e0 / kC;                  // the unit's V slot (half) it reads
+        const int ev = e0 - vh * kC;             // first element within that slot
         const int o = q * 32 + lane;             // output (TMEM lane) within the tile
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
         // This quarter's rows of T for the tile `major` (warps pw < 3, one
@@ -533,10 +594,10 @@ __global__ void __launch_bounds__(kThreads, 1)
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
         const int major0 = (int)(u0 / sk.major_units());
-        RingPos<kVStages> vr;
+        RingPos<kVStages / 2> ur;
         RingPos<kNB> qr;
         int segs = 0, tiles = 0, prev_t = -1;
-        // A finished segment waiting to be drained (one chunk late).
+        // A finished segment waiting to be drained (one unit late).
         bool pend = false, pend_last_tile = false;
         int pend_x = 0, pend_major = 0;
         uint32_t pend_par = 0;
@@ -588,72 +649,84 @@ __global__ void __launch_bounds__(kThreads, 1)
         while (ok && w.ok && !*abort_flag) {
             const ChunkInfo c = take(w, sk, kext, prev_t);
             prev_t = c.t;
-            const int s = vr.slot;
+            const int s = 2 * ur.slot + vh;
             const int qb = qr.slot;
             const uint32_t qpar = qr.par;
-            // V first: its slot is refilled as soon as every epilogue warp
-            // has read it.
-            if (!warp_wait(&bars.vfull[s], vr.par)) {
+            // V first: its slot is refilled as soon as the eight warps that
+            // read it are done.
+            if (!warp_wait(&bars.vfull[s], ur.par)) {
                 ok = false;
                 break;
             }
             const unsigned char *vs = smem + s * V_BYTES;
-            float v[16];
-            if (HPASS) {
-                const float *vf = reinterpret_cast<const float *>(vs);
+            // This warp's 32 elements, 16 at a time: V, W H from tensor
+            // memory, Q written over it.  The V slot is released after the
+            // second group's read, W H is awaited before the first group's.
+#pragma unroll 1
+            for (int g = 0; g < kPartElems / 16; g++) {
+                float v[16];
+                if (HPASS) {
+                    const float *vf = reinterpret_cast<const float *>(vs);
 #pragma unroll
-                for (int i = 0; i < 16; i++) v[i] = vf[(e0 + i) * kM + o];
-            } else {
-                // Box e0 / 32 holds columns (e0 / 32) * 32 .. +31 of rows
-                // 0..127, 16-byte chunk ch of row o at (ch ^ (o & 7)).
-                const unsigned char *row = vs + (e0 >> 5) * (V_BYTES / 2) + o * 128;
+                    for (int i = 0; i < 16; i++) v[i] = vf[(ev + 16 * g + i) * kM + o];
+                } else {
+                    // Box ev / 32 holds columns (ev / 32) * 32 .. +31 of rows
+                    // 0..127, 16-byte chunk ch of row o at (ch ^ (o & 7)).
+                    const unsigned char *row = vs + (ev >> 5) * (V_BYTES / 2) + o * 128;
 #pragma unroll
-                for (int c4 = 0; c4 < 4; c4++) {
-                    const int ch = ((e0 & 31) >> 2) + c4;
-                    const float4 x = *reinterpret_cast<const float4 *>(row + ((ch ^ (o & 7)) << 4));
-                    v[4 * c4] = x.x;
-                    v[4 * c4 + 1] = x.y;
-                    v[4 * c4 + 2] = x.z;
-                    v[4 * c4 + 3] = x.w;
+                    for (int c4 = 0; c4 < 4; c4++) {
+                        const int ch = 4 * g + c4;
+                        const float4 x =
+                            *reinterpret_cast<const float4 *>(row + ((ch ^ (o & 7)) << 4));
+                        v[4 * c4] = x.x;
+                        v[4 * c4 + 1] = x.y;
+                        v[4 * c4 + 2] = x.z;
+                        v[4 * c4 + 3] = x.w;
+                    }
                 }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars.vempty[s]);
-            // W H of this warp's 16 elements, then Q over it.
-            if (!warp_wait(&bars.d1full[qb], qpar)) {
-                ok = false;
-                break;
-            }
-            tc::tc_fence_after();
-            const uint32_t ta = tmem + lane_off + (uint32_t)qb * kQCols + (uint32_t)e0;
-            float wh[16];
-            tc::tmem_ld16(ta, wh);
-            tc::tmem_wait_ld();
-            uint32_t qp[16];  // [0, 8): hi pairs, [8, 16): lo pairs
+                if (g == kPartElems / 16 - 1) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&bars.vempty[s]);
+                }
+                if (g == 0) {
+                    if (!warp_wait(&bars.d1full[qb], qpar)) {
+                        ok = false;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                }
+                const uint32_t ta =
+                    tmem + lane_off + (uint32_t)qb * kQCols + (uint32_t)(e0 + 16 * g);
+                float wh[16];
+                tc::tmem_ld16(ta, wh);
+                tc::tmem_wait_ld();
+                uint32_t qp[16];  // [0, 8): hi pairs, [8, 16): lo pairs
 #pragma unroll
-            for (int i = 0; i < 16; i += 2) {
-                // q = v / wh as v times an approximate reciprocal (two
-                // elements a packed multiply), 0 where wh is 0.
-                float2 qv = __fmul2_rn(make_float2(v[i], v[i + 1]),
-                                       make_float2(rcp_approx(wh[i]), rcp_approx(wh[i + 1])));
-                qv.x = (wh[i] != 0.f) ? qv.x : 0.f;
-                qv.y = (wh[i + 1] != 0.f) ? qv.y : 0.f;
-                const __nv_bfloat162 hi = __float22bfloat162_rn(qv);
-                const uint32_t hb = *reinterpret_cast<const uint32_t *>(&hi);
-                const float2 hf = make_float2(__uint_as_float(hb << 16),
-                                              __uint_as_float(hb & 0xffff0000u));
-                // lo = bf16(q - hi); q - hi is exact in f32.
-                const __nv_bfloat162 lo =
-                    __float22bfloat162_rn(__ffma2_rn(hf, make_float2(-1.f, -1.f), qv));
-                qp[i / 2] = hb;
-                qp[8 + i / 2] = *reinterpret_cast<const uint32_t *>(&lo);
+                for (int i = 0; i < 16; i += 2) {
+                    // q = v / wh as v times an approximate reciprocal (two
+                    // elements a packed multiply), 0 where wh is 0.
+                    float2 qv = __fmul2_rn(make_float2(v[i], v[i + 1]),
+                                           make_float2(rcp_approx(wh[i]), rcp_approx(wh[i + 1])));
+                    qv.x = (wh[i] != 0.f) ? qv.x : 0.f;
+                    qv.y = (wh[i + 1] != 0.f) ? qv.y : 0.f;
+                    const __nv_bfloat162 hi = __float22bfloat162_rn(qv);
+                    const uint32_t hb = *reinterpret_cast<const uint32_t *>(&hi);
+                    const float2 hf = make_float2(__uint_as_float(hb << 16),
+                                                  __uint_as_float(hb & 0xffff0000u));
+                    // lo = bf16(q - hi); q - hi is exact in f32.
+                    const __nv_bfloat162 lo =
+                        __float22bfloat162_rn(__ffma2_rn(hf, make_float2(-1.f, -1.f), qv));
+                    qp[i / 2] = hb;
+                    qp[8 + i / 2] = *reinterpret_cast<const uint32_t *>(&lo);
+                }
+                tmem_st16_wait(ta, qp);
             }
-            tmem_st16_wait(ta, qp);
+            if (!ok) break;
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars.qfull[qb]);
-            // The segment finished one chunk ago (its MMA2 has had this
-            // chunk's ratio step to complete).
+            // The segment finished one unit ago (its MMA2 has had this
+            // unit's ratio step to complete).
             if (pend && !drain()) {
                 ok = false;
                 break;
@@ -674,7 +747,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 }
                 ++tiles;
             }
-            vr.next();
+            ur.next();
             qr.next();
         }
         if (ok && pend && !*abort_flag && !drain()) ok = false;
