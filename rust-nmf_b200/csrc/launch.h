@@ -75,18 +75,24 @@ void tc_split_v(const double *V, int64_t ldv, void *Vh, void *Vl, int64_t ldb, v
 void tc_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *out, int RPN,
                      int64_t ldk, const RunState *st, int sms, cudaStream_t s);
 
-// brunet's tensor-core passes (stream_tcr.cu), on the stream-K split of the
-// split-bf16 passes.  hpass: N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j];
-// otherwise N[i][k] = sum_j H[k][j] V[i][j] / (W H)[i][j].  v: the f32 V (H
-// pass box {128, 64}; W pass box {32, 128}, 128-B swizzle); t: the tile
-// factor's [3][xpadT][32] bf16 terms, f1: the chunk factor's [3][xpadF][32]
-// terms (device pointers, 16-byte aligned).
-cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t, const void *f1, int xpadT, int xpadF, int kext, int RP,
-                            const StreamK &sk, double *part, RunState *st, cudaStream_t s);
-// F(k, x) = F[k * fk + x * fx] (R x K) -> three bf16 terms as [3][RPN][ldk]
-// (kx) and as [3][xpad][32] (xk); either may be null.
-void tcr_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *kx, int RPN,
-                      int64_t ldk, void *xk, int64_t xpad, const RunState *st, int sms,
-                      cudaStream_t s);
+// brunet's tensor-core passes (stream_tcr.cu), on their own stream-K split
+// (units of kTcrUnit elements, kTcrSegUnits units a segment).  hpass:
+// N[j][k] = sum_i W[i][k] V[i][j] / (W H)[i][j]; otherwise N[i][k] =
+// sum_j H[k][j] V[i][j] / (W H)[i][j].  v: the f32 V (H pass box {128, 64};
+// W pass box {32, 128}, 128-B swizzle); t: the tile factor's rows in the
+// tile layout (device pointer, rows of tcr_concat_rank(rank) bf16, from
+// tcr_split_factor); f1: the unit factor's rows in the unit layout (box
+// {64, 128}, 128-B swizzle).
+cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t,
+                            const CUtensorMap &f1, int kext, int rank, int RP, const StreamK &sk,
+                            double *part, RunState *st, cudaStream_t s);
+// The padded concatenated rank (row length, bf16) of the two layouts:
+// 128 for rank <= 21, 192 up to 32.
+int tcr_concat_rank(int rank);
+// F(k, x) = F[k * fk + x * fx] (R x K) -> xpad rows of tcr_concat_rank(R)
+// bf16 in the tile layout ([Th Th Th Tm Tm Tl], blocks of R) and the unit
+// layout ([Fh Fm Fl Fh Fm Fh]), zero-padded; either output may be null.
+void tcr_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, int64_t xpad,
+                      void *tile, void *unit, const RunState *st, int sms, cudaStream_t s);
 
 }  // namespace nmfcu

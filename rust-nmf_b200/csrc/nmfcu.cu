@@ -423,7 +423,7 @@ struct nmfcu_context {
     DevBuf V64, V32, W, H, part, pg, ps, Gw, sw, Gh, sh, Gw2, sw2, obj, dev, state;
     DevBuf Wf32, Ht64, Ht32;
     DevBuf Vs, Fs;     // split-bf16 form: V hi/lo, the factor's three terms
-    DevBuf Xs;         // split-bf16 brunet: W and H as [3][xpad][32] bf16 terms
+    DevBuf Xs;         // split-bf16 brunet: W and H in the tcr tile and unit layouts
     DevBuf Wns, Hns;   // nsNMF: W S (n x RP), S H (RP x p)
     DevBuf off, rsv, addon;  // offset: row offsets, row sums of V, W^T off
     DevBuf Wprev, Hprev;     // ehals: the iterate before the last extrapolation
@@ -532,7 +532,7 @@ struct PassSet {
     // planes as tile (box 128 rows) and chunk (box 64 rows) operands.
     bool tcr = false;
     int64_t xpadW = 0, xpadH = 0;
-    CUtensorMap tmVrH, tmVrW;
+    CUtensorMap tmVrH, tmVrW, tmXwU, tmXhU;  // tcr: V (f32), W / H unit layouts
 };
 
 // The split-bf16 form runs lee / offset / hals / dnmf on the tensor cores;
@@ -665,6 +665,23 @@ nmfcu_status make_tc_passset(nmfcu_context *c, const Plan &pl, const double *V64
     return NMFCU_OK;
 }
 
+// The split factors of brunet's tensor-core passes in c->Xs: W's rows then
+// H's, each in the tile layout then the unit layout (xpad rows of
+// tcr_concat_rank(r) bf16).
+struct TcrTerms {
+    void *w_tile, *w_unit, *h_tile, *h_unit;
+};
+TcrTerms tcr_terms(nmfcu_context *c, const PassSet &ps, int r) {
+    const size_t row = 2 * (size_t)tcr_concat_rank(r);
+    unsigned char *base = c->Xs.as<unsigned char>();
+    TcrTerms x;
+    x.w_tile = base;
+    x.w_unit = base + row * ps.xpadW;
+    x.h_tile = base + 2 * row * ps.xpadW;
+    x.h_unit = base + 2 * row * ps.xpadW + row * ps.xpadH;
+    return x;
+}
+
 // brunet's split-bf16 passes (tensor cores) over the f32 V (leading
 // dimension ld32): added to the f32 pass set `ps` made for that V.
 nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, int64_t ld32,
@@ -680,6 +697,10 @@ nmfcu_status add_tcr_passes(nmfcu_context *c, const Plan &pl, const void *V32, i
     NMF_TRY(encode_2d(&ps->tmVrH, V32, true, pl.n, pl.p, ld32, 128, 64));
     NMF_TRY(encode_2d(&ps->tmVrW, V32, true, pl.n, pl.p, ld32, 32, 128,
                       CU_TENSOR_MAP_SWIZZLE_128B));
+    const int kc = tcr_concat_rank(pl.r);
+    const TcrTerms x = tcr_terms(c, *ps, pl.r);
+    NMF_TRY(encode_2d_bf16(&ps->tmXwU, x.w_unit, ps->xpadW, kc, kc, 64, 128));
+    NMF_TRY(encode_2d_bf16(&ps->tmXhU, x.h_unit, ps->xpadH, kc, kc, 64, 128));
     return NMFCU_OK;
 }
 
@@ -775,23 +796,22 @@ nmfcu_status h_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     if (ps.tcr) {
-        // brunet, split-bf16 form: the bf16 terms of W (the chunk operand of
-        // both MMAs) and of H (the tile operand of W H); tensor-core ratio
-        // pass; update.
+        // brunet, split-bf16 form: W's bf16 terms in the unit layout (the
+        // streamed operand of both MMAs) and H's in the tile layout (the
+        // tile operand of W H); tensor-core ratio pass; update.
         const StreamK sk = plan_tcr_h(pl.n, pl.p, c->sms);
-        unsigned char *xw = c->Xs.as<unsigned char>();
-        unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
+        const TcrTerms x = tcr_terms(c, ps, pl.r);
         {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, nullptr, kTcrRank, 0, xw, ps.xpadW, st,
-                             c->sms, s);
-            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, nullptr, kTcrRank, 0, xh, ps.xpadH, st,
-                             c->sms, s);
+            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, ps.xpadW, nullptr, x.w_unit, st, c->sms,
+                             s);
+            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, ps.xpadH, x.h_tile, nullptr, st, c->sms,
+                             s);
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_HSTEP);
-            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, xh, xw, (int)ps.xpadH,
-                                     (int)ps.xpadW, pl.n, pl.RP, sk, c->part.as<double>(), st, s));
+            CUDA_TRY(tcr_pass_launch(true, ps.tmVrH, x.h_tile, ps.tmXwU, pl.n, pl.r, pl.RP, sk,
+                                     c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
         ps.so->h_epi(a.H, nullptr, pl.p, c->part.as<double>(), sk, kTcTile, e, st, s);
@@ -842,22 +862,22 @@ nmfcu_status w_step(nmfcu_context *c, const RunArgs &a, const PassSet &ps, const
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
     if (ps.tcr) {
-        // brunet, split-bf16 form: the bf16 terms of H (the chunk operand)
-        // and of W (the tile operand); tensor-core ratio pass; update.
+        // brunet, split-bf16 form: H's bf16 terms in the unit layout (the
+        // streamed operand) and W's in the tile layout; tensor-core ratio
+        // pass; update.
         const StreamK sk = plan_tcr_w(pl.n, pl.p, c->sms);
-        unsigned char *xw = c->Xs.as<unsigned char>();
-        unsigned char *xh = xw + (size_t)3 * ps.xpadW * kTcrRank * 2;
+        const TcrTerms x = tcr_terms(c, ps, pl.r);
         {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
-            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, nullptr, kTcrRank, 0, xh, ps.xpadH, st,
-                             c->sms, s);
-            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, nullptr, kTcrRank, 0, xw, ps.xpadW, st,
-                             c->sms, s);
+            tcr_split_factor(a.H, pl.p, 1, pl.r, pl.p, ps.xpadH, nullptr, x.h_unit, st, c->sms,
+                             s);
+            tcr_split_factor(a.W, 1, pl.RP, pl.r, pl.n, ps.xpadW, x.w_tile, nullptr, st, c->sms,
+                             s);
         }
         if (sk.G > 0) {
             nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_WSTEP);
-            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, xw, xh, (int)ps.xpadW,
-                                     (int)ps.xpadH, pl.p, pl.RP, sk, c->part.as<double>(), st, s));
+            CUDA_TRY(tcr_pass_launch(false, ps.tmVrW, x.w_tile, ps.tmXhU, pl.p, pl.r, pl.RP, sk,
+                                     c->part.as<double>(), st, s));
         }
         nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
         ps.so->w_epi(a.Wout ? a.Wout : a.W, pl.n, c->part.as<double>(), sk, kTcTile, e, st, s);
@@ -1089,7 +1109,7 @@ std::vector<WsNeed> workspace_needs(nmfcu_context *c, const Plan &pl, bool need_
         v.push_back({&c->Vs, 2 * 2 * ((size_t)pl.n * (size_t)round8(pl.p) +
                                       (size_t)pl.p * (size_t)round8(pl.n))});
     if (need_tcr)
-        v.push_back({&c->Xs, 3 * 2 * (size_t)kTcrRank *
+        v.push_back({&c->Xs, 4 * (size_t)tcr_concat_rank(std::min(pl.r, kTcrRank)) *
                                  (size_t)(round128(pl.n) + round128(pl.p))});
     v.push_back({&c->Ht64, sizeof(double) * (size_t)pl.p * stream_ops_f64(pl.RP)->rps()});
     if (need_f32) {

@@ -1,5 +1,5 @@
 // stream_tcr.cu -- launch of brunet's tensor-core passes (tcr.cuh) and the
-// split of a factor into the two bf16 term layouts they read.
+// split of a factor into the two concatenated bf16 term layouts they read.
 #include <atomic>
 #include <algorithm>
 
@@ -20,35 +20,41 @@ __device__ __forceinline__ void split3(double f, __nv_bfloat16 &h, __nv_bfloat16
     l = __double2bfloat16(r1 - (double)__bfloat162float(m));
 }
 
-__global__ void split_factor_both(const double *__restrict__ F, int64_t fk, int64_t fx, int R,
-                                  int K, __nv_bfloat16 *__restrict__ kx, int RPN, int64_t ldk,
-                                  __nv_bfloat16 *__restrict__ xk, int64_t xpad,
-                                  const RunState *st) {
+// F (f64, logically R x K with F(k, x) = F[k * fk + x * fx]) -> rows x of
+// KC bf16 in the two layouts of tcr.cuh: element b * R + k (block b < 6,
+// k < R) holds term tile_term[b] of F(k, x) in `tile` and term unit_term[b]
+// in `unit`; everything else (x >= K, positions >= 6 R) is zero.  Either
+// output may be null.
+__global__ void split_factor_concat(const double *__restrict__ F, int64_t fk, int64_t fx, int R,
+                                    int K, int KC, int64_t xpad,
+                                    __nv_bfloat16 *__restrict__ tile,
+                                    __nv_bfloat16 *__restrict__ unit, const RunState *st) {
     if (run_stopped(st)) return;
+    const int64_t total = xpad * KC;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (kx) {
-        const int64_t plane = (int64_t)RPN * ldk;
-        for (int64_t t = t0; t < plane; t += stride) {
-            const int64_t k = t / ldk, x = t - k * ldk;
-            const double f = (k < R && x < K) ? F[k * fk + x * fx] : 0.0;
-            split3(f, kx[t], kx[plane + t], kx[2 * plane + t]);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const int64_t x = t / KC;
+        const int p = (int)(t - x * KC);
+        __nv_bfloat16 vt = __float2bfloat16(0.f), vu = vt;
+        if (x < K && p < 6 * R) {
+            const int blk = p / R, k = p - blk * R;
+            __nv_bfloat16 th[3];
+            split3(F[k * fk + x * fx], th[0], th[1], th[2]);
+            // Products Th Fh, Th Fm, Th Fl, Tm Fh, Tm Fm, Tl Fh.
+            constexpr int tile_term[6] = {0, 0, 0, 1, 1, 2};
+            constexpr int unit_term[6] = {0, 1, 2, 0, 1, 0};
+            vt = th[tile_term[blk]];
+            vu = th[unit_term[blk]];
         }
-    }
-    if (xk) {
-        const int64_t plane = xpad * kR;
-        for (int64_t t = t0; t < plane; t += stride) {
-            const int64_t x = t / kR, k = t - x * kR;
-            const double f = (k < R && x < K) ? F[k * fk + x * fx] : 0.0;
-            split3(f, xk[t], xk[plane + t], xk[2 * plane + t]);
-        }
+        if (tile) tile[t] = vt;
+        if (unit) unit[t] = vu;
     }
 }
 
-template <bool HPASS>
-cudaError_t launch_one(const CUtensorMap &v, const void *t, const void *f1,
-                       int xpadT, int xpadF, int kext, int RP, const StreamK &sk, double *part,
-                       RunState *st, cudaStream_t s) {
+template <bool HPASS, int KC>
+cudaError_t launch_one(const CUtensorMap &v, const void *t, const CUtensorMap &f1, int kext,
+                       int rank, int RP, const StreamK &sk, double *part, RunState *st,
+                       cudaStream_t s) {
     // The attribute lives in each device's context: set it once per device
     // and instantiation.  Serving worker threads launch these passes
     // concurrently, so the flags are atomics (a repeated set is harmless).
@@ -57,35 +63,41 @@ cudaError_t launch_one(const CUtensorMap &v, const void *t, const void *f1,
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kAttrDevices || !configured[dev].load(std::memory_order_acquire)) {
-        e = cudaFuncSetAttribute(tcr_pass<HPASS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 SMEM);
+        e = cudaFuncSetAttribute(tcr_pass<HPASS, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 Cfg<KC>::SMEM);
         if (e != cudaSuccess) return e;
         if (dev >= 0 && dev < kAttrDevices) configured[dev].store(true, std::memory_order_release);
     }
-    tcr_pass<HPASS><<<sk.G, kThreads, SMEM, s>>>(v, static_cast<const __nv_bfloat16 *>(t),
-                                                  static_cast<const __nv_bfloat16 *>(f1), xpadT,
-                                                  xpadF, kext, RP, sk, part, st);
+    tcr_pass<HPASS, KC><<<sk.G, kThreads, Cfg<KC>::SMEM, s>>>(
+        v, static_cast<const __nv_bfloat16 *>(t), f1, kext, rank, RP, sk, part, st);
     return cudaGetLastError();
 }
 
 }  // namespace tcr
 
-cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t, const void *f1, int xpadT, int xpadF, int kext, int RP,
-                            const StreamK &sk, double *part, RunState *st, cudaStream_t s) {
+int tcr_concat_rank(int rank) { return rank <= 21 ? 128 : 192; }
+
+cudaError_t tcr_pass_launch(bool hpass, const CUtensorMap &v, const void *t,
+                            const CUtensorMap &f1, int kext, int rank, int RP, const StreamK &sk,
+                            double *part, RunState *st, cudaStream_t s) {
     if (sk.G <= 0) return cudaSuccess;
-    return hpass ? tcr::launch_one<true>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st, s)
-                 : tcr::launch_one<false>(v, t, f1, xpadT, xpadF, kext, RP, sk, part, st, s);
+    if (rank < 1 || rank > tcr::kMaxRank) return cudaErrorInvalidValue;
+    if (tcr_concat_rank(rank) == 128)
+        return hpass ? tcr::launch_one<true, 128>(v, t, f1, kext, rank, RP, sk, part, st, s)
+                     : tcr::launch_one<false, 128>(v, t, f1, kext, rank, RP, sk, part, st, s);
+    return hpass ? tcr::launch_one<true, 192>(v, t, f1, kext, rank, RP, sk, part, st, s)
+                 : tcr::launch_one<false, 192>(v, t, f1, kext, rank, RP, sk, part, st, s);
 }
 
-void tcr_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, void *kx, int RPN,
-                      int64_t ldk, void *xk, int64_t xpad, const RunState *st, int sms,
-                      cudaStream_t s) {
-    const int64_t work = std::max<int64_t>(kx ? (int64_t)RPN * ldk : 0, xk ? xpad * tcr::kR : 0);
+void tcr_split_factor(const double *F, int64_t fk, int64_t fx, int R, int K, int64_t xpad,
+                      void *tile, void *unit, const RunState *st, int sms, cudaStream_t s) {
+    const int KC = tcr_concat_rank(R);
+    const int64_t work = xpad * KC;
     const unsigned blocks =
         (unsigned)std::max<int64_t>(1, std::min<int64_t>((work + 255) / 256, (int64_t)sms * 8));
-    tcr::split_factor_both<<<blocks, 256, 0, s>>>(F, fk, fx, R, K,
-                                                  static_cast<__nv_bfloat16 *>(kx), RPN, ldk,
-                                                  static_cast<__nv_bfloat16 *>(xk), xpad, st);
+    tcr::split_factor_concat<<<blocks, 256, 0, s>>>(F, fk, fx, R, K, KC, xpad,
+                                                    static_cast<__nv_bfloat16 *>(tile),
+                                                    static_cast<__nv_bfloat16 *>(unit), st);
 }
 
 }  // namespace nmfcu

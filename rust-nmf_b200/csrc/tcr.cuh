@@ -45,7 +45,7 @@
 //
 // One CTA per SM, twenty warps: warp 0 loads V by TMA into a ring of
 // half-unit slots (a slot is refilled as soon as the ratio step has read
-// it), warp 1 copies the unit factor terms with plain asynchronous copies,
+// it), warp 1 loads the unit factor rows by TMA into a ring of their own,
 // warp 2 owns the tensor memory and issues MMA1 as soon as a buffer is free,
 // warp 3 issues MMA2 behind the ratio step, warps 4..19 form Q and drain the
 // contraction: warp w reads tensor-memory lanes 32 (w mod 4) .. +31 and the
@@ -67,94 +67,77 @@ namespace tcr {
 constexpr int kM = 128;        // outputs per tile (TMEM lanes, MMA M)
 constexpr int kU = 128;        // streamed elements per unit (one stream-K unit; MMA1's N)
 constexpr int kC = 64;         // streamed elements per V ring slot (half a unit)
-constexpr int kR = 32;         // padded rank: MMA1's K, MMA2's N per factor term
+constexpr int kMaxRank = 32;
 constexpr int kVStages = 4;    // V ring (half units): freed as soon as the ratio step has read V
-constexpr int kFStages = 3;    // factor ring (units): freed when the unit's MMA2 is done
-constexpr int kNB = 2;         // W H / Q buffers (units) in tensor memory
 // Warp roles: V producer, factor producer, MMA1 issuer (and the tensor
 // memory's owner), MMA2 issuer, then the epilogue warps.
 constexpr int kVProdWarp = 0, kFProdWarp = 1, kMma1Warp = 2, kMma2Warp = 3, kEpiWarp0 = 4;
 constexpr int kEpiWarps = 16;
-constexpr int kParts = kEpiWarps / 4;       // epilogue warps per TMEM lane quarter
-constexpr int kPartElems = kU / kParts;    // unit elements per epilogue warp (32)
-constexpr int kPartRanks = kR / kParts;    // contraction ranks per epilogue warp
-constexpr int kTWarps = 3;                 // warps of a lane quarter that write T
+constexpr int kParts = kEpiWarps / 4;          // epilogue warps per TMEM lane quarter
+constexpr int kPartElems = kU / kParts;       // unit elements per epilogue warp (32)
+constexpr int kPartRanks = kMaxRank / kParts;  // contraction ranks per epilogue warp
 constexpr int kWarps = kEpiWarp0 + kEpiWarps;
 constexpr int kThreads = kWarps * 32;
 constexpr int kSegUnits = 16;  // units per segment: 2048 terms per f32 sum
 static_assert(kPartElems == 32 && kVStages == 4,
               "a warp's share of a unit is two 16-element MMA2 K steps of one V slot");
-
-// Tensor-memory columns.
 constexpr int kTmemCols = 512;
-constexpr uint32_t kQCols = kU;          // one W H / Q buffer
-constexpr uint32_t kTOff = kNB * kQCols;  // T: three terms of 16 columns
-constexpr uint32_t kTCols = 3 * (kR / 2);
-constexpr uint32_t kD2Off = 320;          // two segment accumulators of 96 columns
-constexpr uint32_t kD2Cols = 3 * kR;
-static_assert(kTOff + kTCols <= kD2Off && kD2Off + 2 * kD2Cols <= (uint32_t)kTmemCols,
-              "tensor memory budget");
+constexpr int V_BYTES = kC * kM * 4;  // half a unit of f32 V (one V ring slot)
+constexpr int kKBlock = 16384;        // one 64-element K block of a factor slot (128 rows x 128 B)
 
-// Shared memory, from a 1 KB-aligned base.
-constexpr int V_BYTES = kC * kM * 4;      // half a unit of f32 V (one V ring slot)
-// One factor term of a unit: 128 rows x 32 k, 64-B swizzle.  MMA1 reads it
-// K-major (B = F, K = k); MMA2 reads the same tile MN-major (B[k][e], N = k
-// along a row, K = e down the rows), the three terms one 32-wide N block
-// apart.
-constexpr int F1_TERM = kU * kR * 2;
-constexpr int F_SLOT = 3 * F1_TERM;       // one factor ring slot: the three terms
-constexpr int kFPieces = F_SLOT / 16;      // 16-byte copies a factor slot takes
-constexpr int kFLag = 1;                   // factor slots in flight before one is announced
-static_assert(kFPieces % 32 == 0 && kFLag < kFStages, "factor producer shape");
-constexpr int OFF_F = kVStages * V_BYTES;
-constexpr int OFF_BARS = OFF_F + kFStages * F_SLOT;
-static_assert(V_BYTES % 1024 == 0 && F_SLOT % 1024 == 0 && OFF_F % 1024 == 0 &&
-                  F1_TERM % 512 == 0,
-              "swizzle atoms need their alignment");
-
-struct Bars {
-    uint64_t vfull[kVStages];   // V slot loaded (TMA bytes)
-    uint64_t vempty[kVStages];  // V slot read (one arrival per epilogue warp that reads it)
-    uint64_t ffull[kFStages];   // factor slot landed (one arrival by the factor producer)
-    uint64_t fempty[kFStages];  // factor slot free (MMA2 of its unit done)
-    uint64_t tfull, tempty;     // T written (T-writing warps) / free (last MMA1 of its tile done)
-    uint64_t d1full[kNB];       // W H of buffer b written (MMA1 commit)
-    uint64_t qfull[kNB];        // Q of buffer b written (one arrival per epilogue warp)
-    uint64_t qempty[kNB];       // buffer b free again (MMA2 commit)
-    uint64_t d2full[2], d2empty[2];  // a segment's contraction done / drained
-    uint64_t drain[2];          // every MMA of an issuer done (abort path)
-    uint32_t tmem_base;
-    int abort;
+// The shape of the pass for a padded concatenated rank KC (128: rank <= 21,
+// 192: rank <= 32).  A factor row in the pass's two layouts holds six
+// blocks of `rank` bf16 each, zero-padded to KC:
+//   tile layout  [Th Th Th Tm Tm Tl]   (MMA1's A, in tensor memory)
+//   unit layout  [Fh Fm Fl Fh Fm Fh]   (MMA1's B and MMA2's B, in shared memory)
+// so MMA1 adds the six products Th Fh, Th Fm, Th Fl, Tm Fh, Tm Fm, Tl Fh in
+// ceil(6 rank / 16) K steps into one accumulator, and the first three
+// blocks of the unit layout are [Fh; Fm; Fl] along MMA2's N.
+template <int KC>
+struct Cfg {
+    static_assert(KC == 128 || KC == 192, "concatenated rank");
+    static constexpr int kFStages = KC == 128 ? 3 : 2;  // factor ring (units)
+    static constexpr int kNB = KC == 128 ? 3 : 2;       // W H / Q buffers (units)
+    static constexpr int kD2Buf = 1;                    // segment accumulators
+    static constexpr int kN2Max = KC == 128 ? 64 : 96;  // MMA2's N: round16(3 rank)
+    // Tensor-memory columns: W H / Q buffers, then T, then the segment
+    // accumulators.
+    static constexpr uint32_t kQCols = kU;
+    static constexpr uint32_t kTOff = kNB * kQCols;
+    static constexpr uint32_t kTCols = KC / 2;
+    static constexpr uint32_t kD2Off = kTOff + kTCols;
+    static constexpr uint32_t kD2Cols = kN2Max;
+    static_assert(kD2Off + kD2Buf * kD2Cols <= (uint32_t)kTmemCols, "tensor memory budget");
+    // Shared memory, from a 1 KB-aligned base: the V ring, the factor ring
+    // (a unit's rows in the unit layout, 128-B swizzle, K blocks of 64).
+    static constexpr int F_SLOT = (KC / 64) * kKBlock;
+    static constexpr int OFF_F = kVStages * V_BYTES;
+    static constexpr int OFF_BARS = OFF_F + kFStages * F_SLOT;
+    struct Bars {
+        uint64_t vfull[kVStages];   // V slot loaded (TMA bytes)
+        uint64_t vempty[kVStages];  // V slot read (one arrival per epilogue warp that reads it)
+        uint64_t ffull[kFStages];   // factor slot loaded (TMA bytes)
+        uint64_t fempty[kFStages];  // factor slot free (MMA2 of its unit done)
+        uint64_t tfull, tempty;     // T written (epilogue warps) / free (last MMA1 of its tile done)
+        uint64_t d1full[kNB];       // W H of buffer b written (MMA1 commit)
+        uint64_t qfull[kNB];        // Q of buffer b written (one arrival per epilogue warp)
+        uint64_t qempty[kNB];       // buffer b free again (MMA2 commit)
+        uint64_t d2full[kD2Buf], d2empty[kD2Buf];  // a segment's contraction done / drained
+        uint64_t drain[2];          // every MMA of an issuer done (abort path)
+        uint32_t tmem_base;
+        int abort;
+    };
+    static constexpr int SMEM = OFF_BARS + (int)sizeof(Bars) + 1024;  // + alignment slack
+    static_assert(SMEM <= 232448, "shared memory per CTA");
+    static_assert(V_BYTES % 1024 == 0 && F_SLOT % 1024 == 0 && OFF_F % 1024 == 0,
+                  "swizzle atoms need their alignment");
 };
-constexpr int SMEM = OFF_BARS + (int)sizeof(Bars) + 1024;  // + alignment slack
-static_assert(SMEM <= 232448, "shared memory per CTA");
 
-// K-major shared-memory descriptor, 64-byte swizzle (rows of 32 bf16): 8-row
-// groups 512 bytes apart.
-__device__ __forceinline__ uint64_t desc_sw64(uint32_t addr) {
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;               // leading byte offset (unused when swizzled)
-    d |= (uint64_t)(512 >> 4) << 32;      // stride byte offset
-    d |= (uint64_t)1 << 46;               // descriptor version (sm_100)
-    d |= (uint64_t)4 << 61;               // 64-byte swizzle
-    return d;
-}
-// MN-major, 64-byte swizzle: rows of 32 MN elements, one per K; 32-wide MN
-// blocks `lbo` bytes apart, 8-K groups 512 bytes apart.
-__device__ __forceinline__ uint64_t desc_sw64_mn(uint32_t addr, uint32_t lbo) {
-    uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)(512 >> 4) << 32;
-    d |= (uint64_t)1 << 46;
-    d |= (uint64_t)4 << 61;
-    return d;
-}
-// Instruction descriptor as tc::instr_desc, with B read MN-major.
-template <int N>
-__host__ __device__ constexpr uint32_t instr_desc_bmn() {
-    return tc::instr_desc<N, false>() | (1u << 16);
+// Instruction descriptor as tc::instr_desc, for a run-time N, with B read
+// MN-major when `b_mn`.
+__device__ __forceinline__ uint32_t instr_desc_rt(int n, bool b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (b_mn ? (1u << 16) : 0u) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kM >> 4) << 24);
 }
 
 // MMA with A read from tensor memory (rows in lanes, two bf16 K elements a
@@ -168,13 +151,11 @@ __device__ __forceinline__ void umma_ts(uint32_t d_tmem, uint32_t a_tmem, uint64
         : "memory");
 }
 
-// 8 consecutive 32-bit columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7])
-        : "r"(taddr));
+// One 32-bit column of this thread's tensor-memory lane.
+__device__ __forceinline__ uint32_t tmem_ld1(uint32_t taddr) {
+    uint32_t r;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    return r;
 }
 // Writes 16 consecutive 32-bit columns of this thread's lane and waits until
 // the writes are done.
@@ -187,18 +168,6 @@ __device__ __forceinline__ void tmem_st16_wait(uint32_t taddr, const uint32_t (&
         "r"(r[15])
         : "memory");
     asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-
-// 16-byte asynchronous copy global -> shared (L2 only), and its groups.
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() {
-    asm volatile("cp.async.commit_group;" ::: "memory");
-}
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // 1 / y to about 1 ulp (approximate reciprocal, subnormals flushed).
@@ -294,20 +263,21 @@ __device__ __forceinline__ ChunkInfo take(ChunkWalker &w, const StreamK &sk, int
 // unit = 128 columns.
 //   tmV   the f32 V: HPASS box {128, 64}, no swizzle; else box {32, 128},
 //         128-B swizzle (two boxes a V slot)
-//   xT    the tile factor's terms as [3][xpadT][32] bf16 (rows of 64 bytes)
-//   xF    the unit factor's terms as [3][xpadF][32] bf16 (rows of 64 bytes)
+//   xT    the tile factor's rows in the tile layout (KC bf16 a row)
+//   tmF   the unit factor's rows in the unit layout, box {64, 128}, 128-B swizzle
 //   kext  streamed extent (n for the H pass, p for the W pass)
-template <bool HPASS>
+template <bool HPASS, int KC>
 __global__ void __launch_bounds__(kThreads, 1)
     tcr_pass(const __grid_constant__ CUtensorMap tmV, const __nv_bfloat16 *__restrict__ xT,
-             const __nv_bfloat16 *__restrict__ xF,
-             int xpadT, int xpadF, int kext, int RP, StreamK sk, double *__restrict__ part,
-             RunState *st) {
+             const __grid_constant__ CUtensorMap tmF, int kext, int rank,
+             int RP, StreamK sk, double *__restrict__ part, RunState *st) {
+    using C = Cfg<KC>;
+    constexpr int kFStages = C::kFStages, kNB = C::kNB, kD2Buf = C::kD2Buf;
     extern __shared__ unsigned char tcr_smem_raw[];
     if (run_stopped(st)) return;
     const uint32_t raw = smem_u32(tcr_smem_raw);
     unsigned char *smem = tcr_smem_raw + ((1024 - (raw & 1023)) & 1023);
-    Bars &bars = *reinterpret_cast<Bars *>(smem + OFF_BARS);
+    typename C::Bars &bars = *reinterpret_cast<typename C::Bars *>(smem + C::OFF_BARS);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int b = blockIdx.x;
     const long long u0 = sk.start(b), u1 = sk.start(b + 1);
@@ -321,18 +291,19 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(&bars.ffull[s], 1);
             mbar_init(&bars.fempty[s], 1);
         }
-        mbar_init(&bars.tfull, 4 * kTWarps);
+        mbar_init(&bars.tfull, kEpiWarps);
         mbar_init(&bars.tempty, 1);
         for (int a = 0; a < kNB; a++) {
             mbar_init(&bars.d1full[a], 1);
             mbar_init(&bars.qfull[a], kEpiWarps);
             mbar_init(&bars.qempty[a], 1);
         }
-        for (int a = 0; a < 2; a++) {
+        for (int a = 0; a < kD2Buf; a++) {
             mbar_init(&bars.d2full[a], 1);
             mbar_init(&bars.d2empty[a], kEpiWarps);
-            mbar_init(&bars.drain[a], 1);
         }
+        mbar_init(&bars.drain[0], 1);
+        mbar_init(&bars.drain[1], 1);
         bars.abort = 0;
         fence_mbar_init();
     }
@@ -387,72 +358,44 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int i = 0; i < kVStages; i++)
                 if (issued[i] > 0) mbar_sleep_wait(&bars.vfull[i], (uint32_t)((issued[i] - 1) & 1));
         }
-    } else if (warp == kFProdWarp) {
-        // ---- producer of the unit factor terms (L2-resident) ----------------
-        // Plain 16-byte asynchronous copies by the whole warp, not TMA: the
-        // factor slot of a unit is needed by MMA1 long before its V, and TMA
-        // copies would queue behind the V stream's.  Each lane copies 48 of
-        // the slot's 1536 16-byte pieces into the 64-byte-swizzled layout the
-        // MMAs read (16-byte piece j of row r at r * 64 + ((j ^ (r / 2 % 4))
-        // * 16)).  A slot is announced once its copies have landed, kFLag
-        // units later or before the warp would wait for a free slot: wait
-        // for them, order them before the tensor cores' reads (proxy fence),
-        // then one arrival.
+    } else if (warp == kFProdWarp && lane == 0) {
+        // ---- TMA producer of the unit factor terms (L2-resident) ------------
+        // The unit layout's rows along * 128 .. +127, one 64-column box (a K
+        // block, 128-B swizzle) at a time.
+        const uint64_t pol_f = l2_evict_last_policy();
         ChunkWalker w;
         w.init(sk, u0, u1, kext);
-        RingPos<kFStages> fr, sig;
-        int unsig = 0;
-        auto announce = [&]() {
-            fence_proxy_async_smem();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bars.ffull[sig.slot]);
-            sig.next();
-            --unsig;
-        };
+        RingPos<kFStages> fr;
+        int issued[kFStages] = {0};
         while (w.ok && !*abort_flag) {
             const int along = w.cur.along(sk);
-            // Never hold landed-but-unannounced slots while waiting for a
-            // free one: MMA1 may need them to make progress.
-            if (unsig > 0 &&
-                !__all_sync(0xffffffffu, mbar_try_wait(&bars.fempty[fr.slot], fr.par ^ 1u))) {
-                cp_async_wait<0>();
-                while (unsig > 0) announce();
-            }
-            if (!warp_wait(&bars.fempty[fr.slot], fr.par ^ 1u)) {
-                if (lane == 0) give_up();
+            if (!mbar_sleep_wait(&bars.fempty[fr.slot], fr.par ^ 1u)) {
+                give_up();
                 break;
             }
-            const uint32_t dst0 = smem_u32(smem + OFF_F + fr.slot * F_SLOT);
-#pragma unroll
-            for (int i = 0; i < kFPieces / 32; i++) {
-                const int k = lane + 32 * i;
-                const int t = k / (kU * 4), r = (k >> 2) & (kU - 1), j = k & 3;
-                const __nv_bfloat16 *src =
-                    xF + (((size_t)t * xpadF + (size_t)along * kU + r) * kR + j * 8);
-                cp_async16(dst0 + (uint32_t)(t * F1_TERM + r * 64 + ((j ^ ((r >> 1) & 3)) << 4)),
-                           src);
-            }
-            cp_async_commit();
+            unsigned char *base = smem + C::OFF_F + fr.slot * C::F_SLOT;
+            mbar_expect_tx(&bars.ffull[fr.slot], C::F_SLOT);
+            for (int kb = 0; kb < KC / 64; kb++)
+                tma_load_2d_hint(base + kb * kKBlock, &tmF, &bars.ffull[fr.slot], kb * 64,
+                                 along * kU, pol_f);
+            issued[fr.slot]++;
             fr.next();
-            ++unsig;
-            if (unsig > kFLag) {
-                cp_async_wait<kFLag>();
-                announce();
-            }
             w.advance(sk, kext);
         }
-        // The remaining slots (or, after a give-up, only this warp's own
-        // copies) land before the CTA exits.
-        cp_async_wait<0>();
-        while (unsig > 0 && !*abort_flag) announce();
+        if (*abort_flag) {
+            // Let this thread's own loads land before the CTA exits.
+            for (int i = 0; i < kFStages; i++)
+                if (issued[i] > 0) mbar_sleep_wait(&bars.ffull[i], (uint32_t)((issued[i] - 1) & 1));
+        }
     } else if ((warp == kMma1Warp || warp == kMma2Warp) && lane == 0) {
         // ---- MMA issuers ------------------------------------------------------
         // MMA1 (W H of a unit) runs ahead, held back only by free buffers,
         // the tile's T and landed factor terms; MMA2 (the contraction)
         // follows the ratio step.  Each commit covers its own thread's MMAs.
         constexpr uint32_t id128 = tc::instr_desc<kU, false>();
-        constexpr uint32_t id96m = instr_desc_bmn<96>();  // MMA2: B = F MN-major
-        constexpr uint32_t id64m = instr_desc_bmn<64>();
+        const int nks1 = (6 * rank + 15) / 16;          // MMA1's K steps
+        const int n2 = (3 * rank + 15) / 16 * 16;       // MMA2's N: [Fh; Fm; Fl]
+        const uint32_t id2 = instr_desc_rt(n2, true);  // MMA2: B = F MN-major
         const uint32_t sbase = smem_u32(smem);
         const bool first = (warp == kMma1Warp);
         ChunkWalker w;
@@ -468,8 +411,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             const int s = fr.slot;
             const int qb = qr.slot;
             const uint32_t qpar = qr.par;
-            const uint32_t fB = sbase + OFF_F + s * F_SLOT;
-            const uint32_t qcol = tmem + (uint32_t)qb * kQCols;
+            const uint32_t fB = sbase + C::OFF_F + s * C::F_SLOT;
+            const uint32_t qcol = tmem + (uint32_t)qb * C::kQCols;
             if (first) {
                 // MMA1 of unit ci into buffer qb (N = the unit's 128 elements).
                 if (!mbar_sleep_wait(&bars.ffull[s], fr.par)) {
@@ -489,30 +432,24 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc::tc_fence_after();
-                // Products (T term, F term): hh, hm, hl, mh, mm, lh; two K
-                // steps of 16 ranks each.
-                constexpr int ta[6] = {0, 0, 0, 1, 1, 2};
-                constexpr int fa[6] = {0, 1, 2, 0, 1, 0};
-#pragma unroll
-                for (int pr = 0; pr < 6; pr++) {
-#pragma unroll
-                    for (int ks = 0; ks < kR / 16; ks++) {
-                        const uint32_t a =
-                            tmem + kTOff + (uint32_t)(ta[pr] * (kR / 2) + ks * 8);
-                        const uint64_t bdesc =
-                            desc_sw64(fB + (uint32_t)(fa[pr] * F1_TERM) + (uint32_t)ks * 32u);
-                        umma_ts(qcol, a, bdesc, id128, (pr > 0 || ks > 0) ? 1u : 0u);
-                    }
+                // The six term products, concatenated along K: K step ks
+                // reads T columns 8 ks .. +7 and the unit rows' elements
+                // 16 ks .. +15 (K block ks / 4, 32 bytes a step within it).
+                for (int ks = 0; ks < nks1; ks++) {
+                    const uint64_t bdesc = tc::smem_desc(
+                        fB + (uint32_t)((ks >> 2) * kKBlock + (ks & 3) * 32), 16, 1024);
+                    umma_ts(qcol, tmem + C::kTOff + (uint32_t)(ks * 8), bdesc, id128,
+                            ks > 0 ? 1u : 0u);
                 }
                 tc::umma_commit(&bars.d1full[qb]);
                 if (c.last_tile) tc::umma_commit(&bars.tempty);
             } else {
-                // MMA2 of unit ci into segment accumulator segs & 1.  The
-                // factor slot landed before MMA1 of this unit, which the
-                // ratio step waited for.
-                const int x = segs & 1;
+                // MMA2 of unit ci into segment accumulator segs % kD2Buf.
+                // The factor slot landed before MMA1 of this unit, which
+                // the ratio step waited for.
+                const int x = segs % kD2Buf;
                 if (c.first_seg &&
-                    !mbar_sleep_wait(&bars.d2empty[x], (uint32_t)(((segs >> 1) & 1) ^ 1))) {
+                    !mbar_sleep_wait(&bars.d2empty[x], (uint32_t)(((segs / kD2Buf) & 1) ^ 1))) {
                     ok = false;
                     break;
                 }
@@ -521,14 +458,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                     break;
                 }
                 tc::tc_fence_after();
-                const uint32_t d2 = tmem + kD2Off + (uint32_t)x * kD2Cols;
+                const uint32_t d2 = tmem + C::kD2Off + (uint32_t)x * C::kD2Cols;
 #pragma unroll
                 for (int ks = 0; ks < kU / 16; ks++) {
-                    // K step: unit elements 16 ks .. +15; 16 rows (1 KB) down F.
-                    const uint64_t bdesc = desc_sw64_mn(fB + (uint32_t)ks * 1024u, F1_TERM);
-                    umma_ts(d2, qcol + (uint32_t)ks * 16u, bdesc, id96m,
+                    // K step: unit elements 16 ks .. +15, 16 rows (2 KB) down
+                    // the unit rows read MN-major (N blocks of 64 elements one
+                    // K block apart).
+                    const uint64_t bdesc = tc::smem_desc(fB + (uint32_t)ks * 2048u, kKBlock, 1024);
+                    umma_ts(d2, qcol + (uint32_t)ks * 16u, bdesc, id2,
                             (c.first_seg && ks == 0) ? 0u : 1u);
-                    umma_ts(d2, qcol + (uint32_t)ks * 16u + 8u, bdesc, id64m, 1u);
+                    umma_ts(d2, qcol + (uint32_t)ks * 16u + 8u, bdesc, id2, 1u);
                 }
                 tc::umma_commit(&bars.qempty[qb]);
                 tc::umma_commit(&bars.fempty[s]);
@@ -567,25 +506,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int ev = e0 - vh * kC;             // first element within that slot
         const int o = q * 32 + lane;             // output (TMEM lane) within the tile
         const uint32_t lane_off = (uint32_t)(q * 32) << 16;
-        // This quarter's rows of T for the tile `major` (warps pw < 3, one
-        // term each), after the last MMA1 of the previous tile.
+        // This quarter's rows of T for the tile `major` (the tile layout, KC
+        // bf16 a row: 16-column pieces pw, pw + 4, ...), after the last MMA1
+        // of the previous tile.
         auto write_t = [&](int major, int tiles_done) -> bool {
-            if (pw >= kTWarps) return true;
             if (tiles_done > 0 && !warp_wait(&bars.tempty, (uint32_t)((tiles_done - 1) & 1)))
                 return false;
             tc::tc_fence_after();
-            const uint4 *src = reinterpret_cast<const uint4 *>(
-                xT + ((size_t)pw * xpadT + (size_t)major * kM + o) * kR);
-            uint32_t r[16];
+            for (int piece = pw; piece < KC / 32; piece += kParts) {
+                const uint4 *src = reinterpret_cast<const uint4 *>(
+                    xT + ((size_t)major * kM + o) * KC + piece * 32);
+                uint32_t r[16];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                const uint4 x = __ldg(src + i);
-                r[4 * i] = x.x;
-                r[4 * i + 1] = x.y;
-                r[4 * i + 2] = x.z;
-                r[4 * i + 3] = x.w;
+                for (int i = 0; i < 4; i++) {
+                    const uint4 x = __ldg(src + i);
+                    r[4 * i] = x.x;
+                    r[4 * i + 1] = x.y;
+                    r[4 * i + 2] = x.z;
+                    r[4 * i + 3] = x.w;
+                }
+                tmem_st16_wait(tmem + lane_off + C::kTOff + (uint32_t)(piece * 16), r);
             }
-            tmem_st16_wait(tmem + lane_off + kTOff + (uint32_t)(pw * (kR / 2)), r);
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars.tfull);
@@ -607,22 +548,27 @@ __global__ void __launch_bounds__(kThreads, 1)
         auto drain = [&]() -> bool {
             if (!warp_wait(&bars.d2full[pend_x], pend_par)) return false;
             tc::tc_fence_after();
-            // Ranks pw * 8 .. +7 of the three groups (the products with Fh,
-            // Fm, Fl); their sum is the contraction.
-            uint32_t x0[8], x1[8], x2[8];
-            const uint32_t ta = tmem + lane_off + kD2Off + (uint32_t)pend_x * kD2Cols +
-                                (uint32_t)(pw * kPartRanks);
-            tmem_ld8(ta, x0);
-            tmem_ld8(ta + kR, x1);
-            tmem_ld8(ta + 2 * kR, x2);
-            tc::tmem_wait_ld();
+            // Ranks pw * 8 .. +7: columns k, rank + k and 2 rank + k hold
+            // the products with Fh, Fm and Fl; their sum is the contraction.
+            float xs[kPartRanks];
+            const uint32_t ta = tmem + lane_off + C::kD2Off + (uint32_t)pend_x * C::kD2Cols;
+#pragma unroll
+            for (int i = 0; i < kPartRanks; i++) {
+                const int k = pw * kPartRanks + i;
+                xs[i] = 0.f;
+                if (k < rank) {  // the same for the whole warp
+                    const uint32_t a0 = tmem_ld1(ta + (uint32_t)k);
+                    const uint32_t a1 = tmem_ld1(ta + (uint32_t)(rank + k));
+                    const uint32_t a2 = tmem_ld1(ta + (uint32_t)(2 * rank + k));
+                    tc::tmem_wait_ld();
+                    xs[i] = __uint_as_float(a0) + __uint_as_float(a1) + __uint_as_float(a2);
+                }
+            }
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&bars.d2empty[pend_x]);
 #pragma unroll
-            for (int i = 0; i < kPartRanks; i++)
-                sum[i] += (double)(__uint_as_float(x0[i]) + __uint_as_float(x1[i]) +
-                                   __uint_as_float(x2[i]));
+            for (int i = 0; i < kPartRanks; i++) sum[i] += (double)xs[i];
             if (pend_last_tile) {
                 double *dst = part + ((size_t)b * sk.slots + (size_t)(pend_major - major0)) *
                                          (size_t)kM * RP;
@@ -696,7 +642,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     tc::tc_fence_after();
                 }
                 const uint32_t ta =
-                    tmem + lane_off + (uint32_t)qb * kQCols + (uint32_t)(e0 + 16 * g);
+                    tmem + lane_off + (uint32_t)qb * C::kQCols + (uint32_t)(e0 + 16 * g);
                 float wh[16];
                 tc::tmem_ld16(ta, wh);
                 tc::tmem_wait_ld();
@@ -733,8 +679,8 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             if (c.last_seg) {
                 pend = true;
-                pend_x = segs & 1;
-                pend_par = (uint32_t)((segs >> 1) & 1);
+                pend_x = segs % kD2Buf;
+                pend_par = (uint32_t)((segs / kD2Buf) & 1);
                 pend_last_tile = c.last_tile;
                 pend_major = c.major;
                 ++segs;
@@ -761,15 +707,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::tmem_dealloc(tmem, kTmemCols);
     }
 }
-
-// The factor F (f64, logically R x K with F(k, x) = F[k * fk + x * fx]) as
-// three bf16 terms in both layouts the passes read: kx = [3][RPN][ldk]
-// (k-rows, as the split-bf16 lee passes) and xk = [3][xpad][32] (x-rows);
-// zero outside k < R, x < K.  Either output may be null.
-__global__ void split_factor_both(const double *__restrict__ F, int64_t fk, int64_t fx, int R,
-                                  int K, __nv_bfloat16 *__restrict__ kx, int RPN, int64_t ldk,
-                                  __nv_bfloat16 *__restrict__ xk, int64_t xpad,
-                                  const RunState *st);
 
 }  // namespace tcr
 }  // namespace nmfcu
