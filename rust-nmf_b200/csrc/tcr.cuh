@@ -19,29 +19,29 @@
 // the factors are L2-resident.  Factor operands are three bf16 terms each
 // (Fh + Fm + Fl ~ F to about 2^-24).
 //
-// A tcgen05 MMA (M = 128, K = 16) costs about the same issue time for any N
-// up to 128, so the pass is shaped to issue few, wide MMAs: a 128-element
-// unit makes MMA1 N = 128 (12 MMAs a unit: six term products x two 16-rank
-// K steps), MMA2 is 8 K steps x 2 (Qh, Ql) with N = 96 / 64.
+// A tcgen05 MMA (M = 128, K = 16) takes about 125 cycles of tensor-pipe
+// time for any N up to 128 (measured), so the pass is shaped to issue few,
+// wide MMAs: a 128-element unit makes MMA1 N = 128, and the six term
+// products are concatenated along K (ceil(6 r / 16) MMAs a unit: 8 at rank
+// 20, not 6 x 2); MMA2 is 8 K steps x 2 (Qh, Ql) with N = round16(3 r).
 //
 // Tensor memory carries everything that is not streamed, so shared memory
-// holds only the two rings (V and the unit factor F) and its bandwidth goes
-// to the streams:
+// holds only the two TMA rings (V, and the unit factor rows):
 //   * T, the tile operand of MMA1, sits in tensor memory for the whole tile
-//     (MMA1 reads A from tensor memory): its three terms, 16 columns each.
-//   * MMA1 adds the six products Th Fh, Th Fm, Th Fl, Tm Fh, Tm Fm, Tl Fh
-//     (products down to 2^-16 x 2^-8) into ONE 128-column accumulator per
+//     (MMA1 reads A from tensor memory) in the tile layout.
+//   * MMA1 sums the six term products into ONE 128-column accumulator per
 //     unit, so the ratio step reads one value an element.
 //   * The ratio step writes Q back over the W H it has just read, as bf16
 //     pairs: for unit elements 16g .. 16g + 15 the hi terms fill columns
 //     16g .. 16g + 7 and the lo terms 16g + 8 .. 16g + 15 of the same
 //     buffer, and MMA2 reads them as its A operand (K step g: Qh at 16g, Ql
 //     at 16g + 8).  Each epilogue warp reads and rewrites only its own 32
-//     columns.  MMA2 contracts Qh [Fh; Fm; Fl] + Ql [Fh; Fm] (N = 96 / 64,
-//     B = F read MN-major) into a segment accumulator of three column groups.
-//   * Two W H / Q buffers (a buffer is freed by the MMA2 that read its Q),
-//     two segment accumulators (drained one unit late, so MMA2 of the next
-//     segment never waits on the drain).
+//     columns.  MMA2 contracts Qh [Fh; Fm; Fl] + Ql [Fh; Fm; Fl] (B = the
+//     unit rows read MN-major) into a segment accumulator whose columns k,
+//     r + k, 2 r + k hold rank k's three terms.
+//   * Two W H / Q buffers (a buffer is freed by the MMA2 that read its Q);
+//     two segment accumulators at ranks up to 21 (drained one unit late, so
+//     MMA2 of the next segment does not wait on the drain), one above.
 //
 // One CTA per SM, twenty warps: warp 0 loads V by TMA into a ring of
 // half-unit slots (a slot is refilled as soon as the ratio step has read
@@ -97,8 +97,8 @@ template <int KC>
 struct Cfg {
     static_assert(KC == 128 || KC == 192, "concatenated rank");
     static constexpr int kFStages = KC == 128 ? 3 : 2;  // factor ring (units)
-    static constexpr int kNB = KC == 128 ? 3 : 2;       // W H / Q buffers (units)
-    static constexpr int kD2Buf = 1;                    // segment accumulators
+    static constexpr int kNB = 2;                       // W H / Q buffers (units)
+    static constexpr int kD2Buf = KC == 128 ? 2 : 1;    // segment accumulators
     static constexpr int kN2Max = KC == 128 ? 64 : 96;  // MMA2's N: round16(3 rank)
     // Tensor-memory columns: W H / Q buffers, then T, then the segment
     // accumulators.
