@@ -102,7 +102,7 @@ def parse():
                                        "sparse"],
                     default="iterate")
     ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the stream")
-    ap.add_argument("--slots", type=int, default=4, help="serve: server slots")
+    ap.add_argument("--slots", type=int, default=8, help="serve: server slots")
     ap.add_argument("--load", type=float, default=0.8,
                     help="serve: Poisson arrival rate as a fraction of the measured capacity")
     ap.add_argument("--runs", type=int, default=64, help="consensus restarts per rank")
@@ -638,6 +638,13 @@ def run_ours(args, world, rank, local):
             extra["rel_objective_vs_fp64"] = abs(o_m - o_plain) / abs(o_plain)
             extra["max_rel_dW_vs_fp64"] = float((W - W64).abs().max() / W64.abs().max())
 
+    if atlas and not args.no_fp64_compare and args.workload == "atlas":
+        # The 2000 x 7750 rank-10 workload (brunet and hals, FP64, 100
+        # iterations from the seeded uniform start), measured beside the
+        # headline: iterations/s and the fused KL ratio passes' GB/s and
+        # FP64 TFLOP/s.
+        extra["pbmc8k"] = small_workload_extra(ctx, local, dev, fp64_tflops, world)
+
     # End to end through the host-pointer C ABI.
     e2e = None
     if not args.no_e2e:
@@ -718,6 +725,68 @@ def run_ours(args, world, rank, local):
         }
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def small_workload_extra(ctx, local, dev, fp64_tflops, world):
+    """brunet and hals in FP64 on the 2000 x 7750 rank-10 workload, 100
+    timed iterations each (after 3 untimed), with the dominant pass's
+    achieved GB/s (one f64 read of V a launch; V fits in L2, so this is L2
+    and HBM together) and, for brunet's fused ratio passes, FP64 TFLOP/s
+    (4 n p r a launch) against a cuBLAS f64 GEMM measured in the same run."""
+    import torch
+
+    from nmf_rs import _native
+
+    n, p, k, alpha, r, iters = WORKLOADS["pbmc8k"]
+    V64, ld64, _, _, W0, H0 = device_workload(n, p, k, alpha, r, 4321, dev)
+    stream = torch.cuda.current_stream(dev)
+    out = {"n": n, "p": p, "rank": r, "iterations": iters, "precision": "fp64",
+           "start": "seeded uniform", "regime": "V (124 MB f64) fits in the 126 MB L2"}
+    for method in ("brunet", "hals"):
+        o = _native.default_options()
+        o.method = _native.parse_method(method)
+        o.stop = 0
+        o.precision = _native.PRECISIONS["fp64"]
+        o.device = local
+
+        def run(iters_, W, H):
+            o.max_iter = iters_
+            ctx.run(o, n, p, r, V64.data_ptr(), _native.F64, ld64, W.data_ptr(), H.data_ptr(),
+                    stream=stream.cuda_stream)
+
+        W, H = W0.clone(), H0.clone()
+        run(3, W, H)
+        W, H = W0.clone(), H0.clone()
+        torch.cuda.synchronize()
+        ctx.reset_timing()
+        ctx.set_timing(True)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run(iters, W, H)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
+        classes = {name: ctx.kernel_time(kc) for name, kc in
+                   (("hstep", _native.KCLASS_HSTEP), ("wstep", _native.KCLASS_WSTEP))}
+        ctx.set_timing(False)
+        dom = max(classes, key=lambda c: classes[c][1])
+        nl, tot = classes[dom]
+        avg = tot / max(nl, 1)
+        line = {"iters_per_s": world * iters / (ms / 1000.0),
+                "dominant_pass": {"kernel": ("h" if dom == "hstep" else "w") + "pass_dmma" +
+                                  ("_ratio" if method == "brunet" else ""),
+                                  "avg_launch_ms": avg,
+                                  "achieved_gbs": n * p * 8 / (avg / 1000.0) / 1e9,
+                                  "pass_share_of_step": (classes["hstep"][1] +
+                                                         classes["wstep"][1]) / ms}}
+        if method == "brunet" and fp64_tflops:
+            tf = 4.0 * n * p * r / (avg / 1000.0) / 1e12
+            line["dominant_pass"]["fp64_tflops"] = tf
+            line["dominant_pass"]["fp64_frac"] = tf / fp64_tflops
+        out[method] = line
+    del V64
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -991,6 +1060,7 @@ def run_consensus(args, world, rank, local):
 # ---------------------------------------------------------------------------
 
 SERVE_METHODS = (("lee", 0.4), ("brunet", 0.3), ("hals", 0.2), ("dnmf", 0.1))
+SERVE_CAL = 64  # requests in the closed-loop capacity sample
 SERVE_MAX = (5000, 50000)
 
 
@@ -1069,6 +1139,8 @@ def run_serve(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     reqs = serve_requests(args.requests)
+    # A fixed sample of the same mix, run closed-loop to measure capacity.
+    cal = serve_requests(SERVE_CAL, seed=23)
     N, P = SERVE_MAX
     # One pinned host V; request i reads its top-left n x p block (ldv = P).
     V64, ld64, V32, ld32, _, _ = device_workload(N, P, 12, 0.3, 5, 4321 + rank, dev)
@@ -1082,7 +1154,7 @@ def run_serve(args, world, rank, local):
     _native.check(lib.nmfcu_server_create(local, args.slots, 0, ctypes.byref(h)))
     gen = np.random.default_rng(5)
     bufs = []
-    for n, p, r, m, it in reqs:
+    for n, p, r, m, it in reqs + cal:
         top = 1.0
         W0 = gen.uniform(0, top, (n, r))
         H0 = gen.uniform(0, top, (r, p))
@@ -1096,7 +1168,7 @@ def run_serve(args, world, rank, local):
     dp = _native._ptr
 
     def submit(i):
-        n, p, r, m, it = reqs[i]
+        n, p, r, m, it = (reqs + cal)[i]
         o, W0, H0, W, H = bufs[i]
         rid = ctypes.c_int64(0)
         _native.check(lib.nmfcu_server_submit(
@@ -1109,17 +1181,20 @@ def run_serve(args, world, rank, local):
         _native.check(lib.nmfcu_server_wait(h, rid, -1, ctypes.byref(ni), ctypes.byref(nd)))
         return ni.value
 
-    # Warm-up and capacity: the first requests as one burst.
+    # Warm-up: the first requests as one burst (untimed).
     warm = list(range(min(len(reqs), max(3, args.warmup) * args.slots)))
-    t0 = time.perf_counter()
     ids = [submit(i) for i in warm]
     for rid in ids:
         wait(rid)
-    burst_s = time.perf_counter() - t0
-    # Capacity in requests/s: work units (rows x columns x rank x iterations)
-    # per second in the burst, over the mean work of a request of the mix.
+    # Capacity: the calibration sample submitted at once (closed loop), in
+    # work units (rows x columns x rank x iterations) per second, over the
+    # mean work of a request of the stream: requests per second.
+    t0 = time.perf_counter()
+    ids = [submit(len(reqs) + j) for j in range(len(cal))]
+    cal_iters = sum(wait(rid) for rid in ids)
+    cal_s = time.perf_counter() - t0
     units = [n * p * r * it for n, p, r, _, it in reqs]
-    rate_cap = sum(units[i] for i in warm) / burst_s / float(np.mean(units))
+    rate_cap = sum(n * p * r * it for n, p, r, _, it in cal) / cal_s / float(np.mean(units))
     lam = args.load * rate_cap  # requests per second
     _native.check(lib.nmfcu_server_reset_stats(h))
     arrivals = np.cumsum(np.random.default_rng(17).exponential(1.0 / lam, len(reqs)))
@@ -1169,9 +1244,13 @@ def run_serve(args, world, rank, local):
                        "shapes": "log-uniform 500x1000..5000x50000", "ranks": "5..30",
                        "iters": "25..200", "mix": "lee .4 brunet .3 hals .2 dnmf .1",
                        "arrival_rate_per_s": lam, "load": args.load,
+                       "capacity": (f"{len(cal)} requests of the same mix (another seed) "
+                                    "submitted at once: " f"{cal_iters / cal_s:.0f} iters/s, "
+                                    f"{rate_cap:.2f} stream requests/s"),
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "max": st.max_ms,
                            "mean_queue": st.mean_queue_ms},
+            "closed_loop_iters_per_s": cal_iters / cal_s,
             "server": {"completed": st.completed, "failed": st.failed,
                        "peak_running": st.peak_running, "peak_bytes": st.peak_bytes,
                        "budget_bytes": st.budget_bytes},

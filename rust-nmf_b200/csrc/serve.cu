@@ -13,8 +13,11 @@
 //     the engine workspace of that shape, computed from the same list the
 //     engine allocates from) fit in the server's budget next to what every
 //     slot holds; requests that arrive while others run are admitted as
-//     slots and memory free up, smallest work first, with a bypass
-//     limit so a large request is not starved by small ones;
+//     slots and memory free up, first come first served within two size
+//     classes: large requests (V of at least 2^25 elements, whose passes
+//     alone keep HBM busy) run on at most a quarter of the slots, so a
+//     small request never queues behind a run of large ones and a large
+//     one is never overtaken by later large ones;
 //   * a slot keeps its buffers for the next request (no allocation on the
 //     common path) and releases them when the request at the head of the
 //     queue cannot fit otherwise;
@@ -50,9 +53,12 @@ using Clock = std::chrono::steady_clock;
 // Scratch slots of a worker's context holding the request's device copies
 // (offset method: the row offsets in and out).
 constexpr int kSlotV = 12, kSlotW = 13, kSlotH = 14, kSlotDev = 15, kSlotOff = 16;
-// A queued request may be passed over this many times by later, smaller
-// ones; after that nothing behind it is admitted before it.
+// A queued request that does not fit in device memory may be passed over
+// this many times by later ones that do; after that nothing behind it is
+// admitted before it.
 constexpr int kMaxBypass = 8;
+// Requests whose V has at least this many elements are "large".
+constexpr int64_t kLargeElems = int64_t(1) << 25;
 
 enum ReqState { kQueued = 0, kRunning = 1, kDone = 2 };
 
@@ -96,6 +102,8 @@ size_t growth_on(nmfcu_context *c, const Request &q) {
                   : 0);
 }
 
+bool is_large(const Request &q) { return q.n * q.p >= kLargeElems; }
+
 double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -122,7 +130,7 @@ struct nmfcu_server {
     std::vector<Slot> slots;
     nmfcu_context *probe = nullptr;  // never runs: sizes a request from nothing
     size_t in_use = 0, peak = 0;
-    int running = 0, peak_running = 0;
+    int running = 0, peak_running = 0, running_large = 0;
 
     // Statistics since creation or the last reset.
     int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, iterations = 0;
@@ -136,44 +144,31 @@ struct nmfcu_server {
     void run(int k, Request *q);
 };
 
-// Work of a request for the shortest-first order: V elements x rank x
-// iterations (each iteration streams V twice at a cost that grows with the
-// rank).
-double work_of(const Request &q) {
-    return (double)q.n * (double)q.p * (double)q.r * (double)std::max<int64_t>(1, q.opt.max_iter);
-}
-
-// The queued request with the least work that fits next to what the slots
-// hold (ties: the earlier one), so small requests are not held behind large
-// ones.  A request passed over kMaxBypass times is taken first if it fits,
-// and while it does not fit nothing behind it starts, so no request waits
+// The oldest queued request that may start on slot k: a large one only
+// while fewer than a quarter of the slots run large ones (later small ones
+// go past it meanwhile), and only if what it adds fits in the budget next
+// to what every slot holds.  A request passed over kMaxBypass times for
+// memory blocks everything behind it until it fits, so no request waits
 // for ever.
 Request *nmfcu_server::pick(int k, size_t *growth) {
     Slot &sl = slots[k];
-    auto best = queue.end();
-    size_t best_g = 0;
+    const int max_large = std::max<int>(1, (int)slots.size() / 4);
     for (auto it = queue.begin(); it != queue.end(); ++it) {
         Request *q = *it;
+        if (is_large(*q) && running_large >= max_large) continue;
         const size_t g = growth_on(sl.ctx, *q);
-        const bool fits = in_use + g <= budget;
-        if (q->bypassed >= kMaxBypass) {
-            if (!fits) return nullptr;  // the starved request blocks the rest
-            best = it;
-            best_g = g;
-            break;
+        if (in_use + g > budget) {
+            if (q->bypassed >= kMaxBypass) return nullptr;
+            continue;
         }
-        if (fits && (best == queue.end() || work_of(*q) < work_of(**best))) {
-            best = it;
-            best_g = g;
-        }
+        // Requests ahead of it that did not fit were passed over once more.
+        for (auto jt = queue.begin(); jt != it; ++jt)
+            if (!(is_large(**jt) && running_large >= max_large)) (*jt)->bypassed++;
+        queue.erase(it);
+        *growth = g;
+        return q;
     }
-    if (best == queue.end()) return nullptr;
-    // Every earlier request (the queue is in arrival order) was overtaken.
-    for (auto jt = queue.begin(); jt != best; ++jt) (*jt)->bypassed++;
-    Request *q = *best;
-    queue.erase(best);
-    *growth = best_g;
-    return q;
+    return nullptr;
 }
 
 void nmfcu_server::worker(int k) {
@@ -203,6 +198,8 @@ void nmfcu_server::worker(int k) {
         peak = std::max(peak, in_use);
         sl.busy = true;
         running++;
+        const bool large = is_large(*q);
+        if (large) running_large++;
         peak_running = std::max(peak_running, running);
         q->state = kRunning;
         q->t_start = Clock::now();
@@ -217,6 +214,7 @@ void nmfcu_server::worker(int k) {
         peak = std::max(peak, in_use);
         sl.busy = false;
         running--;
+        if (large) running_large--;
         q->t_done = Clock::now();
         q->state = kDone;
         if (q->status == NMFCU_OK) {
