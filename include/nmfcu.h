@@ -357,7 +357,9 @@ int64_t nmfcu_context_launch_count(nmfcu_context *ctx);
  * rank sweep of the reference's consensus workflow, which calls nmf() once
  * per (rank, run) in a Python loop (examples/build_scaling_notebook.py:
  * 157-208, each call nmf_run_brunet lib.rs:1529-1586 with stop="max_iter").
- * Solve s has rank ranks[s] (1..16); the factors of all solves are stacked:
+ * Solve s has rank ranks[s] (1..NMFCU_MAX_WIDE_RANK); ranks 1..16 run in the
+ * batched kernels, higher ones one at a time through the single-solve
+ * engine in FP64 within the same call.  The factors of all solves are stacked:
  *   W0, W  n x R f64, R = sum(ranks), solve s in columns [off_s, off_s + r_s)
  *   H0, H  R x p f64, solve s in rows [off_s, off_s + r_s)
  * with off_s = ranks[0] + ... + ranks[s-1].  Every solve runs exactly

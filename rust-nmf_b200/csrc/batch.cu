@@ -754,8 +754,9 @@ nmfcu_status validate_batch(int32_t method, int32_t precision, int64_t max_iter,
     if (nsolves < 1 || !ranks) return fail(NMFCU_ERR_INVALID_ARG, "need at least one solve");
     int64_t rtot = 0;
     for (int s = 0; s < nsolves; s++) {
-        if (ranks[s] < 1 || ranks[s] > kMaxBatchRank)
-            return fail(NMFCU_ERR_UNSUPPORTED, "batched ranks must be in [1, 16]");
+        if (ranks[s] < 1 || ranks[s] > NMFCU_MAX_WIDE_RANK)
+            return fail(NMFCU_ERR_UNSUPPORTED,
+                        "batched ranks must be in [1, " + std::to_string(NMFCU_MAX_WIDE_RANK) + "]");
         rtot += ranks[s];
     }
     if (rtot > INT32_MAX) return fail(NMFCU_ERR_INVALID_ARG, "sum of ranks must fit in 32 bits");
@@ -781,14 +782,14 @@ int32_t nmfcu_batch_last_shape(void) {
     return g_last_shape;
 }
 
-nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t precision,
-                                    int64_t max_iter, int64_t n, int64_t p, const double *dV,
-                                    int64_t ldv, int32_t nsolves, const int32_t *ranks,
-                                    double *dW, double *dH, void *stream) {
-    if (!ctx) return fail(NMFCU_ERR_INVALID_ARG, "NULL context");
-    NMFCU_TRY(validate_batch(method, precision, max_iter, n, p, nsolves, ranks));
-    if (!dV || !dW || !dH) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
-    if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
+}  // extern "C"
+
+namespace {
+
+// The batched kernels on solves of ranks 1..kMaxBatchRank (checked).
+nmfcu_status run_batch_narrow(nmfcu_context *ctx, int32_t precision, int64_t max_iter, int64_t n,
+                              int64_t p, const double *dV, int64_t ldv, int32_t nsolves,
+                              const int32_t *ranks, double *dW, double *dH, void *stream) {
     std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
     nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -819,6 +820,117 @@ nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t 
     NMFCU_CUDA_TRY(cudaGetLastError());
     NMFCU_CUDA_TRY(cudaStreamSynchronize(s));
     return NMFCU_OK;
+}
+
+// A batch with solves above kMaxBatchRank: the others run through the
+// batched kernels on compacted copies of their stacked factors (context
+// slots 20, 21); each wide solve runs alone through the single-solve engine
+// in FP64 (ranks above 32 run only there) on a compact copy of its W
+// (slot 22) and its rows of H in place.  Results are copied back into the
+// stacked arrays.
+nmfcu_status run_batch_mixed(nmfcu_context *ctx, int32_t precision, int64_t max_iter, int64_t n,
+                             int64_t p, const double *dV, int64_t ldv, int32_t nsolves,
+                             const int32_t *ranks, double *dW, double *dH, void *stream) {
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    std::vector<int64_t> off(nsolves);
+    std::vector<int32_t> nranks;
+    std::vector<int> nidx, widx;
+    int64_t rtot = 0, rtot_n = 0, rmax_w = 0;
+    for (int i = 0; i < nsolves; i++) {
+        off[i] = rtot;
+        rtot += ranks[i];
+        if (ranks[i] <= kMaxBatchRank) {
+            nidx.push_back(i);
+            nranks.push_back(ranks[i]);
+            rtot_n += ranks[i];
+        } else {
+            widx.push_back(i);
+            rmax_w = std::max<int64_t>(rmax_w, ranks[i]);
+        }
+    }
+    const size_t d8 = sizeof(double);
+    void *wn = nullptr, *hn = nullptr, *ws = nullptr;
+    // Copies of solve i's W columns between the stacked W (pitch rtot) and a
+    // compact buffer (pitch `pitch`, first column `col`), either way.
+    auto w_copy = [&](int i, double *buf, int64_t pitch, int64_t col, bool to_buf) {
+        const size_t width = d8 * (size_t)ranks[i];
+        if (to_buf)
+            return cudaMemcpy2DAsync(buf + col, d8 * pitch, dW + off[i], d8 * rtot, width,
+                                     (size_t)n, cudaMemcpyDeviceToDevice, s);
+        return cudaMemcpy2DAsync(dW + off[i], d8 * rtot, buf + col, d8 * pitch, width, (size_t)n,
+                                 cudaMemcpyDeviceToDevice, s);
+    };
+    if (!nidx.empty()) {
+        {
+            std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
+            nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
+            NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 20, d8 * (size_t)(n * rtot_n), &wn));
+            NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 21, d8 * (size_t)(rtot_n * p), &hn));
+            int64_t o = 0;
+            for (int i : nidx) {
+                NMFCU_CUDA_TRY(w_copy(i, (double *)wn, rtot_n, o, true));
+                NMFCU_CUDA_TRY(cudaMemcpyAsync((double *)hn + o * p, dH + off[i] * p,
+                                               d8 * (size_t)(ranks[i] * p),
+                                               cudaMemcpyDeviceToDevice, s));
+                o += ranks[i];
+            }
+        }
+        NMFCU_TRY(run_batch_narrow(ctx, precision, max_iter, n, p, dV, ldv, (int32_t)nidx.size(),
+                                   nranks.data(), (double *)wn, (double *)hn, stream));
+        std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
+        nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
+        int64_t o = 0;
+        for (int i : nidx) {
+            NMFCU_CUDA_TRY(w_copy(i, (double *)wn, rtot_n, o, false));
+            NMFCU_CUDA_TRY(cudaMemcpyAsync(dH + off[i] * p, (double *)hn + o * p,
+                                           d8 * (size_t)(ranks[i] * p), cudaMemcpyDeviceToDevice,
+                                           s));
+            o += ranks[i];
+        }
+    }
+    nmfcu_options opt;
+    nmfcu_options_default(&opt);
+    opt.method = NMFCU_BRUNET;
+    opt.stop = NMFCU_STOP_MAX_ITER;
+    opt.max_iter = max_iter;
+    opt.precision = NMFCU_PREC_FP64;
+    opt.device = nmfcu_internal::context_device(ctx);
+    for (int i : widx) {
+        {
+            std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
+            nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
+            NMFCU_TRY(nmfcu_internal::context_buffer(ctx, 22, d8 * (size_t)(n * rmax_w), &ws));
+            NMFCU_CUDA_TRY(w_copy(i, (double *)ws, ranks[i], 0, true));
+        }
+        int64_t ndev = 0, nit = 0;
+        NMFCU_TRY(nmfcu_run_device(ctx, &opt, n, p, ranks[i], dV, NMFCU_F64, ldv, nullptr, 0,
+                                   (double *)ws, dH + off[i] * p, nullptr, &ndev, &nit, stream));
+        std::lock_guard<std::mutex> lk(nmfcu_internal::context_mutex(ctx));
+        nmfcu_internal::DeviceScope dg(nmfcu_internal::context_device(ctx));
+        NMFCU_CUDA_TRY(w_copy(i, (double *)ws, ranks[i], 0, false));
+    }
+    NMFCU_CUDA_TRY(cudaStreamSynchronize(s));
+    return NMFCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nmfcu_status nmfcu_run_batch_device(nmfcu_context *ctx, int32_t method, int32_t precision,
+                                    int64_t max_iter, int64_t n, int64_t p, const double *dV,
+                                    int64_t ldv, int32_t nsolves, const int32_t *ranks,
+                                    double *dW, double *dH, void *stream) {
+    if (!ctx) return fail(NMFCU_ERR_INVALID_ARG, "NULL context");
+    NMFCU_TRY(validate_batch(method, precision, max_iter, n, p, nsolves, ranks));
+    if (!dV || !dW || !dH) return fail(NMFCU_ERR_INVALID_ARG, "NULL pointer");
+    if (ldv < p) return fail(NMFCU_ERR_INVALID_ARG, "ldv must be >= p");
+    for (int i = 0; i < nsolves; i++)
+        if (ranks[i] > kMaxBatchRank)
+            return run_batch_mixed(ctx, precision, max_iter, n, p, dV, ldv, nsolves, ranks, dW,
+                                   dH, stream);
+    return run_batch_narrow(ctx, precision, max_iter, n, p, dV, ldv, nsolves, ranks, dW, dH,
+                            stream);
 }
 
 nmfcu_status nmfcu_run_batch(int32_t method, int32_t precision, int64_t max_iter, int64_t n,

@@ -65,18 +65,20 @@ __device__ inline void fc_cssls(int l, const double *__restrict__ ctc,
         if (pset >> i & 1u) act[m++] = i;
     }
     if (m == 0) return;
-    double g[kFcMax * kFcMax], b[kFcMax], rhs[kFcMax], dreg[kFcMax];
+    // The (regularised) sub-Gram is the passive rows and columns of ctc with
+    // the diagonal dreg; each try rebuilds it in f and factors it in place
+    // (one m x m array a thread).
+    double f[kFcMax * kFcMax], b[kFcMax], rhs[kFcMax], dreg[kFcMax];
     for (int a = 0; a < m; a++) {
-        for (int c = 0; c < m; c++) g[a * m + c] = ctc[act[a] * l + act[c]];
         rhs[a] = cta[act[a] * cs + j * js];
-        dreg[a] = g[a * m + a];
+        dreg[a] = ctc[act[a] * l + act[a]];
     }
     double eps = 1e-12;
     bool first = true;
     for (int tries = 0; tries < 64; tries++) {
-        // g holds the (regularised) sub-Gram; factor a copy in place.
-        double f[kFcMax * kFcMax];
-        for (int t = 0; t < m * m; t++) f[t] = g[t];
+        for (int a = 0; a < m; a++)
+            for (int c = 0; c < m; c++)
+                f[a * m + c] = (a == c) ? dreg[a] : ctc[act[a] * l + act[c]];
         if (fc_chol(f, m)) {
             for (int a = 0; a < m; a++) b[a] = rhs[a];
             fc_chol_solve(f, m, b);
@@ -84,10 +86,7 @@ __device__ inline void fc_cssls(int l, const double *__restrict__ ctc,
             return;
         }
         if (!first) {
-            for (int a = 0; a < m; a++) {
-                dreg[a] += eps;
-                g[a * m + a] = dreg[a];
-            }
+            for (int a = 0; a < m; a++) dreg[a] += eps;
             eps *= 10.0;
             if (eps > 1e6) return;  // zeros
         }

@@ -62,6 +62,22 @@ def test_batch_fp64_mixed_ranks_match_oracle(oracle, iters):
         assert ok, vals
 
 
+def test_batch_wide_ranks_match_oracle(oracle):
+    """Ranks above the batched kernels' 16 run through the single-solve
+    engine in FP64 inside the same call (40 takes the wide loop above 32);
+    the rest of the batch is unchanged."""
+    V = _counts(200, 300, 21)
+    ranks = [3, 17, 5, 20, 40, 2]
+    starts = _starts(V, ranks, 6)
+    for precision in ("fp64", "fp32"):
+        got = consensus.run_batch(V, starts, 12, precision=precision)
+        for r, (W0, H0), (W, H) in zip(ranks, starts, got):
+            ref = oracle.nmf_method("brunet", V, W0, H0, 12)
+            tol = FACTOR_TOL if (precision == "fp64" or r > 16) else 1e-3
+            assert rel_max(W, ref["W"]) <= tol, (precision, r, rel_max(W, ref["W"]))
+            assert rel_max(H, ref["H"]) <= tol, (precision, r, rel_max(H, ref["H"]))
+
+
 def test_batch_fp64_many_restarts_one_rank(oracle):
     """23 restarts of rank 3: several CTA groups, the last one padded."""
     V = _counts(257, 513, 3)

@@ -187,8 +187,9 @@ def test_batch_rejects_unsupported_before_touching_a_device():
     starts = [(np.ones((4, 2)), np.ones((2, 5)))]
     with pytest.raises(NotImplementedError):
         consensus.run_batch(V, starts, 3, method="lee")
+    # Ranks above the largest supported one (NMFCU_MAX_WIDE_RANK, 256).
     with pytest.raises(NotImplementedError):
-        consensus.run_batch(V, [(np.ones((4, 17)), np.ones((17, 5)))], 3)
+        consensus.run_batch(V, [(np.ones((4, 257)), np.ones((257, 5)))], 3)
     with pytest.raises(ValueError):
         consensus.run_batch(V, starts, -1)
 
