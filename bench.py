@@ -1060,7 +1060,6 @@ def run_consensus(args, world, rank, local):
 # ---------------------------------------------------------------------------
 
 SERVE_METHODS = (("lee", 0.4), ("brunet", 0.3), ("hals", 0.2), ("dnmf", 0.1))
-SERVE_CAL = 64  # requests in the closed-loop capacity sample
 SERVE_MAX = (5000, 50000)
 
 
@@ -1139,8 +1138,6 @@ def run_serve(args, world, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     reqs = serve_requests(args.requests)
-    # A fixed sample of the same mix, run closed-loop to measure capacity.
-    cal = serve_requests(SERVE_CAL, seed=23)
     N, P = SERVE_MAX
     # One pinned host V; request i reads its top-left n x p block (ldv = P).
     V64, ld64, V32, ld32, _, _ = device_workload(N, P, 12, 0.3, 5, 4321 + rank, dev)
@@ -1154,7 +1151,7 @@ def run_serve(args, world, rank, local):
     _native.check(lib.nmfcu_server_create(local, args.slots, 0, ctypes.byref(h)))
     gen = np.random.default_rng(5)
     bufs = []
-    for n, p, r, m, it in reqs + cal:
+    for n, p, r, m, it in reqs:
         top = 1.0
         W0 = gen.uniform(0, top, (n, r))
         H0 = gen.uniform(0, top, (r, p))
@@ -1168,7 +1165,7 @@ def run_serve(args, world, rank, local):
     dp = _native._ptr
 
     def submit(i):
-        n, p, r, m, it = (reqs + cal)[i]
+        n, p, r, m, it = reqs[i]
         o, W0, H0, W, H = bufs[i]
         rid = ctypes.c_int64(0)
         _native.check(lib.nmfcu_server_submit(
@@ -1186,15 +1183,43 @@ def run_serve(args, world, rank, local):
     ids = [submit(i) for i in warm]
     for rid in ids:
         wait(rid)
-    # Capacity: the calibration sample submitted at once (closed loop), in
-    # work units (rows x columns x rank x iterations) per second, over the
-    # mean work of a request of the stream: requests per second.
+    # Capacity: the whole stream run closed-loop at constant concurrency (a
+    # new request is submitted whenever one completes, so the server never
+    # has a choice of order): work units (rows x columns x rank x
+    # iterations) completed per second until the last submission, over the
+    # mean work of a request: requests per second.  The open-loop stream
+    # below then arrives at args.load of that.
+    def poll(rid):
+        state = ctypes.c_int32(0)
+        _native.check(lib.nmfcu_server_poll(h, rid, ctypes.byref(state)))
+        return state.value
+
+    cal = reqs
+    cal_work = [n * p * r * it for n, p, r, _, it in cal]
     t0 = time.perf_counter()
-    ids = [submit(len(reqs) + j) for j in range(len(cal))]
-    cal_iters = sum(wait(rid) for rid in ids)
+    inflight = {}
+    nxt = 0
+    work_done = iters_done = 0
+    while nxt < len(cal) and len(inflight) < args.slots:
+        inflight[submit(nxt)] = nxt
+        nxt += 1
+    while nxt < len(cal):
+        finished = [rid for rid in inflight if poll(rid) == 2]
+        if not finished:
+            time.sleep(0.0002)
+            continue
+        for rid in finished:
+            iters_done += wait(rid)
+            work_done += cal_work[inflight.pop(rid)]
+            if nxt < len(cal):
+                inflight[submit(nxt)] = nxt
+                nxt += 1
     cal_s = time.perf_counter() - t0
+    cal_iters = iters_done
+    for rid in list(inflight):
+        wait(rid)
     units = [n * p * r * it for n, p, r, _, it in reqs]
-    rate_cap = sum(n * p * r * it for n, p, r, _, it in cal) / cal_s / float(np.mean(units))
+    rate_cap = work_done / cal_s / float(np.mean(units))
     lam = args.load * rate_cap  # requests per second
     _native.check(lib.nmfcu_server_reset_stats(h))
     arrivals = np.cumsum(np.random.default_rng(17).exponential(1.0 / lam, len(reqs)))
@@ -1244,9 +1269,10 @@ def run_serve(args, world, rank, local):
                        "shapes": "log-uniform 500x1000..5000x50000", "ranks": "5..30",
                        "iters": "25..200", "mix": "lee .4 brunet .3 hals .2 dnmf .1",
                        "arrival_rate_per_s": lam, "load": args.load,
-                       "capacity": (f"{len(cal)} requests of the same mix (another seed) "
-                                    "submitted at once: " f"{cal_iters / cal_s:.0f} iters/s, "
-                                    f"{rate_cap:.2f} stream requests/s"),
+                       "capacity": (f"the {len(cal)} requests run closed-loop with "
+                                    f"{args.slots} in flight, measured until the last "
+                                    f"submission: {cal_iters / cal_s:.0f} iters/s, "
+                                    f"{rate_cap:.2f} requests/s"),
                        "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": st.p50_ms, "p99": st.p99_ms, "max": st.max_ms,
                            "mean_queue": st.mean_queue_ms},
