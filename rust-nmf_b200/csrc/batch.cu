@@ -112,15 +112,19 @@ __device__ __forceinline__ float &plane(F4 &a, int c) {
 __device__ __forceinline__ double &plane(double &a, int) { return a; }
 
 // The brunet ratio V / (WH), 0 where WH == 0 (lib.rs:93-99).  f32 uses the
-// hardware reciprocal approximation (rcp.approx.ftz.f32, about 1 ulp).
-__device__ __forceinline__ float ratio1(float v, float wh) {
+// hardware reciprocal approximation (rcp.approx.ftz.f32, about 1 ulp); for a
+// pack of four columns the reciprocals are taken one by one and the
+// products v * (1 / wh) as two packed f32x2 multiplies.
+__device__ __forceinline__ float rcp1(float wh) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(wh));
-    return (wh != 0.f) ? v * r : 0.f;
+    return r;
 }
 __device__ __forceinline__ F4 ratio(F4 v, F4 wh) {
-    return F4{make_float2(ratio1(v.a.x, wh.a.x), ratio1(v.a.y, wh.a.y)),
-              make_float2(ratio1(v.b.x, wh.b.x), ratio1(v.b.y, wh.b.y))};
+    const float2 qa = __fmul2_rn(v.a, make_float2(rcp1(wh.a.x), rcp1(wh.a.y)));
+    const float2 qb = __fmul2_rn(v.b, make_float2(rcp1(wh.b.x), rcp1(wh.b.y)));
+    return F4{make_float2(wh.a.x != 0.f ? qa.x : 0.f, wh.a.y != 0.f ? qa.y : 0.f),
+              make_float2(wh.b.x != 0.f ? qb.x : 0.f, wh.b.y != 0.f ? qb.y : 0.f)};
 }
 // f64: v * (1 / wh) with the reciprocal from the hardware approximation
 // (rcp.approx.ftz.f64) refined by two Newton-Raphson steps
