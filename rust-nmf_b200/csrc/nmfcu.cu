@@ -1365,6 +1365,65 @@ nmfcu_status run_snmf(nmfcu_context *c, RunArgs &a, cudaStream_t s, double *dev)
     return finish_checked(c, s);
 }
 
+// Iterations whose kernels repeat with this period: the only iteration-
+// dependent work is brunet's clamp every 10 iterations.
+constexpr long long kGraphPeriod = 10;
+
+// The main-precision iterations of a fixed-length run as a CUDA graph: the
+// first iteration is enqueued directly (its launches set the kernels'
+// one-time attributes), the next kGraphPeriod are captured and the graph is
+// launched while a whole period of main-precision iterations remains; *it
+// is the next iteration still to enqueue.  Small problems are bound by
+// launch overhead, which the graph's launches cut.  If capture or
+// instantiation fails nothing of the captured work ran: *it stays at the
+// first captured iteration and the caller enqueues the rest directly.
+nmfcu_status run_graphed(nmfcu_context *c, RunArgs &a, long long refine_from, cudaStream_t s,
+                         long long *it) {
+    const nmfcu_options *o = a.opt;
+    const long long main_end = std::min<long long>(o->max_iter, refine_from);
+    if (main_end < 1 + 3 * kGraphPeriod) return NMFCU_OK;
+    // Not on the legacy or per-thread default streams (they cannot be
+    // captured), nor on a stream the caller is capturing already.
+    if (s == nullptr || s == cudaStreamLegacy || s == cudaStreamPerThread) return NMFCU_OK;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return NMFCU_OK;
+    const bool fp64 = (o->precision == NMFCU_PREC_FP64);
+    NMF_TRY(enqueue_iteration(c, a, 1, fp64, s));
+    *it = 2;
+    const int64_t launches0 = c->launch_total;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    nmfcu_status st = NMFCU_OK;
+    for (long long k = 0; k < kGraphPeriod && st == NMFCU_OK; k++)
+        st = enqueue_iteration(c, a, *it + k, fp64, s);
+    const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+    if (st == NMFCU_OK && ec == cudaSuccess && graph &&
+        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        const int64_t per_graph = c->launch_total - launches0;
+        c->launch_total = launches0;
+        cudaError_t el = cudaSuccess;
+        while (el == cudaSuccess && *it + kGraphPeriod - 1 <= main_end) {
+            el = cudaGraphLaunch(exec, s);
+            if (el == cudaSuccess) {
+                c->launch_total += per_graph;
+                *it += kGraphPeriod;
+            }
+        }
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        CUDA_TRY(el);
+        return NMFCU_OK;
+    }
+    // Capture did not give a graph: nothing captured ran; enqueue directly.
+    c->launch_total = launches0;
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return NMFCU_OK;
+}
+
 nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_dev,
                       int64_t *n_iter) {
     const nmfcu_options *o = a.opt;
@@ -1373,7 +1432,9 @@ nmfcu_status run_loop(nmfcu_context *c, RunArgs &a, cudaStream_t s, int64_t *n_d
     if (stat) NMF_TRY(enqueue_objective(c, a, 0, s));
     const long long refine_from =
         (o->precision != NMFCU_PREC_FP64) ? (long long)o->max_iter - o->refine_iters : LLONG_MAX;
-    for (long long it = 1; it <= o->max_iter; it++) {
+    long long it = 1;
+    if (!stat && !c->timing) NMF_TRY(run_graphed(c, a, refine_from, s, &it));
+    for (; it <= o->max_iter; it++) {
         const bool fp64 = (o->precision == NMFCU_PREC_FP64) || (it > refine_from);
         NMF_TRY(enqueue_iteration(c, a, it, fp64, s));
         if (stat) NMF_TRY(enqueue_objective(c, a, it, s));
