@@ -966,7 +966,9 @@ def run_consensus(args, world, rank, local):
     ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
     value = world * nsolves / (ms / 1000.0)
 
-    # The same solves one by one through the single-solve engine.
+    # The same solves one by one through the single-solve engine, on a
+    # stream of their own so that each solve replays its iterations as a
+    # CUDA graph, as nmf() does (the best single-solve path).
     seq_runs = min(runs, runs if args.seq_runs is None else args.seq_runs)
     seq_value = dh_rel = t_seq_solves = t_post = None
     if seq_runs > 0:
@@ -978,13 +980,17 @@ def run_consensus(args, world, rank, local):
         o.refine_iters = 0
         o.device = local
         pick = [ci * runs + i for ci in range(len(c["ranks"])) for i in range(seq_runs)]
+        side = torch.cuda.Stream(dev)
+
+        side.wait_stream(stream)
 
         def one(s_):
             a, r = int(offs[s_]), int(ranks[s_])
-            w = dW0[:, a:a + r].contiguous()
-            h = dH0[a:a + r].contiguous()
-            ctx.run(o, n, p, r, dV.data_ptr(), _native.F64, p, w.data_ptr(), h.data_ptr(),
-                    stream=stream.cuda_stream)
+            with torch.cuda.stream(side):  # the copies and the solve on the side stream
+                w = dW0[:, a:a + r].contiguous()
+                h = dH0[a:a + r].contiguous()
+                ctx.run(o, n, p, r, dV.data_ptr(), _native.F64, p, w.data_ptr(), h.data_ptr(),
+                        stream=side.cuda_stream)
             return h
 
         one(0)
