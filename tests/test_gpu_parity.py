@@ -15,7 +15,7 @@ max(G_kk, eps) = eps and amplifies rounding by ~1e9.  The oracle itself then
 moves by up to ~1e-3 when W0 is perturbed by one ulp, and so would the
 reference (whose W^T V / V H^T summation order, matrixmultiply's, is not
 pinned either).  For those two methods the bound is therefore
-max(north-star tolerance, 100 x the oracle's own one-ulp sensitivity),
+max(1e-10, 100 x the oracle's own one-ulp sensitivity),
 measured in the test; from NNDSVD starts HALS is well conditioned and is
 held to the plain tolerance.
 """
