@@ -60,8 +60,9 @@ def test_brunet_one_iteration_matches_oracle(oracle, n, p, r):
     assert rel_max(got.W, ref["W"]) <= ONE_ITER_TOL, rel_max(got.W, ref["W"])
 
 
-# nsNMF's split-bf16 form runs the same passes on W S (H pass) and S H (W pass).
-@pytest.mark.parametrize("n,p,r", [(700, 900, 8), (257, 1301, 3)])
+# nsNMF's split-bf16 form runs the same passes on W S (H pass) and S H (W pass);
+# rank 24 takes the 192-wide concatenated layouts.
+@pytest.mark.parametrize("n,p,r", [(700, 900, 8), (257, 1301, 3), (600, 1100, 24)])
 def test_nsnmf_one_iteration_matches_oracle(oracle, n, p, r):
     V = synthetic.counts_matrix(n, p, max(2, r // 2), 0.3, seed=n + p) + 0.01
     W0, H0 = nmf_rs.random_init(V, r, seed=3)
@@ -82,6 +83,31 @@ def test_split_bf16_form(oracle, method):
     o_ref = _objective(oracle, method, V, ref["W"], ref["H"])
     o_got = _objective(oracle, method, V, got.W, got.H)
     assert rel(o_got, o_ref) <= 1e-5, rel(o_got, o_ref)
+
+
+# Many iterations through the rank > 21 variant of the tensor-core ratio
+# passes (192-wide concatenated rows, one segment accumulator).
+def test_brunet_split_bf16_rank_26_many_iterations(oracle):
+    V = synthetic.counts_matrix(900, 1400, 12, 0.3, seed=5)
+    W0, H0 = nmf_rs.random_init(V, 26, seed=6)
+    ref = oracle.nmf_method("brunet", V, W0, H0, 40)
+    got = nmf_rs.nmf(V, 26, "brunet", W0=W0, H0=H0, max_iter=40, precision="bf16x3")
+    o_ref = oracle.kl_divergence(V, ref["W"], ref["H"])
+    o_got = oracle.kl_divergence(V, got.W, got.H)
+    assert rel(o_got, o_ref) <= 1e-5, rel(o_got, o_ref)
+
+
+def test_brunet_split_bf16_stationary_and_deterministic():
+    # The stationary stop evaluates the objective on the device each
+    # iteration, so these iterations are launched one by one.
+    V, W0, H0 = synthetic.make(synthetic.PBMC_SUBSET)
+    kw = dict(max_iter=60, precision="bf16x3", stop="stationary", check_interval=10,
+              check_niter=3, stationary_th=1e-12)
+    a = nmf_rs.nmf(V, 8, "brunet", W0=W0, H0=H0, **kw)
+    b = nmf_rs.nmf(V, 8, "brunet", W0=W0, H0=H0, **kw)
+    np.testing.assert_array_equal(a.W, b.W)
+    np.testing.assert_array_equal(a.deviances, b.deviances)
+    assert a.deviances.size == a.n_iter + 1
 
 
 def test_split_bf16_stationary_and_deterministic(oracle):
