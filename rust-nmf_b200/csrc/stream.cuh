@@ -735,11 +735,13 @@ __global__ void __launch_bounds__(WCfg<T, RP, RATIO>::kWarps * 32, 1)
 // D[g][2q + e] with g = lane / 4, q = lane % 4).  One instruction does 256
 // FMAs, where the CUDA-core passes issue one DFMA (and its operand loads)
 // per 32; the ring, stream-K split and partial layouts are the CUDA-core
-// passes' own, so the epilogues are shared.
+// passes' own, so the epilogues are shared.  The asm has no side effects
+// beyond its operands (not volatile), so independent MMAs may be scheduled
+// across one another; each accumulator's chain keeps its order.
 __device__ __forceinline__ void dmma_8x8x4(double (&d)[2], double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(d[0]), "+d"(d[1])
-                 : "d"(a), "d"(b));
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+        : "+d"(d[0]), "+d"(d[1])
+        : "d"(a), "d"(b));
 }
 
 // H pass: A[k][j] = sum_u W[u][k] V[u][j] with M = k (rank tiles of 8), N = j
@@ -1202,25 +1204,35 @@ __global__ void __launch_bounds__(DHRCfg<RP>::kWarps * 32, 1)
                 for (int e = 0; e < 2; e++)
                     a2[mt][e] = (k < RP) ? sw[(r0 + 2 * q4 + e) * C::RPS + k] : 0.0;
             }
+            // The column tiles' WH chains interleaved (independent), then
+            // their ratios, then MMA 2: the tensor pipe has a second chain
+            // to issue while one waits.  Each accumulator sees the same
+            // operations in the same order as tile by tile.
+            double wh[C::NT][2];
 #pragma unroll
-            for (int nt = 0; nt < C::NT; nt++) {
-                double wh[2] = {0.0, 0.0};
+            for (int nt = 0; nt < C::NT; nt++) wh[nt][0] = wh[nt][1] = 0.0;
 #pragma unroll
-                for (int ks = 0; ks < C::KST; ks++) dmma_8x8x4(wh, hreg[nt][ks], b1[ks]);
-                double qv[2];
+            for (int ks = 0; ks < C::KST; ks++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++) dmma_8x8x4(wh[nt], hreg[nt][ks], b1[ks]);
+            double qv[C::NT][2];
+#pragma unroll
+            for (int nt = 0; nt < C::NT; nt++)
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
                     const double v = sv[(r0 + 2 * q4 + e) * C::BOXC + nt * 8];
                     if constexpr (WEIGHTED)
-                        qv[e] = v * wh[e];
+                        qv[nt][e] = v * wh[nt][e];
                     else
-                        qv[e] = (wh[e] != 0.0) ? ratio_div(v, wh[e]) : 0.0;
+                        qv[nt][e] = (wh[nt][e] != 0.0) ? ratio_div(v, wh[nt][e]) : 0.0;
                 }
 #pragma unroll
-                for (int e = 0; e < 2; e++)
+            for (int e = 0; e < 2; e++)
 #pragma unroll
-                    for (int mt = 0; mt < C::MT; mt++) dmma_8x8x4(acc[mt][nt], a2[mt][e], qv[e]);
-            }
+                for (int mt = 0; mt < C::MT; mt++)
+#pragma unroll
+                    for (int nt = 0; nt < C::NT; nt++)
+                        dmma_8x8x4(acc[mt][nt], a2[mt][e], qv[nt][e]);
         }
         __syncwarp();
         if (lane == 0)
@@ -1383,28 +1395,37 @@ __global__ void __launch_bounds__(DWRCfg<RP>::kWarps * 32, 1)
             }
             // V[row][j0 + 2 q4 + e], e = 0, 1: one 16-byte chunk of the row.
             const int chunk = (j0 >> 1) + q4;
+            // The row tiles' WH chains interleaved, then their ratios, then
+            // MMA 2 (the same operations per accumulator, in the same order).
+            double wh[C::MW][2];
+#pragma unroll
+            for (int mw = 0; mw < C::MW; mw++) wh[mw][0] = wh[mw][1] = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < C::KST; ks++)
+#pragma unroll
+                for (int mw = 0; mw < C::MW; mw++) dmma_8x8x4(wh[mw], wreg[mw][ks], b1[ks]);
+            double qv[C::MW][2];
 #pragma unroll
             for (int mw = 0; mw < C::MW; mw++) {
                 const int row = rbase + mw * 8;
-                double wh[2] = {0.0, 0.0};
-#pragma unroll
-                for (int ks = 0; ks < C::KST; ks++) dmma_8x8x4(wh, wreg[mw][ks], b1[ks]);
                 const double2 v2 = *reinterpret_cast<const double2 *>(
                     stg + row * C::ROWB + ((chunk ^ g) << 4));
-                double qv[2];
                 const double vv[2] = {v2.x, v2.y};
 #pragma unroll
                 for (int e = 0; e < 2; e++) {
                     if constexpr (WEIGHTED)
-                        qv[e] = vv[e] * wh[e];
+                        qv[mw][e] = vv[e] * wh[mw][e];
                     else
-                        qv[e] = (wh[e] != 0.0) ? ratio_div(vv[e], wh[e]) : 0.0;
+                        qv[mw][e] = (wh[mw][e] != 0.0) ? ratio_div(vv[e], wh[mw][e]) : 0.0;
                 }
-#pragma unroll
-                for (int e = 0; e < 2; e++)
-#pragma unroll
-                    for (int nt = 0; nt < C::NT; nt++) dmma_8x8x4(acc[mw][nt], qv[e], b2[nt][e]);
             }
+#pragma unroll
+            for (int e = 0; e < 2; e++)
+#pragma unroll
+                for (int nt = 0; nt < C::NT; nt++)
+#pragma unroll
+                    for (int mw = 0; mw < C::MW; mw++)
+                        dmma_8x8x4(acc[mw][nt], qv[mw][e], b2[nt][e]);
         }
         __syncwarp();
         if (lane == 0)
