@@ -432,7 +432,7 @@ nmfcu_status nmfcu_consensus_stats_batch_device(nmfcu_context *ctx, int32_t coun
                                                 void *stream);
 
 /* ---------------------------------------------------------------------- */
-/* Serving: continuous batching of independent factorisations              */
+/* Serving: continuous admission of independent factorisations            */
 /* ---------------------------------------------------------------------- */
 
 /*

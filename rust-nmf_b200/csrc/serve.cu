@@ -1,4 +1,6 @@
-// serve.cu -- continuous-batching request server for single factorisations.
+// serve.cu -- request server for single factorisations, with continuous
+// admission (each request still runs alone on its slot's stream; requests
+// are not fused into shared launches).
 //
 // The reference has no server: every nmf() call runs to completion on the
 // calling thread (python/nmf_rs/__init__.py:396-568, lib.rs:1934-2169).

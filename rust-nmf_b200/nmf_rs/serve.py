@@ -91,7 +91,8 @@ class Request:
 
 
 class Server:
-    """A continuous-batching server on one GPU.
+    """A request server on one GPU with continuous admission (requests run
+    concurrently, each alone on its slot's stream).
 
     slots         concurrent requests (one engine context and stream each)
     budget_bytes  device memory the slots may hold (0: 90% of free memory)
