@@ -309,26 +309,25 @@ __device__ __forceinline__ void mu_item(BSmem<T> &sm, const MuArgs<T> &a,
 #define BATCH_RANK_CASES(X) \
     X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10) X(11) X(12) X(13) X(14) X(15) X(16)
 
-// Rank buckets: ranks 1..8 and 9..16 run as separate kernels, so the
-// register budget of one bucket is not set by the other's largest rank.
+// Rank buckets: ranks 1..8, 9..10 and 11..16 run as separate kernels, so
+// the register budget of one bucket is not set by another's largest rank.
 // Within a bucket one launch covers every rank class: CTA b runs item b.
-// Ranks form two buckets with a launch each, so that a launch's register
-// cap fits its ranks.
-constexpr int kBucketSplit = 8;  // largest rank of the low bucket
+constexpr int kBuckets = 3;
+constexpr int kBucketHi[kBuckets] = {8, 10, kMaxBatchRank};  // largest rank of each
 template <int B>
 struct BBucket {
-    static constexpr int kLo = B == 0 ? 1 : kBucketSplit + 1;
-    static constexpr int kHi = B == 0 ? kBucketSplit : kMaxBatchRank;
+    static constexpr int kLo = B == 0 ? 1 : kBucketHi[B - 1] + 1;
+    static constexpr int kHi = kBucketHi[B];
 };
-constexpr int bucket_of(int R) { return R <= kBucketSplit ? 0 : 1; }
+constexpr int bucket_of(int R) { return R <= kBucketHi[0] ? 0 : R <= kBucketHi[1] ? 1 : 2; }
 
 // CTAs a multiprocessor keeps resident (the register cap) for a bucket and
-// shape.  f32 carries four columns a thread: ranks 9..16 hold up to 16
-// components in x and acc (128 registers of packs) and get two CTAs; the
-// low bucket keeps four.
+// shape.  f32 carries four columns a thread, x and acc holding 8 R
+// registers of packs: ranks 1..8 keep four CTAs (128 registers), 9..10
+// three (168), 11..16 two (255).
 template <typename T, int B, int SHAPE>
 constexpr int min_blocks_for() {
-    if constexpr (sizeof(T) == 4) return B == 0 ? 4 : 2;
+    if constexpr (sizeof(T) == 4) return B == 0 ? 4 : B == 1 ? 3 : 2;
     return BShapes<T>::min_blocks[SHAPE];
 }
 
@@ -461,8 +460,8 @@ int ns_for(int R, int comp) { return comp / R > 0 ? comp / R : 1; }
 struct BatchPlan {
     int rtot = 0;
     std::vector<int> group_off;           // per group, NS offsets (-1 padded)
-    std::vector<BItem> hitems, witems;    // bucket 0 items, then bucket 1 items
-    int nh[2] = {0, 0}, nw[2] = {0, 0};   // items per bucket
+    std::vector<BItem> hitems, witems;    // bucket 0 items, then bucket 1, then 2
+    int nh[kBuckets] = {}, nw[kBuckets] = {};  // items per bucket
 };
 
 // Solves of one rank form a class; a class is cut into groups of NS solves;
@@ -478,7 +477,7 @@ BatchPlan plan_batch(int n, int p, int nsolves, const int32_t *ranks, int comp) 
         by_rank[ranks[s]].push_back(s);
     }
     const int htiles = (p + kTile<T> - 1) / kTile<T>, wtiles = (n + kTile<T> - 1) / kTile<T>;
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kBuckets; b++) {
         // Larger ranks first: their CTAs are the longest, so they start first.
         for (auto it = by_rank.rbegin(); it != by_rank.rend(); ++it) {
             const int R = it->first;
@@ -512,6 +511,21 @@ struct BatchSteps {
     MuArgs<T> h, w;  // the H step streams V, the W step streams V^T
 };
 
+// One step's launches, one per bucket with items (bucket b's items follow
+// those of the buckets before it).
+template <typename T, int SHAPE, bool kComponentFast>
+void launch_buckets(const MuArgs<T> &a, const int *off, const BItem *items,
+                    const int (&count)[kBuckets], cudaStream_t s, int64_t *launches) {
+    static_assert(kBuckets == 3, "one launch per bucket");
+    const BItem *at = items;
+    if (count[0]) batch_mu<T, 0, SHAPE, kComponentFast><<<count[0], kThreads, 0, s>>>(a, off, at);
+    at += count[0];
+    if (count[1]) batch_mu<T, 1, SHAPE, kComponentFast><<<count[1], kThreads, 0, s>>>(a, off, at);
+    at += count[1];
+    if (count[2]) batch_mu<T, 2, SHAPE, kComponentFast><<<count[2], kThreads, 0, s>>>(a, off, at);
+    *launches += (count[0] > 0) + (count[1] > 0) + (count[2] > 0);
+}
+
 // Enqueue iterations [it0, it1] of the batched brunet loop with shape SHAPE.
 template <typename T, int SHAPE>
 void enqueue_batch_iters_s(long long it0, long long it1, const BatchPlan &bp, const BatchDev &d,
@@ -520,18 +534,10 @@ void enqueue_batch_iters_s(long long it0, long long it1, const BatchPlan &bp, co
     const int rtot = bp.rtot;
     for (long long it = it0; it <= it1; it++) {
         batch_colsum<T><<<(rtot + 127) / 128, 128, 0, s>>>(W, n, rtot, rtot, sw);
-        if (bp.nh[0])
-            batch_mu<T, 0, SHAPE, true><<<bp.nh[0], kThreads, 0, s>>>(st.h, d.off, d.hitems);
-        if (bp.nh[1])
-            batch_mu<T, 1, SHAPE, true><<<bp.nh[1], kThreads, 0, s>>>(st.h, d.off,
-                                                                     d.hitems + bp.nh[0]);
+        launch_buckets<T, SHAPE, true>(st.h, d.off, d.hitems, bp.nh, s, launches);
         batch_rowsum<T><<<(rtot + 7) / 8, 256, 0, s>>>(H, p, rtot, sh);
-        if (bp.nw[0])
-            batch_mu<T, 0, SHAPE, false><<<bp.nw[0], kThreads, 0, s>>>(st.w, d.off, d.witems);
-        if (bp.nw[1])
-            batch_mu<T, 1, SHAPE, false><<<bp.nw[1], kThreads, 0, s>>>(st.w, d.off,
-                                                                      d.witems + bp.nw[0]);
-        *launches += 2 + (bp.nh[0] > 0) + (bp.nh[1] > 0) + (bp.nw[0] > 0) + (bp.nw[1] > 0);
+        launch_buckets<T, SHAPE, false>(st.w, d.off, d.witems, bp.nw, s, launches);
+        *launches += 2;
         if (it % 10 == 0) {
             batch_clamp<T><<<592, 256, 0, s>>>(W, (int64_t)n * rtot, H, (int64_t)rtot * p,
                                                (T)DBL_EPSILON);

@@ -51,7 +51,7 @@ def _kl_close(oracle, V, W, H, Wr, Hr, tol):
 @pytest.mark.parametrize("iters", [0, 7, 37])
 def test_batch_fp64_mixed_ranks_match_oracle(oracle, iters):
     V = _counts(300, 700, 11)
-    ranks = [1, 2, 3, 3, 5, 7, 8, 16, 16, 4, 12]
+    ranks = [1, 2, 3, 3, 5, 7, 8, 16, 16, 4, 12, 9, 10, 11]  # every rank bucket
     starts = _starts(V, ranks, 5)
     got = consensus.run_batch(V, starts, iters, precision="fp64")
     for (W0, H0), (W, H) in zip(starts, got):
