@@ -43,7 +43,7 @@ struct RunState {
     int stopped;       // 1 once the loop has stopped
     int error;         // 1: `iter % check_interval` with check_interval == 0
     int timeout;       // a bounded mbarrier wait gave up (stream.cuh codes)
-    int pad1;
+    unsigned gram_ticket;  // blocks of the running Gram launch that are done
 };
 
 // Fixed constants of the streaming kernels.
@@ -709,11 +709,43 @@ __global__ void __launch_bounds__(kThreads)
 // Gram matrices and sums (two-stage, fixed order).
 // ---------------------------------------------------------------------------
 
-// W^T W and colsum(W) partials over a row range.  block RP*RP threads.
+// The second stage inside the first stage's launch: each block publishes
+// its partials and takes a ticket; the block that takes the last ticket sums
+// the B = gridDim.x partials in block order (the sums gram_finalize forms,
+// bit for bit) and resets the ticket for the next launch.  No block waits
+// on another.  G == nullptr leaves the partials for the caller (lee's and
+// nsNMF's col_rescale read them).
+template <int RP>
+__device__ __forceinline__ void gram_finish_last(const double *pg, const double *ps, double *G,
+                                                 double *sums, unsigned *ticket) {
+    if (G == nullptr) return;
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int tid = threadIdx.x;
+    const int B = (int)gridDim.x;
+    double g = 0.0;
+    for (int b = 0; b < B; b++) g += __ldcg(&pg[(int64_t)b * RP * RP + tid]);
+    G[tid] = g;
+    if (tid < RP) {
+        double t = 0.0;
+        for (int b = 0; b < B; b++) t += __ldcg(&ps[(int64_t)b * RP + tid]);
+        sums[tid] = t;
+    }
+    if (tid == 0) *ticket = 0u;
+}
+
+// W^T W and colsum(W) partials over a row range, and with G given the
+// finished Gram and sums (gram_finish_last).  block RP*RP threads.
 template <int RP>
 __global__ void gram_w_partial(const double *__restrict__ W, int n, int rows_per_block,
                                double *__restrict__ pg, double *__restrict__ ps,
-                               const RunState *st) {
+                               const RunState *st, double *G = nullptr, double *sums = nullptr,
+                               unsigned *ticket = nullptr) {
     if (run_stopped(st)) return;
     constexpr int CH = 64;
     __shared__ double sW[CH][RP];
@@ -735,13 +767,16 @@ __global__ void gram_w_partial(const double *__restrict__ W, int n, int rows_per
     }
     pg[(int64_t)blockIdx.x * RP * RP + tid] = g;
     if (tid < RP) ps[(int64_t)blockIdx.x * RP + tid] = s;
+    gram_finish_last<RP>(pg, ps, G, sums, ticket);
 }
 
-// H H^T and rowsum(H) partials over a column range.  block RP*RP threads.
+// H H^T and rowsum(H) partials over a column range, and with G given the
+// finished Gram and sums.  block RP*RP threads.
 template <int RP>
 __global__ void gram_h_partial(const double *__restrict__ H, int p, int cols_per_block,
                                double *__restrict__ pg, double *__restrict__ ps,
-                               const RunState *st) {
+                               const RunState *st, double *G = nullptr, double *sums = nullptr,
+                               unsigned *ticket = nullptr) {
     if (run_stopped(st)) return;
     constexpr int CC = 64;
     __shared__ double sH[RP][CC + 1];
@@ -765,6 +800,7 @@ __global__ void gram_h_partial(const double *__restrict__ H, int p, int cols_per
     }
     pg[(int64_t)blockIdx.x * RP * RP + tid] = g;
     if (tid < RP) ps[(int64_t)blockIdx.x * RP + tid] = s;
+    gram_finish_last<RP>(pg, ps, G, sums, ticket);
 }
 
 // Sum B partial Grams / sums in block order.  block RP*RP threads.

@@ -126,8 +126,14 @@ struct Ops {
                         double *ps, const RunState *st, cudaStream_t s) const = 0;
     virtual void gram_h(const double *H, int p, int B, int cols_per_block, double *pg,
                         double *ps, const RunState *st, cudaStream_t s) const = 0;
-    virtual void gram_fin(const double *pg, const double *ps, int B, double *G, double *sums,
-                          const RunState *st, cudaStream_t s) const = 0;
+    // The same partials, and the finished Gram G and sums from the launch's
+    // last block (one launch; ticket zero before and after).
+    virtual void gram_w_fin(const double *W, int n, int B, int rows_per_block, double *pg,
+                            double *ps, double *G, double *sums, unsigned *ticket,
+                            const RunState *st, cudaStream_t s) const = 0;
+    virtual void gram_h_fin(const double *H, int p, int B, int cols_per_block, double *pg,
+                            double *ps, double *G, double *sums, unsigned *ticket,
+                            const RunState *st, cudaStream_t s) const = 0;
     virtual void rescale(double *W, int n, int r, const double *ps, int B, const RunState *st,
                          cudaStream_t s) const = 0;
     virtual void dnmf_scale(double *W, double *H, int n, int p, int r, const double *Gw,
@@ -186,9 +192,17 @@ struct OpsT final : Ops {
                 const RunState *st, cudaStream_t s) const override {
         gram_h_partial<RP><<<B, RP * RP, 0, s>>>(H, p, cols_per_block, pg, ps, st);
     }
-    void gram_fin(const double *pg, const double *ps, int B, double *G, double *sums,
-                  const RunState *st, cudaStream_t s) const override {
-        gram_finalize<RP><<<1, RP * RP, 0, s>>>(pg, ps, B, G, sums, st);
+    void gram_w_fin(const double *W, int n, int B, int rows_per_block, double *pg, double *ps,
+                    double *G, double *sums, unsigned *ticket, const RunState *st,
+                    cudaStream_t s) const override {
+        gram_w_partial<RP><<<B, RP * RP, 0, s>>>(W, n, rows_per_block, pg, ps, st, G, sums,
+                                                 ticket);
+    }
+    void gram_h_fin(const double *H, int p, int B, int cols_per_block, double *pg, double *ps,
+                    double *G, double *sums, unsigned *ticket, const RunState *st,
+                    cudaStream_t s) const override {
+        gram_h_partial<RP><<<B, RP * RP, 0, s>>>(H, p, cols_per_block, pg, ps, st, G, sums,
+                                                 ticket);
     }
     void rescale(double *W, int n, int r, const double *ps, int B, const RunState *st,
                  cudaStream_t s) const override {
@@ -775,19 +789,21 @@ nmfcu_status enqueue_objective(nmfcu_context *c, const RunArgs &a, long long ite
     return NMFCU_OK;
 }
 
+// The Grams and sums in one launch each; the ticket lives in the run state,
+// which every run zeroes before its first launch.
 void gram_w_full(nmfcu_context *c, const RunArgs &a, double *G, double *sums, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
-    a.ops->gram_w(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(), c->ps.as<double>(), st, s);
-    a.ops->gram_fin(c->pg.as<double>(), c->ps.as<double>(), pl.Bw, G, sums, st, s);
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    a.ops->gram_w_fin(a.W, pl.n, pl.Bw, pl.rows_per_gram, c->pg.as<double>(), c->ps.as<double>(),
+                      G, sums, &st->gram_ticket, st, s);
 }
 void gram_h_full(nmfcu_context *c, const RunArgs &a, double *G, double *sums, cudaStream_t s) {
     const Plan &pl = a.pl;
     RunState *st = c->state.as<RunState>();
-    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER, 2);
-    a.ops->gram_h(a.H, pl.p, pl.Bh, pl.cols_per_gram, c->pg.as<double>(), c->ps.as<double>(), st, s);
-    a.ops->gram_fin(c->pg.as<double>(), c->ps.as<double>(), pl.Bh, G, sums, st, s);
+    nmfcu_context::Scope sc(c, s, NMFCU_KCLASS_OTHER);
+    a.ops->gram_h_fin(a.H, pl.p, pl.Bh, pl.cols_per_gram, c->pg.as<double>(), c->ps.as<double>(),
+                      G, sums, &st->gram_ticket, st, s);
 }
 
 // H step: the streaming contraction over all rows, then the per-column update.
